@@ -1,0 +1,216 @@
+/*
+ * ppmg.h -- C-ABI of the B200-native particle<->mesh interpolation and
+ * remeshing library (libppmg.so).  A drop-in replacement for the hot path of
+ * PPM (PPMLibrary/ppm_legacy): ppm_interp_p2m, ppm_interp_m2p,
+ * ppm_rmsh_comp_weights, ppm_rmsh_remesh, ppm_rmsh_create_part, the periodic
+ * ghost get/put of ppm_map_field_ghost and the cell ranking of
+ * ppm_neighlist_clist / ppm_util_rank{2,3}d.
+ *
+ * Conventions (shared by every entry point):
+ *  - Arrays keep the reference's Fortran column-major layout.  `xp` points at
+ *    xp(1,1) of xp(ldxp, Np); `up` at up(1,1) of up(ldup, Np) (scalar variants:
+ *    up(Np)); `field_up` at the first element of field_up(ldf, lb(1):ub(1),
+ *    lb(2):ub(2)[, lb(3):ub(3)], 1:1), i.e. one subdomain, with the spatial
+ *    bounds passed in f_lb[dim] / f_ub[dim] (the allocation may be larger than
+ *    the 1-g:Nm+g box the routine writes; nothing outside the box is touched).
+ *  - Geometry comes from ppmg_mesh_register (the module state that
+ *    ppm_topo_mkfield / ppm_mesh_on_subs leave behind in the reference).
+ *  - `info` follows the reference: 0 on success, else a severity
+ *    (-1 fatal, -2 error; ppm_param.h:372-375) with the reference error number
+ *    (ppm_error.h, e.g. 503 ppm_err_argument, 405 ppm_err_part_unass) and a
+ *    message retrievable through ppmg_last_error.  The library never aborts
+ *    (the reference calls MPI_Abort on fatal errors, ppm_error.f:195-199).
+ *  - Plain entry points take HOST pointers, are synchronous and do their own
+ *    host<->device copies.  `_dev` twins take DEVICE pointers and a
+ *    cudaStream_t (as void*), enqueue asynchronously on that stream and report
+ *    data-dependent errors (e.g. particles outside the subdomain) through
+ *    ppmg_sync_status.
+ *  - Supported: one subdomain per GPU with periodic boundaries on every face,
+ *    kernels M'4 (2) and B-spline 2 (1); anything else returns info = -2 with
+ *    errno 503 and does no work (no CPU fallback).
+ *  - Precision of the double-precision ('d') variants: PPMG_PREC_FP64 computes
+ *    weights and sums in FP64; PPMG_PREC_MIXED forms cell offsets in FP64 and
+ *    weights/products in FP32 with compensated FP32 accumulation per node.
+ *    Single-precision ('s') variants compute in FP32.
+ */
+#ifndef PPMG_H
+#define PPMG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PPMG_PREC_FP64 0
+#define PPMG_PREC_MIXED 1
+
+/* ---- status, configuration ------------------------------------------- */
+
+/* Version of this library (major*10000 + minor*100 + patch). */
+int ppmg_version(void);
+
+/* Last error of the calling thread: returns its info, writes errno and a
+ * NUL-terminated message (ppm_error.f:90-199 keeps the same triple). */
+int ppmg_last_error(int* errnum, char* msg, int msglen);
+
+/* Precision of the 'd' variants (default PPMG_PREC_FP64, or the
+ * PPMG_PRECISION environment variable "fp64" / "mixed" at load time). */
+void ppmg_set_precision(int mode, int* info);
+int ppmg_get_precision(void);
+
+/* Number of CUDA kernels this library launched so far (all threads). */
+int64_t ppmg_launch_count(void);
+
+/* ---- geometry (replaces ppm_topo_mkfield / ppm_mesh_on_subs state) -------
+ * min_sub/max_sub: [nsubs][3]; subs_bc: [nsubs][6]; istart/nnodes: [nsubs][3]
+ * (C row-major = Fortran (3,nsubs) column-major).  Nm: global nodes per axis;
+ * bcdef: 2*dim codes (ppm_param.h:333-338). */
+void ppmg_mesh_register(int topo_id, int mesh_id, int dim, const double* min_phys,
+                        const double* max_phys, const int* Nm, const int* bcdef, int nsubs,
+                        const double* min_sub, const double* max_sub, const int* subs_bc,
+                        const int* istart, const int* nnodes, int* info);
+void ppmg_mesh_unregister(int topo_id, int mesh_id, int* info);
+
+/* Wait for all work of the handle's `_dev` calls on `stream` and return the
+ * data-dependent status latched since the last call (info/errno as above). */
+void ppmg_sync_status(int topo_id, int mesh_id, void* stream, int* info);
+
+/* ---- ppm_interp_p2m  (ppm/src/ppm_interp_p2m.f:127-163) ------------------
+ * field_up(1-g:Nm+g) is overwritten: real nodes hold the periodic sum
+ * (node Nm equals node 1), ghost layers hold the periodic images of the real
+ * nodes (the state a following ghost get would leave). */
+#define PPMG_P2M_V_ARGS(R)                                                          \
+  const R *xp, int64_t ldxp, int64_t Np, const R *up, int64_t ldup, int lda,       \
+      int topo_id, int mesh_id, int kernel, const int *ghostsize, R *field_up,      \
+      int64_t ldf, const int64_t *f_lb, const int64_t *f_ub, int *info
+#define PPMG_P2M_S_ARGS(R)                                                          \
+  const R *xp, int64_t ldxp, int64_t Np, const R *up, int topo_id, int mesh_id,     \
+      int kernel, const int *ghostsize, R *field_up, const int64_t *f_lb,           \
+      const int64_t *f_ub, int *info
+
+void ppmg_interp_p2m_dv_3d(PPMG_P2M_V_ARGS(double)); /* ppm_interp_p2m.f:159 */
+void ppmg_interp_p2m_sv_3d(PPMG_P2M_V_ARGS(float));  /* ppm_interp_p2m.f:156 */
+void ppmg_interp_p2m_ds_3d(PPMG_P2M_S_ARGS(double)); /* ppm_interp_p2m.f:151 */
+void ppmg_interp_p2m_ss_3d(PPMG_P2M_S_ARGS(float));  /* ppm_interp_p2m.f:148 */
+void ppmg_interp_p2m_dv_2d(PPMG_P2M_V_ARGS(double)); /* ppm_interp_p2m.f:141 */
+void ppmg_interp_p2m_sv_2d(PPMG_P2M_V_ARGS(float));  /* ppm_interp_p2m.f:138 */
+void ppmg_interp_p2m_ds_2d(PPMG_P2M_S_ARGS(double)); /* ppm_interp_p2m.f:133 */
+void ppmg_interp_p2m_ss_2d(PPMG_P2M_S_ARGS(float));  /* ppm_interp_p2m.f:130 */
+void ppmg_interp_p2m_dv_3d_dev(PPMG_P2M_V_ARGS(double), void* stream);
+void ppmg_interp_p2m_sv_3d_dev(PPMG_P2M_V_ARGS(float), void* stream);
+void ppmg_interp_p2m_dv_2d_dev(PPMG_P2M_V_ARGS(double), void* stream);
+void ppmg_interp_p2m_sv_2d_dev(PPMG_P2M_V_ARGS(float), void* stream);
+
+/* ---- ppm_interp_m2p  (ppm/src/ppm_interp_m2p.f:126-162) ------------------
+ * up is overwritten (zeroed, then the gather).  Reads the real nodes 1..Nm-1
+ * of field_up with periodic wrap, i.e. the result of the reference's M2P
+ * after a ghost get. */
+#define PPMG_M2P_V_ARGS(R)                                                          \
+  const R *xp, int64_t ldxp, int64_t Np, R *up, int64_t ldup, int lda, int topo_id, \
+      int mesh_id, int kernel, const int *ghostsize, const R *field_up, int64_t ldf, \
+      const int64_t *f_lb, const int64_t *f_ub, int *info
+#define PPMG_M2P_S_ARGS(R)                                                          \
+  const R *xp, int64_t ldxp, int64_t Np, R *up, int topo_id, int mesh_id,           \
+      int kernel, const int *ghostsize, const R *field_up, const int64_t *f_lb,     \
+      const int64_t *f_ub, int *info
+
+void ppmg_interp_m2p_dv_3d(PPMG_M2P_V_ARGS(double)); /* ppm_interp_m2p.f:158 */
+void ppmg_interp_m2p_sv_3d(PPMG_M2P_V_ARGS(float));  /* ppm_interp_m2p.f:155 */
+void ppmg_interp_m2p_ds_3d(PPMG_M2P_S_ARGS(double)); /* ppm_interp_m2p.f:150 */
+void ppmg_interp_m2p_ss_3d(PPMG_M2P_S_ARGS(float));  /* ppm_interp_m2p.f:147 */
+void ppmg_interp_m2p_dv_2d(PPMG_M2P_V_ARGS(double)); /* ppm_interp_m2p.f:140 */
+void ppmg_interp_m2p_sv_2d(PPMG_M2P_V_ARGS(float));  /* ppm_interp_m2p.f:137 */
+void ppmg_interp_m2p_ds_2d(PPMG_M2P_S_ARGS(double)); /* ppm_interp_m2p.f:132 */
+void ppmg_interp_m2p_ss_2d(PPMG_M2P_S_ARGS(float));  /* ppm_interp_m2p.f:129 */
+void ppmg_interp_m2p_dv_3d_dev(PPMG_M2P_V_ARGS(double), void* stream);
+void ppmg_interp_m2p_sv_3d_dev(PPMG_M2P_V_ARGS(float), void* stream);
+void ppmg_interp_m2p_dv_2d_dev(PPMG_M2P_V_ARGS(double), void* stream);
+void ppmg_interp_m2p_sv_2d_dev(PPMG_M2P_V_ARGS(float), void* stream);
+
+/* ---- adjoint of P2M (no reference counterpart) -----------------------------
+ * Given the adjoint field r = dL/dfield (real nodes, periodic), returns
+ * dw(lda,Np) = M2P(r) (the exact transpose of P2M) and
+ * dx(dim,Np) = sum_a up(a,p) * sum_n grad_x W(xi_p - n) r(a,n).
+ * Weights are recomputed (nothing is stored between forward and backward). */
+void ppmg_interp_p2m_adjoint_dv_3d(const double* xp, int64_t ldxp, int64_t Np,
+                                   const double* up, int64_t ldup, int lda, int topo_id,
+                                   int mesh_id, int kernel, const double* r_field,
+                                   int64_t ldf, const int64_t* f_lb, const int64_t* f_ub,
+                                   double* dw, int64_t lddw, double* dx, int64_t lddx,
+                                   int* info);
+void ppmg_interp_p2m_adjoint_dv_3d_dev(const double* xp, int64_t ldxp, int64_t Np,
+                                       const double* up, int64_t ldup, int lda, int topo_id,
+                                       int mesh_id, int kernel, const double* r_field,
+                                       int64_t ldf, const int64_t* f_lb, const int64_t* f_ub,
+                                       double* dw, int64_t lddw, double* dx, int64_t lddx,
+                                       int* info, void* stream);
+
+/* ---- ppm_map_field_ghost (ppm/src/ppm_map_field_ghost.f:61-89) -----------
+ * maptype ppm_param_map_ghost_get (5): ghost and duplicate nodes <- periodic
+ * images of the real nodes; ppm_param_map_ghost_put (6): real nodes += their
+ * periodic images in the ghost box (node Nm and node 1 both get the sum), the
+ * ghost layers are left unchanged -- the reference's init/put/push/send/pop
+ * cycle for one periodic subdomain. */
+void ppmg_map_field_ghost_d(double* field_up, int64_t ldf, int lda, const int64_t* f_lb,
+                            const int64_t* f_ub, int topo_id, int mesh_id,
+                            const int* ghostsize, int maptype, int* info);
+void ppmg_map_field_ghost_s(float* field_up, int64_t ldf, int lda, const int64_t* f_lb,
+                            const int64_t* f_ub, int topo_id, int mesh_id,
+                            const int* ghostsize, int maptype, int* info);
+void ppmg_map_field_ghost_d_dev(double* field_up, int64_t ldf, int lda, const int64_t* f_lb,
+                                const int64_t* f_ub, int topo_id, int mesh_id,
+                                const int* ghostsize, int maptype, int* info, void* stream);
+
+/* ---- ppm_rmsh_comp_weights (ppm/src/ppm_rmsh_comp_weights.f:96-103) ------
+ * Computes the per-particle 1D weights and keeps them (with the particle
+ * list) in the handle, like the reference's module state
+ * (ppm_module_data_rmsh.f:47-73).  wx1/wx2/wx3 may be NULL; when given they
+ * receive the reference layout wx(1:2ks, 1:1, 1-ks:Np+ks) (ks = 2 for M'4,
+ * 1 for bsp2), indexed by the particle's position in the sub list, which for
+ * one subdomain is the particle index. */
+void ppmg_rmsh_comp_weights_d(const double* xp, int64_t ldxp, int64_t Np, int topo_id,
+                              int mesh_id, int kernel, double* wx1, double* wx2,
+                              double* wx3, int* info);
+
+/* ---- ppm_rmsh_remesh (ppm/src/ppm_rmsh_remesh.f:90-124) ------------------
+ * Scatter with the weights of the last comp_weights call of this handle;
+ * the field box is overwritten as in P2M. */
+void ppmg_rmsh_remesh_dv_3d(const double* xp, int64_t ldxp, int64_t Np, const double* up,
+                            int64_t ldup, int lda, int topo_id, int mesh_id, int kernel,
+                            const int* ghostsize, double* field_up, int64_t ldf,
+                            const int64_t* f_lb, const int64_t* f_ub, int* info);
+void ppmg_rmsh_remesh_dv_2d(const double* xp, int64_t ldxp, int64_t Np, const double* up,
+                            int64_t ldup, int lda, int topo_id, int mesh_id, int kernel,
+                            const int* ghostsize, double* field_up, int64_t ldf,
+                            const int64_t* f_lb, const int64_t* f_ub, int* info);
+
+/* ---- ppm_rmsh_create_part (ppm/src/ppm_rmsh_create_part.f:90-171) --------
+ * Two calls: with up == NULL it only returns the new particle count in *np;
+ * then the caller allocates up(lda, np) [, xp(dim, np), wp(lda2, np)] and
+ * calls again to fill them.  Nodes are visited k, j, i with i fastest, node
+ * Nm excluded on periodic axes; a node becomes a particle when
+ * cutoff[0] < strength < cutoff[1], strength = |u|_2 (or |u*cutoff_weights|_2). */
+void ppmg_rmsh_create_part_d(const double* field_up, int64_t ldf, int lda,
+                             const int64_t* f_lb, const int64_t* f_ub, int topo_id,
+                             int mesh_id, const double* cutoff, const double* cutoff_weights,
+                             int resetpos, const double* field_wp, int64_t ldfw, int lda2,
+                             int64_t* np, double* up, double* xp, double* wp, int* info);
+
+/* ---- ppm_neighlist_clist / ppm_util_rank3d (ppm/src/ppm_neighlist_clist.f:
+ * 371-429, ppm/src/ppm_util_rank3d.f:353-533) ------------------------------
+ * Stable counting sort of particles into the cells of a box: lpdx receives
+ * the 1-based ids of the particles inside the mesh (ascending id within each
+ * cell), lhbx(1:nbox+1) the 1-based first position of each cell; returns the
+ * count of particles inside in *icount.  Bit-identical to the reference. */
+void ppmg_util_rank3d_d(const double* xp, int64_t ldxp, int64_t Np, const double* xmin,
+                        const double* xmax, const int* Nm, const int* Ngl, int* lpdx,
+                        int* lhbx, int64_t* icount, int* info);
+void ppmg_util_rank2d_d(const double* xp, int64_t ldxp, int64_t Np, const double* xmin,
+                        const double* xmax, const int* Nm, const int* Ngl, int* lpdx,
+                        int* lhbx, int64_t* icount, int* info);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PPMG_H */

@@ -1,0 +1,1099 @@
+// ppmg_api.cu -- the C-ABI of libppmg (declared in include/ppmg.h): handle
+// registry (the geometry state the reference keeps in ppm_module_data*),
+// argument validation with the reference's info/errno conventions, and the
+// host-pointer (synchronous) and device-pointer (stream-ordered) pipelines.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "ppmg_common.cuh"
+#include "ppmg_m2p.cuh"
+#include "ppmg_p2m.cuh"
+#include "ppmg_rmsh.cuh"
+#include "ppmg_sort.cuh"
+
+namespace ppmg {
+
+std::atomic<int64_t> g_launches{0};
+
+namespace {
+
+struct ErrState {
+  int info = 0;
+  int errnum = 0;
+  std::string msg;
+};
+thread_local ErrState t_err;
+
+int initial_precision() {
+  const char* e = std::getenv("PPMG_PRECISION");
+  if (e && (std::strcmp(e, "mixed") == 0 || std::strcmp(e, "MIXED") == 0))
+    return PPMG_PREC_MIXED;
+  return PPMG_PREC_FP64;
+}
+std::atomic<int> g_precision{initial_precision()};
+
+struct Handle {
+  int topo_id = 0, mesh_id = 0;
+  int dim = 0, nsubs = 0;
+  int Nm[3] = {1, 1, 1};
+  int bcdef[6] = {0, 0, 0, 0, 0, 0};
+  std::vector<double> min_sub, max_sub;
+  std::vector<int> subs_bc, istart, nnodes;
+  Geom g{};
+  Workspace ws;       // P2M / M2P / adjoint / ghost / clist scratch
+  Workspace ws_rmsh;  // comp_weights -> remesh state (ppm_module_data_rmsh)
+  cudaStream_t stream = nullptr;
+  int* d_status = nullptr;  // [0] particles outside the sub, [1] non-finite
+  std::mutex mu;
+  // comp_weights state
+  bool w_valid = false;
+  int w_kernel = 0;
+  int64_t w_np = 0;
+  ~Handle() {
+    if (stream) cudaStreamDestroy(stream);
+    if (d_status) cudaFree(d_status);
+  }
+};
+
+std::mutex g_mu;
+std::map<std::pair<int, int>, std::unique_ptr<Handle>> g_handles;
+
+int fail(int* info, int sev, int errnum, const std::string& msg) {
+  set_error(sev, errnum, msg);
+  if (info) *info = sev;
+  return sev;
+}
+
+int cuda_fail(int* info, cudaError_t e, const char* where) {
+  const int errnum = e == cudaErrorMemoryAllocation ? kErrAlloc : 602;
+  std::string m = std::string(where) + ": CUDA error: " + cudaGetErrorString(e);
+  cudaGetLastError();  // clear a sticky launch error of this thread
+  return fail(info, kErrorFatal, errnum, m);
+}
+
+Handle* find_handle(int topo_id, int mesh_id) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_handles.find({topo_id, mesh_id});
+  return it == g_handles.end() ? nullptr : it->second.get();
+}
+
+// Checks shared by every hot-path entry point (the ppm_debug > 0 checks of
+// ppm_interp_p2m.f:338-410, always on here).
+Handle* get_checked(int topo_id, int mesh_id, int dim, const char* caller, int* info) {
+  Handle* h = find_handle(topo_id, mesh_id);
+  if (!h) {
+    fail(info, kErrorError, kErrArgument, std::string(caller) + ": topo_id/mesh_id is invalid");
+    return nullptr;
+  }
+  if (h->dim != dim) {
+    fail(info, kErrorError, kErrArgument,
+         std::string(caller) + ": routine dimension does not match the registered mesh");
+    return nullptr;
+  }
+  if (h->nsubs != 1) {
+    fail(info, kErrorError, kErrArgument,
+         std::string(caller) + ": one subdomain per GPU is supported (nsubs must be 1)");
+    return nullptr;
+  }
+  for (int f = 0; f < 2 * dim; ++f)
+    if (h->bcdef[f] != kBcPeriodic) {
+      fail(info, kErrorError, kErrArgument,
+           std::string(caller) + ": only periodic boundary conditions are supported");
+      return nullptr;
+    }
+  return h;
+}
+
+bool check_kernel(int kernel, const char* caller, int* info) {
+  if (kernel != kKernelMp4 && kernel != kKernelBsp2) {
+    fail(info, kErrorError, kErrArgument,
+         std::string(caller) + ": wrong kernel definition (only M'4 = 2 and bsp2 = 1)");
+    return false;
+  }
+  return true;
+}
+
+// field_up(ldf, lb:ub, ...) descriptor; `need_lo/hi` is the index box the
+// routine touches.  Returns false (info set) when the allocation is too small.
+bool make_fd(const Handle& h, int64_t ldf, const int64_t* f_lb, const int64_t* f_ub,
+             const int need_lo[3], const int need_hi[3], FieldDesc& fd, const char* caller,
+             int* info) {
+  int64_t s = ldf;
+  for (int a = 0; a < 3; ++a) {
+    fd.s[a] = 0;
+    fd.lb[a] = 0;
+    fd.ub[a] = 0;
+    fd.box_lo[a] = 0;
+    fd.box_hi[a] = 0;
+  }
+  for (int a = 0; a < h.dim; ++a) {
+    if (f_ub[a] < f_lb[a]) {
+      fail(info, kErrorError, kErrArgument, std::string(caller) + ": field bounds are empty");
+      return false;
+    }
+    fd.s[a] = s;
+    fd.lb[a] = (int)f_lb[a];
+    fd.ub[a] = (int)f_ub[a];
+    fd.box_lo[a] = need_lo[a];
+    fd.box_hi[a] = need_hi[a];
+    if (f_lb[a] > need_lo[a] || f_ub[a] < need_hi[a]) {
+      fail(info, kErrorError, kErrArgument,
+           std::string(caller) + ": field_up bounds do not cover the required index box");
+      return false;
+    }
+    s *= (f_ub[a] - f_lb[a] + 1);
+  }
+  return true;
+}
+
+int64_t field_elems(const Handle& h, int64_t ldf, const int64_t* f_lb, const int64_t* f_ub) {
+  int64_t n = ldf;
+  for (int a = 0; a < h.dim; ++a) n *= (f_ub[a] - f_lb[a] + 1);
+  return n;
+}
+
+KeyParams make_kp(const Handle& h, int mode, bool quirk) {
+  KeyParams kp{};
+  kp.dim = h.dim;
+  kp.mode = mode;
+  for (int a = 0; a < 3; ++a) {
+    kp.N[a] = a < h.dim ? h.g.N[a] : 1;
+    kp.min[a] = a < h.dim ? h.g.min_sub[a] : 0.0;
+    kp.max[a] = a < h.dim ? h.g.max_sub[a] : 1.0;
+    kp.dxi[a] = a < h.dim ? (quirk ? h.g.dxiq_d[a] : h.g.dxi_d[a]) : 1.0;
+    kp.minf[a] = (float)kp.min[a];
+    kp.maxf[a] = (float)kp.max[a];
+    kp.dxif[a] = a < h.dim ? (quirk ? h.g.dxiq_f[a] : h.g.dxi_f[a]) : 1.0f;
+  }
+  return kp;
+}
+
+const int* d_nvalid_of(const Workspace& ws, int64_t ncell) {
+  return ws.start.as<int>() + ncell;
+}
+
+template <class T>
+constexpr bool is_f32() { return sizeof(T) == 4; }
+
+// ---------------------------------------------------------------------------
+// P2M pipeline (stream-ordered).  Returns 0 or the argument-error info.
+// ---------------------------------------------------------------------------
+template <class T>
+int p2m_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, const T* up, int64_t ldup,
+                 int lda, int kernel, const int* ghost, T* field, int64_t ldf,
+                 const int64_t* f_lb, const int64_t* f_ub, bool remesh, cudaStream_t st,
+                 int* info, const char* caller) {
+  int lo[3], hi[3];
+  for (int a = 0; a < h.dim; ++a) {
+    lo[a] = 1 - ghost[a];
+    hi[a] = h.Nm[a] + ghost[a];
+  }
+  FieldDesc fd;
+  if (!make_fd(h, ldf, f_lb, f_ub, lo, hi, fd, caller, info)) return *info;
+  const P2MPrec prec = is_f32<T>() ? P2M_FP32
+                                   : (g_precision.load() == PPMG_PREC_MIXED ? P2M_MIXED
+                                                                            : P2M_FP64);
+  Workspace& ws = remesh ? h.ws_rmsh : h.ws;
+  cudaError_t e;
+  if (remesh) {
+    // zero the whole allocation (ppm_rmsh_remesh.f:582: field_up = 0)
+    e = cudaMemsetAsync(field, 0, sizeof(T) * (size_t)field_elems(h, ldf, f_lb, f_ub), st);
+    if (e) return cuda_fail(info, e, caller);
+  } else {
+    KeyParams kp = make_kp(h, KEY_INTERP_CHECKED, false);
+    e = bin_sort<T>(kp, xp, ldxp, Np, h.g.ncell, ws, h.d_status + 0, st);
+    if (e) return cuda_fail(info, e, caller);
+  }
+  KeyParams kp = make_kp(h, KEY_INTERP_CHECKED, false);
+  const int* dnv = d_nvalid_of(ws, h.g.ncell);
+  if (prec == P2M_FP64)
+    e = pack_records<T, double>(kp, xp, ldxp, up, ldup, lda, Np, dnv, ws, st);
+  else
+    e = pack_records<T, float>(kp, xp, ldxp, up, ldup, lda, Np, dnv, ws, st);
+  if (e) return cuda_fail(info, e, caller);
+  P2MParams P{};
+  for (int a = 0; a < 3; ++a) P.N[a] = a < h.dim ? h.g.N[a] : 1;
+  P.TZ = p2m_tile_depth(h.dim, P.N);
+  P.cap = prec == P2M_FP64 ? 448 : 896;
+  P.c0 = 0;
+  P.start = ws.start.as<int>();
+  P.rec = remesh ? (const void*)ws.w1d.p : ws.rec.p;
+  P.us = ws.us.p;
+  P.field = field;
+  P.fd = fd;
+  e = launch_p2m(P, h.dim, kernel, prec, lda, Np > 0 ? Np : 1, remesh, st);
+  if (e) return cuda_fail(info, e, caller);
+  return 0;
+}
+
+template <class T>
+int m2p_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, T* up, int64_t ldup,
+                 int lda, int kernel, const T* field, int64_t ldf, const int64_t* f_lb,
+                 const int64_t* f_ub, cudaStream_t st, int* info, const char* caller) {
+  int lo[3], hi[3];
+  for (int a = 0; a < h.dim; ++a) {
+    lo[a] = 1;
+    hi[a] = h.g.N[a];
+  }
+  FieldDesc fd;
+  if (!make_fd(h, ldf, f_lb, f_ub, lo, hi, fd, caller, info)) return *info;
+  if (Np == 0) return 0;
+  const M2PPrec prec = is_f32<T>() ? M2P_FP32
+                                   : (g_precision.load() == PPMG_PREC_MIXED ? M2P_MIXED
+                                                                            : M2P_FP64);
+  KeyParams kp = make_kp(h, KEY_INTERP_WRAP, true);
+  cudaError_t e = bin_sort<T>(kp, xp, ldxp, Np, h.g.ncell, h.ws, h.d_status + 1, st, up, ldup,
+                              lda);
+  if (e) return cuda_fail(info, e, caller);
+  const int* dnv = d_nvalid_of(h.ws, h.g.ncell);
+  if (prec == M2P_FP64)
+    e = pack_records<T, double>(kp, xp, ldxp, (const T*)nullptr, 0, 0, Np, dnv, h.ws, st);
+  else
+    e = pack_records<T, float>(kp, xp, ldxp, (const T*)nullptr, 0, 0, Np, dnv, h.ws, st);
+  if (e) return cuda_fail(info, e, caller);
+  M2PParams P{};
+  for (int a = 0; a < 3; ++a) P.N[a] = a < h.dim ? h.g.N[a] : 1;
+  P.nvalid = Np;
+  P.d_nvalid = dnv;
+  P.idx = h.ws.idx.as<int>();
+  P.rec = h.ws.rec.p;
+  P.field = field;
+  P.fd = fd;
+  P.up = up;
+  P.ldup = ldup;
+  P.lda = lda;
+  e = launch_m2p(P, h.dim, kernel, prec, st);
+  if (e) return cuda_fail(info, e, caller);
+  return 0;
+}
+
+// Device status -> info (synchronises the stream).
+int read_status(Handle& h, cudaStream_t st, int* info, const char* caller) {
+  int hs[2] = {0, 0};
+  cudaError_t e = cudaMemcpyAsync(hs, h.d_status, sizeof(hs), cudaMemcpyDeviceToHost, st);
+  if (!e) e = cudaStreamSynchronize(st);
+  if (e) return cuda_fail(info, e, caller);
+  if (hs[0] || hs[1]) {
+    e = cudaMemsetAsync(h.d_status, 0, 2 * sizeof(int), st);
+    cudaStreamSynchronize(st);
+  }
+  if (hs[0] > 0) {
+    return fail(info, kErrorFatal, kErrPartUnass,
+                std::string(caller) + ": " + std::to_string(hs[0]) +
+                    " particles lie outside the subdomain (unassigned)");
+  }
+  if (hs[1] > 0) {
+    return fail(info, kErrorError, kErrArgument,
+                std::string(caller) + ": " + std::to_string(hs[1]) +
+                    " particles have non-finite positions");
+  }
+  if (info) *info = 0;
+  return 0;
+}
+
+template <class T>
+T* mirror(DevBuf& b, const T* host, int64_t n, cudaStream_t st, cudaError_t& e) {
+  e = b.ensure(sizeof(T) * (size_t)(n > 0 ? n : 1));
+  if (e) return nullptr;
+  if (host && n > 0) e = cudaMemcpyAsync(b.p, host, sizeof(T) * (size_t)n,
+                                         cudaMemcpyHostToDevice, st);
+  return b.as<T>();
+}
+
+bool field_is_box(const Handle& h, const int64_t* f_lb, const int64_t* f_ub, const int* ghost) {
+  for (int a = 0; a < h.dim; ++a)
+    if (f_lb[a] != 1 - ghost[a] || f_ub[a] != h.Nm[a] + ghost[a]) return false;
+  return true;
+}
+
+template <class T>
+void p2m_host(const T* xp, int64_t ldxp, int64_t Np, const T* up, int64_t ldup, int lda,
+              int topo_id, int mesh_id, int kernel, const int* ghostsize, T* field_up,
+              int64_t ldf, const int64_t* f_lb, const int64_t* f_ub, int* info, int dim,
+              const char* caller) {
+  clear_error();
+  if (info) *info = 0;
+  if (Np < 0) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": particles must be specified"); return; }
+  if (Np > 0 && ldxp < dim) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": leading dimension of xp insufficient"); return; }
+  if (lda < 1 || ldup < lda || ldf < lda) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": lda / leading dimensions inconsistent"); return; }
+  if (Np >= (int64_t)1 << 31) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": Np must be < 2^31"); return; }
+  if (!check_kernel(kernel, caller, info)) return;
+  if (dim == 2 && kernel != kKernelMp4) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": Only Mp4 is available in 2D"); return; }
+  Handle* h = get_checked(topo_id, mesh_id, dim, caller, info);
+  if (!h) return;
+  std::lock_guard<std::mutex> lk(h->mu);
+  cudaStream_t st = h->stream;
+  cudaError_t e;
+  const T* dxp = mirror<T>(h->ws.h_xp, xp, ldxp * Np, st, e);
+  if (e) { cuda_fail(info, e, caller); return; }
+  const T* dup = mirror<T>(h->ws.h_up, up, ldup * Np, st, e);
+  if (e) { cuda_fail(info, e, caller); return; }
+  const int64_t nf = field_elems(*h, ldf, f_lb, f_ub);
+  // the written box is all of field_up in the common case; otherwise bring the
+  // untouched surroundings along so the copy back preserves them
+  const bool whole = field_is_box(*h, f_lb, f_ub, ghostsize) && ldf == lda;
+  T* dfield = mirror<T>(h->ws.h_field, whole ? (const T*)nullptr : field_up, nf, st, e);
+  if (e) { cuda_fail(info, e, caller); return; }
+  if (p2m_pipeline<T>(*h, dxp, ldxp, Np, dup, ldup, lda, kernel, ghostsize, dfield, ldf, f_lb,
+                      f_ub, false, st, info, caller))
+    return;
+  e = cudaMemcpyAsync(field_up, dfield, sizeof(T) * (size_t)nf, cudaMemcpyDeviceToHost, st);
+  if (e) { cuda_fail(info, e, caller); return; }
+  read_status(*h, st, info, caller);
+}
+
+template <class T>
+void p2m_dev(const T* xp, int64_t ldxp, int64_t Np, const T* up, int64_t ldup, int lda,
+             int topo_id, int mesh_id, int kernel, const int* ghostsize, T* field_up,
+             int64_t ldf, const int64_t* f_lb, const int64_t* f_ub, int* info, int dim,
+             cudaStream_t st, const char* caller) {
+  clear_error();
+  if (info) *info = 0;
+  if (Np < 0 || (Np > 0 && ldxp < dim) || lda < 1 || ldup < lda || ldf < lda ||
+      Np >= (int64_t)1 << 31) {
+    fail(info, kErrorError, kErrArgument, std::string(caller) + ": invalid sizes");
+    return;
+  }
+  if (!check_kernel(kernel, caller, info)) return;
+  if (dim == 2 && kernel != kKernelMp4) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": Only Mp4 is available in 2D"); return; }
+  Handle* h = get_checked(topo_id, mesh_id, dim, caller, info);
+  if (!h) return;
+  std::lock_guard<std::mutex> lk(h->mu);
+  p2m_pipeline<T>(*h, xp, ldxp, Np, up, ldup, lda, kernel, ghostsize, field_up, ldf, f_lb,
+                  f_ub, false, st, info, caller);
+}
+
+template <class T>
+void m2p_host(const T* xp, int64_t ldxp, int64_t Np, T* up, int64_t ldup, int lda,
+              int topo_id, int mesh_id, int kernel, const int* ghostsize, const T* field_up,
+              int64_t ldf, const int64_t* f_lb, const int64_t* f_ub, int* info, int dim,
+              const char* caller) {
+  (void)ghostsize;
+  clear_error();
+  if (info) *info = 0;
+  if (Np < 0) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": particles must be specified"); return; }
+  if (Np > 0 && ldxp < dim) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": leading dimension of xp insufficient"); return; }
+  if (lda < 1 || ldup < lda || ldf < lda) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": lda / leading dimensions inconsistent"); return; }
+  if (Np >= (int64_t)1 << 31) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": Np must be < 2^31"); return; }
+  if (!check_kernel(kernel, caller, info)) return;
+  Handle* h = get_checked(topo_id, mesh_id, dim, caller, info);
+  if (!h) return;
+  std::lock_guard<std::mutex> lk(h->mu);
+  cudaStream_t st = h->stream;
+  cudaError_t e;
+  const T* dxp = mirror<T>(h->ws.h_xp, xp, ldxp * Np, st, e);
+  if (e) { cuda_fail(info, e, caller); return; }
+  // up is overwritten column by column; rows beyond lda (ldup > lda) are kept
+  T* dup = mirror<T>(h->ws.h_up, ldup == lda ? (const T*)nullptr : (const T*)up, ldup * Np, st, e);
+  if (e) { cuda_fail(info, e, caller); return; }
+  const int64_t nf = field_elems(*h, ldf, f_lb, f_ub);
+  const T* dfield = mirror<T>(h->ws.h_field, field_up, nf, st, e);
+  if (e) { cuda_fail(info, e, caller); return; }
+  if (m2p_pipeline<T>(*h, dxp, ldxp, Np, dup, ldup, lda, kernel, dfield, ldf, f_lb, f_ub, st,
+                      info, caller))
+    return;
+  if (Np > 0) {
+    e = cudaMemcpyAsync(up, dup, sizeof(T) * (size_t)(ldup * Np), cudaMemcpyDeviceToHost, st);
+    if (e) { cuda_fail(info, e, caller); return; }
+  }
+  read_status(*h, st, info, caller);
+}
+
+template <class T>
+void m2p_dev(const T* xp, int64_t ldxp, int64_t Np, T* up, int64_t ldup, int lda, int topo_id,
+             int mesh_id, int kernel, const int* ghostsize, const T* field_up, int64_t ldf,
+             const int64_t* f_lb, const int64_t* f_ub, int* info, int dim, cudaStream_t st,
+             const char* caller) {
+  (void)ghostsize;
+  clear_error();
+  if (info) *info = 0;
+  if (Np < 0 || (Np > 0 && ldxp < dim) || lda < 1 || ldup < lda || ldf < lda ||
+      Np >= (int64_t)1 << 31) {
+    fail(info, kErrorError, kErrArgument, std::string(caller) + ": invalid sizes");
+    return;
+  }
+  if (!check_kernel(kernel, caller, info)) return;
+  Handle* h = get_checked(topo_id, mesh_id, dim, caller, info);
+  if (!h) return;
+  std::lock_guard<std::mutex> lk(h->mu);
+  m2p_pipeline<T>(*h, xp, ldxp, Np, up, ldup, lda, kernel, field_up, ldf, f_lb, f_ub, st, info,
+                  caller);
+}
+
+int adjoint_pipeline(Handle& h, const double* xp, int64_t ldxp, int64_t Np, const double* up,
+                     int64_t ldup, int lda, int kernel, const double* r, int64_t ldf,
+                     const int64_t* f_lb, const int64_t* f_ub, double* dw, int64_t lddw,
+                     double* dx, int64_t lddx, cudaStream_t st, int* info, const char* caller) {
+  int lo[3], hi[3];
+  for (int a = 0; a < h.dim; ++a) {
+    lo[a] = 1;
+    hi[a] = h.g.N[a];
+  }
+  FieldDesc fd;
+  if (!make_fd(h, ldf, f_lb, f_ub, lo, hi, fd, caller, info)) return *info;
+  if (Np == 0) return 0;
+  const M2PPrec prec = g_precision.load() == PPMG_PREC_MIXED ? M2P_MIXED : M2P_FP64;
+  // the transpose of P2M: P2M's stencil (FP64 mesh spacing), periodic wrap
+  KeyParams kp = make_kp(h, KEY_INTERP_WRAP, false);
+  cudaError_t e = bin_sort<double>(kp, xp, ldxp, Np, h.g.ncell, h.ws, h.d_status + 1, st, dw,
+                                   lddw, lda);
+  if (e) return cuda_fail(info, e, caller);
+  const int* dnv = d_nvalid_of(h.ws, h.g.ncell);
+  if (prec == M2P_FP64)
+    e = pack_records<double, double>(kp, xp, ldxp, nullptr, 0, 0, Np, dnv, h.ws, st);
+  else
+    e = pack_records<double, float>(kp, xp, ldxp, nullptr, 0, 0, Np, dnv, h.ws, st);
+  if (e) return cuda_fail(info, e, caller);
+  M2PParams P{};
+  for (int a = 0; a < 3; ++a) P.N[a] = h.g.N[a];
+  P.nvalid = Np;
+  P.d_nvalid = dnv;
+  P.idx = h.ws.idx.as<int>();
+  P.rec = h.ws.rec.p;
+  P.field = r;
+  P.fd = fd;
+  P.up = dw;
+  P.ldup = lddw;
+  P.lda = lda;
+  P.upin = up;
+  P.ldupin = ldup;
+  P.dx = dx;
+  P.lddx = lddx;
+  for (int a = 0; a < 3; ++a) P.dxi[a] = h.g.dxi_d[a];
+  e = launch_adjoint(P, kernel, prec, st);
+  if (e) return cuda_fail(info, e, caller);
+  return 0;
+}
+
+template <class T>
+int ghost_pipeline(Handle& h, T* field, int64_t ldf, int lda, const int64_t* f_lb,
+                   const int64_t* f_ub, const int* ghost, int maptype, cudaStream_t st,
+                   int* info, const char* caller) {
+  if (maptype != kMapGhostGet && maptype != kMapGhostPut)
+    return fail(info, kErrorError, kErrArgument,
+                std::string(caller) + ": maptype must be ghost_get (5) or ghost_put (6)");
+  int lo[3], hi[3];
+  for (int a = 0; a < h.dim; ++a) {
+    lo[a] = 1 - ghost[a];
+    hi[a] = h.Nm[a] + ghost[a];
+  }
+  FieldDesc fd;
+  if (!make_fd(h, ldf, f_lb, f_ub, lo, hi, fd, caller, info)) return *info;
+  GhostParams P{};
+  P.dim = h.dim;
+  P.lda = lda;
+  for (int a = 0; a < 3; ++a) {
+    P.N[a] = a < h.dim ? h.g.N[a] : 1;
+    P.lo[a] = a < h.dim ? lo[a] : 0;
+    P.hi[a] = a < h.dim ? hi[a] : 0;
+  }
+  P.fd = fd;
+  T* tmp = nullptr;
+  if (maptype == kMapGhostPut) {
+    int64_t n = lda;
+    for (int a = 0; a < h.dim; ++a) n *= h.Nm[a];
+    cudaError_t e = h.ws.h_aux.ensure(sizeof(T) * (size_t)n);
+    if (e) return cuda_fail(info, e, caller);
+    tmp = h.ws.h_aux.as<T>();
+  }
+  cudaError_t e = launch_ghost<T>(P, maptype, field, tmp, st);
+  if (e) return cuda_fail(info, e, caller);
+  return 0;
+}
+
+template <class T>
+void ghost_host(T* field_up, int64_t ldf, int lda, const int64_t* f_lb, const int64_t* f_ub,
+                int topo_id, int mesh_id, const int* ghostsize, int maptype, int* info,
+                const char* caller) {
+  clear_error();
+  if (info) *info = 0;
+  Handle* hh = find_handle(topo_id, mesh_id);
+  if (!hh) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": topo_id/mesh_id is invalid"); return; }
+  Handle* h = get_checked(topo_id, mesh_id, hh->dim, caller, info);
+  if (!h) return;
+  if (lda < 1 || ldf < lda) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": lda inconsistent"); return; }
+  std::lock_guard<std::mutex> lk(h->mu);
+  cudaStream_t st = h->stream;
+  cudaError_t e;
+  const int64_t nf = field_elems(*h, ldf, f_lb, f_ub);
+  T* dfield = mirror<T>(h->ws.h_field, field_up, nf, st, e);
+  if (e) { cuda_fail(info, e, caller); return; }
+  if (ghost_pipeline<T>(*h, dfield, ldf, lda, f_lb, f_ub, ghostsize, maptype, st, info, caller))
+    return;
+  e = cudaMemcpyAsync(field_up, dfield, sizeof(T) * (size_t)nf, cudaMemcpyDeviceToHost, st);
+  if (!e) e = cudaStreamSynchronize(st);
+  if (e) cuda_fail(info, e, caller);
+}
+
+}  // namespace
+
+void set_error(int info, int errnum, const std::string& msg) {
+  t_err.info = info;
+  t_err.errnum = errnum;
+  t_err.msg = msg;
+}
+void clear_error() {
+  t_err.info = 0;
+  t_err.errnum = 0;
+  t_err.msg.clear();
+}
+
+}  // namespace ppmg
+
+using namespace ppmg;
+
+extern "C" {
+
+int ppmg_version(void) { return 10000; }
+
+int ppmg_last_error(int* errnum, char* msg, int msglen) {
+  if (errnum) *errnum = t_err.errnum;
+  if (msg && msglen > 0) {
+    std::strncpy(msg, t_err.msg.c_str(), (size_t)msglen - 1);
+    msg[msglen - 1] = '\0';
+  }
+  return t_err.info;
+}
+
+void ppmg_set_precision(int mode, int* info) {
+  clear_error();
+  if (mode != PPMG_PREC_FP64 && mode != PPMG_PREC_MIXED) {
+    fail(info, kErrorError, kErrArgument, "ppmg_set_precision: mode must be 0 or 1");
+    return;
+  }
+  g_precision.store(mode);
+  if (info) *info = 0;
+}
+
+int ppmg_get_precision(void) { return g_precision.load(); }
+
+int64_t ppmg_launch_count(void) { return g_launches.load(); }
+
+void ppmg_mesh_register(int topo_id, int mesh_id, int dim, const double* min_phys,
+                        const double* max_phys, const int* Nm, const int* bcdef, int nsubs,
+                        const double* min_sub, const double* max_sub, const int* subs_bc,
+                        const int* istart, const int* nnodes, int* info) {
+  clear_error();
+  if (info) *info = 0;
+  if (dim != 2 && dim != 3) { fail(info, kErrorError, ppmg::kErrArgument, "ppmg_mesh_register: dim must be 2 or 3"); return; }
+  if (nsubs < 1) { fail(info, kErrorError, ppmg::kErrArgument, "ppmg_mesh_register: nsubs must be >= 1"); return; }
+  for (int a = 0; a < dim; ++a) {
+    if (Nm[a] < 2) { fail(info, kErrorError, ppmg::kErrArgument, "ppmg_mesh_register: Nm must be >= 2"); return; }
+    if (!(max_phys[a] > min_phys[a])) { fail(info, kErrorError, ppmg::kErrArgument, "ppmg_mesh_register: max_phys must exceed min_phys"); return; }
+  }
+  int64_t ncell = 1;
+  for (int a = 0; a < dim; ++a) ncell *= (int64_t)(Nm[a] - 1);
+  if (ncell >= ((int64_t)1 << 31) - 1) { fail(info, kErrorError, ppmg::kErrArgument, "ppmg_mesh_register: mesh has >= 2^31 cells"); return; }
+  auto h = std::make_unique<Handle>();
+  h->topo_id = topo_id;
+  h->mesh_id = mesh_id;
+  h->dim = dim;
+  h->nsubs = nsubs;
+  for (int a = 0; a < 3; ++a) h->Nm[a] = a < dim ? Nm[a] : 2;
+  for (int f = 0; f < 6; ++f) h->bcdef[f] = f < 2 * dim ? bcdef[f] : kBcPeriodic;
+  h->min_sub.assign(min_sub, min_sub + 3 * nsubs);
+  h->max_sub.assign(max_sub, max_sub + 3 * nsubs);
+  h->subs_bc.assign(subs_bc, subs_bc + 6 * nsubs);
+  h->istart.assign(istart, istart + 3 * nsubs);
+  h->nnodes.assign(nnodes, nnodes + 3 * nsubs);
+  Geom& g = h->g;
+  g.dim = dim;
+  g.ncell = ncell;
+  for (int a = 0; a < 3; ++a) {
+    const bool on = a < dim;
+    g.N[a] = on ? Nm[a] - 1 : 1;
+    g.min_phys[a] = on ? min_phys[a] : 0.0;
+    g.max_phys[a] = on ? max_phys[a] : 1.0;
+    g.min_sub[a] = on ? min_sub[a] : 0.0;
+    g.max_sub[a] = on ? max_sub[a] : 1.0;
+    // P2M / remesh: dx = len/Nc, dxi = 1/dx in the routine's kind
+    const double len = g.max_phys[a] - g.min_phys[a];
+    g.dxi_d[a] = 1.0 / (len / (double)g.N[a]);
+    const float lenf = (float)g.max_phys[a] - (float)g.min_phys[a];
+    g.dxi_f[a] = 1.0f / (lenf / (float)g.N[a]);
+    // M2P / comp_weights: len_phys, dx, dxi are default REAL (FP32)
+    const float len32 = (float)len;
+    const float dx32 = (float)((double)len32 / (double)g.N[a]);
+    g.dxiq_d[a] = (double)(float)(1.0 / (double)dx32);
+    g.dxiq_f[a] = 1.0f / (lenf / (float)g.N[a]);
+    g.h_d[a] = len / (double)(on ? Nm[a] - 1 : 1);
+  }
+  cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (!e) e = cudaMalloc(&h->d_status, 4 * sizeof(int));
+  if (!e) e = cudaMemset(h->d_status, 0, 4 * sizeof(int));
+  if (e) { cuda_fail(info, e, "ppmg_mesh_register"); return; }
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_handles[{topo_id, mesh_id}] = std::move(h);
+}
+
+void ppmg_mesh_unregister(int topo_id, int mesh_id, int* info) {
+  clear_error();
+  if (info) *info = 0;
+  std::unique_ptr<Handle> h;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_handles.find({topo_id, mesh_id});
+    if (it == g_handles.end()) {
+      fail(info, kErrorError, ppmg::kErrArgument, "ppmg_mesh_unregister: unknown handle");
+      return;
+    }
+    h = std::move(it->second);
+    g_handles.erase(it);
+  }
+  if (h->stream) cudaStreamSynchronize(h->stream);
+}
+
+void ppmg_sync_status(int topo_id, int mesh_id, void* stream, int* info) {
+  clear_error();
+  Handle* h = find_handle(topo_id, mesh_id);
+  if (!h) { fail(info, kErrorError, ppmg::kErrArgument, "ppmg_sync_status: topo_id/mesh_id is invalid"); return; }
+  std::lock_guard<std::mutex> lk(h->mu);
+  read_status(*h, (cudaStream_t)stream, info, "ppmg_sync_status");
+}
+
+// ---- P2M ------------------------------------------------------------------
+#define P2M_V_HOST(NAME, R, DIM)                                                             \
+  void NAME(const R* xp, int64_t ldxp, int64_t Np, const R* up, int64_t ldup, int lda,     \
+            int topo_id, int mesh_id, int kernel, const int* ghostsize, R* field_up,        \
+            int64_t ldf, const int64_t* f_lb, const int64_t* f_ub, int* info) {             \
+    p2m_host<R>(xp, ldxp, Np, up, ldup, lda, topo_id, mesh_id, kernel, ghostsize, field_up, \
+                ldf, f_lb, f_ub, info, DIM, #NAME);                                        \
+  }
+#define P2M_S_HOST(NAME, R, DIM)                                                             \
+  void NAME(const R* xp, int64_t ldxp, int64_t Np, const R* up, int topo_id, int mesh_id,   \
+            int kernel, const int* ghostsize, R* field_up, const int64_t* f_lb,             \
+            const int64_t* f_ub, int* info) {                                               \
+    p2m_host<R>(xp, ldxp, Np, up, 1, 1, topo_id, mesh_id, kernel, ghostsize, field_up, 1,   \
+                f_lb, f_ub, info, DIM, #NAME);                                             \
+  }
+#define P2M_V_DEV(NAME, R, DIM)                                                              \
+  void NAME(const R* xp, int64_t ldxp, int64_t Np, const R* up, int64_t ldup, int lda,     \
+            int topo_id, int mesh_id, int kernel, const int* ghostsize, R* field_up,        \
+            int64_t ldf, const int64_t* f_lb, const int64_t* f_ub, int* info,              \
+            void* stream) {                                                                 \
+    p2m_dev<R>(xp, ldxp, Np, up, ldup, lda, topo_id, mesh_id, kernel, ghostsize, field_up,  \
+               ldf, f_lb, f_ub, info, DIM, (cudaStream_t)stream, #NAME);                   \
+  }
+
+P2M_V_HOST(ppmg_interp_p2m_dv_3d, double, 3)
+P2M_V_HOST(ppmg_interp_p2m_sv_3d, float, 3)
+P2M_S_HOST(ppmg_interp_p2m_ds_3d, double, 3)
+P2M_S_HOST(ppmg_interp_p2m_ss_3d, float, 3)
+P2M_V_HOST(ppmg_interp_p2m_dv_2d, double, 2)
+P2M_V_HOST(ppmg_interp_p2m_sv_2d, float, 2)
+P2M_S_HOST(ppmg_interp_p2m_ds_2d, double, 2)
+P2M_S_HOST(ppmg_interp_p2m_ss_2d, float, 2)
+P2M_V_DEV(ppmg_interp_p2m_dv_3d_dev, double, 3)
+P2M_V_DEV(ppmg_interp_p2m_sv_3d_dev, float, 3)
+P2M_V_DEV(ppmg_interp_p2m_dv_2d_dev, double, 2)
+P2M_V_DEV(ppmg_interp_p2m_sv_2d_dev, float, 2)
+
+// ---- M2P ------------------------------------------------------------------
+#define M2P_V_HOST(NAME, R, DIM)                                                            \
+  void NAME(const R* xp, int64_t ldxp, int64_t Np, R* up, int64_t ldup, int lda,           \
+            int topo_id, int mesh_id, int kernel, const int* ghostsize, const R* field_up,  \
+            int64_t ldf, const int64_t* f_lb, const int64_t* f_ub, int* info) {             \
+    m2p_host<R>(xp, ldxp, Np, up, ldup, lda, topo_id, mesh_id, kernel, ghostsize, field_up, \
+                ldf, f_lb, f_ub, info, DIM, #NAME);                                        \
+  }
+#define M2P_S_HOST(NAME, R, DIM)                                                            \
+  void NAME(const R* xp, int64_t ldxp, int64_t Np, R* up, int topo_id, int mesh_id,         \
+            int kernel, const int* ghostsize, const R* field_up, const int64_t* f_lb,       \
+            const int64_t* f_ub, int* info) {                                               \
+    m2p_host<R>(xp, ldxp, Np, up, 1, 1, topo_id, mesh_id, kernel, ghostsize, field_up, 1,   \
+                f_lb, f_ub, info, DIM, #NAME);                                             \
+  }
+#define M2P_V_DEV(NAME, R, DIM)                                                             \
+  void NAME(const R* xp, int64_t ldxp, int64_t Np, R* up, int64_t ldup, int lda,           \
+            int topo_id, int mesh_id, int kernel, const int* ghostsize, const R* field_up,  \
+            int64_t ldf, const int64_t* f_lb, const int64_t* f_ub, int* info,              \
+            void* stream) {                                                                 \
+    m2p_dev<R>(xp, ldxp, Np, up, ldup, lda, topo_id, mesh_id, kernel, ghostsize, field_up,  \
+               ldf, f_lb, f_ub, info, DIM, (cudaStream_t)stream, #NAME);                   \
+  }
+
+M2P_V_HOST(ppmg_interp_m2p_dv_3d, double, 3)
+M2P_V_HOST(ppmg_interp_m2p_sv_3d, float, 3)
+M2P_S_HOST(ppmg_interp_m2p_ds_3d, double, 3)
+M2P_S_HOST(ppmg_interp_m2p_ss_3d, float, 3)
+M2P_V_HOST(ppmg_interp_m2p_dv_2d, double, 2)
+M2P_V_HOST(ppmg_interp_m2p_sv_2d, float, 2)
+M2P_S_HOST(ppmg_interp_m2p_ds_2d, double, 2)
+M2P_S_HOST(ppmg_interp_m2p_ss_2d, float, 2)
+M2P_V_DEV(ppmg_interp_m2p_dv_3d_dev, double, 3)
+M2P_V_DEV(ppmg_interp_m2p_sv_3d_dev, float, 3)
+M2P_V_DEV(ppmg_interp_m2p_dv_2d_dev, double, 2)
+M2P_V_DEV(ppmg_interp_m2p_sv_2d_dev, float, 2)
+
+// ---- adjoint ----------------------------------------------------------------
+static void adjoint_common(const double* xp, int64_t ldxp, int64_t Np, const double* up,
+                           int64_t ldup, int lda, int topo_id, int mesh_id, int kernel,
+                           const double* r_field, int64_t ldf, const int64_t* f_lb,
+                           const int64_t* f_ub, double* dw, int64_t lddw, double* dx,
+                           int64_t lddx, int* info, bool dev, cudaStream_t ust) {
+  const char* caller = dev ? "ppmg_interp_p2m_adjoint_dv_3d_dev" : "ppmg_interp_p2m_adjoint_dv_3d";
+  clear_error();
+  if (info) *info = 0;
+  if (Np < 0 || (Np > 0 && ldxp < 3) || lda < 1 || ldup < lda || ldf < lda || lddw < lda ||
+      lddx < 3 || Np >= (int64_t)1 << 31) {
+    fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": invalid sizes");
+    return;
+  }
+  if (!check_kernel(kernel, caller, info)) return;
+  Handle* h = get_checked(topo_id, mesh_id, 3, caller, info);
+  if (!h) return;
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (dev) {
+    adjoint_pipeline(*h, xp, ldxp, Np, up, ldup, lda, kernel, r_field, ldf, f_lb, f_ub, dw,
+                     lddw, dx, lddx, ust, info, caller);
+    return;
+  }
+  cudaStream_t st = h->stream;
+  cudaError_t e;
+  const double* dxp = mirror<double>(h->ws.h_xp, xp, ldxp * Np, st, e);
+  if (e) { cuda_fail(info, e, caller); return; }
+  const double* dup = mirror<double>(h->ws.h_up, up, ldup * Np, st, e);
+  if (e) { cuda_fail(info, e, caller); return; }
+  const int64_t nf = field_elems(*h, ldf, f_lb, f_ub);
+  const double* dr = mirror<double>(h->ws.h_field, r_field, nf, st, e);
+  if (e) { cuda_fail(info, e, caller); return; }
+  double* ddw = mirror<double>(h->ws.h_aux, (const double*)nullptr, lddw * Np + lddx * Np, st, e);
+  if (e) { cuda_fail(info, e, caller); return; }
+  double* ddx = ddw + lddw * Np;
+  if (adjoint_pipeline(*h, dxp, ldxp, Np, dup, ldup, lda, kernel, dr, ldf, f_lb, f_ub, ddw, lddw,
+                       ddx, lddx, st, info, caller))
+    return;
+  if (Np > 0) {
+    e = cudaMemcpyAsync(dw, ddw, sizeof(double) * (size_t)(lddw * Np), cudaMemcpyDeviceToHost, st);
+    if (!e) e = cudaMemcpyAsync(dx, ddx, sizeof(double) * (size_t)(lddx * Np), cudaMemcpyDeviceToHost, st);
+    if (e) { cuda_fail(info, e, caller); return; }
+  }
+  read_status(*h, st, info, caller);
+}
+
+void ppmg_interp_p2m_adjoint_dv_3d(const double* xp, int64_t ldxp, int64_t Np,
+                                   const double* up, int64_t ldup, int lda, int topo_id,
+                                   int mesh_id, int kernel, const double* r_field,
+                                   int64_t ldf, const int64_t* f_lb, const int64_t* f_ub,
+                                   double* dw, int64_t lddw, double* dx, int64_t lddx,
+                                   int* info) {
+  adjoint_common(xp, ldxp, Np, up, ldup, lda, topo_id, mesh_id, kernel, r_field, ldf, f_lb, f_ub,
+                 dw, lddw, dx, lddx, info, false, nullptr);
+}
+
+void ppmg_interp_p2m_adjoint_dv_3d_dev(const double* xp, int64_t ldxp, int64_t Np,
+                                       const double* up, int64_t ldup, int lda, int topo_id,
+                                       int mesh_id, int kernel, const double* r_field,
+                                       int64_t ldf, const int64_t* f_lb, const int64_t* f_ub,
+                                       double* dw, int64_t lddw, double* dx, int64_t lddx,
+                                       int* info, void* stream) {
+  adjoint_common(xp, ldxp, Np, up, ldup, lda, topo_id, mesh_id, kernel, r_field, ldf, f_lb, f_ub,
+                 dw, lddw, dx, lddx, info, true, (cudaStream_t)stream);
+}
+
+// ---- ghost ------------------------------------------------------------------
+void ppmg_map_field_ghost_d(double* field_up, int64_t ldf, int lda, const int64_t* f_lb,
+                            const int64_t* f_ub, int topo_id, int mesh_id,
+                            const int* ghostsize, int maptype, int* info) {
+  ghost_host<double>(field_up, ldf, lda, f_lb, f_ub, topo_id, mesh_id, ghostsize, maptype, info,
+                     "ppmg_map_field_ghost_d");
+}
+void ppmg_map_field_ghost_s(float* field_up, int64_t ldf, int lda, const int64_t* f_lb,
+                            const int64_t* f_ub, int topo_id, int mesh_id,
+                            const int* ghostsize, int maptype, int* info) {
+  ghost_host<float>(field_up, ldf, lda, f_lb, f_ub, topo_id, mesh_id, ghostsize, maptype, info,
+                    "ppmg_map_field_ghost_s");
+}
+void ppmg_map_field_ghost_d_dev(double* field_up, int64_t ldf, int lda, const int64_t* f_lb,
+                                const int64_t* f_ub, int topo_id, int mesh_id,
+                                const int* ghostsize, int maptype, int* info, void* stream) {
+  const char* caller = "ppmg_map_field_ghost_d_dev";
+  clear_error();
+  if (info) *info = 0;
+  Handle* hh = find_handle(topo_id, mesh_id);
+  if (!hh) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": topo_id/mesh_id is invalid"); return; }
+  Handle* h = get_checked(topo_id, mesh_id, hh->dim, caller, info);
+  if (!h) return;
+  if (lda < 1 || ldf < lda) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": lda inconsistent"); return; }
+  std::lock_guard<std::mutex> lk(h->mu);
+  ghost_pipeline<double>(*h, field_up, ldf, lda, f_lb, f_ub, ghostsize, maptype,
+                         (cudaStream_t)stream, info, caller);
+}
+
+// ---- comp_weights / remesh ---------------------------------------------------
+void ppmg_rmsh_comp_weights_d(const double* xp, int64_t ldxp, int64_t Np, int topo_id,
+                              int mesh_id, int kernel, double* wx1, double* wx2,
+                              double* wx3, int* info) {
+  const char* caller = "ppmg_rmsh_comp_weights_d";
+  clear_error();
+  if (info) *info = 0;
+  Handle* hh = find_handle(topo_id, mesh_id);
+  if (!hh) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": topo_id/mesh_id is invalid"); return; }
+  const int dim = hh->dim;
+  if (Np < 0 || (Np > 0 && ldxp < dim) || Np >= (int64_t)1 << 31) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": invalid sizes"); return; }
+  if (!check_kernel(kernel, caller, info)) return;
+  Handle* h = get_checked(topo_id, mesh_id, dim, caller, info);
+  if (!h) return;
+  std::lock_guard<std::mutex> lk(h->mu);
+  cudaStream_t st = h->stream;
+  cudaError_t e;
+  const double* dxp = mirror<double>(h->ws_rmsh.h_xp, xp, ldxp * Np, st, e);
+  if (e) { cuda_fail(info, e, caller); return; }
+  KeyParams kp = make_kp(*h, KEY_INTERP_CHECKED, false);
+  e = bin_sort<double>(kp, dxp, ldxp, Np, h->g.ncell, h->ws_rmsh, h->d_status + 0, st);
+  if (e) { cuda_fail(info, e, caller); return; }
+  const int S = kernel == kKernelMp4 ? 4 : 2;
+  e = h->ws_rmsh.w1d.ensure(sizeof(double) * (size_t)(Np > 0 ? Np : 1) * dim * S);
+  if (e) { cuda_fail(info, e, caller); return; }
+  CWParams P{};
+  P.dim = dim;
+  P.S = S;
+  P.nvalid = Np;
+  P.d_nvalid = d_nvalid_of(h->ws_rmsh, h->g.ncell);
+  P.idx = h->ws_rmsh.idx.as<int>();
+  P.xp = dxp;
+  P.ldxp = ldxp;
+  for (int a = 0; a < 3; ++a) {
+    P.min_phys[a] = h->g.min_phys[a];
+    P.dxiq[a] = h->g.dxiq_d[a];
+    P.istart[a] = h->istart[a];
+  }
+  P.w = h->ws_rmsh.w1d.as<double>();
+  if ((e = launch_comp_weights(P, st))) { cuda_fail(info, e, caller); return; }
+  double* user[3] = {wx1, wx2, wx3};
+  const int ks = S / 2;
+  const int64_t nu = (int64_t)S * (Np + 2 * ks);
+  for (int a = 0; a < dim; ++a) {
+    if (!user[a]) continue;
+    double* dtmp = mirror<double>(h->ws_rmsh.h_aux, (const double*)nullptr, nu, st, e);
+    if (!e) e = cudaMemsetAsync(dtmp, 0, sizeof(double) * (size_t)nu, st);
+    if (!e) e = launch_weights_to_user(P.w, P.idx, Np, P.d_nvalid, dim, S, a, dtmp, st);
+    if (!e) e = cudaMemcpyAsync(user[a], dtmp, sizeof(double) * (size_t)nu,
+                                cudaMemcpyDeviceToHost, st);
+    if (!e) e = cudaStreamSynchronize(st);
+    if (e) { cuda_fail(info, e, caller); return; }
+  }
+  h->w_valid = true;
+  h->w_kernel = kernel;
+  h->w_np = Np;
+  read_status(*h, st, info, caller);
+}
+
+static void remesh_common(const double* xp, int64_t ldxp, int64_t Np, const double* up,
+                          int64_t ldup, int lda, int topo_id, int mesh_id, int kernel,
+                          const int* ghostsize, double* field_up, int64_t ldf,
+                          const int64_t* f_lb, const int64_t* f_ub, int* info, int dim,
+                          const char* caller) {
+  clear_error();
+  if (info) *info = 0;
+  if (Np < 0 || (Np > 0 && ldxp < dim) || lda < 1 || ldup < lda || ldf < lda) {
+    fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": invalid sizes");
+    return;
+  }
+  if (!check_kernel(kernel, caller, info)) return;
+  const int ks = kernel == kKernelMp4 ? 2 : 1;
+  for (int a = 0; a < dim; ++a)
+    if (ghostsize[a] < ks - 1) {  // ppm_rmsh_remesh.f:340-347
+      fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": ghostsize too small for this kernel");
+      return;
+    }
+  Handle* h = get_checked(topo_id, mesh_id, dim, caller, info);
+  if (!h) return;
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (!h->w_valid || h->w_kernel != kernel || h->w_np != Np) {
+    fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": compute weights before remeshing");
+    return;
+  }
+  cudaStream_t st = h->stream;
+  cudaError_t e;
+  const double* dxp = mirror<double>(h->ws_rmsh.h_xp, xp, ldxp * Np, st, e);
+  if (e) { cuda_fail(info, e, caller); return; }
+  const double* dup = mirror<double>(h->ws_rmsh.h_up, up, ldup * Np, st, e);
+  if (e) { cuda_fail(info, e, caller); return; }
+  const int64_t nf = field_elems(*h, ldf, f_lb, f_ub);
+  double* dfield = mirror<double>(h->ws_rmsh.h_field, (const double*)nullptr, nf, st, e);
+  if (e) { cuda_fail(info, e, caller); return; }
+  if (p2m_pipeline<double>(*h, dxp, ldxp, Np, dup, ldup, lda, kernel, ghostsize, dfield, ldf,
+                           f_lb, f_ub, true, st, info, caller))
+    return;
+  e = cudaMemcpyAsync(field_up, dfield, sizeof(double) * (size_t)nf, cudaMemcpyDeviceToHost, st);
+  if (e) { cuda_fail(info, e, caller); return; }
+  read_status(*h, st, info, caller);
+}
+
+void ppmg_rmsh_remesh_dv_3d(const double* xp, int64_t ldxp, int64_t Np, const double* up,
+                            int64_t ldup, int lda, int topo_id, int mesh_id, int kernel,
+                            const int* ghostsize, double* field_up, int64_t ldf,
+                            const int64_t* f_lb, const int64_t* f_ub, int* info) {
+  remesh_common(xp, ldxp, Np, up, ldup, lda, topo_id, mesh_id, kernel, ghostsize, field_up, ldf,
+                f_lb, f_ub, info, 3, "ppmg_rmsh_remesh_dv_3d");
+}
+void ppmg_rmsh_remesh_dv_2d(const double* xp, int64_t ldxp, int64_t Np, const double* up,
+                            int64_t ldup, int lda, int topo_id, int mesh_id, int kernel,
+                            const int* ghostsize, double* field_up, int64_t ldf,
+                            const int64_t* f_lb, const int64_t* f_ub, int* info) {
+  remesh_common(xp, ldxp, Np, up, ldup, lda, topo_id, mesh_id, kernel, ghostsize, field_up, ldf,
+                f_lb, f_ub, info, 2, "ppmg_rmsh_remesh_dv_2d");
+}
+
+// ---- create_part ---------------------------------------------------------------
+void ppmg_rmsh_create_part_d(const double* field_up, int64_t ldf, int lda,
+                             const int64_t* f_lb, const int64_t* f_ub, int topo_id,
+                             int mesh_id, const double* cutoff, const double* cutoff_weights,
+                             int resetpos, const double* field_wp, int64_t ldfw, int lda2,
+                             int64_t* np, double* up, double* xp, double* wp, int* info) {
+  const char* caller = "ppmg_rmsh_create_part_d";
+  clear_error();
+  if (info) *info = 0;
+  Handle* hh = find_handle(topo_id, mesh_id);
+  if (!hh) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": topo_id/mesh_id is invalid"); return; }
+  Handle* h = get_checked(topo_id, mesh_id, hh->dim, caller, info);
+  if (!h) return;
+  if (lda < 1 || ldf < lda || (field_wp && (lda2 < 1 || ldfw < lda2))) {
+    fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": lda / lda2 inconsistent");
+    return;
+  }
+  std::lock_guard<std::mutex> lk(h->mu);
+  const int dim = h->dim;
+  int lo[3] = {1, 1, 1}, hi[3];
+  for (int a = 0; a < dim; ++a) hi[a] = h->g.N[a];
+  FieldDesc fd, fdw;
+  if (!make_fd(*h, ldf, f_lb, f_ub, lo, hi, fd, caller, info)) return;
+  if (field_wp && !make_fd(*h, ldfw, f_lb, f_ub, lo, hi, fdw, caller, info)) return;
+  cudaStream_t st = h->stream;
+  cudaError_t e;
+  const int64_t nf = field_elems(*h, ldf, f_lb, f_ub);
+  const double* dfield = mirror<double>(h->ws.h_field, field_up, nf, st, e);
+  if (e) { cuda_fail(info, e, caller); return; }
+  const double* dfw = nullptr;
+  if (field_wp) {
+    dfw = mirror<double>(h->ws.h_xp, field_wp, field_elems(*h, ldfw, f_lb, f_ub), st, e);
+    if (e) { cuda_fail(info, e, caller); return; }
+  }
+  const double* dcw = nullptr;
+  if (cutoff_weights) {
+    dcw = mirror<double>(h->ws.w1d, cutoff_weights, lda, st, e);
+    if (e) { cuda_fail(info, e, caller); return; }
+  }
+  CPParams P{};
+  P.dim = dim;
+  P.lda = lda;
+  P.lda2 = lda2;
+  for (int a = 0; a < 3; ++a) {
+    // periodic axes visit nodes 1..Nm-1 (ppm_rmsh_create_part.f:433-453)
+    P.nn[a] = a < dim ? h->g.N[a] : 1;
+    P.h[a] = h->g.h_d[a];
+    P.min_sub[a] = h->g.min_sub[a];
+  }
+  P.field = dfield;
+  P.fd = fd;
+  P.field_wp = dfw;
+  P.fdw = fdw;
+  P.cw = dcw;
+  P.cut0 = cutoff[0];
+  P.cut1 = cutoff[1];
+  const int64_t nq = (int64_t)P.nn[0] * P.nn[1] * P.nn[2];
+  if ((e = h->ws.count.ensure(sizeof(int) * (size_t)(nq + 1))) ||
+      (e = h->ws.start.ensure(sizeof(int) * (size_t)(nq + 1)))) { cuda_fail(info, e, caller); return; }
+  int* flag = h->ws.count.as<int>();
+  int* pos = h->ws.start.as<int>();
+  if ((e = cudaMemsetAsync(flag + nq, 0, sizeof(int), st))) { cuda_fail(info, e, caller); return; }
+  if ((e = launch_cp_flag(P, flag, st))) { cuda_fail(info, e, caller); return; }
+  if ((e = scan_exclusive(flag, pos, nq + 1, h->ws, st))) { cuda_fail(info, e, caller); return; }
+  int total = 0;
+  e = cudaMemcpyAsync(&total, pos + nq, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (!e) e = cudaStreamSynchronize(st);
+  if (e) { cuda_fail(info, e, caller); return; }
+  if (np) *np = total;
+  if (!up) return;  // counting call
+  double* dout = mirror<double>(h->ws.h_aux, (const double*)nullptr,
+                                (int64_t)total * (lda + dim + (field_wp ? lda2 : 0)), st, e);
+  if (e) { cuda_fail(info, e, caller); return; }
+  P.up = dout;
+  P.xp = resetpos ? dout + (int64_t)total * lda : nullptr;
+  P.wp = field_wp ? dout + (int64_t)total * (lda + dim) : nullptr;
+  if ((e = launch_cp_fill(P, flag, pos, st))) { cuda_fail(info, e, caller); return; }
+  if (total > 0) {
+    e = cudaMemcpyAsync(up, P.up, sizeof(double) * (size_t)total * lda, cudaMemcpyDeviceToHost, st);
+    if (!e && resetpos && xp)
+      e = cudaMemcpyAsync(xp, P.xp, sizeof(double) * (size_t)total * dim, cudaMemcpyDeviceToHost, st);
+    if (!e && field_wp && wp)
+      e = cudaMemcpyAsync(wp, P.wp, sizeof(double) * (size_t)total * lda2, cudaMemcpyDeviceToHost, st);
+  }
+  if (!e) e = cudaStreamSynchronize(st);
+  if (e) cuda_fail(info, e, caller);
+}
+
+// ---- cell lists -------------------------------------------------------------------
+static void rank_common(int dim, const double* xp, int64_t ldxp, int64_t Np, const double* xmin,
+                        const double* xmax, const int* Nm, const int* Ngl, int* lpdx, int* lhbx,
+                        int64_t* icount, int* info, const char* caller) {
+  clear_error();
+  if (info) *info = 0;
+  if (Np < 0 || (Np > 0 && ldxp < dim) || Np >= (int64_t)1 << 31) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": invalid sizes"); return; }
+  ClistParams cp{};
+  cp.dim = dim;
+  int64_t nbox = 1;
+  for (int a = 0; a < 3; ++a) {
+    cp.Nm[a] = a < dim ? Nm[a] : 1;
+    cp.Nt[a] = a < dim ? Nm[a] + Ngl[a] + Ngl[dim + a] : 1;
+    cp.xmin[a] = a < dim ? xmin[a] : 0.0;
+    cp.xmax[a] = a < dim ? xmax[a] : 1.0;
+    cp.rd[a] = a < dim ? (double)Nm[a] / (xmax[a] - xmin[a]) : 1.0;
+    nbox *= cp.Nt[a];
+  }
+  for (int a = 0; a < dim; ++a) {
+    cp.Ngl[a] = Ngl[a];
+    if (Nm[a] <= 0 || !(xmax[a] > xmin[a])) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": Nm must be > 0 and xmax > xmin"); return; }
+  }
+  if (nbox >= ((int64_t)1 << 31) - 1) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": too many boxes"); return; }
+  // a private workspace per call: cell lists are independent of any mesh handle
+  static std::mutex mu;
+  static Workspace ws;
+  static cudaStream_t st = nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  cudaError_t e = cudaSuccess;
+  if (!st) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  if (e) { cuda_fail(info, e, caller); return; }
+  const double* dxp = mirror<double>(ws.h_xp, xp, ldxp * Np, st, e);
+  if (e) { cuda_fail(info, e, caller); return; }
+  if ((e = clist_sort(cp, dxp, ldxp, Np, nbox, ws, st))) { cuda_fail(info, e, caller); return; }
+  int nin = 0;
+  e = cudaMemcpyAsync(&nin, ws.err.p, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (!e) e = ws.h_aux.ensure(sizeof(int) * (size_t)(Np + nbox + 2));
+  if (e) { cuda_fail(info, e, caller); return; }
+  int* dl = ws.h_aux.as<int>();
+  int* dh = dl + (Np > 0 ? Np : 1);
+  if ((e = launch_plus_one(ws.idx.as<int>(), dl, Np, st)) ||
+      (e = launch_plus_one(ws.start.as<int>(), dh, nbox + 1, st))) { cuda_fail(info, e, caller); return; }
+  e = cudaStreamSynchronize(st);
+  if (!e && nin > 0) e = cudaMemcpy(lpdx, dl, sizeof(int) * (size_t)nin, cudaMemcpyDeviceToHost);
+  if (!e) e = cudaMemcpy(lhbx, dh, sizeof(int) * (size_t)(nbox + 1), cudaMemcpyDeviceToHost);
+  if (e) { cuda_fail(info, e, caller); return; }
+  if (icount) *icount = nin;
+}
+
+void ppmg_util_rank3d_d(const double* xp, int64_t ldxp, int64_t Np, const double* xmin,
+                        const double* xmax, const int* Nm, const int* Ngl, int* lpdx,
+                        int* lhbx, int64_t* icount, int* info) {
+  rank_common(3, xp, ldxp, Np, xmin, xmax, Nm, Ngl, lpdx, lhbx, icount, info,
+              "ppmg_util_rank3d_d");
+}
+void ppmg_util_rank2d_d(const double* xp, int64_t ldxp, int64_t Np, const double* xmin,
+                        const double* xmax, const int* Nm, const int* Ngl, int* lpdx,
+                        int* lhbx, int64_t* icount, int* info) {
+  rank_common(2, xp, ldxp, Np, xmin, xmax, Nm, Ngl, lpdx, lhbx, icount, info,
+              "ppmg_util_rank2d_d");
+}
+
+}  // extern "C"

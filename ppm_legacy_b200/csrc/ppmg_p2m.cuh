@@ -1,0 +1,35 @@
+// ppmg_p2m.cuh -- launch interface of the particle -> mesh tile gather.
+#pragma once
+
+#include "ppmg_common.cuh"
+
+namespace ppmg {
+
+enum P2MPrec {
+  P2M_FP64 = 0,   // FP64 weights and sums
+  P2M_MIXED = 1,  // FP32 weights/products, compensated FP32 sums, FP64 field
+  P2M_FP32 = 2,   // single-precision API: FP32 throughout
+};
+
+struct P2MParams {
+  int N[3];            // cells per axis
+  int TZ;              // tile depth along the sweep axis (z in 3D, y in 2D)
+  int cap;             // staging capacity (particles per chunk)
+  int c0;              // first component written by this launch
+  const int* start;    // cell offsets into the sorted particle order
+  const void* rec;     // Vec4 (fx, fy, fz, cell) per sorted particle
+  const void* us;      // Vec4 strengths (4 components of one chunk)
+  void* field;         // field_up base (element (1, lb...))
+  FieldDesc fd;
+};
+
+// Tile depth (nodes along the sweep axis per CTA) for a mesh of N cells.
+int p2m_tile_depth(int dim, const int N[3]);
+
+// Launch the gather for all components (chunks of 4) of a P2M / remesh.
+// stored_weights: P.rec holds FP64 1D weights per sorted particle
+// (wx[S], wy[S][, wz[S]]) from comp_weights instead of offset records.
+cudaError_t launch_p2m(const P2MParams& P, int dim, int kernel, P2MPrec prec, int lda,
+                       int64_t nvalid, bool stored_weights, cudaStream_t st);
+
+}  // namespace ppmg

@@ -1,0 +1,329 @@
+"""Host mirror of the reference's interpolation / remeshing API.
+
+Each function keeps the reference routine's name and argument list
+(ppm/src/ppm_interp_p2m.f:127-163, ppm_interp_m2p.f:126-162,
+ppm_rmsh_comp_weights.f:96-103, ppm_rmsh_remesh.f:90-124,
+ppm_rmsh_create_part.f:90-171, ppm_map_field_ghost.f:61-89) and resolves the
+specific variant the way the Fortran generic interface does: kind from the
+array type (float64 'd' / float32 's'), scalar or vector from the rank of
+``up`` (vector variants take ``lda``), 2D or 3D from the rank of ``field_up``.
+Every call goes through libppmg.so; ``info`` is returned (0 on success, the
+reference's severities otherwise; see ``last_error``).
+
+Arrays use the Fortran layout: ``xp`` (ldxp, Np), ``up`` (lda, Np) or (Np,),
+``field_up`` (lda, nx, ny[, nz], 1) (vector) or (nx, ny[, nz], 1) (scalar),
+all column-major.  ``field_up``'s lower bounds default to 1-ghostsize as the
+reference allocates them; pass ``field_lb`` for a different allocation.
+numpy arrays run the synchronous host entry points; CUDA torch tensors run the
+``_dev`` entry points on the current torch stream.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import params as P
+from ._lib import int_array, last_error, lib  # noqa: F401
+
+try:  # torch is optional: only the device-pointer path needs it
+    import torch
+except Exception:  # pragma: no cover
+    torch = None
+
+
+def _is_dev(a) -> bool:
+    return torch is not None and isinstance(a, torch.Tensor) and a.is_cuda
+
+
+def _colmajor(a) -> bool:
+    if _is_dev(a) or (torch is not None and isinstance(a, torch.Tensor)):
+        exp = 1
+        for n, s in zip(a.shape, a.stride()):
+            if n > 1 and s != exp:
+                return False
+            exp *= n
+        return True
+    return a.flags.f_contiguous
+
+
+def _addr(a) -> int:
+    if torch is not None and isinstance(a, torch.Tensor):
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+def _kind(a) -> str:
+    dt = a.dtype
+    if torch is not None and isinstance(a, torch.Tensor):
+        if dt == torch.float64:
+            return "d"
+        if dt == torch.float32:
+            return "s"
+    else:
+        if dt == np.float64:
+            return "d"
+        if dt == np.float32:
+            return "s"
+    raise TypeError(f"unsupported dtype {dt}")
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _bounds(field, dim, vector, ghostsize, field_lb):
+    shape = tuple(field.shape)
+    sp = shape[1:1 + dim] if vector else shape[:dim]
+    lb = [1 - int(ghostsize[a]) for a in range(dim)] if field_lb is None else list(field_lb)
+    ub = [lb[a] + int(sp[a]) - 1 for a in range(dim)]
+    return int_array(lb, C.c_int64), int_array(ub, C.c_int64)
+
+
+def _check(*arrays):
+    for a in arrays:
+        if a is not None and not _colmajor(a):
+            raise ValueError("arrays must be column-major (Fortran order)")
+
+
+def _split(up, args, name):
+    if len(args) == 6:
+        lda, topo_id, mesh_id, kernel, ghostsize, field_up = args
+        return True, int(lda), topo_id, mesh_id, kernel, ghostsize, field_up
+    if len(args) == 5:
+        topo_id, mesh_id, kernel, ghostsize, field_up = args
+        return False, 1, topo_id, mesh_id, kernel, ghostsize, field_up
+    raise TypeError(f"{name}: wrong number of arguments")
+
+
+def ppm_interp_p2m(xp, Np, up, *args, field_lb=None):
+    """ppm_interp_p2m(xp, Np, up, [lda,] topo_id, mesh_id, kernel, ghostsize, field_up)."""
+    vector, lda, topo_id, mesh_id, kernel, ghostsize, field_up = _split(up, args, "ppm_interp_p2m")
+    _check(xp, up, field_up)
+    dim = field_up.ndim - (2 if vector else 1)
+    k = _kind(xp)
+    lb, ub = _bounds(field_up, dim, vector, ghostsize, field_lb)
+    info = C.c_int(0)
+    g = int_array(ghostsize)
+    dev = _is_dev(xp)
+    name = f"ppmg_interp_p2m_{k}{'v' if vector else 's'}_{dim}d"
+    if vector:
+        a = (_addr(xp), xp.shape[0], int(Np), _addr(up), up.shape[0], lda, topo_id, mesh_id,
+             kernel, g, _addr(field_up), field_up.shape[0], lb, ub, C.byref(info))
+        if dev:
+            getattr(lib(), name + "_dev")(*a, _stream())
+        else:
+            getattr(lib(), name)(*a)
+    else:
+        if dev:
+            raise TypeError("device (torch) arrays use the vector variant (pass lda)")
+        getattr(lib(), name)(_addr(xp), xp.shape[0], int(Np), _addr(up), topo_id, mesh_id,
+                             kernel, g, _addr(field_up), lb, ub, C.byref(info))
+    return info.value
+
+
+def ppm_interp_m2p(xp, Np, up, *args, field_lb=None):
+    """ppm_interp_m2p(xp, Np, up, [lda,] topo_id, mesh_id, kernel, ghostsize, field_up)."""
+    vector, lda, topo_id, mesh_id, kernel, ghostsize, field_up = _split(up, args, "ppm_interp_m2p")
+    _check(xp, up, field_up)
+    dim = field_up.ndim - (2 if vector else 1)
+    k = _kind(xp)
+    lb, ub = _bounds(field_up, dim, vector, ghostsize, field_lb)
+    info = C.c_int(0)
+    g = int_array(ghostsize)
+    dev = _is_dev(xp)
+    name = f"ppmg_interp_m2p_{k}{'v' if vector else 's'}_{dim}d"
+    if vector:
+        a = (_addr(xp), xp.shape[0], int(Np), _addr(up), up.shape[0], lda, topo_id, mesh_id,
+             kernel, g, _addr(field_up), field_up.shape[0], lb, ub, C.byref(info))
+        if dev:
+            getattr(lib(), name + "_dev")(*a, _stream())
+        else:
+            getattr(lib(), name)(*a)
+    else:
+        if dev:
+            raise TypeError("device (torch) arrays use the vector variant (pass lda)")
+        getattr(lib(), name)(_addr(xp), xp.shape[0], int(Np), _addr(up), topo_id, mesh_id,
+                             kernel, g, _addr(field_up), lb, ub, C.byref(info))
+    return info.value
+
+
+def ppm_interp_p2m_adjoint(xp, Np, up, lda, topo_id, mesh_id, kernel, r_field, dw, dx,
+                           ghostsize=(0, 0, 0), field_lb=None):
+    """Adjoint of P2M (3D, FP64): dw = M2P(r), dx = sum_a up(a) grad_x W . r(a)."""
+    _check(xp, up, r_field, dw, dx)
+    lb, ub = _bounds(r_field, 3, True, ghostsize, field_lb)
+    info = C.c_int(0)
+    a = (_addr(xp), xp.shape[0], int(Np), _addr(up), up.shape[0], int(lda), topo_id, mesh_id,
+         kernel, _addr(r_field), r_field.shape[0], lb, ub, _addr(dw), dw.shape[0], _addr(dx),
+         dx.shape[0], C.byref(info))
+    if _is_dev(xp):
+        lib().ppmg_interp_p2m_adjoint_dv_3d_dev(*a, _stream())
+    else:
+        lib().ppmg_interp_p2m_adjoint_dv_3d(*a)
+    return info.value
+
+
+def ppm_map_field_ghost(field_up, *args, field_lb=None):
+    """ppm_map_field_ghost(field_up, [lda,] topo_id, mesh_id, ghostsize, maptype).
+
+    maptype ppm_param_map_ghost_get or ppm_param_map_ghost_put; the
+    init/push/send/pop steps of the reference happen inside the call.
+    """
+    if len(args) == 5:
+        lda, topo_id, mesh_id, ghostsize, maptype = args
+        vector = True
+    else:
+        topo_id, mesh_id, ghostsize, maptype = args
+        lda, vector = 1, False
+    _check(field_up)
+    dim = field_up.ndim - (2 if vector else 1)
+    lb, ub = _bounds(field_up, dim, vector, ghostsize, field_lb)
+    info = C.c_int(0)
+    ldf = field_up.shape[0] if vector else 1
+    a = (_addr(field_up), ldf, int(lda), lb, ub, topo_id, mesh_id, int_array(ghostsize),
+         int(maptype), C.byref(info))
+    k = _kind(field_up)
+    if _is_dev(field_up):
+        if k != "d":
+            raise TypeError("device ghost mapping supports float64 fields")
+        lib().ppmg_map_field_ghost_d_dev(*a, _stream())
+    else:
+        getattr(lib(), f"ppmg_map_field_ghost_{k}")(*a)
+    return info.value
+
+
+def ppm_rmsh_comp_weights(xp, Np, topo_id, mesh_id, kernel, wx1_user=None, wx2_user=None,
+                          wx3_user=None):
+    """ppm_rmsh_comp_weights(xp, Np, topo_id, mesh_id, kernel[, wx1, wx2, wx3]).
+
+    The weights stay in the library (like the reference's module state); user
+    arrays, when given, must be float64 (2ks, 1, Np+2ks) column-major.
+    """
+    _check(xp)
+    info = C.c_int(0)
+    w = [None if u is None else _addr(u) for u in (wx1_user, wx2_user, wx3_user)]
+    lib().ppmg_rmsh_comp_weights_d(_addr(xp), xp.shape[0], int(Np), topo_id, mesh_id, kernel,
+                                   w[0], w[1], w[2], C.byref(info))
+    return info.value
+
+
+def ppm_rmsh_remesh(xp, Np, up, *args, field_lb=None):
+    """ppm_rmsh_remesh(xp, Np, up, [lda,] topo_id, mesh_id, kernel, ghostsize, field_up).
+
+    The reference puts ``info`` before ``field_up``; here ``field_up`` must be
+    preallocated by the caller (the reference's ppm_alloc grow step) and is
+    overwritten entirely (zeroed, then the remeshed field).
+    """
+    vector, lda, topo_id, mesh_id, kernel, ghostsize, field_up = _split(up, args, "ppm_rmsh_remesh")
+    _check(xp, up, field_up)
+    dim = field_up.ndim - (2 if vector else 1)
+    lb, ub = _bounds(field_up, dim, vector, ghostsize, field_lb)
+    info = C.c_int(0)
+    ldup = up.shape[0] if vector else 1
+    ldf = field_up.shape[0] if vector else 1
+    getattr(lib(), f"ppmg_rmsh_remesh_dv_{dim}d")(
+        _addr(xp), xp.shape[0], int(Np), _addr(up), ldup, lda, topo_id, mesh_id, kernel,
+        int_array(ghostsize), _addr(field_up), ldf, lb, ub, C.byref(info))
+    return info.value
+
+
+def ppm_rmsh_create_part(field_up, topo_id, mesh_id, cutoff, lda=None, resetpos=False,
+                         cutoff_weights=None, field_wp=None, ghostsize=(0, 0, 0),
+                         field_lb=None):
+    """ppm_rmsh_create_part: returns (info, np, up, xp, wp).
+
+    The reference reallocates xp/up/wp in place (POINTER arguments); this
+    mirror returns the new arrays: up (lda, np), xp (dim, np) when resetpos,
+    wp (lda2, np) when field_wp is given.
+    """
+    vector = lda is not None
+    lda = int(lda) if vector else 1
+    _check(field_up)
+    dim = field_up.ndim - (2 if vector else 1)
+    lb, ub = _bounds(field_up, dim, vector, ghostsize, field_lb)
+    ldf = field_up.shape[0] if vector else 1
+    cut = np.asarray(cutoff, dtype=np.float64)
+    cw = None if cutoff_weights is None else np.ascontiguousarray(cutoff_weights, dtype=np.float64)
+    lda2 = 0
+    ldfw = 0
+    if field_wp is not None:
+        _check(field_wp)
+        lda2 = field_wp.shape[0] if field_wp.ndim == dim + 2 else 1
+        ldfw = lda2
+    n = C.c_int64(0)
+    info = C.c_int(0)
+    fn = lib().ppmg_rmsh_create_part_d
+    common = (_addr(field_up), ldf, lda, lb, ub, topo_id, mesh_id, cut.ctypes.data,
+              None if cw is None else cw.ctypes.data, int(bool(resetpos)),
+              None if field_wp is None else _addr(field_wp), ldfw, lda2)
+    fn(*common, C.byref(n), None, None, None, C.byref(info))
+    if info.value != 0:
+        return info.value, 0, None, None, None
+    npn = n.value
+    up = np.zeros((lda, npn), order="F")
+    xp = np.zeros((dim, npn), order="F") if resetpos else None
+    wp = np.zeros((max(lda2, 1), npn), order="F") if field_wp is not None else None
+    fn(*common, C.byref(n), up.ctypes.data, None if xp is None else xp.ctypes.data,
+       None if wp is None else wp.ctypes.data, C.byref(info))
+    if not vector:
+        up = up.reshape(-1)
+    return info.value, npn, up, xp, wp
+
+
+def ppm_util_rank(xp, Np, xmin, xmax, Nm, Ngl):
+    """ppm_util_rank{2,3}d: returns (info, lpdx, lhbx) with 1-based entries."""
+    _check(xp)
+    dim = len(Nm)
+    nbox = 1
+    for a in range(dim):
+        nbox *= int(Nm[a]) + int(Ngl[a]) + int(Ngl[dim + a])
+    lpdx = np.zeros(max(int(Np), 1), dtype=np.int32)
+    lhbx = np.zeros(nbox + 1, dtype=np.int32)
+    ic = C.c_int64(0)
+    info = C.c_int(0)
+    xmin = np.ascontiguousarray(xmin, dtype=np.float64)
+    xmax = np.ascontiguousarray(xmax, dtype=np.float64)
+    getattr(lib(), f"ppmg_util_rank{dim}d_d")(
+        _addr(xp), xp.shape[0], int(Np), xmin.ctypes.data, xmax.ctypes.data, int_array(Nm),
+        int_array(Ngl), lpdx.ctypes.data, lhbx.ctypes.data, C.byref(ic), C.byref(info))
+    return info.value, lpdx[: ic.value], lhbx
+
+
+def ppm_neighlist_clist(xp, Np, cutoff, lsymm, topo, isub=0):
+    """ppm_neighlist_clist for one sub (ppm/src/ppm_neighlist_clist.f:300-440).
+
+    Returns (info, lpdx, lhbx, Nm): cells of size >= cutoff over the sub,
+    one ghost layer on every side (or only on the upper sides when lsymm).
+    """
+    dim = topo.dim
+    xmin = topo.min_sub[isub, :dim]
+    xmax = topo.max_sub[isub, :dim]
+    cutoff = np.resize(np.asarray(cutoff, dtype=np.float64), dim)
+    Nm = [max(int((xmax[a] - xmin[a]) / cutoff[a]), 1) for a in range(dim)]
+    if lsymm:
+        Ngl = [0] * dim + [1] * dim
+    else:
+        Ngl = [1] * (2 * dim)
+    info, lpdx, lhbx = ppm_util_rank(xp, Np, xmin, xmax, Nm, Ngl)
+    Nm_out = [Nm[a] + Ngl[a] + Ngl[dim + a] for a in range(dim)]
+    return info, lpdx, lhbx, Nm_out
+
+
+def set_precision(mode: int) -> int:
+    """0 = FP64 (default), 1 = mixed (FP64 offsets, FP32 weights, compensated sums)."""
+    info = C.c_int(0)
+    lib().ppmg_set_precision(int(mode), C.byref(info))
+    return info.value
+
+
+def sync_status(topo_id, mesh_id, stream=None) -> int:
+    """Waits for a handle's device-pointer calls and returns their data-dependent info."""
+    info = C.c_int(0)
+    if stream is None and torch is not None and torch.cuda.is_available():
+        stream = _stream()
+    lib().ppmg_sync_status(topo_id, mesh_id, stream, C.byref(info))
+    return info.value
+
+
+PPM = P  # the reference constants, e.g. PPM.ppm_param_rmsh_kernel_mp4

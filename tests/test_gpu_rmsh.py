@@ -1,0 +1,164 @@
+"""GPU parity of remeshing, ghost get/put, cell ranking and the P2M adjoint."""
+import numpy as np
+import pytest
+
+import ppm_legacy_b200 as ppmg
+from _util import (box_bounds, golden_cases, max_rel, periodic_fill, random_particles, topo_for,
+                   unique_view)
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+_next_id = [500]
+
+
+def registered(dim, nc, lo=None, hi=None):
+    _next_id[0] += 1
+    t = topo_for(dim, nc, lo, hi, topo_id=_next_id[0], mesh_id=1)
+    assert ppmg.register(t) == 0, ppmg.last_error()
+    return t
+
+
+@pytest.mark.parametrize("dim,kernel,nc,box", [
+    (3, 2, 16, None), (3, 1, 12, None), (2, 2, 24, None),
+    (3, 2, 10, ([0.0, 0.0, 0.0], [1.3, 1.0, 0.7])),
+])
+def test_comp_weights_and_remesh_match_oracle(dim, kernel, nc, box):
+    rng = np.random.default_rng(40 + nc)
+    lo, hi = box if box else (None, None)
+    t = registered(dim, nc, lo, hi)
+    g = [2] * dim
+    xp = random_particles(rng, dim, 2 * nc ** dim, t.min_phys[:dim], t.max_phys[:dim])
+    up = rng.standard_normal((3, xp.shape[1]))
+    np_ = xp.shape[1]
+    ks = 2 if kernel == 2 else 1
+    wx = [np.zeros((2 * ks, 1, np_ + 2 * ks), order="F") for _ in range(3)]
+    info = ppmg.ppm_rmsh_comp_weights(xp, np_, t.topo_id, t.mesh_id, kernel, wx[0], wx[1],
+                                      wx[2] if dim == 3 else None)
+    assert info == 0, ppmg.last_error()
+    wo, lst, si = O.comp_weights(t, xp, kernel)
+    for a in range(dim):
+        # the oracle's list is ascending particle id, as is the user layout here
+        assert np.array_equal(wx[a], wo[a])
+    lb, ub = box_bounds(t, g)
+    f = np.full((3,) + tuple(ub[a] - lb[a] + 1 for a in range(dim)) + (1,), 5.0, order="F")
+    info = ppmg.ppm_rmsh_remesh(xp, np_, up, 3, t.topo_id, t.mesh_id, kernel, g, f)
+    assert info == 0, ppmg.last_error()
+    fo, lbo, ubo = O.remesh(t, xp, up, kernel, g, wo, lst, si)
+    real = (slice(None),) + tuple(slice(1 - lb[a], t.Nm[a] + 1 - lb[a]) for a in range(dim)) + (0,)
+    assert max_rel(f[real], fo[real]) < 1e-13
+
+
+def test_remesh_without_weights_is_refused():
+    t = registered(3, 8)
+    xp = random_particles(np.random.default_rng(0), 3, 10)
+    f = np.zeros((1, 13, 13, 13, 1), order="F")
+    info = ppmg.ppm_rmsh_remesh(xp, 10, np.ones((1, 10), order="F"), 1, t.topo_id, t.mesh_id, 2,
+                                [2, 2, 2], f)
+    assert info == -2 and "weights" in ppmg.last_error()[2]
+
+
+@pytest.mark.parametrize("dim,lda,weights", [(3, 3, False), (3, 1, False), (2, 2, True)])
+def test_create_part_matches_oracle(dim, lda, weights):
+    rng = np.random.default_rng(50 + lda)
+    nc = 12
+    t = registered(dim, nc)
+    g = [1] * dim
+    lb, ub = box_bounds(t, g)
+    U = rng.standard_normal((lda,) + (nc,) * dim)
+    U[np.abs(U) < 0.8] = 0.0
+    F = periodic_fill(U, lb, ub, dim)
+    cw = [0.5, 2.0][:lda] if weights else None
+    cut = [0.3, 2.5]
+    info, n, up, xp, _ = ppmg.ppm_rmsh_create_part(F, t.topo_id, t.mesh_id, cut, lda=lda,
+                                                   resetpos=True, cutoff_weights=cw, ghostsize=g)
+    assert info == 0, ppmg.last_error()
+    no, upo, xpo, _ = O.create_part(t, F, lb, ub, cut, cutoff_weights=cw)
+    assert n == no and n > 0
+    assert np.array_equal(up.reshape(lda, -1), upo)
+    assert np.array_equal(xp, xpo)
+
+
+@pytest.mark.parametrize("dim,lda", [(3, 3), (2, 1)])
+def test_ghost_get_put_match_oracle(dim, lda):
+    rng = np.random.default_rng(60 + dim)
+    nc = 10
+    t = registered(dim, nc)
+    g = [2] * dim
+    lb, ub = box_bounds(t, g)
+    # put: start from an arbitrary box (stale ghosts, as after a deposit)
+    F = np.asfortranarray(rng.standard_normal((lda,) + tuple(ub[a] - lb[a] + 1 for a in range(dim)) + (1,)))
+    Fo = F.copy(order="F")
+    O.ghost_put(t, Fo, lb, ub, g)
+    Fg = F.copy(order="F")
+    assert ppmg.ppm_map_field_ghost(Fg, lda, t.topo_id, t.mesh_id, g,
+                                    ppmg.params.ppm_param_map_ghost_put) == 0
+    assert max_rel(Fg, Fo) < 1e-15
+    # get on a consistent field reproduces the periodic images exactly
+    U = rng.standard_normal((lda,) + (nc,) * dim)
+    G = periodic_fill(U, lb, ub, dim)
+    G2 = np.zeros_like(G, order="F")
+    real = (slice(None),) + tuple(slice(1 - lb[a], 1 - lb[a] + nc) for a in range(dim)) + (0,)
+    G2[real] = U  # only the real unique nodes are set; ghosts and node Nm are stale
+    assert ppmg.ppm_map_field_ghost(G2, lda, t.topo_id, t.mesh_id, g,
+                                    ppmg.params.ppm_param_map_ghost_get) == 0
+    assert np.array_equal(G2, G)
+
+
+@pytest.mark.parametrize("case", golden_cases("rank"), ids=lambda c: c["name"])
+def test_util_rank_bit_exact(case):
+    xp = np.asfortranarray(np.array(case["xp"]).T)
+    info, lpdx, lhbx = ppmg.ppm_util_rank(xp, xp.shape[1], case["xmin"], case["xmax"],
+                                          case["Nm"], case["Ngl"])
+    assert info == 0, ppmg.last_error()
+    assert lpdx.tolist() == case["lpdx"]
+    assert lhbx.tolist() == case["lhbx"]
+
+
+def test_neighlist_clist_large_bit_exact():
+    rng = np.random.default_rng(70)
+    t = topo_for(3, 64)
+    xp = random_particles(rng, 3, 300000)
+    xp[:, :1000] = 0.5  # a crowded cell (block-cooperative sort path)
+    info, lpdx, lhbx, Nm = ppmg.ppm_neighlist_clist(xp, xp.shape[1], 1.0 / 40, False, t)
+    assert info == 0
+    ref_l, ref_h, ic = O.rank(xp, t.min_sub[0], t.max_sub[0], [40, 40, 40], [1] * 6)
+    assert np.array_equal(lpdx, ref_l) and np.array_equal(lhbx, ref_h)
+
+
+@pytest.mark.parametrize("kernel", [2, 1])
+def test_adjoint_matches_oracle_and_finite_differences(kernel):
+    rng = np.random.default_rng(80 + kernel)
+    nc = 16
+    t = registered(3, nc)
+    lb = [1, 1, 1]
+    np_ = 3000
+    xp = random_particles(rng, 3, np_, 0.05, 0.95)
+    up = np.asfortranarray(rng.standard_normal((2, np_)))
+    R = np.asfortranarray(rng.standard_normal((2, nc, nc, nc, 1)))
+    dw = np.zeros((2, np_), order="F")
+    dx = np.zeros((3, np_), order="F")
+    info = ppmg.ppm_interp_p2m_adjoint(xp, np_, up, 2, t.topo_id, t.mesh_id, kernel, R, dw, dx,
+                                       field_lb=lb)
+    assert info == 0, ppmg.last_error()
+    dwo, dxo = O.p2m_adjoint(t, xp, up, R, lb, [nc] * 3, kernel)
+    assert max_rel(dw, dwo) < 1e-13
+    assert max_rel(dx, dxo) < 1e-12
+    # central finite differences of L = <P2M(x, w), R> in FP64 (step 1e-6 h)
+    h = 1.0 / nc
+    g = [2, 2, 2]
+    Ru = R[..., 0]
+
+    def loss(xq):
+        f, lbq, _ = O.p2m(t, xq, up[:, :5], kernel, g)
+        return float((unique_view(f, lbq, [nc] * 3, 3) * Ru).sum())
+
+    for p in range(5):
+        for a in range(3):
+            e = 1e-6 * h
+            xa = xp[:, :5].copy(order="F")
+            xb = xp[:, :5].copy(order="F")
+            xa[a, p] += e
+            xb[a, p] -= e
+            fd = (loss(xa) - loss(xb)) / (2 * e)
+            assert abs(fd - dx[a, p]) <= 1e-4 * max(1.0, abs(fd))
