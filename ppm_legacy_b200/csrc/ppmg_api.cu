@@ -65,8 +65,13 @@ struct Handle {
   }
 };
 
+// Heap-allocated and never destroyed: handle destructors call into the CUDA
+// runtime, which must not happen from static destructors at process exit.
 std::mutex g_mu;
-std::map<std::pair<int, int>, std::unique_ptr<Handle>> g_handles;
+std::map<std::pair<int, int>, std::unique_ptr<Handle>>& handles() {
+  static auto* m = new std::map<std::pair<int, int>, std::unique_ptr<Handle>>();
+  return *m;
+}
 
 int fail(int* info, int sev, int errnum, const std::string& msg) {
   set_error(sev, errnum, msg);
@@ -83,8 +88,8 @@ int cuda_fail(int* info, cudaError_t e, const char* where) {
 
 Handle* find_handle(int topo_id, int mesh_id) {
   std::lock_guard<std::mutex> lk(g_mu);
-  auto it = g_handles.find({topo_id, mesh_id});
-  return it == g_handles.end() ? nullptr : it->second.get();
+  auto it = handles().find({topo_id, mesh_id});
+  return it == handles().end() ? nullptr : it->second.get();
 }
 
 // Checks shared by every hot-path entry point (the ppm_debug > 0 checks of
@@ -188,11 +193,24 @@ constexpr bool is_f32() { return sizeof(T) == 4; }
 // ---------------------------------------------------------------------------
 // P2M pipeline (stream-ordered).  Returns 0 or the argument-error info.
 // ---------------------------------------------------------------------------
+// ghostsize(1:dim) must be >= 0 and small against the mesh (the periodic
+// image arithmetic of the fused ghost write assumes g < 16 * Nc).
+bool check_ghost(const Handle& h, const int* ghost, const char* caller, int* info) {
+  for (int a = 0; a < h.dim; ++a)
+    if (ghost[a] < 0 || ghost[a] > 16 * h.g.N[a]) {
+      fail(info, kErrorError, kErrArgument,
+           std::string(caller) + ": ghostsize must be >= 0 and <= 16 * (Nm - 1)");
+      return false;
+    }
+  return true;
+}
+
 template <class T>
 int p2m_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, const T* up, int64_t ldup,
                  int lda, int kernel, const int* ghost, T* field, int64_t ldf,
                  const int64_t* f_lb, const int64_t* f_ub, bool remesh, cudaStream_t st,
                  int* info, const char* caller) {
+  if (!check_ghost(h, ghost, caller, info)) return *info;
   int lo[3], hi[3];
   for (int a = 0; a < h.dim; ++a) {
     lo[a] = 1 - ghost[a];
@@ -482,6 +500,7 @@ int ghost_pipeline(Handle& h, T* field, int64_t ldf, int lda, const int64_t* f_l
   if (maptype != kMapGhostGet && maptype != kMapGhostPut)
     return fail(info, kErrorError, kErrArgument,
                 std::string(caller) + ": maptype must be ghost_get (5) or ghost_put (6)");
+  if (!check_ghost(h, ghost, caller, info)) return *info;
   int lo[3], hi[3];
   for (int a = 0; a < h.dim; ++a) {
     lo[a] = 1 - ghost[a];
@@ -633,7 +652,7 @@ void ppmg_mesh_register(int topo_id, int mesh_id, int dim, const double* min_phy
   if (!e) e = cudaMemset(h->d_status, 0, 4 * sizeof(int));
   if (e) { cuda_fail(info, e, "ppmg_mesh_register"); return; }
   std::lock_guard<std::mutex> lk(g_mu);
-  g_handles[{topo_id, mesh_id}] = std::move(h);
+  handles()[{topo_id, mesh_id}] = std::move(h);
 }
 
 void ppmg_mesh_unregister(int topo_id, int mesh_id, int* info) {
@@ -642,13 +661,13 @@ void ppmg_mesh_unregister(int topo_id, int mesh_id, int* info) {
   std::unique_ptr<Handle> h;
   {
     std::lock_guard<std::mutex> lk(g_mu);
-    auto it = g_handles.find({topo_id, mesh_id});
-    if (it == g_handles.end()) {
+    auto it = handles().find({topo_id, mesh_id});
+    if (it == handles().end()) {
       fail(info, kErrorError, ppmg::kErrArgument, "ppmg_mesh_unregister: unknown handle");
       return;
     }
     h = std::move(it->second);
-    g_handles.erase(it);
+    handles().erase(it);
   }
   if (h->stream) cudaStreamSynchronize(h->stream);
 }
@@ -1059,7 +1078,7 @@ static void rank_common(int dim, const double* xp, int64_t ldxp, int64_t Np, con
   if (nbox >= ((int64_t)1 << 31) - 1) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": too many boxes"); return; }
   // a private workspace per call: cell lists are independent of any mesh handle
   static std::mutex mu;
-  static Workspace ws;
+  static Workspace& ws = *new Workspace();  // never destroyed (see handles())
   static cudaStream_t st = nullptr;
   std::lock_guard<std::mutex> lk(mu);
   cudaError_t e = cudaSuccess;

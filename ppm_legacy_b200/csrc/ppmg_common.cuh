@@ -92,16 +92,20 @@ __device__ __forceinline__ void mp4_weights_exact(T f, T w[4]) {
   w[3] = radd(T(2), rmul(radd(T(4), rmul(radd(T(2.5), rmul(T(0.5), x13)), x13)), x13));
 }
 
-// The same polynomials, free to contract (FP32 mixed form).
+// The same polynomials, free to contract (FP32 mixed form).  The weight of
+// node i0+2 is taken as 1 - (w0 + w1 + w2): that weight lies in [-2/27, 0],
+// so the partial sum lies in [1, 1.075], the subtraction is exact (Sterbenz)
+// and the four FP32 weights
+// sum to exactly 1, which keeps the deposited total strength conserved to
+// the rounding of the tensor products only.
 template <class T>
 __device__ __forceinline__ void mp4_weights_fast(T f, T w[4]) {
   const T s0 = f + T(1);
   const T s2 = f - T(1);
-  const T s3 = f - T(2);
   w[0] = T(2) + (T(-4) + (T(2.5) - T(0.5) * s0) * s0) * s0;
   w[1] = T(1) + (T(-2.5) + T(1.5) * f) * (f * f);
   w[2] = T(1) + (T(-2.5) - T(1.5) * s2) * (s2 * s2);
-  w[3] = T(2) + (T(4) + (T(2.5) + T(0.5) * s3) * s3) * s3;
+  w[3] = T(1) - ((w[0] + w[1]) + w[2]);
 }
 
 // B-spline 2 weights (ppm_interp_p2m.f:3080-3110): a10 = 1 - f, a11 = 1 + (f - 1).

@@ -29,7 +29,7 @@ def test_comp_weights_and_remesh_match_oracle(dim, kernel, nc, box):
     t = registered(dim, nc, lo, hi)
     g = [2] * dim
     xp = random_particles(rng, dim, 2 * nc ** dim, t.min_phys[:dim], t.max_phys[:dim])
-    up = rng.standard_normal((3, xp.shape[1]))
+    up = np.asfortranarray(rng.standard_normal((3, xp.shape[1])))
     np_ = xp.shape[1]
     ks = 2 if kernel == 2 else 1
     wx = [np.zeros((2 * ks, 1, np_ + 2 * ks), order="F") for _ in range(3)]
