@@ -54,6 +54,16 @@ struct Handle {
   Workspace ws_rmsh;  // comp_weights -> remesh state (ppm_module_data_rmsh)
   cudaStream_t stream = nullptr;
   int* d_status = nullptr;  // [0] particles outside the sub, [1] non-finite
+  // position fingerprints: [0] of the sort held in ws, [1] of an M2P's xp
+  unsigned long long* d_hash = nullptr;
+  unsigned long long* h_small = nullptr;  // pinned host copy (hashes + status)
+  // The cell order, packed records and work items in `ws` belong to the
+  // positions fingerprinted in d_hash[0]; an M2P of the same positions reuses
+  // them (same key arithmetic: M2P's FP32 spacing equals P2M's spacing).
+  bool sort_cached = false;
+  int cache_prec = -1;        // record precision: 0 FP64 (double4), 1 FP32 (float4)
+  int64_t cache_np = -1, cache_ldxp = -1;
+  bool dxi_same_d = false, dxi_same_f = false;
   std::mutex mu;
   // comp_weights state
   bool w_valid = false;
@@ -62,6 +72,8 @@ struct Handle {
   ~Handle() {
     if (stream) cudaStreamDestroy(stream);
     if (d_status) cudaFree(d_status);
+    if (d_hash) cudaFree(d_hash);
+    if (h_small) cudaFreeHost(h_small);
   }
 };
 
@@ -228,8 +240,10 @@ int p2m_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, const T* up, 
     e = cudaMemsetAsync(field, 0, sizeof(T) * (size_t)field_elems(h, ldf, f_lb, f_ub), st);
     if (e) return cuda_fail(info, e, caller);
   } else {
+    h.sort_cached = false;
     KeyParams kp = make_kp(h, KEY_INTERP_CHECKED, false);
-    e = bin_sort<T>(kp, xp, ldxp, Np, h.g.ncell, ws, h.d_status + 0, st);
+    e = bin_sort<T>(kp, xp, ldxp, Np, h.g.ncell, ws, h.d_status + 0, st, (T*)nullptr, 0, 0,
+                    h.d_hash + 0);
     if (e) return cuda_fail(info, e, caller);
   }
   KeyParams kp = make_kp(h, KEY_INTERP_CHECKED, false);
@@ -242,16 +256,48 @@ int p2m_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, const T* up, 
   P2MParams P{};
   for (int a = 0; a < 3; ++a) P.N[a] = a < h.dim ? h.g.N[a] : 1;
   P.TZ = p2m_tile_depth(h.dim, P.N);
-  P.cap = prec == P2M_FP64 ? 448 : 896;
+  // staging slots per CTA (4 vectors per particle): ~72 KB for 3D, 2 CTAs / SM
+  if (h.dim == 3)
+    P.cap = prec == P2M_FP64 ? 544 : 1088;
+  else
+    P.cap = prec == P2M_FP64 ? 448 : 896;
   P.c0 = 0;
   P.start = ws.start.as<int>();
   P.rec = remesh ? (const void*)ws.w1d.p : ws.rec.p;
   P.us = ws.us.p;
   P.field = field;
   P.fd = fd;
-  e = launch_p2m(P, h.dim, kernel, prec, lda, Np > 0 ? Np : 1, remesh, st);
+  if ((e = ws.tiles.ensure(p2m_scratch_bytes(h.dim, P.N)))) return cuda_fail(info, e, caller);
+  e = launch_p2m(P, h.dim, kernel, prec, lda, Np > 0 ? Np : 1, remesh, ws.tiles.p, st);
   if (e) return cuda_fail(info, e, caller);
+  if (!remesh) {
+    h.sort_cached = true;
+    h.cache_prec = prec == P2M_FP64 ? 0 : 1;
+    h.cache_np = Np;
+    h.cache_ldxp = ldxp;
+  }
   return 0;
+}
+
+// Whether the cell order held in h.ws can serve an M2P of these positions:
+// same count, layout, record precision and key arithmetic, no invalid
+// particle in the sort, and an equal position fingerprint.  Synchronises the
+// stream once (a 24-byte read-back).
+template <class T>
+bool can_reuse_sort(Handle& h, const T* xp, int64_t ldxp, int64_t Np, int rec_prec,
+                    cudaStream_t st) {
+  if (!h.sort_cached || h.cache_np != Np || h.cache_ldxp != ldxp || h.cache_prec != rec_prec)
+    return false;
+  if (!(is_f32<T>() ? h.dxi_same_f : h.dxi_same_d)) return false;
+  if (position_hash<T>(xp, ldxp, Np, h.dim, h.d_hash + 1, st)) return false;
+  if (cudaMemcpyAsync(h.h_small, h.d_hash, 2 * sizeof(unsigned long long),
+                      cudaMemcpyDeviceToHost, st))
+    return false;
+  if (cudaMemcpyAsync(h.h_small + 2, h.d_status, sizeof(int), cudaMemcpyDeviceToHost, st))
+    return false;
+  if (cudaStreamSynchronize(st)) return false;
+  const int bad = *reinterpret_cast<const int*>(h.h_small + 2);
+  return h.h_small[0] == h.h_small[1] && bad == 0;
 }
 
 template <class T>
@@ -269,16 +315,24 @@ int m2p_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, T* up, int64_
   const M2PPrec prec = is_f32<T>() ? M2P_FP32
                                    : (g_precision.load() == PPMG_PREC_MIXED ? M2P_MIXED
                                                                             : M2P_FP64);
+  const int rec_prec = prec == M2P_FP64 ? 0 : 1;
+  const bool reuse = can_reuse_sort<T>(h, xp, ldxp, Np, rec_prec, st);
+  cudaError_t e = cudaSuccess;
   KeyParams kp = make_kp(h, KEY_INTERP_WRAP, true);
-  cudaError_t e = bin_sort<T>(kp, xp, ldxp, Np, h.g.ncell, h.ws, h.d_status + 1, st, up, ldup,
-                              lda);
-  if (e) return cuda_fail(info, e, caller);
+  if (!reuse) {
+    h.sort_cached = false;
+    e = bin_sort<T>(kp, xp, ldxp, Np, h.g.ncell, h.ws, h.d_status + 1, st, up, ldup, lda,
+                    h.d_hash + 0);
+    if (e) return cuda_fail(info, e, caller);
+  }
   const int* dnv = d_nvalid_of(h.ws, h.g.ncell);
-  if (prec == M2P_FP64)
-    e = pack_records<T, double>(kp, xp, ldxp, (const T*)nullptr, 0, 0, Np, dnv, h.ws, st);
-  else
-    e = pack_records<T, float>(kp, xp, ldxp, (const T*)nullptr, 0, 0, Np, dnv, h.ws, st);
-  if (e) return cuda_fail(info, e, caller);
+  if (!reuse) {
+    if (prec == M2P_FP64)
+      e = pack_records<T, double>(kp, xp, ldxp, (const T*)nullptr, 0, 0, Np, dnv, h.ws, st);
+    else
+      e = pack_records<T, float>(kp, xp, ldxp, (const T*)nullptr, 0, 0, Np, dnv, h.ws, st);
+    if (e) return cuda_fail(info, e, caller);
+  }
   M2PParams P{};
   for (int a = 0; a < 3; ++a) P.N[a] = a < h.dim ? h.g.N[a] : 1;
   P.nvalid = Np;
@@ -290,6 +344,26 @@ int m2p_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, T* up, int64_
   P.up = up;
   P.ldup = ldup;
   P.lda = lda;
+  if (h.dim == 3) {
+    TileItems ti;
+    if ((e = h.ws.tiles.ensure(tile_items_bytes(P.N)))) return cuda_fail(info, e, caller);
+    if (reuse) {
+      ti = tile_items_view(h.ws.tiles.p, P.N);
+    } else if ((e = make_tile_items(h.ws.start.as<int>(), P.N, Np, h.ws.tiles.p, ti, st))) {
+      return cuda_fail(info, e, caller);
+    }
+    P.start = h.ws.start.as<int>();
+    P.items = ti.items;
+    P.nitems = ti.nitems;
+    P.item_cap = ti.cap;
+  }
+  if (!reuse && h.dim == 3) {
+    // the M2P sort (with its items) is now what ws holds
+    h.sort_cached = true;
+    h.cache_prec = rec_prec;
+    h.cache_np = Np;
+    h.cache_ldxp = ldxp;
+  }
   e = launch_m2p(P, h.dim, kernel, prec, st);
   if (e) return cuda_fail(info, e, caller);
   return 0;
@@ -461,6 +535,7 @@ int adjoint_pipeline(Handle& h, const double* xp, int64_t ldxp, int64_t Np, cons
   if (!make_fd(h, ldf, f_lb, f_ub, lo, hi, fd, caller, info)) return *info;
   if (Np == 0) return 0;
   const M2PPrec prec = g_precision.load() == PPMG_PREC_MIXED ? M2P_MIXED : M2P_FP64;
+  h.sort_cached = false;
   // the transpose of P2M: P2M's stencil (FP64 mesh spacing), periodic wrap
   KeyParams kp = make_kp(h, KEY_INTERP_WRAP, false);
   cudaError_t e = bin_sort<double>(kp, xp, ldxp, Np, h.g.ncell, h.ws, h.d_status + 1, st, dw,
@@ -647,8 +722,16 @@ void ppmg_mesh_register(int topo_id, int mesh_id, int dim, const double* min_phy
     g.dxiq_f[a] = 1.0f / (lenf / (float)g.N[a]);
     g.h_d[a] = len / (double)(on ? Nm[a] - 1 : 1);
   }
+  h->dxi_same_d = true;
+  h->dxi_same_f = true;
+  for (int a = 0; a < dim; ++a) {
+    h->dxi_same_d = h->dxi_same_d && g.dxi_d[a] == g.dxiq_d[a];
+    h->dxi_same_f = h->dxi_same_f && g.dxi_f[a] == g.dxiq_f[a];
+  }
   cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
   if (!e) e = cudaMalloc(&h->d_status, 4 * sizeof(int));
+  if (!e) e = cudaMalloc(&h->d_hash, 2 * sizeof(unsigned long long));
+  if (!e) e = cudaMallocHost(&h->h_small, 4 * sizeof(unsigned long long));
   if (!e) e = cudaMemset(h->d_status, 0, 4 * sizeof(int));
   if (e) { cuda_fail(info, e, "ppmg_mesh_register"); return; }
   std::lock_guard<std::mutex> lk(g_mu);
@@ -1024,6 +1107,7 @@ void ppmg_rmsh_create_part_d(const double* field_up, int64_t ldf, int lda,
   const int64_t nq = (int64_t)P.nn[0] * P.nn[1] * P.nn[2];
   if ((e = h->ws.count.ensure(sizeof(int) * (size_t)(nq + 1))) ||
       (e = h->ws.start.ensure(sizeof(int) * (size_t)(nq + 1)))) { cuda_fail(info, e, caller); return; }
+  h->sort_cached = false;  // flag / positions reuse the cell-order buffers
   int* flag = h->ws.count.as<int>();
   int* pos = h->ws.start.as<int>();
   if ((e = cudaMemsetAsync(flag + nq, 0, sizeof(int), st))) { cuda_fail(info, e, caller); return; }

@@ -23,6 +23,10 @@ constexpr int kErrArgument = 503;
 constexpr int kMapGhostGet = 5;
 constexpr int kMapGhostPut = 6;
 
+// xy tile (in cells / node columns) of the 3D gather kernels
+constexpr int kTileX = 32;
+constexpr int kTileY = 16;
+
 // Geometry of one registered (topo_id, mesh_id), one subdomain.
 struct Geom {
   int dim;
@@ -92,20 +96,29 @@ __device__ __forceinline__ void mp4_weights_exact(T f, T w[4]) {
   w[3] = radd(T(2), rmul(radd(T(4), rmul(radd(T(2.5), rmul(T(0.5), x13)), x13)), x13));
 }
 
-// The same polynomials, free to contract (FP32 mixed form).  The weight of
-// node i0+2 is taken as 1 - (w0 + w1 + w2): that weight lies in [-2/27, 0],
-// so the partial sum lies in [1, 1.075], the subtraction is exact (Sterbenz)
-// and the four FP32 weights
-// sum to exactly 1, which keeps the deposited total strength conserved to
-// the rounding of the tensor products only.
+// The same polynomials in factored form for the FP32 mixed form.  With
+// g = 1 - f the four M'4 pieces factor as
+//   W(f+1) = -1/2 g^2 f,        W(f)   = g (1 + f - 3/2 f^2),
+//   W(f-1) = f (1 + g - 3/2 g^2), W(f-2) = -1/2 f^2 g,
+// products of well-conditioned factors, so every weight carries a few ulp of
+// relative error; the Horner forms above lose up to ulp(4) absolute to
+// cancellation, which in FP32 is ~1e-6 of the stencil sum.
+// The partition-of-unity defect 1 - sum(w) (exact by Sterbenz: the sum is
+// within a few ulp of 1) is then added to the largest weight, so the stored
+// weights sum to 1 up to a single rounding: the deposited total strength is
+// conserved to the rounding of the tensor products.
 template <class T>
 __device__ __forceinline__ void mp4_weights_fast(T f, T w[4]) {
-  const T s0 = f + T(1);
-  const T s2 = f - T(1);
-  w[0] = T(2) + (T(-4) + (T(2.5) - T(0.5) * s0) * s0) * s0;
-  w[1] = T(1) + (T(-2.5) + T(1.5) * f) * (f * f);
-  w[2] = T(1) + (T(-2.5) - T(1.5) * s2) * (s2 * s2);
-  w[3] = T(1) - ((w[0] + w[1]) + w[2]);
+  const T g = T(1) - f;
+  w[0] = T(-0.5) * (g * g) * f;
+  w[1] = g * (T(1) + f - T(1.5) * (f * f));
+  w[2] = f * (T(1) + g - T(1.5) * (g * g));
+  w[3] = T(-0.5) * (f * f) * g;
+  const T defect = T(1) - ((w[0] + w[3]) + (w[1] + w[2]));
+  if (f < T(0.5))
+    w[1] += defect;
+  else
+    w[2] += defect;
 }
 
 // B-spline 2 weights (ppm_interp_p2m.f:3080-3110): a10 = 1 - f, a11 = 1 + (f - 1).

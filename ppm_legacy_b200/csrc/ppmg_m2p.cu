@@ -220,6 +220,237 @@ __global__ void __launch_bounds__(256) k_adjoint3d(M2PParams P) {
   dx[2] = (double)g[2];
 }
 
+// --------------------------------------------------------------------------
+// 3D tile gather (M2P).  A CTA owns the particles of a work item's cells
+// (kTileX x kTileY cells over [Z0, Z1)).  The nodes their stencils read are
+// staged in shared memory as a ring of S node planes along z: per node column
+// (x, y) the S ring slots x LC components are contiguous, so a particle reads
+// each of its S x S columns with LC*S/4 vector loads and consecutive
+// particles (consecutive cells) hit disjoint banks.  One new plane is loaded
+// per cell layer; particles of the layer are spread over all threads.
+// EXACT (FP64 form): the terms are summed per component in the reference's
+// order (x outer, z inner) with the reference's association, no contraction.
+// --------------------------------------------------------------------------
+template <int S, class CT, bool EXACT, class FT, int LC>
+__global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
+  using V = typename Vec4<CT>::type;
+  constexpr int HL = S / 2;
+  constexpr int HH = S / 2 - 1;
+  constexpr int WX = kTileX + S - 1;
+  constexpr int WY = kTileY + S - 1;
+  constexpr int NCOL = WX * WY;
+  constexpr int R = S + 1;                     // ring slots: S in use + 1 being filled
+  constexpr int CS = R * LC;                   // CT values per node column
+  constexpr int PER = (NCOL + 255) / 256;      // columns per thread when loading a plane
+
+  if ((int)blockIdx.x >= *P.nitems) return;
+  const int4 it = P.items[blockIdx.x];
+  const int tiles_x = (P.N[0] + kTileX - 1) / kTileX;
+  const int X0 = (it.x % tiles_x) * kTileX;
+  const int Y0 = (it.x / tiles_x) * kTileY;
+  const int Z0 = it.y, Z1 = it.z;
+  const int XW = min(kTileX, P.N[0] - X0);  // cells of the tile inside the mesh
+  const int YW = min(kTileY, P.N[1] - Y0);
+
+  extern __shared__ __align__(16) unsigned char smem[];
+  CT* ring = reinterpret_cast<CT*>(smem);  // [NCOL][R][LC]
+  __shared__ int rbeg[2][kTileY], rpre[2][kTileY + 1];
+
+  const int tid = threadIdx.x;
+  const FT* F = static_cast<const FT*>(P.field);
+
+  // global offset of node column q of plane z (component c0)
+  auto col_off = [&](int q, int64_t oz) {
+    const int r = q / WX, qx = q - r * WX;
+    const int xw = wrap_index(X0 - (HL - 1) + qx, P.N[0]);
+    const int yw = wrap_index(Y0 - (HL - 1) + r, P.N[1]);
+    return (int64_t)(xw + 1 - P.fd.lb[0]) * P.fd.s[0] +
+           (int64_t)(yw + 1 - P.fd.lb[1]) * P.fd.s[1] + oz + P.c0;
+  };
+  auto plane_oz = [&](int z) {
+    return (int64_t)(wrap_index(z, P.N[2]) + 1 - P.fd.lb[2]) * P.fd.s[2];
+  };
+  // row ranges of cell layer cz: thread t < 16 loads row t
+  auto row_load = [&](int cz, int& b, int& n) {
+    b = 0;
+    n = 0;
+    if (tid < YW && cz < Z1) {
+      const int64_t c0 = (int64_t)X0 + (int64_t)P.N[0] * (Y0 + tid + (int64_t)P.N[1] * cz);
+      b = P.start[c0];
+      n = P.start[c0 + XW] - b;
+    }
+  };
+  auto row_store = [&](int buf, int b, int n) {
+    if (tid < kTileY) {
+      rbeg[buf][tid] = b;
+      int inc = n;
+#pragma unroll
+      for (int o = 1; o < kTileY; o <<= 1) {
+        const int t = __shfl_up_sync(0x0000ffffu, inc, o);
+        if (tid >= o) inc += t;
+      }
+      rpre[buf][tid + 1] = inc;
+      if (tid == 0) rpre[buf][0] = 0;
+    }
+  };
+
+  // prologue: planes Z0-(HL-1) .. Z0+HH+1 (the S planes of layer Z0) and its rows
+  for (int z = Z0 - (HL - 1); z <= Z0 + HH + 1; ++z) {
+    const int slot = wrap_index(z, R);
+    const int64_t oz = plane_oz(z);
+    for (int q = tid; q < NCOL; q += 256) {
+      const int64_t o = col_off(q, oz);
+      CT* d = ring + (size_t)q * CS + slot * LC;
+#pragma unroll
+      for (int a = 0; a < LC; ++a) d[a] = (CT)__ldg(F + o + a);
+    }
+  }
+  {
+    int b, n;
+    row_load(Z0, b, n);
+    row_store(Z0 & 1, b, n);
+  }
+  __syncthreads();
+
+  FT* up = static_cast<FT*>(P.up);
+  const V* rec = static_cast<const V*>(P.rec);
+
+  for (int cz = Z0; cz < Z1; ++cz) {
+    const int buf = cz & 1;
+    // prefetch the next layer's new plane and rows into registers
+    const bool more = cz + 1 < Z1;
+    const int zn = cz + HH + 2;
+    CT pre[PER][LC];
+    if (more) {
+      const int64_t oz = plane_oz(zn);
+#pragma unroll
+      for (int k = 0; k < PER; ++k) {
+        const int q = tid + 256 * k;
+        if (q < NCOL) {
+          const int64_t o = col_off(q, oz);
+#pragma unroll
+          for (int a = 0; a < LC; ++a) pre[k][a] = (CT)__ldg(F + o + a);
+        }
+      }
+    }
+    int nb, nn;
+    row_load(cz + 1, nb, nn);
+
+    const int ntot = rpre[buf][kTileY];
+    int slot_k[S];
+#pragma unroll
+    for (int k = 0; k < S; ++k) slot_k[k] = wrap_index(cz - (HL - 1) + k, R);
+    // software-pipelined particle loop: the next record is loaded while the
+    // current particle is gathered
+    auto locate = [&](int i, int& r) {
+      r = 0;
+#pragma unroll
+      for (int t = 1; t < kTileY; ++t) r += (i >= rpre[buf][t]) ? 1 : 0;
+      return (int64_t)rbeg[buf][r] + (i - rpre[buf][r]);
+    };
+    int rcur = 0;
+    int64_t scur = 0;
+    V rvcur;
+    if (tid < ntot) {
+      scur = locate(tid, rcur);
+      rvcur = rec[scur];
+    }
+    for (int i = tid; i < ntot; i += 256) {
+      int rnext = 0;
+      int64_t snext = 0;
+      V rvnext;
+      if (i + 256 < ntot) {
+        snext = locate(i + 256, rnext);
+        rvnext = rec[snext];
+      }
+      {
+        int cell;
+        if constexpr (sizeof(CT) == 4) cell = __float_as_int(rvcur.w); else cell = (int)rvcur.w;
+        const int qx0 = cell % P.N[0] - X0;  // local column of the first stencil node
+        const int qy0 = rcur;                // row of the cell inside the tile
+        CT wx[S], wy[S], wz[S];
+        m2p_weights<S, CT, EXACT>(rvcur.x, wx);
+        m2p_weights<S, CT, EXACT>(rvcur.y, wy);
+        m2p_weights<S, CT, EXACT>(rvcur.z, wz);
+        FT* out = up + (int64_t)P.idx[scur] * P.ldup + P.c0;
+        if constexpr (EXACT) {
+#pragma unroll
+          for (int a = 0; a < LC; ++a) {
+            CT acc = CT(0);
+#pragma unroll 1
+            for (int ii = 0; ii < S; ++ii)
+#pragma unroll
+              for (int jj = 0; jj < S; ++jj) {
+                const CT wij = rmul(wx[ii], wy[jj]);
+                const CT* col = ring + (size_t)((qy0 + jj) * WX + qx0 + ii) * CS + a;
+#pragma unroll
+                for (int kk = 0; kk < S; ++kk)
+                  acc = radd(acc, rmul(rmul(wij, wz[kk]), col[slot_k[kk] * LC]));
+              }
+            out[a] = (FT)acc;
+          }
+        } else {
+          CT acc[LC];
+#pragma unroll
+          for (int a = 0; a < LC; ++a) acc[a] = CT(0);
+#pragma unroll
+          for (int ii = 0; ii < S; ++ii)
+#pragma unroll
+            for (int jj = 0; jj < S; ++jj) {
+              const CT wij = wx[ii] * wy[jj];
+              const CT* col = ring + (size_t)((qy0 + jj) * WX + qx0 + ii) * CS;
+#pragma unroll
+              for (int a = 0; a < LC; ++a) {
+                CT part = CT(0);
+#pragma unroll
+                for (int k = 0; k < S; ++k) part = fma(wz[k], col[slot_k[k] * LC + a], part);
+                acc[a] = fma(wij, part, acc[a]);
+              }
+            }
+#pragma unroll
+          for (int a = 0; a < LC; ++a) out[a] = (FT)acc[a];
+        }
+      }
+      rcur = rnext;
+      scur = snext;
+      rvcur = rvnext;
+    }
+    // publish the prefetched plane (its slot is not read by this layer) and rows
+    if (more) {
+      const int slot = wrap_index(zn, R);
+#pragma unroll
+      for (int k = 0; k < PER; ++k) {
+        const int q = tid + 256 * k;
+        if (q < NCOL) {
+          CT* d = ring + (size_t)q * CS + slot * LC;
+#pragma unroll
+          for (int a = 0; a < LC; ++a) d[a] = pre[k][a];
+        }
+      }
+    }
+    row_store(buf ^ 1, nb, nn);
+    __syncthreads();
+  }
+}
+
+template <int S, class CT, bool EXACT, class FT>
+cudaError_t launch_tile_lc(const M2PParams& P, int lc, cudaStream_t st) {
+  auto go = [&](auto kern, int LCv) {
+    const size_t smem = (size_t)(kTileX + S - 1) * (kTileY + S - 1) * (S + 1) * LCv * sizeof(CT);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e) return e;
+    kern<<<P.item_cap, 256, smem, st>>>(P);
+    return cudaGetLastError();
+  };
+  switch (lc) {
+    case 1: return go(k_m2p3d_tile<S, CT, EXACT, FT, 1>, 1);
+    case 2: return go(k_m2p3d_tile<S, CT, EXACT, FT, 2>, 2);
+    case 3: return go(k_m2p3d_tile<S, CT, EXACT, FT, 3>, 3);
+    default: return go(k_m2p3d_tile<S, CT, EXACT, FT, 4>, 4);
+  }
+}
+
 int blocks_for(int64_t n) {
   int64_t b = (n + 255) / 256;
   return (int)(b < 1 ? 1 : b);
@@ -227,36 +458,46 @@ int blocks_for(int64_t n) {
 
 }  // namespace
 
-cudaError_t launch_m2p(const M2PParams& P, int dim, int kernel, M2PPrec prec, cudaStream_t st) {
-  if (P.nvalid <= 0) return cudaSuccess;
-  const int nb = blocks_for(P.nvalid);
+cudaError_t launch_m2p(const M2PParams& P0, int dim, int kernel, M2PPrec prec, cudaStream_t st) {
+  if (P0.nvalid <= 0) return cudaSuccess;
+  cudaError_t e = cudaSuccess;
   if (dim == 3) {
-    if (kernel == kKernelMp4) {
-      switch (prec) {
-        case M2P_FP64: k_m2p3d<4, double, true, double><<<nb, 256, 0, st>>>(P); break;
-        case M2P_MIXED: k_m2p3d<4, float, false, double><<<nb, 256, 0, st>>>(P); break;
-        case M2P_FP32: k_m2p3d<4, float, false, float><<<nb, 256, 0, st>>>(P); break;
+    // tiled gather: one launch per chunk of up to 4 components
+    for (int c0 = 0; c0 < P0.lda; c0 += 4) {
+      M2PParams P = P0;
+      P.c0 = c0;
+      const int lc = P0.lda - c0 < 4 ? P0.lda - c0 : 4;
+      if (kernel == kKernelMp4) {
+        switch (prec) {
+          case M2P_FP64: e = launch_tile_lc<4, double, true, double>(P, lc, st); break;
+          case M2P_MIXED: e = launch_tile_lc<4, float, false, double>(P, lc, st); break;
+          case M2P_FP32: e = launch_tile_lc<4, float, false, float>(P, lc, st); break;
+        }
+      } else {
+        switch (prec) {
+          case M2P_FP64: e = launch_tile_lc<2, double, true, double>(P, lc, st); break;
+          case M2P_MIXED: e = launch_tile_lc<2, float, false, double>(P, lc, st); break;
+          case M2P_FP32: e = launch_tile_lc<2, float, false, float>(P, lc, st); break;
+        }
       }
-    } else {
-      switch (prec) {
-        case M2P_FP64: k_m2p3d<2, double, true, double><<<nb, 256, 0, st>>>(P); break;
-        case M2P_MIXED: k_m2p3d<2, float, false, double><<<nb, 256, 0, st>>>(P); break;
-        case M2P_FP32: k_m2p3d<2, float, false, float><<<nb, 256, 0, st>>>(P); break;
-      }
+      count_launch();
+      if (e) return e;
+    }
+    return e;
+  }
+  const M2PParams& P = P0;
+  const int nb = blocks_for(P.nvalid);
+  if (kernel == kKernelMp4) {
+    switch (prec) {
+      case M2P_FP64: k_m2p2d<4, double, true, double><<<nb, 256, 0, st>>>(P); break;
+      case M2P_MIXED: k_m2p2d<4, float, false, double><<<nb, 256, 0, st>>>(P); break;
+      case M2P_FP32: k_m2p2d<4, float, false, float><<<nb, 256, 0, st>>>(P); break;
     }
   } else {
-    if (kernel == kKernelMp4) {
-      switch (prec) {
-        case M2P_FP64: k_m2p2d<4, double, true, double><<<nb, 256, 0, st>>>(P); break;
-        case M2P_MIXED: k_m2p2d<4, float, false, double><<<nb, 256, 0, st>>>(P); break;
-        case M2P_FP32: k_m2p2d<4, float, false, float><<<nb, 256, 0, st>>>(P); break;
-      }
-    } else {
-      switch (prec) {
-        case M2P_FP64: k_m2p2d<2, double, true, double><<<nb, 256, 0, st>>>(P); break;
-        case M2P_MIXED: k_m2p2d<2, float, false, double><<<nb, 256, 0, st>>>(P); break;
-        case M2P_FP32: k_m2p2d<2, float, false, float><<<nb, 256, 0, st>>>(P); break;
-      }
+    switch (prec) {
+      case M2P_FP64: k_m2p2d<2, double, true, double><<<nb, 256, 0, st>>>(P); break;
+      case M2P_MIXED: k_m2p2d<2, float, false, double><<<nb, 256, 0, st>>>(P); break;
+      case M2P_FP32: k_m2p2d<2, float, false, float><<<nb, 256, 0, st>>>(P); break;
     }
   }
   count_launch();

@@ -22,6 +22,12 @@ struct M2PParams {
   void* up;           // output up(ldup, Np) (adjoint: dw)
   int64_t ldup;
   int lda;
+  int c0;             // first component of this launch (tile kernel)
+  // 3D tile kernel: cell offsets and work items
+  const int* start;
+  const int4* items;
+  const int* nitems;
+  int item_cap;
   // adjoint only
   const double* upin;
   int64_t ldupin;

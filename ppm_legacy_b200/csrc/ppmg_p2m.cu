@@ -20,8 +20,6 @@ namespace ppmg {
 
 namespace {
 
-constexpr int kTile = 16;
-constexpr int kThreads = kTile * kTile;
 
 template <class CT>
 __device__ __forceinline__ void two_sum_fold(CT& hi, CT& lo, CT p) {
@@ -82,215 +80,326 @@ __device__ __forceinline__ void emit_node(const P2MParams& P, int x, int y, int 
 
 // --------------------------------------------------------------------------
 // 3D tile gather.
+// A CTA of 16 x 16 threads owns 32 x 16 node columns (two adjacent columns
+// per thread) over a z-range [Z0, Z1) given by its work item.  Per cell layer
+// the particles of the (32+S-1) x (16+S-1) cells whose stencils reach the tile
+// are staged in shared memory as structure-of-arrays (wx, wy, wz, u: one
+// 16-byte vector each per particle, consecutive particles in consecutive
+// slots).  A thread visits the S+1 cells of each of its S rows; the x-weight
+// index of each of its two columns is a compile-time constant per cell, so
+// every particle costs 3 vector loads + 1 scalar load for two columns.
+// Dense layers that do not fit are processed in chunks that take at most k
+// particles from every staged cell, so every thread has work in every chunk.
 // S: stencil width (4 = M'4, 2 = bsp2).  CT: arithmetic type.  COMP:
 // compensated FP32 accumulation (per-layer partial sums folded into a
 // (hi, lo) pair with an error-free TwoSum).  OT: field type.  LC: components
-// handled by this launch (<= 4).
+// handled by this launch (<= 4).  WST: 1D weights come from comp_weights.
 // --------------------------------------------------------------------------
+constexpr int kTX = 16, kTY = 16;
+static_assert(kTileX == 2 * kTX && kTileY == kTY, "tile shape");
+
+template <class CT>
+__device__ __forceinline__ CT vget(const typename Vec4<CT>::type& v, int i) {
+  return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
+}
+
+// Exclusive scan over n <= 3*256 cell values v(q); writes out[0..n] (out[n] =
+// total) and returns the total and the maximum through smem scalars.
+template <class F>
+__device__ __forceinline__ void scan_cells(int n, F val, int* out, int* wsum, int* red) {
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int q0 = 3 * tid;
+  const int v0 = q0 < n ? val(q0) : 0;
+  const int v1 = q0 + 1 < n ? val(q0 + 1) : 0;
+  const int v2 = q0 + 2 < n ? val(q0 + 2) : 0;
+  const int s = v0 + v1 + v2;
+  int m = max(v0, max(v1, v2));
+  int inc = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+    m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  }
+  if (lane == 31) wsum[wid] = inc;
+  if (lane == 0) wsum[8 + wid] = m;
+  __syncthreads();
+  if (tid == 0) {
+    int run = 0, mx = 0;
+    for (int w = 0; w < 8; ++w) {
+      const int t = wsum[w];
+      wsum[w] = run;
+      run += t;
+      mx = max(mx, wsum[8 + w]);
+    }
+    red[0] = run;
+    red[1] = mx;
+  }
+  __syncthreads();
+  const int ex = inc - s + wsum[wid];
+  if (q0 < n) out[q0] = ex;
+  if (q0 + 1 < n) out[q0 + 1] = ex + v0;
+  if (q0 + 2 < n) out[q0 + 2] = ex + v0 + v1;
+  if (tid == 0) out[n] = red[0];
+  __syncthreads();
+}
+
 template <int S, class CT, bool COMP, class OT, int LC, bool WST>
-__global__ void __launch_bounds__(kThreads) k_p2m3d(P2MParams P) {
+__global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
   using V = typename Vec4<CT>::type;
   constexpr int HL = S / 2;
   constexpr int HH = S / 2 - 1;
-  constexpr int WX = kTile + S - 1;
-  constexpr int NSC = WX * WX;
-  constexpr int PS = ((3 * S + 4) + 3) / 4 * 4;  // per-particle stride in CT
-  constexpr int OFF_U = S;                        // [wz(S) | u(4) | wx(S) | wy(S)]
-  constexpr int OFF_WX = S + 4;
-  constexpr int OFF_WY = 2 * S + 4;
+  constexpr int WX = kTileX + S - 1;
+  constexpr int WY = kTileY + S - 1;
+  constexpr int NSC = WX * WY;
+  constexpr int NT = kTX * kTY;
+  constexpr int PERC = (NSC + NT - 1) / NT;  // staged cells per thread (count loads)
+  static_assert(NSC <= 3 * NT, "staged cells exceed the scan width");
+
+  if ((int)blockIdx.x >= *P.nitems) return;
+  const int4 it = P.items[blockIdx.x];
+  const int tiles_x = (P.N[0] + kTileX - 1) / kTileX;
+  const int X0 = (it.x % tiles_x) * kTileX;
+  const int Y0 = (it.x / tiles_x) * kTileY;
+  const int Z0 = it.y, Z1 = it.z;
 
   extern __shared__ __align__(16) unsigned char smem[];
-  int* sc = reinterpret_cast<int*>(smem);  // NSC + 1 prefix offsets
-  int* sb = sc + NSC + 1;                  // NSC global starts
-  size_t off = (size_t)(2 * NSC + 1) * sizeof(int);
-  off = (off + 15) & ~(size_t)15;
-  CT* sw = reinterpret_cast<CT*>(smem + off);
-  unsigned char* sqx = reinterpret_cast<unsigned char*>(sw + (size_t)P.cap * PS);
+  V* sWX = reinterpret_cast<V*>(smem);
+  V* sWY = sWX + P.cap;
+  V* sWZ = sWY + P.cap;
+  V* sU = sWZ + P.cap;
+  int* cnt = reinterpret_cast<int*>(sU + P.cap);
+  int* off = cnt + NSC;        // NSC + 1
+  int* base = off + NSC + 1;   // NSC
+  unsigned char* sQ = reinterpret_cast<unsigned char*>(base + NSC);  // cap: staged column
+  __shared__ int wsum[16];
+  __shared__ int red[2];
 
   const int tid = threadIdx.x;
-  const int tx = tid % kTile, ty = tid / kTile;
-  const int tiles_x = (P.N[0] + kTile - 1) / kTile;
-  const int X0 = (blockIdx.x % tiles_x) * kTile;
-  const int Y0 = (blockIdx.x / tiles_x) * kTile;
-  const int Z0 = blockIdx.y * P.TZ;
-  const int Z1 = min(Z0 + P.TZ, P.N[2]);
-  const int x = X0 + tx, y = Y0 + ty;
-  const bool active = x < P.N[0] && y < P.N[1];
+  const int tx = tid % kTX, ty = tid / kTX;
+  const int x0 = X0 + 2 * tx, y = Y0 + ty;
+  const bool act0 = x0 < P.N[0] && y < P.N[1];
+  const bool act1 = x0 + 1 < P.N[0] && y < P.N[1];
   const V* rec = static_cast<const V*>(P.rec);
   const V* us = static_cast<const V*>(P.us);
 
-  CT acc[S][LC];  // plain window (or per-layer partials when COMP)
-  CT hi[S][LC], lo[S][LC];
+  CT acc[2][S][LC];  // window (or per-layer partials when COMP)
+  CT hi[2][S][LC], lo[2][S][LC];
 #pragma unroll
-  for (int k = 0; k < S; ++k)
+  for (int e = 0; e < 2; ++e)
 #pragma unroll
-    for (int a = 0; a < LC; ++a) acc[k][a] = hi[k][a] = lo[k][a] = CT(0);
+    for (int k = 0; k < S; ++k)
+#pragma unroll
+      for (int a = 0; a < LC; ++a) acc[e][k][a] = hi[e][k][a] = lo[e][k][a] = CT(0);
+
+  // cell offsets of the staged cells of layer cz, kept in registers until stored
+  int pb[PERC], pe[PERC];
+  auto load_counts = [&](int cz) {
+    const int czw = wrap_index(cz, P.N[2]);
+#pragma unroll
+    for (int k = 0; k < PERC; ++k) {
+      const int q = tid + NT * k;
+      pb[k] = pe[k] = 0;
+      if (q < NSC) {
+        const int r = q / WX, qx = q - r * WX;
+        const int cx = wrap_index(X0 - HL + qx, P.N[0]);
+        const int cy = wrap_index(Y0 - HL + r, P.N[1]);
+        const int64_t c = (int64_t)cx + (int64_t)P.N[0] * (cy + (int64_t)P.N[1] * czw);
+        pb[k] = P.start[c];
+        pe[k] = P.start[c + 1];
+      }
+    }
+  };
+  load_counts(Z0 - HL);
 
   for (int cz = Z0 - HL; cz <= Z1 - 1 + HH; ++cz) {
-    const int czw = wrap_index(cz, P.N[2]);
-    // 1. particle counts of the staged cells
-    for (int q = tid; q < NSC; q += kThreads) {
-      const int r = q / WX, qx = q % WX;
-      const int cx = wrap_index(X0 - HL + qx, P.N[0]);
-      const int cy = wrap_index(Y0 - HL + r, P.N[1]);
-      const int64_t c = (int64_t)cx + (int64_t)P.N[0] * (cy + (int64_t)P.N[1] * czw);
-      const int b = P.start[c];
-      sb[q] = b;
-      sc[q] = P.start[c + 1] - b;
+    // 1. publish this layer's cell ranges
+#pragma unroll
+    for (int k = 0; k < PERC; ++k) {
+      const int q = tid + NT * k;
+      if (q < NSC) {
+        base[q] = pb[k];
+        cnt[q] = pe[k] - pb[k];
+      }
     }
     __syncthreads();
-    // 2. exclusive scan of the counts (two per thread, NSC <= 2*kThreads)
-    {
-      const int i0 = 2 * tid, i1 = 2 * tid + 1;
-      const int v0 = i0 < NSC ? sc[i0] : 0;
-      const int v1 = i1 < NSC ? sc[i1] : 0;
-      int v = v0 + v1;
-      // warp inclusive scan
-      const int lane = tid & 31, wid = tid >> 5;
-      int inc = v;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        int t = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += t;
-      }
-      __shared__ int wsum[kThreads / 32 + 1];
-      if (lane == 31) wsum[wid] = inc;
-      __syncthreads();
-      if (tid == 0) {
-        int run = 0;
-        for (int w = 0; w < kThreads / 32; ++w) {
-          int t = wsum[w];
-          wsum[w] = run;
-          run += t;
-        }
-        wsum[kThreads / 32] = run;
-      }
-      __syncthreads();
-      const int ex = inc - v + wsum[wid];
-      if (i0 < NSC) sc[i0] = ex;
-      if (i1 < NSC) sc[i1] = ex + v0;
-      if (tid == 0) sc[NSC] = wsum[kThreads / 32];
-      __syncthreads();
+    scan_cells(NSC, [&](int q) { return cnt[q]; }, off, wsum, red);
+    const int total = red[0], maxc = red[1];
+    int kch = 1 << 30, nch = 1;
+    if (total > P.cap) {
+      kch = P.cap / NSC;
+      nch = (maxc + kch - 1) / kch;
     }
-    const int total = sc[NSC];
-    for (int cb = 0; cb < total; cb += P.cap) {
-      const int n = min(P.cap, total - cb);
-      // 3. stage particles [cb, cb+n) of the layer's staged cells
-      for (int i = tid; i < n; i += kThreads) {
-        const int pos = cb + i;
-        int lo_q = 0, hi_q = NSC;  // largest q with sc[q] <= pos
-        while (hi_q - lo_q > 1) {
-          const int mid = (lo_q + hi_q) >> 1;
-          if (sc[mid] <= pos) lo_q = mid; else hi_q = mid;
-        }
-        const int64_t s = (int64_t)sb[lo_q] + (pos - sc[lo_q]);
-        const V u = us[s];
-        CT w[3][S];
-        if constexpr (WST) {
-          // remesh: the 1D weights of ppm_rmsh_comp_weights, stored per
-          // sorted particle as (wx[S], wy[S], wz[S]) in FP64
-          const double* ws = static_cast<const double*>(P.rec) + s * (3 * S);
+    for (int j = 0; j < nch; ++j) {
+      const int lo_l = nch > 1 ? j * kch : 0;
+      int n = total;
+      if (nch > 1) {
+        scan_cells(NSC, [&](int q) { return min(max(cnt[q] - lo_l, 0), kch); }, off, wsum, red);
+        n = red[0];
+      }
+      // 2. stage particles [0, n) of this chunk, two per thread in flight
+      for (int i0 = tid; i0 < n; i0 += 2 * NT) {
+        int qv[2];
+        int64_t sv[2];
+        V uv[2], rv[2];
 #pragma unroll
-          for (int k = 0; k < S; ++k) {
-            w[0][k] = (CT)ws[k];
-            w[1][k] = (CT)ws[S + k];
-            w[2][k] = (CT)ws[2 * S + k];
+        for (int u2 = 0; u2 < 2; ++u2) {
+          const int i = i0 + NT * u2;
+          int lo_q = 0, hi_q = NSC;  // largest q with off[q] <= i
+          while (hi_q - lo_q > 1) {
+            const int mid = (lo_q + hi_q) >> 1;
+            if (off[mid] <= i) lo_q = mid; else hi_q = mid;
           }
-        } else {
-          const V r = rec[s];
-          weights<S, CT>(r.x, w[0]);
-          weights<S, CT>(r.y, w[1]);
-          weights<S, CT>(r.z, w[2]);
+          qv[u2] = lo_q;
+          sv[u2] = (int64_t)base[lo_q] + lo_l + (i - off[lo_q]);
+          if (i < n) {
+            uv[u2] = us[sv[u2]];
+            if constexpr (!WST) rv[u2] = rec[sv[u2]];
+          }
         }
-        CT* d = sw + (size_t)i * PS;
 #pragma unroll
-        for (int k = 0; k < S; ++k) {
-          d[k] = w[2][k];
-          d[OFF_WX + k] = w[0][k];
-          d[OFF_WY + k] = w[1][k];
+        for (int u2 = 0; u2 < 2; ++u2) {
+          const int i = i0 + NT * u2;
+          if (i >= n) break;
+          CT w[3][S];
+          if constexpr (WST) {
+            const double* wsrc = static_cast<const double*>(P.rec) + sv[u2] * (3 * S);
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+              w[0][k] = (CT)wsrc[k];
+              w[1][k] = (CT)wsrc[S + k];
+              w[2][k] = (CT)wsrc[2 * S + k];
+            }
+          } else {
+            weights<S, CT>(rv[u2].x, w[0]);
+            weights<S, CT>(rv[u2].y, w[1]);
+            weights<S, CT>(rv[u2].z, w[2]);
+          }
+          V a, b, c;
+          a.x = w[0][0]; a.y = w[0][1]; a.z = S > 2 ? w[0][S > 2 ? 2 : 0] : CT(0); a.w = S > 3 ? w[0][S > 3 ? 3 : 0] : CT(0);
+          b.x = w[1][0]; b.y = w[1][1]; b.z = S > 2 ? w[1][S > 2 ? 2 : 0] : CT(0); b.w = S > 3 ? w[1][S > 3 ? 3 : 0] : CT(0);
+          c.x = w[2][0]; c.y = w[2][1]; c.z = S > 2 ? w[2][S > 2 ? 2 : 0] : CT(0); c.w = S > 3 ? w[2][S > 3 ? 3 : 0] : CT(0);
+          sWX[i] = a;
+          sWY[i] = b;
+          sWZ[i] = c;
+          sU[i] = uv[u2];
+          sQ[i] = (unsigned char)(qv[u2] % WX);
         }
-        d[OFF_U + 0] = u.x;
-        d[OFF_U + 1] = u.y;
-        d[OFF_U + 2] = u.z;
-        d[OFF_U + 3] = u.w;
-        sqx[i] = (unsigned char)(lo_q % WX);
       }
       __syncthreads();
-      // 4. accumulate the S x S cells around this thread's column
-      if (active) {
+      // the next layer's cell ranges load while this chunk is accumulated
+      if (j == nch - 1 && cz < Z1 - 1 + HH) load_counts(cz + 1);
+      // 3. accumulate: per row, the particles of cells 2tx..2tx+S (one range)
+      if (act0) {
 #pragma unroll
         for (int dy = 0; dy < S; ++dy) {
-          const int row = ty + dy;
-          const int pb = max(sc[row * WX + tx], cb);
-          const int pe = min(sc[row * WX + tx + S], cb + n);
-          for (int pos = pb; pos < pe; ++pos) {
-            const int i = pos - cb;
-            const CT* d = sw + (size_t)i * PS;
-            const int wi = tx - (int)sqx[i] + S - 1;
-            const CT c = d[OFF_WX + wi] * d[OFF_WY + S - 1 - dy];
-            CT wz[S], uu[4];
-            if constexpr (S == 4 && sizeof(CT) == 4) {
-              const float4 a = *reinterpret_cast<const float4*>(d);
-              wz[0] = a.x; wz[1] = a.y; wz[2] = a.z; wz[3] = a.w;
-            } else {
-#pragma unroll
-              for (int k = 0; k < S; ++k) wz[k] = d[k];
-            }
-            if constexpr (sizeof(CT) == 4) {
-              const float4 b = *reinterpret_cast<const float4*>(d + OFF_U);
-              uu[0] = b.x; uu[1] = b.y; uu[2] = b.z; uu[3] = b.w;
-            } else {
-#pragma unroll
-              for (int a = 0; a < 4; ++a) uu[a] = d[OFF_U + a];
-            }
+          const int row = (ty + dy) * WX + 2 * tx;
+          const int p0 = off[row], p1 = off[row + S + 1];
+          for (int p = p0; p < p1; ++p) {
+            const int d = (int)sQ[p] - 2 * tx;  // cell offset 0..S inside the window
+            const V wx = sWX[p];
+            const V wz = sWZ[p];
+            const V u = sU[p];
+            const CT wy = vget<CT>(sWY[p], S - 1 - dy);
+            const int i0 = S - 1 - d, i1 = S - d;
+            const CT w0 = i0 >= 0 ? vget<CT>(wx, i0 >= 0 ? i0 : 0) : CT(0);
+            const CT w1 = i1 < S ? vget<CT>(wx, i1 < S ? i1 : 0) : CT(0);
+            const CT c0 = w0 * wy, c1 = w1 * wy;
+            const CT wzv[4] = {wz.x, wz.y, wz.z, wz.w};
+            const CT uu[4] = {u.x, u.y, u.z, u.w};
 #pragma unroll
             for (int a = 0; a < LC; ++a) {
-              const CT cu = c * uu[a];
+              const CT cu0 = c0 * uu[a], cu1 = c1 * uu[a];
 #pragma unroll
-              for (int k = 0; k < S; ++k) acc[k][a] += cu * wz[k];
+              for (int k = 0; k < S; ++k) {
+                acc[0][k][a] += cu0 * wzv[k];
+                acc[1][k][a] += cu1 * wzv[k];
+              }
             }
           }
         }
       }
       __syncthreads();
     }
-    // 5. node zc = cz - (HL-1) is complete: fold, emit, shift the window
+    // 4. node zc = cz - (HL-1) of both columns is complete: fold, emit, shift
     const int zc = cz - (HL - 1);
-    if constexpr (COMP) {
 #pragma unroll
-      for (int k = 0; k < S; ++k)
+    for (int e = 0; e < 2; ++e) {
+      if constexpr (COMP) {
+#pragma unroll
+        for (int k = 0; k < S; ++k)
+#pragma unroll
+          for (int a = 0; a < LC; ++a) {
+            two_sum_fold<CT>(hi[e][k][a], lo[e][k][a], acc[e][k][a]);
+            acc[e][k][a] = CT(0);
+          }
+      }
+      if ((e == 0 ? act0 : act1) && zc >= Z0 && zc < Z1) {
+        double v[LC];
+#pragma unroll
+        for (int a = 0; a < LC; ++a)
+          v[a] = COMP ? (double)hi[e][0][a] + (double)lo[e][0][a] : (double)acc[e][0][a];
+        emit_node<3, OT, LC>(P, x0 + e, y, zc, v);
+      }
+#pragma unroll
+      for (int k = 0; k < S - 1; ++k)
 #pragma unroll
         for (int a = 0; a < LC; ++a) {
-          two_sum_fold<CT>(hi[k][a], lo[k][a], acc[k][a]);
-          acc[k][a] = CT(0);
+          if constexpr (COMP) {
+            hi[e][k][a] = hi[e][k + 1][a];
+            lo[e][k][a] = lo[e][k + 1][a];
+          } else {
+            acc[e][k][a] = acc[e][k + 1][a];
+          }
         }
-    }
-    if (active && zc >= Z0 && zc < Z1) {
-      double v[LC];
-#pragma unroll
-      for (int a = 0; a < LC; ++a)
-        v[a] = COMP ? (double)hi[0][a] + (double)lo[0][a] : (double)acc[0][a];
-      emit_node<3, OT, LC>(P, x, y, zc, v);
-    }
-#pragma unroll
-    for (int k = 0; k < S - 1; ++k)
 #pragma unroll
       for (int a = 0; a < LC; ++a) {
         if constexpr (COMP) {
-          hi[k][a] = hi[k + 1][a];
-          lo[k][a] = lo[k + 1][a];
+          hi[e][S - 1][a] = CT(0);
+          lo[e][S - 1][a] = CT(0);
         } else {
-          acc[k][a] = acc[k + 1][a];
+          acc[e][S - 1][a] = CT(0);
         }
       }
-#pragma unroll
-    for (int a = 0; a < LC; ++a) {
-      if constexpr (COMP) {
-        hi[S - 1][a] = CT(0);
-        lo[S - 1][a] = CT(0);
-      } else {
-        acc[S - 1][a] = CT(0);
-      }
+    }
+  }
+}
+
+// Per (xy tile, cell layer): particles in the tile's own cells of that layer.
+__global__ void k_layer_counts(const int* __restrict__ start, int N0, int N1, int N2,
+                               int tiles_x, int ntiles, int* __restrict__ lc) {
+  const int64_t n = (int64_t)ntiles * N2;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int tile = (int)(i / N2), cz = (int)(i % N2);
+    const int X0 = (tile % tiles_x) * kTileX, X1 = min(X0 + kTileX, N0);
+    const int Y0 = (tile / tiles_x) * kTileY, Y1 = min(Y0 + kTileY, N1);
+    int sum = 0;
+    for (int y = Y0; y < Y1; ++y) {
+      const int64_t c0 = (int64_t)X0 + (int64_t)N0 * (y + (int64_t)N1 * cz);
+      sum += start[c0 + (X1 - X0)] - start[c0];
+    }
+    lc[i] = sum;
+  }
+}
+
+// Split every xy tile's z range into work items of about `target` particles
+// (at least min_tz and at most max_tz layers; the halo makes short items dear).
+__global__ void k_make_items(const int* __restrict__ lc, int N2, int ntiles, int target,
+                             int min_tz, int max_tz, int4* __restrict__ items,
+                             int* __restrict__ nitems) {
+  const int tile = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tile >= ntiles) return;
+  int z0 = 0, acc = 0;
+  for (int cz = 0; cz < N2; ++cz) {
+    acc += lc[(int64_t)tile * N2 + cz];
+    const int len = cz + 1 - z0;
+    const bool want = (acc >= target && len >= min_tz) || len >= max_tz;
+    if (cz == N2 - 1 || (want && N2 - (cz + 1) >= min_tz)) {
+      const int q = atomicAdd(nitems, 1);
+      items[q] = make_int4(tile, z0, cz + 1, 0);
+      z0 = cz + 1;
+      acc = 0;
     }
   }
 }
@@ -447,20 +556,19 @@ __global__ void __launch_bounds__(kTile2) k_p2m2d(P2MParams P) {
 template <int S, class CT, bool COMP, class OT, int LC, bool WST>
 cudaError_t launch_lc(const P2MParams& P, int dim, cudaStream_t st) {
   if (dim == 3) {
-    constexpr int WX = kTile + S - 1;
-    constexpr int NSC = WX * WX;
-    constexpr int PS = ((3 * S + 4) + 3) / 4 * 4;
-    size_t off = ((size_t)(2 * NSC + 1) * sizeof(int) + 15) & ~(size_t)15;
-    size_t smem = off + (size_t)P.cap * PS * sizeof(CT) + (size_t)P.cap;
+    constexpr int WX = kTileX + S - 1, WY = kTileY + S - 1;
+    constexpr int NSC = WX * WY;
+    // staging capacity: a whole number of slots per staged cell (chunks of
+    // dense layers take that many particles from every cell); ~85 KB, 2 CTAs/SM
+    P2MParams Q = P;
+    Q.cap = NSC * (sizeof(CT) == 4 ? 2 : 1);
+    const size_t smem = (size_t)Q.cap * 4 * sizeof(typename Vec4<CT>::type) +
+                        (size_t)(3 * NSC + 1) * sizeof(int) + (size_t)Q.cap;
     auto kern = k_p2m3d<S, CT, COMP, OT, LC, WST>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    const int tiles_x = (P.N[0] + kTile - 1) / kTile;
-    const int tiles_y = (P.N[1] + kTile - 1) / kTile;
-    const int tiles_z = (P.N[2] + P.TZ - 1) / P.TZ;
-    dim3 grid(tiles_x * tiles_y, tiles_z);
-    kern<<<grid, kThreads, smem, st>>>(P);
+    kern<<<Q.item_cap, kTX * kTY, smem, st>>>(Q);
   } else {
     constexpr int WX = kTile2 + S - 1;
     constexpr int PS = ((2 * S + 4) + 3) / 4 * 4;
@@ -496,27 +604,79 @@ cudaError_t launch_w(const P2MParams& P, int dim, int lc, bool wst, cudaStream_t
 }  // namespace
 
 int p2m_tile_depth(int dim, const int N[3]) {
-  if (dim == 2) {
-    const int tx = (N[0] + kTile2 - 1) / kTile2;
-    int want = (148 * 8 + tx - 1) / tx;  // ~8 CTAs per SM in total
-    int tz = (N[1] + want - 1) / want;
-    return tz < 8 ? (N[1] < 8 ? N[1] : 8) : tz;
-  }
-  const int txy = ((N[0] + kTile - 1) / kTile) * ((N[1] + kTile - 1) / kTile);
-  int want = (148 * 3 * 8 + txy - 1) / txy;  // ~8 waves of 3 CTAs per SM
-  int tz = (N[2] + want - 1) / want;
-  if (tz < 8) tz = 8;
-  if (tz > 64) tz = 64;
-  if (tz > N[2]) tz = N[2];
-  return tz;
+  const int tx = (N[0] + kTile2 - 1) / kTile2;
+  int want = (148 * 8 + tx - 1) / tx;  // ~8 CTAs per SM in total
+  int tz = (N[1] + want - 1) / want;
+  (void)dim;
+  return tz < 8 ? (N[1] < 8 ? N[1] : 8) : tz;
+}
+
+namespace {
+constexpr int kMinTZ = 8, kMaxTZ = 64;
+int tiles_xy(const int N[3]) {
+  return ((N[0] + kTileX - 1) / kTileX) * ((N[1] + kTileY - 1) / kTileY);
+}
+int item_capacity(const int N[3]) {
+  return tiles_xy(N) * ((N[2] + kMinTZ - 1) / kMinTZ) + 1;
+}
+}  // namespace
+
+size_t tile_items_bytes(const int N[3]) {
+  return sizeof(int4) * (size_t)item_capacity(N) + sizeof(int) * (size_t)tiles_xy(N) * N[2] +
+         64;
+}
+
+size_t p2m_scratch_bytes(int dim, const int N[3]) {
+  return dim == 3 ? tile_items_bytes(N) : 16;
+}
+
+TileItems tile_items_view(void* scratch, const int N[3]) {
+  TileItems t;
+  t.cap = item_capacity(N);
+  t.items = static_cast<const int4*>(scratch);
+  t.nitems = reinterpret_cast<const int*>(t.items + t.cap);
+  return t;
+}
+
+cudaError_t make_tile_items(const int* start, const int N[3], int64_t nvalid, void* scratch,
+                            TileItems& out, cudaStream_t st) {
+  const int nt = tiles_xy(N);
+  const int cap_items = item_capacity(N);
+  int4* items = static_cast<int4*>(scratch);
+  int* nitems = reinterpret_cast<int*>(items + cap_items);
+  int* lc = nitems + 16;
+  cudaError_t e = cudaMemsetAsync(nitems, 0, sizeof(int), st);
+  if (e) return e;
+  const int64_t nl = (int64_t)nt * N[2];
+  const int gl = (int)((nl + 255) / 256 < 148 * 32 ? (nl + 255) / 256 : 148 * 32);
+  k_layer_counts<<<gl, 256, 0, st>>>(start, N[0], N[1], N[2], (N[0] + kTileX - 1) / kTileX, nt,
+                                     lc);
+  const int64_t tgt64 = nvalid / (148 * 2 * 8);
+  const int target = (int)(tgt64 < 4096 ? 4096 : (tgt64 > (1 << 30) ? (1 << 30) : tgt64));
+  k_make_items<<<(nt + 127) / 128, 128, 0, st>>>(lc, N[2], nt, target, kMinTZ, kMaxTZ, items,
+                                                 nitems);
+  count_launch(2);
+  out.items = items;
+  out.nitems = nitems;
+  out.cap = cap_items;
+  return cudaGetLastError();
 }
 
 cudaError_t launch_p2m(const P2MParams& P0, int dim, int kernel, P2MPrec prec, int lda,
-                       int64_t nvalid, bool stored_weights, cudaStream_t st) {
+                       int64_t nvalid, bool stored_weights, void* scratch, cudaStream_t st) {
   cudaError_t e = cudaSuccess;
+  P2MParams Pw = P0;
+  if (dim == 3) {
+    // work items: xy tiles split along z into segments of similar particle count
+    TileItems ti;
+    if ((e = make_tile_items(P0.start, P0.N, nvalid, scratch, ti, st))) return e;
+    Pw.items = ti.items;
+    Pw.nitems = ti.nitems;
+    Pw.item_cap = ti.cap;
+  }
   const int nchunk = (lda + 3) / 4;
   for (int ch = 0; ch < nchunk; ++ch) {
-    P2MParams P = P0;
+    P2MParams P = Pw;
     const int lc = lda - 4 * ch < 4 ? lda - 4 * ch : 4;
     P.c0 = 4 * ch;
     const size_t vsz = prec == P2M_FP64 ? sizeof(double4) : sizeof(float4);

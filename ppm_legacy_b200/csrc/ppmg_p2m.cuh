@@ -21,15 +21,35 @@ struct P2MParams {
   const void* us;      // Vec4 strengths (4 components of one chunk)
   void* field;         // field_up base (element (1, lb...))
   FieldDesc fd;
+  // 3D work items (xy tile, z0, z1), filled by launch_p2m
+  const int4* items;
+  const int* nitems;
+  int item_cap;
 };
 
-// Tile depth (nodes along the sweep axis per CTA) for a mesh of N cells.
+// Device scratch launch_p2m needs (work items, per-layer counts).
+size_t p2m_scratch_bytes(int dim, const int N[3]);
+
+// Work items of the 3D tile kernels: (xy tile of kTileX x kTileY cells,
+// z0, z1) with z ranges split so every item holds a similar particle count.
+struct TileItems {
+  const int4* items;
+  const int* nitems;  // device count
+  int cap;            // grid size to launch (items beyond *nitems exit)
+};
+size_t tile_items_bytes(const int N[3]);
+// The items a previous make_tile_items left in `scratch`.
+TileItems tile_items_view(void* scratch, const int N[3]);
+cudaError_t make_tile_items(const int* start, const int N[3], int64_t nvalid, void* scratch,
+                            TileItems& out, cudaStream_t st);
+
+// Tile depth (nodes along the sweep axis per CTA) of the 2D gather.
 int p2m_tile_depth(int dim, const int N[3]);
 
 // Launch the gather for all components (chunks of 4) of a P2M / remesh.
 // stored_weights: P.rec holds FP64 1D weights per sorted particle
 // (wx[S], wy[S][, wz[S]]) from comp_weights instead of offset records.
 cudaError_t launch_p2m(const P2MParams& P, int dim, int kernel, P2MPrec prec, int lda,
-                       int64_t nvalid, bool stored_weights, cudaStream_t st);
+                       int64_t nvalid, bool stored_weights, void* scratch, cudaStream_t st);
 
 }  // namespace ppmg

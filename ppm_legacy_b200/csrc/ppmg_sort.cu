@@ -34,7 +34,7 @@ void DevBuf::release() {
 
 Workspace::~Workspace() {
   DevBuf* all[] = {&key, &slot, &idx, &count, &start, &bsum, &rec, &us, &err,
-                   &big, &h_xp, &h_up, &h_field, &h_aux, &w1d};
+                   &big, &tiles, &h_xp, &h_up, &h_field, &h_aux, &w1d};
   for (DevBuf* b : all) b->release();
   if (h_err_pinned) cudaFreeHost(h_err_pinned);
 }
@@ -157,10 +157,46 @@ __device__ __forceinline__ bool cell_axis(const KeyParams& kp, int a, T x, int& 
   return true;
 }
 
+// 64-bit fingerprint of a particle's coordinates (splitmix64 finaliser over
+// the coordinate bits and the particle index); summed over particles it
+// identifies a position array (accidental equality ~2^-64).
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+template <class T>
+__device__ __forceinline__ unsigned long long bits64(T v) {
+  if constexpr (sizeof(T) == 8) return (unsigned long long)__double_as_longlong((double)v);
+  else return (unsigned long long)(unsigned)__float_as_int((float)v);
+}
+template <class T>
+__device__ __forceinline__ unsigned long long particle_hash(const T* x, int dim, int64_t p) {
+  unsigned long long h = mix64((unsigned long long)p);
+  for (int a = 0; a < dim; ++a) h = mix64(h ^ bits64<T>(x[a]));
+  return h;
+}
+__device__ __forceinline__ void block_add_hash(unsigned long long v, unsigned long long* out) {
+  __shared__ unsigned long long part[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) part[wid] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += part[w];
+    atomicAdd(out, t);
+  }
+}
+
 template <class T>
 __global__ void k_bin(KeyParams kp, const T* __restrict__ xp, int64_t ldxp, int64_t np,
                       int* __restrict__ key, int* __restrict__ slot, int* __restrict__ count,
-                      int* __restrict__ err, T* __restrict__ zout, int64_t ldz, int nz) {
+                      int* __restrict__ err, T* __restrict__ zout, int64_t ldz, int nz,
+                      unsigned long long* __restrict__ hash) {
+  unsigned long long hacc = 0;
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np;
        p += (int64_t)gridDim.x * blockDim.x) {
     const T* x = xp + p * ldxp;
@@ -168,6 +204,7 @@ __global__ void k_bin(KeyParams kp, const T* __restrict__ xp, int64_t ldxp, int6
     T f;
     bool ok = true;
     for (int a = 0; a < kp.dim; ++a) ok = ok && cell_axis<T>(kp, a, x[a], c[a], f);
+    if (hash) hacc += particle_hash<T>(x, kp.dim, p);
     int k = -1;
     if (ok) {
       k = c[0] + kp.N[0] * (c[1] + kp.N[1] * c[2]);
@@ -179,6 +216,17 @@ __global__ void k_bin(KeyParams kp, const T* __restrict__ xp, int64_t ldxp, int6
     }
     key[p] = k;
   }
+  if (hash) block_add_hash(hacc, hash);
+}
+
+template <class T>
+__global__ void k_hash(const T* __restrict__ xp, int64_t ldxp, int64_t np, int dim,
+                       unsigned long long* __restrict__ hash) {
+  unsigned long long hacc = 0;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np;
+       p += (int64_t)gridDim.x * blockDim.x)
+    hacc += particle_hash<T>(xp + p * ldxp, dim, p);
+  block_add_hash(hacc, hash);
 }
 
 __global__ void k_scatter(const int* __restrict__ key, const int* __restrict__ slot,
@@ -283,7 +331,7 @@ cudaError_t scan_exclusive(const int* in, int* out, int64_t n, Workspace& ws,
 template <class T>
 cudaError_t bin_sort(const KeyParams& kp, const T* xp, int64_t ldxp, int64_t np,
                      int64_t ncell, Workspace& ws, int* err_counter, cudaStream_t st,
-                     T* zout, int64_t ldz, int nz) {
+                     T* zout, int64_t ldz, int nz, unsigned long long* hash) {
   cudaError_t e;
   const size_t pn = sizeof(int) * (size_t)(np > 0 ? np : 1);
   if ((e = ws.key.ensure(pn)) || (e = ws.slot.ensure(pn)) || (e = ws.idx.ensure(pn)) ||
@@ -293,10 +341,11 @@ cudaError_t bin_sort(const KeyParams& kp, const T* xp, int64_t ldxp, int64_t np,
       (e = ws.big.ensure(sizeof(int) * (size_t)(ncell + 1 < 1 << 20 ? ncell + 2 : (1 << 20) + 2))))
     return e;
   if ((e = cudaMemsetAsync(ws.count.p, 0, sizeof(int) * (size_t)(ncell + 1), st))) return e;
+  if (hash && (e = cudaMemsetAsync(hash, 0, sizeof(unsigned long long), st))) return e;
   if (np > 0) {
     k_bin<T><<<grid_for(np, 256), 256, 0, st>>>(kp, xp, ldxp, np, ws.key.as<int>(),
                                                 ws.slot.as<int>(), ws.count.as<int>(),
-                                                err_counter, zout, ldz, nz);
+                                                err_counter, zout, ldz, nz, hash);
     count_launch();
   }
   return sort_tail(np, ncell, ws, st);
@@ -304,10 +353,26 @@ cudaError_t bin_sort(const KeyParams& kp, const T* xp, int64_t ldxp, int64_t np,
 
 template cudaError_t bin_sort<double>(const KeyParams&, const double*, int64_t, int64_t,
                                       int64_t, Workspace&, int*, cudaStream_t, double*,
-                                      int64_t, int);
+                                      int64_t, int, unsigned long long*);
 template cudaError_t bin_sort<float>(const KeyParams&, const float*, int64_t, int64_t,
                                      int64_t, Workspace&, int*, cudaStream_t, float*, int64_t,
-                                     int);
+                                     int, unsigned long long*);
+
+template <class T>
+cudaError_t position_hash(const T* xp, int64_t ldxp, int64_t np, int dim,
+                          unsigned long long* hash, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(hash, 0, sizeof(unsigned long long), st);
+  if (e) return e;
+  if (np > 0) {
+    k_hash<T><<<grid_for(np, 256), 256, 0, st>>>(xp, ldxp, np, dim, hash);
+    count_launch();
+  }
+  return cudaGetLastError();
+}
+template cudaError_t position_hash<double>(const double*, int64_t, int64_t, int,
+                                           unsigned long long*, cudaStream_t);
+template cudaError_t position_hash<float>(const float*, int64_t, int64_t, int,
+                                          unsigned long long*, cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // Sorted records

@@ -23,7 +23,7 @@ struct DevBuf {
 
 // Scratch of one handle (device memory, grown on demand, reused).
 struct Workspace {
-  DevBuf key, slot, idx, count, start, bsum, rec, us, err, big;
+  DevBuf key, slot, idx, count, start, bsum, rec, us, err, big, tiles;
   DevBuf h_xp, h_up, h_field, h_aux;  // device mirrors for host-pointer calls
   DevBuf w1d;                          // comp_weights state: sorted 1D weights
   int* h_err_pinned = nullptr;         // pinned host copy of the error word
@@ -52,11 +52,19 @@ struct KeyParams {
 // valid particles), ws.key the cell of every particle (-1 if invalid).
 // T is the position type (double or float).
 // Invalid particles increment *err_counter (device, not reset here); when
-// zout is given their rows zout(0:nz-1, p) are zeroed (M2P output).
+// zout is given their rows zout(0:nz-1, p) are zeroed (M2P output).  When
+// hash is given it receives the position fingerprint of position_hash.
 template <class T>
 cudaError_t bin_sort(const KeyParams& kp, const T* xp, int64_t ldxp, int64_t np,
                      int64_t ncell, Workspace& ws, int* err_counter, cudaStream_t st,
-                     T* zout = nullptr, int64_t ldz = 0, int nz = 0);
+                     T* zout = nullptr, int64_t ldz = 0, int nz = 0,
+                     unsigned long long* hash = nullptr);
+
+// 64-bit fingerprint of the first `dim` coordinates of xp(ldxp, np) into
+// *hash (device): sum over particles of a mixed hash of (index, coordinates).
+template <class T>
+cudaError_t position_hash(const T* xp, int64_t ldxp, int64_t np, int dim,
+                          unsigned long long* hash, cudaStream_t st);
 
 // Exclusive scan of n ints (in may alias out).
 cudaError_t scan_exclusive(const int* in, int* out, int64_t n, Workspace& ws,

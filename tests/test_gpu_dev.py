@@ -102,3 +102,31 @@ def test_config2_round_trip_properties():
     assert ppmg.ppm_interp_p2m(dxp, n, dup * 2, 3, t.topo_id, t.mesh_id, 2, g, f3) == 0
     assert torch.equal(f3[:, 2:2 + nc, 2:2 + nc, 2:2 + nc, 0].cpu(),
                        torch.from_numpy(res[0][0] * 2))
+
+
+def test_m2p_reuses_p2m_order_only_for_identical_positions():
+    """M2P after P2M of the same positions reuses P2M's cell order (fingerprint
+    match); after the positions change (even one particle, one ulp) it sorts
+    again.  Both must equal the oracle."""
+    rng = np.random.default_rng(95)
+    t = registered(3, 16)
+    g = [2, 2, 2]
+    lb, ub = box_bounds(t, g)
+    xp = random_particles(rng, 3, 20000)
+    up = np.asfortranarray(rng.standard_normal((3, 20000)))
+    shape = (3,) + tuple(ub[a] - lb[a] + 1 for a in range(3)) + (1,)
+    for mode in (0, 1):
+        ppmg.set_precision(mode)
+        f = np.zeros(shape, order="F")
+        assert ppmg.ppm_interp_p2m(xp, 20000, up, 3, t.topo_id, t.mesh_id, 2, g, f) == 0
+        for moved in (False, True):
+            xq = xp.copy(order="F")
+            if moved:
+                xq[0, 7] = np.nextafter(xq[0, 7], 2.0)
+                xq[:, 100:200] = xq[:, 100:200][:, ::-1]
+            out = np.zeros((3, 20000), order="F")
+            assert ppmg.ppm_interp_m2p(xq, 20000, out, 3, t.topo_id, t.mesh_id, 2, g, f) == 0
+            ref = O.m2p(t, xq, f, lb, ub, 3, 2, g)
+            tol = 0.0 if mode == 0 else 1e-6
+            assert max_rel(out, ref) <= tol, (mode, moved)
+    ppmg.set_precision(0)
