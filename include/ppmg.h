@@ -102,6 +102,24 @@ void ppmg_interp_p2m_sv_3d_dev(PPMG_P2M_V_ARGS(float), void* stream);
 void ppmg_interp_p2m_dv_2d_dev(PPMG_P2M_V_ARGS(double), void* stream);
 void ppmg_interp_p2m_sv_2d_dev(PPMG_P2M_V_ARGS(float), void* stream);
 
+/* P2M that allocates nothing.  No counterpart in the reference: this entry
+ * point exists for callers that cannot let the library call cudaMalloc -- a
+ * code that hands nearly all device memory to its own pool at start-up, or a
+ * time-step loop that must not stall on the device-wide synchronisation that
+ * cudaFree (and cudaMalloc, when new memory is mapped) brings.
+ * Same arguments, results and error reporting as ppmg_interp_p2m_dv_3d_dev,
+ * but its sort and tile scratch live in one 16 MiB array compiled into the
+ * library, which every GPU that loads the library holds until exit.  Limits:
+ * Np <= 131072, Nx*Ny*Nz <= 262144 cells, lda <= 4; larger calls return
+ * info = -2 (errnum 503) and launch nothing.
+ * The first call on a device looks up the array's device address (this may
+ * load the library's device code on that device): make it before any stream
+ * capture.  All calls on a device share the array and each overwrites the
+ * previous call's contents (what must start at zero is cleared by the call):
+ * calls whose GPU work overlaps -- different streams, or different host
+ * threads -- race and corrupt each other's results; order them on one stream. */
+void ppmg_interp_p2m_dv_3d_noalloc(PPMG_P2M_V_ARGS(double), void* stream);
+
 /* ---- ppm_interp_m2p  (ppm/src/ppm_interp_m2p.f:126-162) ------------------
  * up is overwritten (zeroed, then the gather).  Reads the real nodes 1..Nm-1
  * of field_up with periodic wrap, i.e. the result of the reference's M2P

@@ -48,6 +48,7 @@ SIGNATURES = {
                                  _pi64, _pd, _pd, _pd, _pi], None),
     "ppmg_util_rank3d_d": (_RANK, None),
     "ppmg_util_rank2d_d": (_RANK, None),
+    "ppmg_interp_p2m_dv_3d_noalloc": (_P2M_V + [_vp], None),
 }
 for _k in ("ss", "sv", "ds", "dv"):
     for _d in ("2d", "3d"):

@@ -1200,3 +1200,164 @@ void ppmg_util_rank2d_d(const double* xp, int64_t ldxp, int64_t Np, const double
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// P2M without allocation (ppmg_interp_p2m_dv_3d_noalloc).
+//
+// Some callers cannot let this library call cudaMalloc: a simulation that
+// hands nearly all of the GPU's memory to its own pool at start-up (a library
+// allocation then fails or fragments that pool), and a time-step loop that
+// must not stall, since cudaFree -- and cudaMalloc when the driver has to map
+// fresh memory -- synchronises the whole device.  This variant of the device
+// P2M keeps its sort and tile scratch in one fixed array compiled into the
+// library instead of the mesh handle's growable workspace.  The array is
+// modest (kNoAllocBytes = 16 MiB) but every GPU that loads the library holds
+// it until the process exits.
+// ===========================================================================
+
+// The scratch of every noalloc call on a device.  In host code this name is a
+// host-side stand-in for the device array, not a device address: the device
+// address comes from cudaGetSymbolAddress, once per device.
+static constexpr size_t kNoAllocBytes = size_t(16) << 20;
+static __device__ __align__(256) unsigned char ppmg_noalloc_scratch[kNoAllocBytes];
+
+namespace ppmg {
+namespace {
+
+constexpr int64_t kNoAllocMaxParticles = 131072;
+constexpr int64_t kNoAllocMaxCells = 262144;
+constexpr int kNoAllocMaxLda = 4;
+constexpr int kNoAllocMaxDevices = 64;
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_base[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device.  The first call
+// on a device looks it up (which may load this library's device code there).
+void* noalloc_scratch(int* info, const char* caller) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) { cuda_fail(info, e, caller); return nullptr; }
+  if (dev < 0 || dev >= kNoAllocMaxDevices) {
+    fail(info, kErrorError, kErrArgument, std::string(caller) + ": device ordinal >= 64");
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (g_noalloc_base[dev] == nullptr) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, ppmg_noalloc_scratch);
+    if (e != cudaSuccess) { cuda_fail(info, e, caller); return nullptr; }
+    if (p == nullptr) {
+      fail(info, kErrorFatal, 602, std::string(caller) + ": scratch array has no device address");
+      return nullptr;
+    }
+    g_noalloc_base[dev] = p;
+  }
+  return g_noalloc_base[dev];
+}
+
+// Carves the sort and tile buffers of one P2M out of the scratch array as
+// fixed views (no buffer can grow, so nothing is allocated).  Returns false
+// when they do not fit.
+bool noalloc_views(Workspace& ws, void* base, int64_t np, int64_t ncell, int lda, bool fp64,
+                   const int N[3]) {
+  size_t off = 0;
+  auto view = [&](DevBuf& b, size_t n) {
+    n = (n + 255) & ~size_t(255);
+    b.fixed = true;
+    b.p = static_cast<unsigned char*>(base) + off;
+    b.bytes = n;
+    off += n;
+  };
+  const size_t pn = sizeof(int) * (size_t)(np > 0 ? np : 1);
+  view(ws.key, pn);
+  view(ws.slot, pn);
+  view(ws.idx, pn);
+  view(ws.count, sizeof(int) * (size_t)(ncell + 1));
+  view(ws.start, sizeof(int) * (size_t)(ncell + 1));
+  view(ws.err, sizeof(int) * 4);
+  view(ws.big, sizeof(int) * (size_t)(ncell + 2));
+  view(ws.bsum, sizeof(int) * (size_t)(ncell / 1024 + 16));  // scan block sums
+  const size_t vsz = fp64 ? sizeof(double4) : sizeof(float4);
+  const size_t n = (size_t)(np > 0 ? np : 1);
+  view(ws.rec, vsz * n);
+  view(ws.us, vsz * n * (size_t)((lda + 3) / 4));
+  view(ws.tiles, p2m_scratch_bytes(3, N));
+  return off <= kNoAllocBytes;
+}
+
+void p2m_noalloc(const double* xp, int64_t ldxp, int64_t Np, const double* up, int64_t ldup,
+                 int lda, int topo_id, int mesh_id, int kernel, const int* ghost, double* field,
+                 int64_t ldf, const int64_t* f_lb, const int64_t* f_ub, int* info,
+                 cudaStream_t st, const char* caller) {
+  clear_error();
+  if (info) *info = 0;
+  if (Np < 0 || (Np > 0 && ldxp < 3) || lda < 1 || ldup < lda || ldf < lda) {
+    fail(info, kErrorError, kErrArgument, std::string(caller) + ": invalid sizes");
+    return;
+  }
+  if (!check_kernel(kernel, caller, info)) return;
+  Handle* h = get_checked(topo_id, mesh_id, 3, caller, info);
+  if (!h) return;
+  if (Np > kNoAllocMaxParticles || h->g.ncell > kNoAllocMaxCells || lda > kNoAllocMaxLda) {
+    fail(info, kErrorError, kErrArgument,
+         std::string(caller) + ": beyond the fixed scratch (Np <= 131072, Nx*Ny*Nz <= 262144 "
+                               "cells, lda <= 4); use ppmg_interp_p2m_dv_3d_dev");
+    return;
+  }
+  void* base = noalloc_scratch(info, caller);
+  if (!base) return;
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (!check_ghost(*h, ghost, caller, info)) return;
+  int lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = 1 - ghost[a];
+    hi[a] = h->Nm[a] + ghost[a];
+  }
+  FieldDesc fd;
+  if (!make_fd(*h, ldf, f_lb, f_ub, lo, hi, fd, caller, info)) return;
+  const P2MPrec prec = g_precision.load() == PPMG_PREC_MIXED ? P2M_MIXED : P2M_FP64;
+  P2MParams P{};
+  for (int a = 0; a < 3; ++a) P.N[a] = h->g.N[a];
+  Workspace ws;  // fixed views only: its destructor frees nothing
+  if (!noalloc_views(ws, base, Np, h->g.ncell, lda, prec == P2M_FP64, P.N)) {
+    fail(info, kErrorError, kErrArgument, std::string(caller) + ": beyond the fixed scratch");
+    return;
+  }
+  // Everything that must start at zero (cell counts, the big-cell list, the
+  // work-item counter) is cleared on the stream by the sort and item builders;
+  // the rest of the array is written before it is read.
+  const KeyParams kp = make_kp(*h, KEY_INTERP_CHECKED, false);
+  cudaError_t e = bin_sort<double>(kp, xp, ldxp, Np, h->g.ncell, ws, h->d_status + 0, st);
+  if (e) { cuda_fail(info, e, caller); return; }
+  const int* dnv = d_nvalid_of(ws, h->g.ncell);
+  if (prec == P2M_FP64)
+    e = pack_records<double, double>(kp, xp, ldxp, up, ldup, lda, Np, dnv, ws, st);
+  else
+    e = pack_records<double, float>(kp, xp, ldxp, up, ldup, lda, Np, dnv, ws, st);
+  if (e) { cuda_fail(info, e, caller); return; }
+  P.TZ = p2m_tile_depth(3, P.N);
+  P.cap = prec == P2M_FP64 ? 544 : 1088;
+  P.c0 = 0;
+  P.start = ws.start.as<int>();
+  P.rec = ws.rec.p;
+  P.us = ws.us.p;
+  P.field = field;
+  P.fd = fd;
+  e = launch_p2m(P, 3, kernel, prec, lda, Np > 0 ? Np : 1, false, ws.tiles.p, st);
+  if (e) { cuda_fail(info, e, caller); return; }
+}
+
+}  // namespace
+}  // namespace ppmg
+
+extern "C" void ppmg_interp_p2m_dv_3d_noalloc(const double* xp, int64_t ldxp, int64_t Np,
+                                              const double* up, int64_t ldup, int lda,
+                                              int topo_id, int mesh_id, int kernel,
+                                              const int* ghostsize, double* field_up,
+                                              int64_t ldf, const int64_t* f_lb,
+                                              const int64_t* f_ub, int* info, void* stream) {
+  ppmg::p2m_noalloc(xp, ldxp, Np, up, ldup, lda, topo_id, mesh_id, kernel, ghostsize,
+                    field_up, ldf, f_lb, f_ub, info, (cudaStream_t)stream,
+                    "ppmg_interp_p2m_dv_3d_noalloc");
+}

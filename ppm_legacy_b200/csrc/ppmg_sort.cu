@@ -8,6 +8,7 @@
 namespace ppmg {
 
 cudaError_t DevBuf::ensure(size_t n) {
+  if (fixed) return n <= bytes && p != nullptr ? cudaSuccess : cudaErrorMemoryAllocation;
   if (n <= bytes && p != nullptr) return cudaSuccess;
   if (p) {
     cudaFree(p);
@@ -27,6 +28,7 @@ cudaError_t DevBuf::ensure(size_t n) {
 }
 
 void DevBuf::release() {
+  if (fixed) return;
   if (p) cudaFree(p);
   p = nullptr;
   bytes = 0;

@@ -11,10 +11,13 @@
 
 namespace ppmg {
 
-// A growable device buffer.
+// A growable device buffer.  A `fixed` buffer is a view of memory it does not
+// own (p and bytes set by its user): ensure() never reallocates it, it only
+// reports whether the request fits, and release() leaves the memory alone.
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  bool fixed = false;
   cudaError_t ensure(size_t n);
   void release();
   template <class T>
