@@ -202,6 +202,26 @@ const int* d_nvalid_of(const Workspace& ws, int64_t ncell) {
 template <class T>
 constexpr bool is_f32() { return sizeof(T) == 4; }
 
+// Cell-order sort of the interpolation entry points into h.ws: radix sort
+// with the records (FP64 or FP32) and, for P2M, the strengths as payload.
+template <class T>
+cudaError_t sort_interp(Handle& h, const KeyParams& kp, const T* xp, int64_t ldxp, const T* up,
+                        int64_t ldup, int lda, int64_t Np, bool fp64_rec, int* err, T* zout,
+                        int64_t ldz, int nz, cudaStream_t st) {
+  unsigned long long* hash = h.d_hash + 0;
+  int* wflag = h.d_status + 2;
+  if constexpr (is_f32<T>()) {
+    return radix_sort_records<T, float>(kp, xp, ldxp, up, ldup, lda, Np, h.g.ncell, h.ws, err,
+                                        wflag, st, zout, ldz, nz, hash);
+  } else {
+    if (fp64_rec)
+      return radix_sort_records<T, double>(kp, xp, ldxp, up, ldup, lda, Np, h.g.ncell, h.ws,
+                                           err, wflag, st, zout, ldz, nz, hash);
+    return radix_sort_records<T, float>(kp, xp, ldxp, up, ldup, lda, Np, h.g.ncell, h.ws, err,
+                                        wflag, st, zout, ldz, nz, hash);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // P2M pipeline (stream-ordered).  Returns 0 or the argument-error info.
 // ---------------------------------------------------------------------------
@@ -239,20 +259,21 @@ int p2m_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, const T* up, 
     // zero the whole allocation (ppm_rmsh_remesh.f:582: field_up = 0)
     e = cudaMemsetAsync(field, 0, sizeof(T) * (size_t)field_elems(h, ldf, f_lb, f_ub), st);
     if (e) return cuda_fail(info, e, caller);
+    // records of the comp_weights order (ws_rmsh holds its sort)
+    KeyParams kp = make_kp(h, KEY_INTERP_CHECKED, false);
+    const int* dnv = d_nvalid_of(ws, h.g.ncell);
+    if (prec == P2M_FP64)
+      e = pack_records<T, double>(kp, xp, ldxp, up, ldup, lda, Np, dnv, ws, st);
+    else
+      e = pack_records<T, float>(kp, xp, ldxp, up, ldup, lda, Np, dnv, ws, st);
+    if (e) return cuda_fail(info, e, caller);
   } else {
     h.sort_cached = false;
     KeyParams kp = make_kp(h, KEY_INTERP_CHECKED, false);
-    e = bin_sort<T>(kp, xp, ldxp, Np, h.g.ncell, ws, h.d_status + 0, st, (T*)nullptr, 0, 0,
-                    h.d_hash + 0);
+    e = sort_interp<T>(h, kp, xp, ldxp, up, ldup, lda, Np, prec == P2M_FP64, h.d_status + 0,
+                       (T*)nullptr, 0, 0, st);
     if (e) return cuda_fail(info, e, caller);
   }
-  KeyParams kp = make_kp(h, KEY_INTERP_CHECKED, false);
-  const int* dnv = d_nvalid_of(ws, h.g.ncell);
-  if (prec == P2M_FP64)
-    e = pack_records<T, double>(kp, xp, ldxp, up, ldup, lda, Np, dnv, ws, st);
-  else
-    e = pack_records<T, float>(kp, xp, ldxp, up, ldup, lda, Np, dnv, ws, st);
-  if (e) return cuda_fail(info, e, caller);
   P2MParams P{};
   for (int a = 0; a < 3; ++a) P.N[a] = a < h.dim ? h.g.N[a] : 1;
   P.TZ = p2m_tile_depth(h.dim, P.N);
@@ -321,18 +342,11 @@ int m2p_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, T* up, int64_
   KeyParams kp = make_kp(h, KEY_INTERP_WRAP, true);
   if (!reuse) {
     h.sort_cached = false;
-    e = bin_sort<T>(kp, xp, ldxp, Np, h.g.ncell, h.ws, h.d_status + 1, st, up, ldup, lda,
-                    h.d_hash + 0);
+    e = sort_interp<T>(h, kp, xp, ldxp, (const T*)nullptr, 0, 0, Np, prec == M2P_FP64,
+                       h.d_status + 1, up, ldup, lda, st);
     if (e) return cuda_fail(info, e, caller);
   }
   const int* dnv = d_nvalid_of(h.ws, h.g.ncell);
-  if (!reuse) {
-    if (prec == M2P_FP64)
-      e = pack_records<T, double>(kp, xp, ldxp, (const T*)nullptr, 0, 0, Np, dnv, h.ws, st);
-    else
-      e = pack_records<T, float>(kp, xp, ldxp, (const T*)nullptr, 0, 0, Np, dnv, h.ws, st);
-    if (e) return cuda_fail(info, e, caller);
-  }
   M2PParams P{};
   for (int a = 0; a < 3; ++a) P.N[a] = a < h.dim ? h.g.N[a] : 1;
   P.nvalid = Np;
@@ -371,13 +385,17 @@ int m2p_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, T* up, int64_
 
 // Device status -> info (synchronises the stream).
 int read_status(Handle& h, cudaStream_t st, int* info, const char* caller) {
-  int hs[2] = {0, 0};
+  int hs[3] = {0, 0, 0};
   cudaError_t e = cudaMemcpyAsync(hs, h.d_status, sizeof(hs), cudaMemcpyDeviceToHost, st);
   if (!e) e = cudaStreamSynchronize(st);
   if (e) return cuda_fail(info, e, caller);
-  if (hs[0] || hs[1]) {
-    e = cudaMemsetAsync(h.d_status, 0, 2 * sizeof(int), st);
+  if (hs[0] || hs[1] || hs[2]) {
+    e = cudaMemsetAsync(h.d_status, 0, 3 * sizeof(int), st);
     cudaStreamSynchronize(st);
+  }
+  if (hs[2] > 0) {
+    return fail(info, kErrorFatal, 602,
+                std::string(caller) + ": a device copy did not complete in time (results invalid)");
   }
   if (hs[0] > 0) {
     return fail(info, kErrorFatal, kErrPartUnass,
@@ -538,15 +556,10 @@ int adjoint_pipeline(Handle& h, const double* xp, int64_t ldxp, int64_t Np, cons
   h.sort_cached = false;
   // the transpose of P2M: P2M's stencil (FP64 mesh spacing), periodic wrap
   KeyParams kp = make_kp(h, KEY_INTERP_WRAP, false);
-  cudaError_t e = bin_sort<double>(kp, xp, ldxp, Np, h.g.ncell, h.ws, h.d_status + 1, st, dw,
-                                   lddw, lda);
+  cudaError_t e = sort_interp<double>(h, kp, xp, ldxp, nullptr, 0, 0, Np, prec == M2P_FP64,
+                                      h.d_status + 1, dw, lddw, lda, st);
   if (e) return cuda_fail(info, e, caller);
   const int* dnv = d_nvalid_of(h.ws, h.g.ncell);
-  if (prec == M2P_FP64)
-    e = pack_records<double, double>(kp, xp, ldxp, nullptr, 0, 0, Np, dnv, h.ws, st);
-  else
-    e = pack_records<double, float>(kp, xp, ldxp, nullptr, 0, 0, Np, dnv, h.ws, st);
-  if (e) return cuda_fail(info, e, caller);
   M2PParams P{};
   for (int a = 0; a < 3; ++a) P.N[a] = h.g.N[a];
   P.nvalid = Np;

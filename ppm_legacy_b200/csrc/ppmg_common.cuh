@@ -138,6 +138,23 @@ __device__ __forceinline__ void mp4_dweights(T f, T d[4]) {
   d[3] = T(4) + T(5) * s3 + T(1.5) * s3 * s3;
 }
 
+// Packed per-particle vectors (sorted records and strength chunks) are kept
+// as planes of 16-byte units, `ps` units apart: a float4 is one unit, a
+// double4 keeps (x, y) in its first plane and (z, w) in its second.  Every
+// plane of a range of sorted particles is then one contiguous block.
+__device__ __forceinline__ float4 load_vec(const float4* b, int64_t s, int64_t) { return b[s]; }
+__device__ __forceinline__ double4 load_vec(const double4* b, int64_t s, int64_t ps) {
+  const double2* p = reinterpret_cast<const double2*>(b);
+  const double2 a = p[s], c = p[ps + s];
+  return make_double4(a.x, a.y, c.x, c.y);
+}
+__device__ __forceinline__ void store_vec(float4* b, int64_t s, int64_t, float4 v) { b[s] = v; }
+__device__ __forceinline__ void store_vec(double4* b, int64_t s, int64_t ps, double4 v) {
+  double2* p = reinterpret_cast<double2*>(b);
+  p[s] = make_double2(v.x, v.y);
+  p[ps + s] = make_double2(v.z, v.w);
+}
+
 __device__ __forceinline__ int wrap_index(int i, int n) {
   int r = i % n;
   return r < 0 ? r + n : r;

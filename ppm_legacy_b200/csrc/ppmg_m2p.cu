@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(256) k_m2p3d(M2PParams P) {
   constexpr int HL = S / 2;
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= P.nvalid || s >= (int64_t)*P.d_nvalid) return;
-  const V r = static_cast<const V*>(P.rec)[s];
+  const V r = load_vec(static_cast<const V*>(P.rec), s, P.nvalid);
   int cell;
   if constexpr (sizeof(CT) == 4) cell = __float_as_int(r.w); else cell = (int)r.w;
   const int cx = cell % P.N[0];
@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(256) k_m2p2d(M2PParams P) {
   constexpr int HL = S / 2;
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= P.nvalid || s >= (int64_t)*P.d_nvalid) return;
-  const V r = static_cast<const V*>(P.rec)[s];
+  const V r = load_vec(static_cast<const V*>(P.rec), s, P.nvalid);
   int cell;
   if constexpr (sizeof(CT) == 4) cell = __float_as_int(r.w); else cell = (int)r.w;
   const int cx = cell % P.N[0];
@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(256) k_adjoint3d(M2PParams P) {
   constexpr int HL = S / 2;
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= P.nvalid || s >= (int64_t)*P.d_nvalid) return;
-  const V r = static_cast<const V*>(P.rec)[s];
+  const V r = load_vec(static_cast<const V*>(P.rec), s, P.nvalid);
   int cell;
   if constexpr (sizeof(CT) == 4) cell = __float_as_int(r.w); else cell = (int)r.w;
   const int cx = cell % P.N[0];
@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
     V rvcur;
     if (tid < ntot) {
       scur = locate(tid, rcur);
-      rvcur = rec[scur];
+      rvcur = load_vec(rec, scur, P.nvalid);
     }
     for (int i = tid; i < ntot; i += 256) {
       int rnext = 0;
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
       V rvnext;
       if (i + 256 < ntot) {
         snext = locate(i + 256, rnext);
-        rvnext = rec[snext];
+        rvnext = load_vec(rec, snext, P.nvalid);
       }
       {
         int cell;

@@ -16,7 +16,7 @@ struct M2PParams {
   int64_t nvalid;      // grid bound (Np); the sorted count is *d_nvalid
   const int* d_nvalid;
   const int* idx;     // sorted position -> particle id
-  const void* rec;    // Vec4 (fx, fy, fz, cell) per sorted particle
+  const void* rec;    // Vec4 (fx, fy, fz, cell) per sorted particle, planes nvalid apart
   const void* field;  // field_up base (element (1, lb...))
   FieldDesc fd;
   void* up;           // output up(ldup, Np) (adjoint: dw)

@@ -253,8 +253,8 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
           qv[u2] = lo_q;
           sv[u2] = (int64_t)base[lo_q] + lo_l + (i - off[lo_q]);
           if (i < n) {
-            uv[u2] = us[sv[u2]];
-            if constexpr (!WST) rv[u2] = rec[sv[u2]];
+            uv[u2] = load_vec(us, sv[u2], P.ps);
+            if constexpr (!WST) rv[u2] = load_vec(rec, sv[u2], P.ps);
           }
         }
 #pragma unroll
@@ -469,7 +469,7 @@ __global__ void __launch_bounds__(kTile2) k_p2m2d(P2MParams P) {
           if (sc[mid] <= pos) lo_q = mid; else hi_q = mid;
         }
         const int64_t s = (int64_t)sb[lo_q] + (pos - sc[lo_q]);
-        const V u = us[s];
+        const V u = load_vec(us, s, P.ps);
         CT w[2][S];
         if constexpr (WST) {
           const double* ws = static_cast<const double*>(P.rec) + s * (2 * S);
@@ -479,7 +479,7 @@ __global__ void __launch_bounds__(kTile2) k_p2m2d(P2MParams P) {
             w[1][k] = (CT)ws[S + k];
           }
         } else {
-          const V r = rec[s];
+          const V r = load_vec(rec, s, P.ps);
           weights<S, CT>(r.x, w[0]);
           weights<S, CT>(r.y, w[1]);
         }
@@ -666,6 +666,7 @@ cudaError_t launch_p2m(const P2MParams& P0, int dim, int kernel, P2MPrec prec, i
                        int64_t nvalid, bool stored_weights, void* scratch, cudaStream_t st) {
   cudaError_t e = cudaSuccess;
   P2MParams Pw = P0;
+  Pw.ps = nvalid;
   if (dim == 3) {
     // work items: xy tiles split along z into segments of similar particle count
     TileItems ti;

@@ -19,6 +19,7 @@ struct P2MParams {
   const int* start;    // cell offsets into the sorted particle order
   const void* rec;     // Vec4 (fx, fy, fz, cell) per sorted particle
   const void* us;      // Vec4 strengths (4 components of one chunk)
+  int64_t ps;          // plane stride of rec / us in 16-byte units (set by launch_p2m)
   void* field;         // field_up base (element (1, lb...))
   FieldDesc fd;
   // 3D work items (xy tile, z0, z1), filled by launch_p2m

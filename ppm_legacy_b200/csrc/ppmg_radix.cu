@@ -1,0 +1,555 @@
+// ppmg_radix.cu -- stable LSD radix sort of particles into cell order that
+// moves their packed records with the keys (declared in ppmg_sort.cuh).
+//
+// The counting sort of ppmg_sort.cu scatters particle ids to random cell
+// slots and then gathers every particle's position and strengths from random
+// addresses; on large unordered particle sets those random accesses, not the
+// arithmetic, set its time.  Here every pass reads its input in order and
+// writes it grouped by one digit of the cell key: a tile of 2048 particles is
+// ranked in shared memory and leaves as runs of equal digit, so both the
+// reads and the writes are coalesced.  The first pass builds the keys and the
+// records from xp / up; the later passes move (key, id, record, strengths).
+// The sort is stable and starts from particle-id order, so particles of one
+// cell end in ascending id -- the fill order of ppm_util_rank3d.f:525-533.
+#include <cuda_runtime.h>
+
+#include "ppmg_sort.cuh"
+#include "ppmg_sort_dev.cuh"
+
+namespace ppmg {
+namespace {
+
+constexpr int kCThreads = 256;                  // count kernel
+constexpr int kRThreads = 512;                  // move kernel
+constexpr int kRWarps = kRThreads / 32;
+constexpr int kRItems = 8;                      // items per thread and sub-tile
+constexpr int kRSub = kRThreads * kRItems;      // 4096 items per sub-tile
+constexpr int kRWarpItems = kRSub / kRWarps;    // 256 consecutive items per warp
+constexpr int kRMaxBits = 9;                    // >= 8 items per digit and sub-tile
+constexpr int kRMaxBuckets = 1 << kRMaxBits;
+constexpr int kRSlots = kRMaxBuckets + 32;      // + the invalid bucket of the first pass
+constexpr int kRDigitsPerThread = (kRMaxBuckets + 1 + kRThreads - 1) / kRThreads;
+constexpr int kRGapRun = 64;                    // longer runs of empty cells: k_fill_gaps
+constexpr int kRWaitLimit = 1 << 22;            // mbarrier polls before a unit is given up
+
+// Cell key of one particle (ncell when it has no cell) and its offsets.
+template <class T>
+__device__ __forceinline__ int particle_key(const KeyParams& kp, const T* x, int ncell,
+                                            T f[3]) {
+  int c[3] = {0, 0, 0};
+  f[0] = f[1] = f[2] = T(0);
+  bool ok = true;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+    if (a < kp.dim) ok = ok && cell_axis<T>(kp, a, x[a], c[a], f[a]);
+  return ok ? c[0] + kp.N[0] * (c[1] + kp.N[1] * c[2]) : ncell;
+}
+
+template <class T, class CT>
+struct CountArgs {
+  using V = typename Vec4<CT>::type;
+  KeyParams kp;
+  const T* xp;
+  int64_t ldxp;
+  const T* up;
+  int64_t ldup;
+  int lda, nchunk;
+  int64_t np;
+  const int* d_nvalid;  // later passes: items [0, *d_nvalid) are sorted
+  int ncell, shift, bits, subs, ntiles;
+  const int* key_in;
+  int* hist;  // [digit * ntiles + tile]
+  // first pass: keys, records and strengths in particle order
+  int* key0;
+  V* rec0;
+  V* us0;
+  int* err;
+  T* zout;
+  int64_t ldz;
+  int nz;
+  unsigned long long* hash;
+};
+
+// Digit of a key; in the first pass invalid particles (key ncell) take the
+// extra bucket nb, which sorts them behind all valid ones.
+template <bool FIRST>
+__device__ __forceinline__ int digit_of(int k, int shift, unsigned mask, int nb, int ncell) {
+  if (FIRST && k == ncell) return nb;
+  return (int)(((unsigned)k >> shift) & mask);
+}
+
+template <class T, class CT>
+__device__ __forceinline__ typename Vec4<CT>::type make_us(const T* u, int lda, int ch) {
+  CT v[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int a = ch * 4 + q;
+    v[q] = a < lda ? (CT)u[a] : CT(0);
+  }
+  typename Vec4<CT>::type w;
+  w.x = v[0];
+  w.y = v[1];
+  w.z = v[2];
+  w.w = v[3];
+  return w;
+}
+
+// Digit histogram of each tile (subs sub-tiles of consecutive items).  The
+// first pass computes the keys from the positions, writes keys, records and
+// strengths in particle order, counts invalid particles, zeroes their output
+// rows and accumulates the position fingerprint.
+template <class T, class CT, bool FIRST>
+__global__ void __launch_bounds__(kCThreads) k_radix_count(CountArgs<T, CT> A) {
+  using V = typename Vec4<CT>::type;
+  __shared__ int sh[kRSlots];
+  const int nb = 1 << A.bits;
+  const int nbk = FIRST ? nb + 1 : nb;
+  const unsigned mask = (unsigned)nb - 1u;
+  for (int d = threadIdx.x; d < nbk; d += kCThreads) sh[d] = 0;
+  __syncthreads();
+  const int64_t n = FIRST ? A.np : (int64_t)*A.d_nvalid;
+  const int64_t t0 = (int64_t)blockIdx.x * A.subs * kRSub;
+  const int64_t t1 = min(n, t0 + (int64_t)A.subs * kRSub);
+  unsigned long long hacc = 0;
+  for (int64_t i = t0 + threadIdx.x; i < t1; i += kCThreads) {
+    int k;
+    if constexpr (FIRST) {
+      const T* x = A.xp + i * A.ldxp;
+      T f[3];
+      k = particle_key<T>(A.kp, x, A.ncell, f);
+      if (A.hash) hacc += particle_hash<T>(x, A.kp.dim, i);
+      if (k == A.ncell) {
+        atomicAdd(A.err, 1);
+        if (A.zout)
+          for (int a = 0; a < A.nz; ++a) A.zout[i * A.ldz + a] = T(0);
+      }
+      A.key0[i] = k;
+      V r;
+      r.x = (CT)f[0];
+      r.y = (CT)f[1];
+      r.z = (CT)f[2];
+      if constexpr (sizeof(CT) == 4)
+        r.w = __int_as_float(k);
+      else
+        r.w = (double)k;
+      store_vec(A.rec0, i, A.np, r);
+      for (int ch = 0; ch < A.nchunk; ++ch)
+        store_vec(A.us0 + (int64_t)ch * A.np, i, A.np, make_us<T, CT>(A.up + i * A.ldup, A.lda, ch));
+    } else {
+      k = A.key_in[i];
+    }
+    atomicAdd(&sh[digit_of<FIRST>(k, A.shift, mask, nb, A.ncell)], 1);
+  }
+  __syncthreads();
+  for (int d = threadIdx.x; d < nbk; d += kCThreads)
+    A.hist[(int64_t)d * A.ntiles + blockIdx.x] = sh[d];
+  if (FIRST && A.hash) block_add_hash(hacc, A.hash);
+}
+
+struct MoveArgs {
+  int64_t np;     // plane stride of the records / strengths (16-byte units)
+  int* d_nvalid;  // written by the first pass, read by the later ones
+  int ncell, shift, bits, subs, ntiles;
+  int rplanes, nplanes;  // record planes; record + strength planes
+  const int* hist;       // exclusive-scanned, [digit * ntiles + tile]
+  const int* key_in;
+  const int* id_in;
+  const uint4* rec_in;
+  const uint4* us_in;
+  int* key_out;
+  int* id_out;
+  uint4* rec_out;
+  uint4* us_out;
+  int* wait_flag;  // set when a bulk copy never completes
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// One-dimensional TMA bulk copy global -> this CTA's shared memory.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes,
+                                          uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}" : "=r"(ok) : "r"(smem_addr(bar)), "r"(parity) : "memory");
+  return ok != 0;
+}
+// Bounded wait for a phase of an mbarrier (false: gave up).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (int it = 0; it < kRWaitLimit; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+constexpr size_t kMoveSmem = sizeof(uint4) * 2 * (size_t)kRSub + sizeof(int) * (size_t)kRSub +
+                             sizeof(int) * (size_t)(kRWarps * kRSlots + 3 * kRSlots + 64) +
+                             2 * sizeof(uint64_t);
+
+// One stable pass.  Every tile walks its sub-tiles in order; the inputs of a
+// sub-tile arrive as 16-byte-unit planes (keys with ids, then every record and
+// strength plane), each by one TMA bulk copy into one of two buffers, two
+// planes ahead of the one being written.  The keys are ranked by digit (warp
+// w owns items [256w, 256w+256), ranked round by round with __match_any_sync);
+// inv[] maps every sorted position of the sub-tile to its item, so each plane
+// is written in digit runs straight from its buffer.
+template <bool FIRST>
+__global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint4* inb = reinterpret_cast<uint4*>(smem);                 // [2][kRSub]
+  int* inv = reinterpret_cast<int*>(inb + 2 * kRSub);          // [kRSub]
+  int* whist = inv + kRSub;                                    // [kRWarps][kRSlots]
+  int* run = whist + kRWarps * kRSlots;                        // next output slot per digit
+  int* dst = run + kRSlots;                                    // digit start in the sub-tile
+  int* tot = dst + kRSlots;                                    // digit count of the sub-tile
+  int* sw = tot + kRSlots;                                     // block scan scratch [33]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sw + 64);        // [2]
+
+  const int nb = 1 << A.bits;
+  const int nbk = FIRST ? nb + 1 : nb;
+  const unsigned mask = (unsigned)nb - 1u;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int w = tid >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  int* wh = whist + w * kRSlots;
+
+  const int64_t n = FIRST ? A.np : (int64_t)*A.d_nvalid;
+  if (FIRST && blockIdx.x == 0 && tid == 0)
+    *A.d_nvalid = A.hist[(int64_t)nb * A.ntiles];  // start of the invalid bucket
+  const int64_t t0 = (int64_t)blockIdx.x * A.subs * kRSub;
+  if (t0 >= n) return;
+  const int nsc = (int)min((int64_t)A.subs, (n - t0 + kRSub - 1) / kRSub);
+  const int NU = 1 + A.nplanes;
+  const int total = nsc * NU;
+
+  for (int d = tid; d < nbk; d += kRThreads) run[d] = A.hist[(int64_t)d * A.ntiles + blockIdx.x];
+  if (tid == 0) {
+    mbar_init(&bar[0]);
+    mbar_init(&bar[1]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  // unit k of this tile: sub-tile k / NU; 0 = keys (+ ids), then the planes
+  auto issue = [&](int k) {
+    if (k >= total) return;
+    const int sub = k / NU, kind = k - sub * NU;
+    const int64_t base = t0 + (int64_t)sub * kRSub;
+    const int subn = (int)min((int64_t)kRSub, n - base);
+    uint4* b = inb + (k & 1) * kRSub;
+    uint64_t* br = &bar[k & 1];
+    if (kind == 0) {
+      const uint32_t kb = (uint32_t)((subn * 4 + 15) & ~15);
+      mbar_expect_tx(br, FIRST ? kb : 2 * kb);
+      bulk_load(b, A.key_in + base, kb, br);
+      if (!FIRST) bulk_load(reinterpret_cast<int*>(b) + kRSub, A.id_in + base, kb, br);
+    } else {
+      const int pl = kind - 1;
+      const uint4* src = pl < A.rplanes ? A.rec_in + (int64_t)pl * A.np
+                                        : A.us_in + (int64_t)(pl - A.rplanes) * A.np;
+      mbar_expect_tx(br, (uint32_t)subn * 16u);
+      bulk_load(b, src + base, (uint32_t)subn * 16u, br);
+    }
+  };
+  // every thread waits; all give up together (the outstanding copy is waited
+  // for once more, with the same bound, before the tile is abandoned)
+  auto wait_unit = [&](int k) -> bool {
+    const bool ok = mbar_wait(&bar[k & 1], (uint32_t)((k >> 1) & 1));
+    if (__syncthreads_and(ok)) return true;
+    if (tid == 0) atomicExch(A.wait_flag, 1);
+    if (k + 1 < total) mbar_wait(&bar[(k + 1) & 1], (uint32_t)(((k + 1) >> 1) & 1));
+    return false;
+  };
+
+  if (tid == 0) {
+    issue(0);
+    issue(1);
+  }
+  int k = 0;
+  for (int sub = 0; sub < nsc; ++sub) {
+    const int64_t base = t0 + (int64_t)sub * kRSub;
+    const int subn = (int)min((int64_t)kRSub, n - base);
+    if (!wait_unit(k)) return;
+    const int* skeys = reinterpret_cast<const int*>(inb + (k & 1) * kRSub);
+    const int* sids = skeys + kRSub;
+    for (int d = lane; d < nbk; d += 32) wh[d] = 0;
+    __syncwarp();
+    int key[kRItems], lpos[kRItems];
+#pragma unroll
+    for (int r = 0; r < kRItems; ++r) {
+      const int li = w * kRWarpItems + r * 32 + lane;
+      const bool valid = li < subn;
+      key[r] = valid ? skeys[li] : 0;
+      const int d = valid ? digit_of<FIRST>(key[r], A.shift, mask, nb, A.ncell) : -1;
+      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      const int before = valid ? wh[d] : 0;
+      __syncwarp();
+      if (valid && lane == __ffs(peers) - 1) wh[d] = before + __popc(peers);
+      __syncwarp();
+      lpos[r] = valid ? before + __popc(peers & lt) : -1;
+    }
+    __syncthreads();
+    // per digit: exclusive prefix over the warps and the sub-tile total
+    for (int d = tid; d < nbk; d += kRThreads) {
+      int s = 0;
+#pragma unroll
+      for (int ww = 0; ww < kRWarps; ++ww) {
+        const int c = whist[ww * kRSlots + d];
+        whist[ww * kRSlots + d] = s;
+        s += c;
+      }
+      tot[d] = s;
+    }
+    __syncthreads();
+    {
+      // digit starts inside the sub-tile: exclusive scan of tot
+      int v[kRDigitsPerThread], sum = 0;
+#pragma unroll
+      for (int q = 0; q < kRDigitsPerThread; ++q) {
+        const int d = tid * kRDigitsPerThread + q;
+        v[q] = d < nbk ? tot[d] : 0;
+        sum += v[q];
+      }
+      int tsum;
+      int ex = block_excl_scan(sum, sw, tsum);
+#pragma unroll
+      for (int q = 0; q < kRDigitsPerThread; ++q) {
+        const int d = tid * kRDigitsPerThread + q;
+        if (d < nbk) dst[d] = ex;
+        ex += v[q];
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kRItems; ++r)
+      if (lpos[r] >= 0) {
+        const int d = digit_of<FIRST>(key[r], A.shift, mask, nb, A.ncell);
+        inv[lpos[r] + dst[d] + wh[d]] = w * kRWarpItems + r * 32 + lane;
+      }
+    __syncthreads();
+    // keys and ids; each thread takes the sorted positions j = tid + 512 q
+    int gdst[kRItems];
+#pragma unroll
+    for (int q = 0; q < kRItems; ++q) {
+      const int j = tid + q * kRThreads;
+      gdst[q] = -1;
+      if (j < subn) {
+        const int li = inv[j];
+        const int kk = skeys[li];
+        const int d = digit_of<FIRST>(kk, A.shift, mask, nb, A.ncell);
+        gdst[q] = run[d] + (j - dst[d]);
+        A.key_out[gdst[q]] = kk;
+        A.id_out[gdst[q]] = FIRST ? (int)(base + li) : sids[li];
+      }
+    }
+    __syncthreads();
+    if (tid == 0) issue(k + 2);
+    ++k;
+    // record and strength planes
+    for (int pl = 0; pl < A.nplanes; ++pl) {
+      if (!wait_unit(k)) return;
+      const uint4* sb = inb + (k & 1) * kRSub;
+      uint4* out = pl < A.rplanes ? A.rec_out + (int64_t)pl * A.np
+                                  : A.us_out + (int64_t)(pl - A.rplanes) * A.np;
+#pragma unroll
+      for (int q = 0; q < kRItems; ++q)
+        if (gdst[q] >= 0) out[gdst[q]] = sb[inv[tid + q * kRThreads]];
+      __syncthreads();
+      if (tid == 0) issue(k + 2);
+      ++k;
+    }
+    for (int d = tid; d < nbk; d += kRThreads) run[d] += tot[d];
+  }
+}
+
+// start[c] = first sorted position whose key is >= c, for c in [0, ncell]
+// (start[ncell] = the valid count): position s writes the cells between the
+// previous key and its own; runs of more than kRGapRun empty cells go to a
+// list that k_fill_gaps writes.
+__global__ void k_cell_starts(const int* __restrict__ key, const int* __restrict__ d_nvalid,
+                              int ncell, int* __restrict__ start, int4* __restrict__ gaps,
+                              int* __restrict__ ngaps, int gapcap) {
+  const int64_t nv = *d_nvalid;
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s <= nv;
+       s += (int64_t)gridDim.x * blockDim.x) {
+    const int kprev = s > 0 ? key[s - 1] : -1;
+    const int kcur = s < nv ? key[s] : ncell;
+    const int c0 = kprev + 1;
+    const int c1 = kcur;
+    if (c1 < c0) continue;
+    if (c1 - c0 < kRGapRun) {
+      for (int c = c0; c <= c1; ++c) start[c] = (int)s;
+    } else {
+      const int g = atomicAdd(ngaps, 1);
+      if (g < gapcap) gaps[g] = make_int4(c0, c1, (int)s, 0);
+    }
+  }
+}
+
+__global__ void k_fill_gaps(const int4* __restrict__ gaps, const int* __restrict__ ngaps,
+                            int gapcap, int* __restrict__ start) {
+  const int n = min(*ngaps, gapcap);
+  for (int g = blockIdx.x; g < n; g += gridDim.x) {
+    const int4 q = gaps[g];
+    for (int c = q.x + threadIdx.x; c <= q.y; c += blockDim.x) start[c] = q.z;
+  }
+}
+
+int bit_length(int64_t v) {
+  int b = 0;
+  while (v > 0) {
+    ++b;
+    v >>= 1;
+  }
+  return b;
+}
+
+}  // namespace
+
+template <class T, class CT>
+cudaError_t radix_sort_records(const KeyParams& kp, const T* xp, int64_t ldxp, const T* up,
+                               int64_t ldup, int lda, int64_t np, int64_t ncell,
+                               Workspace& ws, int* err_counter, int* wait_flag, cudaStream_t st,
+                               T* zout, int64_t ldz, int nz, unsigned long long* hash) {
+  using V = typename Vec4<CT>::type;
+  constexpr int RU = (int)(sizeof(V) / 16);
+  const int nchunk = up ? (lda + 3) / 4 : 0;
+  const size_t n = (size_t)(np > 0 ? np : 1);
+  const size_t nus = n * (size_t)(nchunk > 0 ? nchunk : 1);
+  const size_t nk = n + 16;  // bulk copies of keys round up to 16 bytes
+  cudaError_t e;
+  if ((e = ws.key.ensure(sizeof(int) * nk)) || (e = ws.key2.ensure(sizeof(int) * nk)) ||
+      (e = ws.idx.ensure(sizeof(int) * nk)) || (e = ws.idx2.ensure(sizeof(int) * nk)) ||
+      (e = ws.rec.ensure(sizeof(V) * n)) || (e = ws.rec2.ensure(sizeof(V) * n)) ||
+      (e = ws.us.ensure(sizeof(V) * nus)) || (e = ws.us2.ensure(sizeof(V) * nus)) ||
+      (e = ws.start.ensure(sizeof(int) * (size_t)(ncell + 1))) ||
+      (e = ws.err.ensure(sizeof(int) * 4)))
+    return e;
+  if (hash && (e = cudaMemsetAsync(hash, 0, sizeof(unsigned long long), st))) return e;
+  if (np == 0) return cudaMemsetAsync(ws.start.p, 0, sizeof(int) * (size_t)(ncell + 1), st);
+
+  // digits of the valid keys [0, ncell); the first pass adds an invalid bucket
+  const int nbits = ncell > 1 ? bit_length(ncell - 1) : 1;
+  const int passes = (nbits + kRMaxBits - 1) / kRMaxBits;
+  const int bits = (nbits + passes - 1) / passes;
+  const int64_t nsub = (np + kRSub - 1) / kRSub;
+  const int64_t want_tiles = 148 * 4;
+  const int subs = (int)((nsub + want_tiles - 1) / want_tiles);
+  const int ntiles = (int)((nsub + subs - 1) / subs);
+  if ((e = ws.hist.ensure(sizeof(int) * (size_t)ntiles * (size_t)((1 << bits) + 1)))) return e;
+  if ((e = cudaFuncSetAttribute(k_radix_move<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kMoveSmem)) ||
+      (e = cudaFuncSetAttribute(k_radix_move<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kMoveSmem)))
+    return e;
+  int* d_nvalid = ws.err.as<int>() + 2;
+  DevBuf* keys[2] = {&ws.key, &ws.key2};
+  DevBuf* ids[2] = {&ws.idx, &ws.idx2};
+  DevBuf* recs[2] = {&ws.rec, &ws.rec2};
+  DevBuf* uss[2] = {&ws.us, &ws.us2};
+  for (int p = 0; p < passes; ++p) {
+    const int shift = p * bits;
+    const int pb = nbits - shift < bits ? nbits - shift : bits;
+    const int nbk = p == 0 ? (1 << pb) + 1 : (1 << pb);
+    const int out = (passes - 1 - p) & 1;  // the last pass writes set 0
+    const int in = out ^ 1;
+    CountArgs<T, CT> C{};
+    C.kp = kp;
+    C.xp = xp;
+    C.ldxp = ldxp;
+    C.up = up;
+    C.ldup = ldup;
+    C.lda = lda;
+    C.nchunk = nchunk;
+    C.np = np;
+    C.d_nvalid = d_nvalid;
+    C.ncell = (int)ncell;
+    C.shift = shift;
+    C.bits = pb;
+    C.subs = subs;
+    C.ntiles = ntiles;
+    C.key_in = keys[in]->as<int>();
+    C.hist = ws.hist.as<int>();
+    C.key0 = keys[in]->as<int>();
+    C.rec0 = recs[in]->as<V>();
+    C.us0 = uss[in]->as<V>();
+    C.err = err_counter;
+    C.zout = zout;
+    C.ldz = ldz;
+    C.nz = nz;
+    C.hash = hash;
+    if (p == 0)
+      k_radix_count<T, CT, true><<<ntiles, kCThreads, 0, st>>>(C);
+    else
+      k_radix_count<T, CT, false><<<ntiles, kCThreads, 0, st>>>(C);
+    count_launch();
+    if ((e = scan_exclusive(ws.hist.as<int>(), ws.hist.as<int>(), (int64_t)ntiles * nbk, ws,
+                            st)))
+      return e;
+    MoveArgs M{};
+    M.np = np;
+    M.d_nvalid = d_nvalid;
+    M.ncell = (int)ncell;
+    M.shift = shift;
+    M.bits = pb;
+    M.subs = subs;
+    M.ntiles = ntiles;
+    M.rplanes = RU;
+    M.nplanes = RU * (1 + nchunk);
+    M.hist = ws.hist.as<int>();
+    M.key_in = keys[in]->as<int>();
+    M.id_in = ids[in]->as<int>();
+    M.rec_in = recs[in]->as<uint4>();
+    M.us_in = uss[in]->as<uint4>();
+    M.key_out = keys[out]->as<int>();
+    M.id_out = ids[out]->as<int>();
+    M.rec_out = recs[out]->as<uint4>();
+    M.us_out = uss[out]->as<uint4>();
+    M.wait_flag = wait_flag;
+    if (p == 0)
+      k_radix_move<true><<<ntiles, kRThreads, kMoveSmem, st>>>(M);
+    else
+      k_radix_move<false><<<ntiles, kRThreads, kMoveSmem, st>>>(M);
+    count_launch();
+  }
+  // cell offsets from the sorted keys
+  const int gapcap = (int)((ncell + 1) / (kRGapRun + 1) + 2);
+  if ((e = ws.gaps.ensure(sizeof(int4) * (size_t)gapcap))) return e;
+  if ((e = cudaMemsetAsync(ws.err.as<int>() + 3, 0, sizeof(int), st))) return e;
+  const int64_t gs = (np + 1 + 255) / 256;
+  k_cell_starts<<<(int)(gs < 148 * 16 ? gs : 148 * 16), 256, 0, st>>>(
+      ws.key.as<int>(), d_nvalid, (int)ncell, ws.start.as<int>(), ws.gaps.as<int4>(),
+      ws.err.as<int>() + 3, gapcap);
+  k_fill_gaps<<<148 * 2, 256, 0, st>>>(ws.gaps.as<int4>(), ws.err.as<int>() + 3, gapcap,
+                                       ws.start.as<int>());
+  count_launch(2);
+  return cudaGetLastError();
+}
+
+#define PPMG_RADIX_INST(T, CT)                                                              \
+  template cudaError_t radix_sort_records<T, CT>(const KeyParams&, const T*, int64_t,      \
+                                                 const T*, int64_t, int, int64_t, int64_t, \
+                                                 Workspace&, int*, int*, cudaStream_t, T*, \
+                                                 int64_t, int, unsigned long long*);
+PPMG_RADIX_INST(double, double)
+PPMG_RADIX_INST(double, float)
+PPMG_RADIX_INST(float, float)
+#undef PPMG_RADIX_INST
+
+}  // namespace ppmg

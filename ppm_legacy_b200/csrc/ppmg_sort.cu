@@ -3,6 +3,7 @@
 
 #include <cmath>
 
+#include "ppmg_sort_dev.cuh"
 #include "ppmg_sort.cuh"
 
 namespace ppmg {
@@ -36,7 +37,8 @@ void DevBuf::release() {
 
 Workspace::~Workspace() {
   DevBuf* all[] = {&key, &slot, &idx, &count, &start, &bsum, &rec, &us, &err,
-                   &big, &tiles, &h_xp, &h_up, &h_field, &h_aux, &w1d};
+                   &big, &tiles, &h_xp, &h_up, &h_field, &h_aux, &w1d,
+                   &key2, &idx2, &rec2, &us2, &hist, &gaps};
   for (DevBuf* b : all) b->release();
   if (h_err_pinned) cudaFreeHost(h_err_pinned);
 }
@@ -47,37 +49,6 @@ constexpr int kScanThreads = 512;
 constexpr int kScanRounds = 16;
 constexpr int kScanTile = kScanThreads * kScanRounds;
 constexpr int kSmallCell = 64;
-
-__device__ __forceinline__ int warp_incl_scan(int v) {
-  const unsigned lane = threadIdx.x & 31u;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int n = __shfl_up_sync(0xffffffffu, v, o);
-    if (lane >= (unsigned)o) v += n;
-  }
-  return v;
-}
-
-// Block-wide exclusive scan of one value per thread; returns the block total.
-__device__ __forceinline__ int block_excl_scan(int v, int* smem_warp, int& total) {
-  const int lane = threadIdx.x & 31;
-  const int wid = threadIdx.x >> 5;
-  const int nw = blockDim.x >> 5;
-  int inc = warp_incl_scan(v);
-  if (lane == 31) smem_warp[wid] = inc;
-  __syncthreads();
-  if (wid == 0) {
-    int w = lane < nw ? smem_warp[lane] : 0;
-    int wi = warp_incl_scan(w);
-    if (lane < nw) smem_warp[lane] = wi - w;
-    if (lane == nw - 1) smem_warp[32] = wi;
-  }
-  __syncthreads();
-  int excl = inc - v + smem_warp[wid];
-  total = smem_warp[32];
-  __syncthreads();
-  return excl;
-}
 
 __global__ void k_scan_reduce(const int* __restrict__ in, int64_t n, int* __restrict__ bsum) {
   __shared__ int sw[33];
@@ -117,79 +88,6 @@ __global__ void k_scan_apply(const int* in, int* out, int64_t n, const int* __re
     int ex = block_excl_scan(v, sw, tot);
     if (i < n) out[i] = ex + carry;
     carry += tot;
-  }
-}
-
-template <class T>
-struct KeyArith;
-template <>
-struct KeyArith<double> {
-  __device__ static double mn(const KeyParams& k, int a) { return k.min[a]; }
-  __device__ static double mx(const KeyParams& k, int a) { return k.max[a]; }
-  __device__ static double di(const KeyParams& k, int a) { return k.dxi[a]; }
-};
-template <>
-struct KeyArith<float> {
-  __device__ static float mn(const KeyParams& k, int a) { return k.minf[a]; }
-  __device__ static float mx(const KeyParams& k, int a) { return k.maxf[a]; }
-  __device__ static float di(const KeyParams& k, int a) { return k.dxif[a]; }
-};
-
-// Cell of one particle along one axis, and its offset f from the stencil
-// origin, as the reference computes them (ppm_interp_p2m.f:800-822):
-// xi = (x - min_sub) * dxi, i0 = INT(xi), f = xi - i0.
-template <class T>
-__device__ __forceinline__ bool cell_axis(const KeyParams& kp, int a, T x, int& cell, T& f) {
-  using A = KeyArith<T>;
-  const T xi = rmul(rsub(x, A::mn(kp, a)), A::di(kp, a));
-  const int n = kp.N[a];
-  if (kp.mode == KEY_INTERP_CHECKED) {
-    // closed-lower / open-upper containment (periodic upper face)
-    if (!(x >= A::mn(kp, a) && x < A::mx(kp, a))) return false;
-    int i0 = (int)xi;  // xi >= 0 here: INT == FLOOR
-    f = rsub(xi, (T)i0);
-    cell = i0 >= n ? i0 - n : i0;  // xi may round up to exactly Nc
-    return true;
-  }
-  // periodic wrap of any finite position
-  if (!(fabs((double)xi) < 1.0e9)) return false;
-  T fl = floor(xi);
-  f = rsub(xi, fl);
-  cell = wrap_index((int)fl, n);
-  return true;
-}
-
-// 64-bit fingerprint of a particle's coordinates (splitmix64 finaliser over
-// the coordinate bits and the particle index); summed over particles it
-// identifies a position array (accidental equality ~2^-64).
-__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
-  z += 0x9E3779B97F4A7C15ull;
-  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-  return z ^ (z >> 31);
-}
-template <class T>
-__device__ __forceinline__ unsigned long long bits64(T v) {
-  if constexpr (sizeof(T) == 8) return (unsigned long long)__double_as_longlong((double)v);
-  else return (unsigned long long)(unsigned)__float_as_int((float)v);
-}
-template <class T>
-__device__ __forceinline__ unsigned long long particle_hash(const T* x, int dim, int64_t p) {
-  unsigned long long h = mix64((unsigned long long)p);
-  for (int a = 0; a < dim; ++a) h = mix64(h ^ bits64<T>(x[a]));
-  return h;
-}
-__device__ __forceinline__ void block_add_hash(unsigned long long v, unsigned long long* out) {
-  __shared__ unsigned long long part[32];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (lane == 0) part[wid] = v;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned long long t = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += part[w];
-    atomicAdd(out, t);
   }
 }
 
@@ -406,7 +304,7 @@ __global__ void k_pack(KeyParams kp, const T* __restrict__ xp, int64_t ldxp,
       r.w = __int_as_float(cell);
     else
       r.w = (double)cell;
-    rec[s] = r;
+    store_vec(rec, s, np, r);
     const T* u = up + p * ldup;
     for (int ch = 0; ch < nchunk; ++ch) {
       CT v[4];
@@ -420,7 +318,7 @@ __global__ void k_pack(KeyParams kp, const T* __restrict__ xp, int64_t ldxp,
       w.y = v[1];
       w.z = v[2];
       w.w = v[3];
-      us[(int64_t)ch * np + s] = w;
+      store_vec(us + (int64_t)ch * np, s, np, w);
     }
   }
 }

@@ -27,6 +27,7 @@ struct DevBuf {
 // Scratch of one handle (device memory, grown on demand, reused).
 struct Workspace {
   DevBuf key, slot, idx, count, start, bsum, rec, us, err, big, tiles;
+  DevBuf key2, idx2, rec2, us2, hist, gaps;  // radix sort: second buffer set, histograms
   DevBuf h_xp, h_up, h_field, h_aux;  // device mirrors for host-pointer calls
   DevBuf w1d;                          // comp_weights state: sorted 1D weights
   int* h_err_pinned = nullptr;         // pinned host copy of the error word
@@ -74,12 +75,33 @@ cudaError_t scan_exclusive(const int* in, int* out, int64_t n, Workspace& ws,
                            cudaStream_t st);
 
 // Pack sorted particle records: rec[s] = (fx, fy, fz, cell) of particle idx[s]
-// in CT precision, us[ch*np + s] = up(4ch..4ch+3, idx[s]) (when up != null).
+// in CT precision, us chunk ch (vector offset ch*np) [s] = up(4ch..4ch+3,
+// idx[s]) (when up != null); both in the plane layout of load_vec (stride np).
 // Positions s < *d_nvalid (the sorted count, start[ncell]) are packed.
 template <class T, class CT>
 cudaError_t pack_records(const KeyParams& kp, const T* xp, int64_t ldxp, const T* up,
                          int64_t ldup, int lda, int64_t np, const int* d_nvalid,
                          Workspace& ws, cudaStream_t st);
+
+// Stable LSD radix sort of the particles by cell (the order of bin_sort:
+// ascending id inside a cell) that carries their packed records along.  On
+// return (stream-ordered), for sorted positions s < np:
+//   ws.key[s]  cell of the particle (ncell for an invalid one; those sort last)
+//   ws.idx[s]  particle id
+//   ws.rec     (fx, fy, fz, cell) in CT precision, as pack_records
+//   ws.us      up(4ch..4ch+3, id) in CT precision (when up != null), chunk ch
+//              at vector offset ch*np
+// (rec and us in the 16-byte plane layout of load_vec, plane stride np) and
+// ws.start[0..ncell] the cell offsets (start[ncell] = valid count).
+// Invalid particles increment *err_counter; zout / hash as for bin_sort.
+// *wait_flag is set if a bulk copy of the sort never completes (the sort is
+// then incomplete and must not be used).
+template <class T, class CT>
+cudaError_t radix_sort_records(const KeyParams& kp, const T* xp, int64_t ldxp, const T* up,
+                               int64_t ldup, int lda, int64_t np, int64_t ncell,
+                               Workspace& ws, int* err_counter, int* wait_flag, cudaStream_t st,
+                               T* zout = nullptr, int64_t ldz = 0, int nz = 0,
+                               unsigned long long* hash = nullptr);
 
 // Clist ranking (ppm_util_rank{2,3}d): keys from FLOOR((x-xmin)*rdx)+Ngl with
 // the reference's upper-boundary corrections; -1 outside the mesh.  The
