@@ -348,20 +348,22 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
       for (int t = 1; t < kTileY; ++t) r += (i >= rpre[buf][t]) ? 1 : 0;
       return (int64_t)rbeg[buf][r] + (i - rpre[buf][r]);
     };
-    int rcur = 0;
+    int rcur = 0, idcur = 0;
     int64_t scur = 0;
     V rvcur;
     if (tid < ntot) {
       scur = locate(tid, rcur);
       rvcur = load_vec(rec, scur, P.nvalid);
+      idcur = P.idx[scur];
     }
     for (int i = tid; i < ntot; i += 256) {
-      int rnext = 0;
+      int rnext = 0, idnext = 0;
       int64_t snext = 0;
       V rvnext;
       if (i + 256 < ntot) {
         snext = locate(i + 256, rnext);
         rvnext = load_vec(rec, snext, P.nvalid);
+        idnext = P.idx[snext];
       }
       {
         int cell;
@@ -372,7 +374,7 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
         m2p_weights<S, CT, EXACT>(rvcur.x, wx);
         m2p_weights<S, CT, EXACT>(rvcur.y, wy);
         m2p_weights<S, CT, EXACT>(rvcur.z, wz);
-        FT* out = up + (int64_t)P.idx[scur] * P.ldup + P.c0;
+        FT* out = up + (int64_t)idcur * P.ldup + P.c0;
         if constexpr (EXACT) {
 #pragma unroll
           for (int a = 0; a < LC; ++a) {
@@ -414,6 +416,7 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
       rcur = rnext;
       scur = snext;
       rvcur = rvnext;
+      idcur = idnext;
     }
     // publish the prefetched plane (its slot is not read by this layer) and rows
     if (more) {

@@ -81,17 +81,22 @@ __device__ __forceinline__ void emit_node(const P2MParams& P, int x, int y, int 
 // --------------------------------------------------------------------------
 // 3D tile gather.
 // A CTA of 16 x 16 threads owns 32 x 16 node columns (two adjacent columns
-// per thread) over a z-range [Z0, Z1) given by its work item.  Per cell layer
-// the particles of the (32+S-1) x (16+S-1) cells whose stencils reach the tile
-// are staged in shared memory as structure-of-arrays (wx, wy, wz, u: one
-// 16-byte vector each per particle, consecutive particles in consecutive
-// slots).  A thread visits the S+1 cells of each of its S rows; the x-weight
-// index of each of its two columns is a compile-time constant per cell, so
-// every particle costs 3 vector loads + 1 scalar load for two columns.
-// Dense layers that do not fit are processed in chunks that take at most k
-// particles from every staged cell, so every thread has work in every chunk.
+// per thread) over a z-range [Z0, Z1) given by its work item, and sweeps the
+// cell layers that reach it.  The particles of the (32+S-1) x (16+S-1) cells
+// of a layer whose stencils reach the tile are processed in units of at most
+// `cap` particles (one unit per layer unless the layer is dense).  Units are
+// software-pipelined: while unit u is accumulated, the records and strengths
+// of unit u+1 stream into a raw shared-memory buffer with cp.async; unit u+1
+// then gets its 1D weights computed once per particle into structure-of-
+// arrays slots (wx, wy, wz, u: one 16-byte vector each).  A thread visits the
+// S+1 cells of each of its S rows; the x-weight index of each of its two
+// columns follows from the staged cell column, so every visit costs 3 vector
+// loads + 1 scalar load for two columns.
+// Dense layers are cut into units that give every cell with particles left
+// an equal share (cap / active cells, the remainder one more for the first
+// cells), so every thread has work in every unit.
 // S: stencil width (4 = M'4, 2 = bsp2).  CT: arithmetic type.  COMP:
-// compensated FP32 accumulation (per-layer partial sums folded into a
+// compensated FP32 accumulation (per-unit partial sums folded into a
 // (hi, lo) pair with an error-free TwoSum).  OT: field type.  LC: components
 // handled by this launch (<= 4).  WST: 1D weights come from comp_weights.
 // --------------------------------------------------------------------------
@@ -103,8 +108,22 @@ __device__ __forceinline__ CT vget(const typename Vec4<CT>::type& v, int i) {
   return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
 }
 
-// Exclusive scan over n <= 3*256 cell values v(q); writes out[0..n] (out[n] =
-// total) and returns the total and the maximum through smem scalars.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(smem_dst)),
+               "l"(gmem_src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
+// Exclusive scan over n <= 3*256 cell values v(q) (thread t owns cells 3t ..
+// 3t+2); writes out[0..n] (out[n] = total) and returns the total and the
+// maximum through the smem scalars red[0], red[1].
 template <class F>
 __device__ __forceinline__ void scan_cells(int n, F val, int* out, int* wsum, int* red) {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -144,6 +163,16 @@ __device__ __forceinline__ void scan_cells(int n, F val, int* out, int* wsum, in
   __syncthreads();
 }
 
+// Shared memory of k_p2m3d for `cap` staging slots.
+template <int S, class CT, bool WST>
+constexpr size_t p2m3d_smem(int cap) {
+  using V = typename Vec4<CT>::type;
+  constexpr int NSC = (kTileX + S - 1) * (kTileY + S - 1);
+  constexpr int IU = (WST ? 3 * S * 8 / 16 : (int)sizeof(V) / 16) + (int)sizeof(V) / 16;
+  return (size_t)cap * (3 * sizeof(V) + (S + 2) * sizeof(CT) + 16 * IU + 2) +
+         sizeof(int) * (size_t)(6 * NSC + 2);
+}
+
 template <int S, class CT, bool COMP, class OT, int LC, bool WST>
 __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
   using V = typename Vec4<CT>::type;
@@ -154,6 +183,9 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
   constexpr int NSC = WX * WY;
   constexpr int NT = kTX * kTY;
   constexpr int PERC = (NSC + NT - 1) / NT;  // staged cells per thread (count loads)
+  constexpr int RU = WST ? 3 * S * 8 / 16 : (int)sizeof(V) / 16;  // 16-byte units: record part
+  constexpr int UU = (int)sizeof(V) / 16;                          // strengths part
+  constexpr int IU = RU + UU;
   static_assert(NSC <= 3 * NT, "staged cells exceed the scan width");
 
   if ((int)blockIdx.x >= *P.nitems) return;
@@ -162,16 +194,21 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
   const int X0 = (it.x % tiles_x) * kTileX;
   const int Y0 = (it.x / tiles_x) * kTileY;
   const int Z0 = it.y, Z1 = it.z;
+  const int cap = P.cap;
 
+  constexpr int PXN = S + 2;  // x-weights per slot, zero-padded: [0, w0 .. w(S-1), 0]
   extern __shared__ __align__(16) unsigned char smem[];
-  V* sWX = reinterpret_cast<V*>(smem);
-  V* sWY = sWX + P.cap;
-  V* sWZ = sWY + P.cap;
-  V* sU = sWZ + P.cap;
-  int* cnt = reinterpret_cast<int*>(sU + P.cap);
-  int* off = cnt + NSC;        // NSC + 1
-  int* base = off + NSC + 1;   // NSC
-  unsigned char* sQ = reinterpret_cast<unsigned char*>(base + NSC);  // cap: staged column
+  V* sWY = reinterpret_cast<V*>(smem);
+  V* sWZ = sWY + cap;
+  V* sU = sWZ + cap;
+  CT* sPX = reinterpret_cast<CT*>(sU + cap);           // [cap][PXN]
+  uint4* raw = reinterpret_cast<uint4*>(sPX + (size_t)cap * PXN);  // [cap][IU] next unit
+  int* cnt = reinterpret_cast<int*>(raw + (size_t)cap * IU);  // layer: particles per cell
+  int* done = cnt + NSC;                                // layer: particles already in units
+  int* cbase = done + NSC;                              // layer: first sorted particle per cell
+  int* ubase = cbase + NSC;                             // unit being issued: its first particle per cell
+  int* offU = ubase + NSC;                              // [2][NSC + 1] unit offsets per cell
+  unsigned char* sQ = reinterpret_cast<unsigned char*>(offU + 2 * (NSC + 1));  // [2][cap]
   __shared__ int wsum[16];
   __shared__ int red[2];
 
@@ -180,10 +217,10 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
   const int x0 = X0 + 2 * tx, y = Y0 + ty;
   const bool act0 = x0 < P.N[0] && y < P.N[1];
   const bool act1 = x0 + 1 < P.N[0] && y < P.N[1];
-  const V* rec = static_cast<const V*>(P.rec);
-  const V* us = static_cast<const V*>(P.us);
+  const uint4* grec = static_cast<const uint4*>(P.rec);
+  const uint4* gus = static_cast<const uint4*>(P.us);
 
-  CT acc[2][S][LC];  // window (or per-layer partials when COMP)
+  CT acc[2][S][LC];  // window (or per-unit partials when COMP)
   CT hi[2][S][LC], lo[2][S][LC];
 #pragma unroll
   for (int e = 0; e < 2; ++e)
@@ -192,7 +229,7 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
 #pragma unroll
       for (int a = 0; a < LC; ++a) acc[e][k][a] = hi[e][k][a] = lo[e][k][a] = CT(0);
 
-  // cell offsets of the staged cells of layer cz, kept in registers until stored
+  // cell offsets of the staged cells of layer cz, kept in registers until published
   int pb[PERC], pe[PERC];
   auto load_counts = [&](int cz) {
     const int czw = wrap_index(cz, P.N[2]);
@@ -210,122 +247,201 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
       }
     }
   };
-  load_counts(Z0 - HL);
-
-  for (int cz = Z0 - HL; cz <= Z1 - 1 + HH; ++cz) {
-    // 1. publish this layer's cell ranges
+  auto publish = [&]() {
 #pragma unroll
     for (int k = 0; k < PERC; ++k) {
       const int q = tid + NT * k;
       if (q < NSC) {
-        base[q] = pb[k];
+        cbase[q] = pb[k];
         cnt[q] = pe[k] - pb[k];
+        done[q] = 0;
       }
+    }
+  };
+  // Plans the next unit of the published layer into offU[ob]: returns its
+  // particle count; `left` (particles of the layer not yet in a unit) is
+  // updated.  Thread t plans cells 3t .. 3t+2.
+  int left = 0;
+  auto plan = [&](int ob, bool first) -> int {
+    int* off = offU + ob * (NSC + 1);
+    if (first) {
+      scan_cells(NSC, [&](int q) { return cnt[q]; }, off, wsum, red);
+      left = red[0];
+      if (left <= cap) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          const int q = 3 * tid + i;
+          if (q < NSC) {
+            ubase[q] = cbase[q];
+            done[q] = cnt[q];
+          }
+        }
+        const int n = left;
+        left = 0;
+        __syncthreads();
+        return n;
+      }
+    }
+    // cells with particles left share the unit equally
+    scan_cells(NSC, [&](int q) { return cnt[q] > done[q] ? 1 : 0; }, off, wsum, red);
+    const int A = max(red[0], 1);
+    const int k = cap / A, rem = cap - A * k;
+    auto take_of = [&](int q) {
+      const int l = q < NSC ? cnt[q] - done[q] : 0;
+      return l > 0 ? min(l, k + (off[q] < rem ? 1 : 0)) : 0;
+    };
+    const int t0 = take_of(3 * tid), t1 = take_of(3 * tid + 1), t2 = take_of(3 * tid + 2);
+    __syncthreads();  // the active ranks in off are read
+    scan_cells(NSC, [&](int q) { const int i = q - 3 * tid; return i == 0 ? t0 : (i == 1 ? t1 : t2); },
+               off, wsum, red);
+    const int n = red[0];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const int q = 3 * tid + i;
+      if (q < NSC) {
+        ubase[q] = cbase[q] + done[q];
+        done[q] += i == 0 ? t0 : (i == 1 ? t1 : t2);
+      }
+    }
+    left -= n;
+    __syncthreads();
+    return n;
+  };
+  // cp.async of the planned unit's records and strengths into raw; the
+  // staged column of every slot goes to sQ[ob].  Thread t issues its cells.
+  auto issue = [&](int ob) {
+    const int* off = offU + ob * (NSC + 1);
+    unsigned char* q8 = sQ + ob * cap;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const int q = 3 * tid + i;
+      if (q < NSC) {
+        const int o0 = off[q], o1 = off[q + 1];
+        const int64_t g0 = ubase[q];
+        for (int o = o0; o < o1; ++o) {
+          const int64_t s = g0 + (o - o0);
+          uint4* d = raw + (size_t)o * IU;
+#pragma unroll
+          for (int t = 0; t < RU; ++t) {
+            if constexpr (WST)
+              cp_async16(d + t, grec + s * RU + t);
+            else
+              cp_async16(d + t, grec + t * P.ps + s);
+          }
+#pragma unroll
+          for (int t = 0; t < UU; ++t) cp_async16(d + RU + t, gus + t * P.ps + s);
+          q8[o] = (unsigned char)(q % WX);
+        }
+      }
+    }
+    cp_async_commit();
+  };
+
+  // prologue: layer Z0 - HL published, its first unit in flight, the next
+  // layer's cell ranges in registers
+  int cz = Z0 - HL;
+  const int zlast = Z1 - 1 + HH;
+  load_counts(cz);
+  publish();
+  if (cz < zlast) load_counts(cz + 1);
+  __syncthreads();
+  int n_cur = plan(0, true);
+  bool last_cur = left == 0;  // the unit in flight completes its layer
+  issue(0);
+
+  for (int u = 0;; ++u) {
+    const int ub = u & 1;
+    cp_async_wait_all();
+    __syncthreads();
+    // 1. weights of unit u: raw -> structure-of-arrays slots
+    for (int i = tid; i < n_cur; i += NT) {
+      const uint4* r = raw + (size_t)i * IU;
+      CT w[3][S];
+      if constexpr (WST) {
+        const double* wsrc = reinterpret_cast<const double*>(r);
+#pragma unroll
+        for (int k = 0; k < S; ++k) {
+          w[0][k] = (CT)wsrc[k];
+          w[1][k] = (CT)wsrc[S + k];
+          w[2][k] = (CT)wsrc[2 * S + k];
+        }
+      } else {
+        const V rv = *reinterpret_cast<const V*>(r);
+        weights<S, CT>(rv.x, w[0]);
+        weights<S, CT>(rv.y, w[1]);
+        weights<S, CT>(rv.z, w[2]);
+      }
+      V b, c;
+      b.x = w[1][0]; b.y = w[1][1]; b.z = S > 2 ? w[1][S > 2 ? 2 : 0] : CT(0); b.w = S > 3 ? w[1][S > 3 ? 3 : 0] : CT(0);
+      c.x = w[2][0]; c.y = w[2][1]; c.z = S > 2 ? w[2][S > 2 ? 2 : 0] : CT(0); c.w = S > 3 ? w[2][S > 3 ? 3 : 0] : CT(0);
+      CT* px = sPX + (size_t)i * PXN;
+      px[0] = CT(0);
+#pragma unroll
+      for (int k = 0; k < S; ++k) px[1 + k] = w[0][k];
+      px[S + 1] = CT(0);
+      sWY[i] = b;
+      sWZ[i] = c;
+      sU[i] = *reinterpret_cast<const V*>(r + RU);
     }
     __syncthreads();
-    scan_cells(NSC, [&](int q) { return cnt[q]; }, off, wsum, red);
-    const int total = red[0], maxc = red[1];
-    int kch = 1 << 30, nch = 1;
-    if (total > P.cap) {
-      kch = P.cap / NSC;
-      nch = (maxc + kch - 1) / kch;
-    }
-    for (int j = 0; j < nch; ++j) {
-      const int lo_l = nch > 1 ? j * kch : 0;
-      int n = total;
-      if (nch > 1) {
-        scan_cells(NSC, [&](int q) { return min(max(cnt[q] - lo_l, 0), kch); }, off, wsum, red);
-        n = red[0];
+    // 2. plan and issue unit u+1 (the next layer's first unit when unit u
+    //    completes its layer); its loads fly while unit u is accumulated
+    const int cz_u = cz;
+    const bool last_u = last_cur;
+    const int n_u = n_cur;
+    bool more = true;
+    if (last_u) {
+      if (cz < zlast) {
+        ++cz;
+        publish();
+        if (cz < zlast) load_counts(cz + 1);
+        __syncthreads();
+        n_cur = plan(ub ^ 1, true);
+      } else {
+        more = false;
       }
-      // 2. stage particles [0, n) of this chunk, two per thread in flight
-      for (int i0 = tid; i0 < n; i0 += 2 * NT) {
-        int qv[2];
-        int64_t sv[2];
-        V uv[2], rv[2];
+    } else {
+      n_cur = plan(ub ^ 1, false);
+    }
+    if (more) {
+      last_cur = left == 0;
+      issue(ub ^ 1);
+    }
+    // 3. accumulate unit u: per row, the particles of cells 2tx..2tx+S (one range)
+    if (act0 && n_u > 0) {
+      const int* off = offU + ub * (NSC + 1);
+      const unsigned char* q8 = sQ + ub * cap;
 #pragma unroll
-        for (int u2 = 0; u2 < 2; ++u2) {
-          const int i = i0 + NT * u2;
-          int lo_q = 0, hi_q = NSC;  // largest q with off[q] <= i
-          while (hi_q - lo_q > 1) {
-            const int mid = (lo_q + hi_q) >> 1;
-            if (off[mid] <= i) lo_q = mid; else hi_q = mid;
-          }
-          qv[u2] = lo_q;
-          sv[u2] = (int64_t)base[lo_q] + lo_l + (i - off[lo_q]);
-          if (i < n) {
-            uv[u2] = load_vec(us, sv[u2], P.ps);
-            if constexpr (!WST) rv[u2] = load_vec(rec, sv[u2], P.ps);
-          }
-        }
+      for (int dy = 0; dy < S; ++dy) {
+        const int row = (ty + dy) * WX + 2 * tx;
+        const int p0 = off[row], p1 = off[row + S + 1];
+        for (int p = p0; p < p1; ++p) {
+          const int d = (int)q8[p] - 2 * tx;  // cell offset 0..S inside the window
+          const CT* px = sPX + (size_t)p * PXN;
+          const V wz = sWZ[p];
+          const V uv = sU[p];
+          const CT wy = vget<CT>(sWY[p], S - 1 - dy);
+          // x-weights of the two columns: nodes S-1-d and S-d of the stencil
+          const CT w0 = px[S - d], w1 = px[S + 1 - d];
+          const CT c0 = w0 * wy, c1 = w1 * wy;
+          const CT wzv[4] = {wz.x, wz.y, wz.z, wz.w};
+          const CT uu[4] = {uv.x, uv.y, uv.z, uv.w};
 #pragma unroll
-        for (int u2 = 0; u2 < 2; ++u2) {
-          const int i = i0 + NT * u2;
-          if (i >= n) break;
-          CT w[3][S];
-          if constexpr (WST) {
-            const double* wsrc = static_cast<const double*>(P.rec) + sv[u2] * (3 * S);
+          for (int a = 0; a < LC; ++a) {
+            const CT cu0 = c0 * uu[a], cu1 = c1 * uu[a];
 #pragma unroll
             for (int k = 0; k < S; ++k) {
-              w[0][k] = (CT)wsrc[k];
-              w[1][k] = (CT)wsrc[S + k];
-              w[2][k] = (CT)wsrc[2 * S + k];
-            }
-          } else {
-            weights<S, CT>(rv[u2].x, w[0]);
-            weights<S, CT>(rv[u2].y, w[1]);
-            weights<S, CT>(rv[u2].z, w[2]);
-          }
-          V a, b, c;
-          a.x = w[0][0]; a.y = w[0][1]; a.z = S > 2 ? w[0][S > 2 ? 2 : 0] : CT(0); a.w = S > 3 ? w[0][S > 3 ? 3 : 0] : CT(0);
-          b.x = w[1][0]; b.y = w[1][1]; b.z = S > 2 ? w[1][S > 2 ? 2 : 0] : CT(0); b.w = S > 3 ? w[1][S > 3 ? 3 : 0] : CT(0);
-          c.x = w[2][0]; c.y = w[2][1]; c.z = S > 2 ? w[2][S > 2 ? 2 : 0] : CT(0); c.w = S > 3 ? w[2][S > 3 ? 3 : 0] : CT(0);
-          sWX[i] = a;
-          sWY[i] = b;
-          sWZ[i] = c;
-          sU[i] = uv[u2];
-          sQ[i] = (unsigned char)(qv[u2] % WX);
-        }
-      }
-      __syncthreads();
-      // the next layer's cell ranges load while this chunk is accumulated
-      if (j == nch - 1 && cz < Z1 - 1 + HH) load_counts(cz + 1);
-      // 3. accumulate: per row, the particles of cells 2tx..2tx+S (one range)
-      if (act0) {
-#pragma unroll
-        for (int dy = 0; dy < S; ++dy) {
-          const int row = (ty + dy) * WX + 2 * tx;
-          const int p0 = off[row], p1 = off[row + S + 1];
-          for (int p = p0; p < p1; ++p) {
-            const int d = (int)sQ[p] - 2 * tx;  // cell offset 0..S inside the window
-            const V wx = sWX[p];
-            const V wz = sWZ[p];
-            const V u = sU[p];
-            const CT wy = vget<CT>(sWY[p], S - 1 - dy);
-            const int i0 = S - 1 - d, i1 = S - d;
-            const CT w0 = i0 >= 0 ? vget<CT>(wx, i0 >= 0 ? i0 : 0) : CT(0);
-            const CT w1 = i1 < S ? vget<CT>(wx, i1 < S ? i1 : 0) : CT(0);
-            const CT c0 = w0 * wy, c1 = w1 * wy;
-            const CT wzv[4] = {wz.x, wz.y, wz.z, wz.w};
-            const CT uu[4] = {u.x, u.y, u.z, u.w};
-#pragma unroll
-            for (int a = 0; a < LC; ++a) {
-              const CT cu0 = c0 * uu[a], cu1 = c1 * uu[a];
-#pragma unroll
-              for (int k = 0; k < S; ++k) {
-                acc[0][k][a] += cu0 * wzv[k];
-                acc[1][k][a] += cu1 * wzv[k];
-              }
+              acc[0][k][a] += cu0 * wzv[k];
+              acc[1][k][a] += cu1 * wzv[k];
             }
           }
         }
       }
-      __syncthreads();
     }
-    // 4. node zc = cz - (HL-1) of both columns is complete: fold, emit, shift
-    const int zc = cz - (HL - 1);
+    if constexpr (COMP) {
+      // fold the unit's partial sums
 #pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      if constexpr (COMP) {
+      for (int e = 0; e < 2; ++e)
 #pragma unroll
         for (int k = 0; k < S; ++k)
 #pragma unroll
@@ -333,35 +449,42 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
             two_sum_fold<CT>(hi[e][k][a], lo[e][k][a], acc[e][k][a]);
             acc[e][k][a] = CT(0);
           }
-      }
-      if ((e == 0 ? act0 : act1) && zc >= Z0 && zc < Z1) {
-        double v[LC];
+    }
+    // 4. layer complete: node zc = cz_u - (HL-1) of both columns is final: emit, shift
+    if (last_u) {
+      const int zc = cz_u - (HL - 1);
 #pragma unroll
-        for (int a = 0; a < LC; ++a)
-          v[a] = COMP ? (double)hi[e][0][a] + (double)lo[e][0][a] : (double)acc[e][0][a];
-        emit_node<3, OT, LC>(P, x0 + e, y, zc, v);
-      }
+      for (int e = 0; e < 2; ++e) {
+        if ((e == 0 ? act0 : act1) && zc >= Z0 && zc < Z1) {
+          double v[LC];
 #pragma unroll
-      for (int k = 0; k < S - 1; ++k)
+          for (int a = 0; a < LC; ++a)
+            v[a] = COMP ? (double)hi[e][0][a] + (double)lo[e][0][a] : (double)acc[e][0][a];
+          emit_node<3, OT, LC>(P, x0 + e, y, zc, v);
+        }
+#pragma unroll
+        for (int k = 0; k < S - 1; ++k)
+#pragma unroll
+          for (int a = 0; a < LC; ++a) {
+            if constexpr (COMP) {
+              hi[e][k][a] = hi[e][k + 1][a];
+              lo[e][k][a] = lo[e][k + 1][a];
+            } else {
+              acc[e][k][a] = acc[e][k + 1][a];
+            }
+          }
 #pragma unroll
         for (int a = 0; a < LC; ++a) {
           if constexpr (COMP) {
-            hi[e][k][a] = hi[e][k + 1][a];
-            lo[e][k][a] = lo[e][k + 1][a];
+            hi[e][S - 1][a] = CT(0);
+            lo[e][S - 1][a] = CT(0);
           } else {
-            acc[e][k][a] = acc[e][k + 1][a];
+            acc[e][S - 1][a] = CT(0);
           }
-        }
-#pragma unroll
-      for (int a = 0; a < LC; ++a) {
-        if constexpr (COMP) {
-          hi[e][S - 1][a] = CT(0);
-          lo[e][S - 1][a] = CT(0);
-        } else {
-          acc[e][S - 1][a] = CT(0);
         }
       }
     }
+    if (!more) break;
   }
 }
 
@@ -397,10 +520,40 @@ __global__ void k_make_items(const int* __restrict__ lc, int N2, int ntiles, int
     const bool want = (acc >= target && len >= min_tz) || len >= max_tz;
     if (cz == N2 - 1 || (want && N2 - (cz + 1) >= min_tz)) {
       const int q = atomicAdd(nitems, 1);
-      items[q] = make_int4(tile, z0, cz + 1, 0);
+      // weight: particles of the item's own cells + a per-layer cost
+      items[q] = make_int4(tile, z0, cz + 1, acc + 32 * len);
       z0 = cz + 1;
       acc = 0;
     }
+  }
+}
+
+// Longest items first (a one-CTA bucket sort by log2 weight, heaviest bucket
+// first): heavy items of dense regions start in the first wave instead of
+// stretching the tail.  Items write disjoint nodes, so the order changes
+// only the schedule, never a result.
+__global__ void __launch_bounds__(1024) k_order_items(const int4* __restrict__ tmp,
+                                                      const int* __restrict__ nitems,
+                                                      int4* __restrict__ items) {
+  __shared__ int hist[32];
+  const int n = *nitems;
+  if (threadIdx.x < 32) hist[threadIdx.x] = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    atomicAdd(&hist[31 - __clz(max(tmp[i].w, 1))], 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int b = 31; b >= 0; --b) {
+      const int c = hist[b];
+      hist[b] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int4 t = tmp[i];
+    items[atomicAdd(&hist[31 - __clz(max(t.w, 1))], 1)] = t;
   }
 }
 
@@ -556,14 +709,12 @@ __global__ void __launch_bounds__(kTile2) k_p2m2d(P2MParams P) {
 template <int S, class CT, bool COMP, class OT, int LC, bool WST>
 cudaError_t launch_lc(const P2MParams& P, int dim, cudaStream_t st) {
   if (dim == 3) {
-    constexpr int WX = kTileX + S - 1, WY = kTileY + S - 1;
-    constexpr int NSC = WX * WY;
-    // staging capacity: a whole number of slots per staged cell (chunks of
-    // dense layers take that many particles from every cell); ~85 KB, 2 CTAs/SM
+    // staging slots: as many as fit in ~110 KB (2 CTAs / SM)
     P2MParams Q = P;
-    Q.cap = NSC * (sizeof(CT) == 4 ? 2 : 1);
-    const size_t smem = (size_t)Q.cap * 4 * sizeof(typename Vec4<CT>::type) +
-                        (size_t)(3 * NSC + 1) * sizeof(int) + (size_t)Q.cap;
+    int cap = 2048;
+    while (cap > 64 && p2m3d_smem<S, CT, WST>(cap) > (size_t)110 * 1024) cap -= 16;
+    Q.cap = cap;
+    const size_t smem = p2m3d_smem<S, CT, WST>(cap);
     auto kern = k_p2m3d<S, CT, COMP, OT, LC, WST>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
@@ -621,9 +772,10 @@ int item_capacity(const int N[3]) {
 }
 }  // namespace
 
+// Layout: items[cap] | nitems (64 bytes) | unordered items[cap] | layer counts
 size_t tile_items_bytes(const int N[3]) {
-  return sizeof(int4) * (size_t)item_capacity(N) + sizeof(int) * (size_t)tiles_xy(N) * N[2] +
-         64;
+  return 2 * sizeof(int4) * (size_t)item_capacity(N) +
+         sizeof(int) * (size_t)tiles_xy(N) * N[2] + 64;
 }
 
 size_t p2m_scratch_bytes(int dim, const int N[3]) {
@@ -644,7 +796,8 @@ cudaError_t make_tile_items(const int* start, const int N[3], int64_t nvalid, vo
   const int cap_items = item_capacity(N);
   int4* items = static_cast<int4*>(scratch);
   int* nitems = reinterpret_cast<int*>(items + cap_items);
-  int* lc = nitems + 16;
+  int4* unordered = reinterpret_cast<int4*>(nitems + 16);
+  int* lc = reinterpret_cast<int*>(unordered + cap_items);
   cudaError_t e = cudaMemsetAsync(nitems, 0, sizeof(int), st);
   if (e) return e;
   const int64_t nl = (int64_t)nt * N[2];
@@ -653,9 +806,10 @@ cudaError_t make_tile_items(const int* start, const int N[3], int64_t nvalid, vo
                                      lc);
   const int64_t tgt64 = nvalid / (148 * 2 * 8);
   const int target = (int)(tgt64 < 4096 ? 4096 : (tgt64 > (1 << 30) ? (1 << 30) : tgt64));
-  k_make_items<<<(nt + 127) / 128, 128, 0, st>>>(lc, N[2], nt, target, kMinTZ, kMaxTZ, items,
-                                                 nitems);
-  count_launch(2);
+  k_make_items<<<(nt + 127) / 128, 128, 0, st>>>(lc, N[2], nt, target, kMinTZ, kMaxTZ,
+                                                 unordered, nitems);
+  k_order_items<<<1, 1024, 0, st>>>(unordered, nitems, items);
+  count_launch(3);
   out.items = items;
   out.nitems = nitems;
   out.cap = cap_items;
