@@ -58,6 +58,37 @@ def alg_bytes(np_, nc, lda=3, dim=3, b=8):
     return np_ * (2 * dim * 8 + 2 * lda * b) + (nc ** dim) * lda * 2 * b
 
 
+def kernel_bytes(np_, nc, lda, g, mixed):
+    """Algorithmic bytes of one launch of each timed part (FP64 field and
+    strengths at the API, records in the compute precision):
+    p2m_gather: sorted records + strength chunks read, the written node box
+      (Nm + 2g)^3 x lda x 8 (real nodes and every periodic image);
+    m2p_gather: the unique nodes read once, records and particle ids read,
+      up(lda, Np) written;
+    cell_sort: xp and up read, key, id, record and strengths written, the
+      cell offsets (Nc^3 + 1) written."""
+    v = 16 if mixed else 32
+    chunks = (lda + 3) // 4
+    box = (nc + 1 + 2 * g) ** 3
+    return {
+        "p2m_gather": np_ * v * (1 + chunks) + box * lda * 8,
+        "m2p_gather": nc ** 3 * lda * 8 + np_ * (v + 4 + lda * 8),
+        "cell_sort": np_ * (3 * 8 + lda * 8) + np_ * (8 + v * (1 + chunks)) + (nc ** 3 + 1) * 4,
+    }
+
+
+def measured_traffic(kernel, np_):
+    """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
+    summary (profiles/dram_traffic.json), scaled to np_ particles; None when
+    that kernel has no capture."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "dram_traffic.json")) as fh:
+            d = json.load(fh)[kernel]
+        return d["bytes_per_launch"] * np_ / d["particles"]
+    except Exception:
+        return None
+
+
 def gen_particles(torch, cfg, device, seed):
     nc, n, dist = CONFIGS[cfg]
     g = torch.Generator(device=device)
@@ -261,6 +292,14 @@ def main():
     out = torch.empty((n, 3), device=dev, dtype=torch.float64).t()
     stream = torch.cuda.current_stream()
 
+    def kernel_time(part):
+        """(total ms, launches) the library timed for a part since the last read."""
+        import ctypes as C
+        tot = C.c_double(0.0)
+        cnt = C.c_int64(0)
+        ppmg.lib().ppmg_kernel_timing_read(part, C.byref(tot), C.byref(cnt))
+        return float(tot.value), int(cnt.value)
+
     def step():
         i1 = ppmg.ppm_interp_p2m(xp, n, up, 3, 1, 1, 2, g, field)
         i2 = ppmg.ppm_interp_m2p(xp, n, out, 3, 1, 1, 2, g, field)
@@ -275,6 +314,9 @@ def main():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
+        for part in range(3):  # drop anything recorded before the timed region
+            kernel_time(part)
+        ppmg.lib().ppmg_kernel_timing(1)
         l0 = ppmg.lib().ppmg_launch_count()
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
@@ -292,6 +334,8 @@ def main():
         ev1.record(stream)
         torch.cuda.synchronize()
         launches = ppmg.lib().ppmg_launch_count() - l0
+        ppmg.lib().ppmg_kernel_timing(0)
+        kparts = [kernel_time(part) for part in range(3)]
         assert ppmg.sync_status(1, 1) == 0, ppmg.last_error()
         ms = ev0.elapsed_time(ev1) / args.steps
         if world > 1:
@@ -302,7 +346,7 @@ def main():
                 dist.barrier()
         p2m = float(np.median([a for a, _ in p2m_ms]))
         m2p = float(np.median([b for _, b in p2m_ms]))
-        return ms, p2m, m2p, launches
+        return ms, p2m, m2p, launches, kparts
 
     sampler = ClockSampler(local)
     sampler.start()
@@ -314,18 +358,37 @@ def main():
 
     peak, peak_src = hbm_peak()
     head = precs[0]
-    ms, p2m_ms, m2p_ms, launches = res[head]
+    ms, p2m_ms, m2p_ms, launches, kparts = res[head]
     total = n * world
     value = total / (ms / 1e3)
     B = alg_bytes(n, nc)
-    achieved = B / (ms / 1e3) / 1e9
-    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None,
-            "kernel": "P2M+M2P round trip (all kernels of one step)",
-            "alg_bytes_per_step": B, "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)"}
+    # per-part algorithmic bytes per launch (see kernel_bytes) over the mean
+    # CUDA-event duration of that part's launches in the timed region
+    kb = kernel_bytes(n, nc, 3, 2, head == 1)
+    names = ["p2m_gather", "m2p_gather", "cell_sort"]
+    kinfo = {}
+    for i, nm in enumerate(names):
+        tms, cnt = kparts[i]
+        if cnt == 0:
+            continue
+        avg = tms / cnt
+        ach = kb[nm] / (avg / 1e3) / 1e9
+        kinfo[nm] = {"launches": cnt, "ms_per_launch": avg, "alg_bytes": kb[nm],
+                     "achieved_gbs": ach, "frac": ach / peak,
+                     "share_of_step": tms / (ms * args.steps)}
+    dom = max(kinfo, key=lambda k: kinfo[k]["ms_per_launch"] * kinfo[k]["launches"])
+    traffic = measured_traffic(dom, n)
+    roof = {"bound": "hbm", "achieved": kinfo[dom]["achieved_gbs"], "peak": peak,
+            "unit": "GB/s", "frac": kinfo[dom]["frac"], "traffic": traffic,
+            "kernel": dom, "alg_bytes_per_launch": kb[dom],
+            "ms_per_launch": kinfo[dom]["ms_per_launch"],
+            "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs, of measured)",
+            "parts": kinfo,
+            "step": {"alg_bytes": B, "achieved_gbs": B / (ms / 1e3) / 1e9,
+                     "frac": B / (ms / 1e3) / 1e9 / peak}}
     parts = {}
     for prec in precs:
-        m, a, b, _ = res[prec]
+        m, a, b, _, _ = res[prec]
         nm = "mixed" if prec == 1 else "fp64"
         bp = n * 48 + nc ** 3 * 24
         bm = n * 48 + nc ** 3 * 24

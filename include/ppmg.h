@@ -228,6 +228,18 @@ void ppmg_util_rank2d_d(const double* xp, int64_t ldxp, int64_t Np, const double
                         const double* xmax, const int* Nm, const int* Ngl, int* lpdx,
                         int* lhbx, int64_t* icount, int* info);
 
+/* ---- Instrumentation (no counterpart in the reference) -------------------
+ * ppmg_kernel_timing(1) makes the library bracket, on the launching stream,
+ * every launch of its 3D P2M gather kernel (part 0), its 3D M2P gather
+ * kernel (part 1) and every cell-order sort (part 2, all its kernels) with
+ * CUDA events.  ppmg_kernel_timing_read(part, ...) waits for the recorded
+ * events and returns the summed device time in ms and the number of timed
+ * launches since the last read of that part, then resets them (returns 0, or
+ * -2 for an unknown part).  Off by default; enabling it adds two event
+ * records per timed launch. */
+void ppmg_kernel_timing(int enable);
+int ppmg_kernel_timing_read(int part, double* ms, int64_t* launches);
+
 #ifdef __cplusplus
 }
 #endif

@@ -49,6 +49,8 @@ SIGNATURES = {
     "ppmg_util_rank3d_d": (_RANK, None),
     "ppmg_util_rank2d_d": (_RANK, None),
     "ppmg_interp_p2m_dv_3d_noalloc": (_P2M_V + [_vp], None),
+    "ppmg_kernel_timing": ([_i], None),
+    "ppmg_kernel_timing_read": ([_i, C.POINTER(C.c_double), _pi64], _i),
 }
 for _k in ("ss", "sv", "ds", "dv"):
     for _d in ("2d", "3d"):

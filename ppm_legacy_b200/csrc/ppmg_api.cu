@@ -1215,6 +1215,106 @@ void ppmg_util_rank2d_d(const double* xp, int64_t ldxp, int64_t Np, const double
 }  // extern "C"
 
 // ===========================================================================
+// Device-time instrumentation (ppmg_kernel_timing).
+// ===========================================================================
+namespace ppmg {
+namespace {
+std::atomic<bool> g_timing{false};
+struct TimedPair {
+  int part;
+  cudaEvent_t begin, end;
+};
+std::mutex g_tmu;
+// heap-allocated and never destroyed (no CUDA calls from static destructors)
+std::vector<TimedPair>& pending() {
+  static auto* v = new std::vector<TimedPair>();
+  return *v;
+}
+std::vector<cudaEvent_t>& spare_events() {
+  static auto* v = new std::vector<cudaEvent_t>();
+  return *v;
+}
+cudaEvent_t take_event() {
+  {
+    std::lock_guard<std::mutex> lk(g_tmu);
+    if (!spare_events().empty()) {
+      cudaEvent_t ev = spare_events().back();
+      spare_events().pop_back();
+      return ev;
+    }
+  }
+  cudaEvent_t ev = nullptr;
+  if (cudaEventCreate(&ev) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return ev;
+}
+}  // namespace
+
+TimingScope::TimingScope(int part, cudaStream_t st) : part_(part), st_(st) {
+  if (part < 0 || part >= kTimedParts || !g_timing.load(std::memory_order_relaxed)) return;
+  begin_ = take_event();
+  if (begin_ && cudaEventRecord(begin_, st_) != cudaSuccess) {
+    cudaGetLastError();
+    begin_ = nullptr;
+  }
+}
+
+TimingScope::~TimingScope() {
+  if (!begin_) return;
+  cudaEvent_t end = take_event();
+  if (!end) return;
+  if (cudaEventRecord(end, st_) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  std::lock_guard<std::mutex> lk(g_tmu);
+  pending().push_back({part_, begin_, end});
+}
+}  // namespace ppmg
+
+extern "C" void ppmg_kernel_timing(int enable) { ppmg::g_timing.store(enable != 0); }
+
+extern "C" int ppmg_kernel_timing_read(int part, double* ms, int64_t* launches) {
+  using namespace ppmg;
+  if (part < 0 || part >= kTimedParts) return kErrorError;
+  std::vector<TimedPair> mine;
+  {
+    std::lock_guard<std::mutex> lk(g_tmu);
+    auto& p = pending();
+    for (size_t i = 0; i < p.size();) {
+      if (p[i].part == part) {
+        mine.push_back(p[i]);
+        p[i] = p.back();
+        p.pop_back();
+      } else {
+        ++i;
+      }
+    }
+  }
+  double total = 0.0;
+  for (const TimedPair& t : mine) {
+    float el = 0.f;
+    if (cudaEventSynchronize(t.end) == cudaSuccess &&
+        cudaEventElapsedTime(&el, t.begin, t.end) == cudaSuccess)
+      total += el;
+    else
+      cudaGetLastError();
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_tmu);
+    for (const TimedPair& t : mine) {
+      spare_events().push_back(t.begin);
+      spare_events().push_back(t.end);
+    }
+  }
+  if (ms) *ms = total;
+  if (launches) *launches = (int64_t)mine.size();
+  return 0;
+}
+
+// ===========================================================================
 // P2M without allocation (ppmg_interp_p2m_dv_3d_noalloc).
 //
 // Some callers cannot let this library call cudaMalloc: a simulation that

@@ -58,6 +58,23 @@ void clear_error();
 extern std::atomic<int64_t> g_launches;
 inline void count_launch(int n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+// Device-time instrumentation (ppmg_kernel_timing): while enabled, a scope
+// brackets the work it encloses on stream `st` with CUDA events; the elapsed
+// times accumulate per part until ppmg_kernel_timing_read.
+enum TimedPart { kTimeP2M = 0, kTimeM2P = 1, kTimeSort = 2, kTimedParts = 3 };
+class TimingScope {
+ public:
+  TimingScope(int part, cudaStream_t st);
+  ~TimingScope();
+  TimingScope(const TimingScope&) = delete;
+  TimingScope& operator=(const TimingScope&) = delete;
+
+ private:
+  int part_;
+  cudaStream_t st_;
+  cudaEvent_t begin_ = nullptr;
+};
+
 // -------------------------------------------------------------------------
 // Device helpers
 // -------------------------------------------------------------------------

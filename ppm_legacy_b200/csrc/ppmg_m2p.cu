@@ -466,6 +466,7 @@ cudaError_t launch_m2p(const M2PParams& P0, int dim, int kernel, M2PPrec prec, c
   cudaError_t e = cudaSuccess;
   if (dim == 3) {
     // tiled gather: one launch per chunk of up to 4 components
+    TimingScope timed(kTimeM2P, st);
     for (int c0 = 0; c0 < P0.lda; c0 += 4) {
       M2PParams P = P0;
       P.c0 = c0;

@@ -829,6 +829,7 @@ cudaError_t launch_p2m(const P2MParams& P0, int dim, int kernel, P2MPrec prec, i
     Pw.nitems = ti.nitems;
     Pw.item_cap = ti.cap;
   }
+  TimingScope timed(dim == 3 ? kTimeP2M : kTimedParts, dim == 3 ? st : nullptr);
   const int nchunk = (lda + 3) / 4;
   for (int ch = 0; ch < nchunk; ++ch) {
     P2MParams P = Pw;

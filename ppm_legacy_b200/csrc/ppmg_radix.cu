@@ -443,6 +443,7 @@ cudaError_t radix_sort_records(const KeyParams& kp, const T* xp, int64_t ldxp, c
     return e;
   if (hash && (e = cudaMemsetAsync(hash, 0, sizeof(unsigned long long), st))) return e;
   if (np == 0) return cudaMemsetAsync(ws.start.p, 0, sizeof(int) * (size_t)(ncell + 1), st);
+  TimingScope timed(kTimeSort, st);
 
   // digits of the valid keys [0, ncell); the first pass adds an invalid bucket
   const int nbits = ncell > 1 ? bit_length(ncell - 1) : 1;
