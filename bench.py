@@ -58,6 +58,17 @@ def alg_bytes(np_, nc, lda=3, dim=3, b=8):
     return np_ * (2 * dim * 8 + 2 * lda * b) + (nc ** dim) * lda * 2 * b
 
 
+def max_over_ranks(x, dist=None, device=None):
+    """Max of a per-rank scalar over all ranks of the default process group
+    (every rank receives it); the value itself without a group."""
+    if dist is None or not dist.is_available() or not dist.is_initialized():
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def kernel_bytes(np_, nc, lda, g, mixed):
     """Algorithmic bytes of one launch of each timed part (FP64 field and
     strengths at the API, records in the compute precision):
@@ -251,6 +262,129 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def _cfg3_particles(nc, seed=3):
+    """256^3 remesh workload: particles at cell centres displaced by 8 smooth
+    Fourier modes (max displacement 0.5 h), vortex-tube strengths (lda 3)."""
+    rng = np.random.default_rng(seed)
+    h = 1.0 / nc
+    i = np.arange(nc, dtype=np.float64)
+    X, Y, Z = np.meshgrid((i + 0.5) * h, (i + 0.5) * h, (i + 0.5) * h, indexing="ij")
+    x = np.stack([X.ravel(order="F"), Y.ravel(order="F"), Z.ravel(order="F")])
+    del X, Y, Z
+    d = np.zeros_like(x)
+    amps = rng.random(8)
+    amps *= 0.5 * h / amps.sum()
+    for m in range(8):
+        k = rng.integers(-4, 5, size=3)
+        while np.abs(k).max() < 1:
+            k = rng.integers(-4, 5, size=3)
+        e = rng.standard_normal(3)
+        e /= np.linalg.norm(e)
+        ph = rng.uniform(0, 2 * np.pi)
+        d += amps[m] * e[:, None] * np.sin(2 * np.pi * (k @ x) + ph)[None, :]
+    xp = np.asfortranarray((x + d) % 1.0)
+    xp[xp >= 1.0] = 0.0
+    tp = 2 * np.pi
+    up = np.asfortranarray(np.stack([
+        np.sin(tp * xp[0]) * np.cos(tp * xp[1]) * np.cos(tp * xp[2]),
+        np.cos(tp * xp[0]) * np.sin(tp * xp[1]) * np.cos(tp * xp[2]),
+        -2 * np.cos(tp * xp[0]) * np.cos(tp * xp[1]) * np.sin(tp * xp[2])]))
+    return xp, up
+
+
+def run_remesh(args):
+    """One remeshing step through the reference-facing host entry points:
+    ppm_rmsh_comp_weights + ppm_rmsh_remesh (M'4, lda 3, ghostsize 2) and
+    ppm_rmsh_create_part (cutoff (1e-8, huge), |u|_2, resetpos), host arrays
+    (copies inside the timed region), best of --steps after --warmup."""
+    import ppm_legacy_b200 as ppmg
+    nc = 256
+    xp, up = _cfg3_particles(nc)
+    n = xp.shape[1]
+    t = ppmg.cartesian(3, nc, topo_id=3, mesh_id=1)
+    assert ppmg.register(t) == 0, ppmg.last_error()
+    ppmg.set_precision(1 if args.precision != "fp64" else 0)
+    g = [2, 2, 2]
+    ext = nc + 1 + 2 * g[0]
+    field = np.zeros((3, ext, ext, ext, 1), order="F")
+    times = []
+    npn = 0
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        assert ppmg.ppm_rmsh_comp_weights(xp, n, 3, 1, 2) == 0, ppmg.last_error()
+        assert ppmg.ppm_rmsh_remesh(xp, n, up, 3, 3, 1, 2, g, field) == 0, ppmg.last_error()
+        info, npn, _, _, _ = ppmg.ppm_rmsh_create_part(field, 3, 1, [1e-8, 1e300], lda=3,
+                                                       resetpos=True, ghostsize=g)
+        assert info == 0, ppmg.last_error()
+        t1 = time.perf_counter()
+        if i >= args.warmup:
+            times.append(t1 - t0)
+    best = min(times)
+    print(json.dumps({
+        "workload": "remesh", "metric": "particles/s for one remeshing step",
+        "value": n / best, "unit": "particles/s", "ms_per_step": best * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "dtype": "mixed" if args.precision != "fp64" else "f64",
+        "config": {"mesh": f"{nc}^3 periodic", "particles": n, "lda": 3, "kernel": "M'4",
+                   "ghostsize": 2, "new_particles": npn,
+                   "data": "cell centres + 8 smooth modes (max 0.5 h), vortex-tube strengths"},
+        "path": "host-pointer C-ABI (comp_weights, remesh, create_part): host<->device copies "
+                "inside the timed region"}))
+
+
+def run_adjoint(args):
+    """128^3 adjoint workload: 4,194,304 uniform particles, lda 1, loss
+    0.5 |P2M(x, w) - T|^2 with T ~ N(0, 1); one step = forward P2M, the
+    residual on the device, the adjoint pass (dw, dx); device pointers."""
+    import torch
+    import ppm_legacy_b200 as ppmg
+    dev = torch.device("cuda", 0)
+    nc, n = 128, 4_194_304
+    g = torch.Generator(device=dev)
+    g.manual_seed(4)
+    xp = torch.rand((n, 3), generator=g, device=dev, dtype=torch.float64).t()
+    w = torch.randn((n, 1), generator=g, device=dev, dtype=torch.float64).t()
+    T = torch.randn((nc, nc, nc), generator=g, device=dev, dtype=torch.float64)
+    t = ppmg.cartesian(3, nc, topo_id=4, mesh_id=1)
+    assert ppmg.register(t) == 0, ppmg.last_error()
+    ppmg.set_precision(1 if args.precision != "fp64" else 0)
+    gh = [2, 2, 2]
+    ext = nc + 1 + 4
+    # column-major (Fortran) arrays: allocate the reversed shape, view it transposed
+    field = torch.zeros((1, ext, ext, ext, 1), device=dev, dtype=torch.float64).permute(
+        4, 3, 2, 1, 0)
+    R = torch.empty((1, nc, nc, nc, 1), device=dev, dtype=torch.float64).permute(4, 3, 2, 1, 0)
+    dw = torch.empty((n, 1), device=dev, dtype=torch.float64).t()
+    dx = torch.empty((n, 3), device=dev, dtype=torch.float64).t()
+    stream = torch.cuda.current_stream()
+
+    def step():
+        assert ppmg.ppm_interp_p2m(xp, n, w, 1, 4, 1, 2, gh, field) == 0
+        R[0, :, :, :, 0] = field[0, 2:2 + nc, 2:2 + nc, 2:2 + nc, 0] - T
+        assert ppmg.ppm_interp_p2m_adjoint(xp, n, w, 1, 4, 1, 2, R, dw, dx,
+                                           field_lb=[1, 1, 1]) == 0
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    assert ppmg.sync_status(4, 1) == 0, ppmg.last_error()
+    ms = e0.elapsed_time(e1) / args.steps
+    print(json.dumps({
+        "workload": "adjoint", "metric": "particles/s for forward P2M + adjoint (dL/dw, dL/dx)",
+        "value": n / (ms / 1e3), "unit": "particles/s", "ms_per_step": ms,
+        "steps": args.steps, "warmup": max(args.warmup, 3), "higher_is_better": True,
+        "dtype": "mixed" if args.precision != "fp64" else "f64",
+        "config": {"mesh": f"{nc}^3 periodic", "particles": n, "lda": 1,
+                   "data": "uniform positions, w ~ N(0,1), target T ~ N(0,1) per node"}}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -264,9 +398,17 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--cpu-warmup", type=int, default=0)
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--workload", default="roundtrip", choices=["roundtrip", "remesh", "adjoint"],
+                    help="roundtrip: the metric (default); remesh / adjoint: the 256^3 remesh "
+                         "and 128^3 adjoint workloads, one JSON line each")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "remesh":
+        return run_remesh(args)
+    if args.workload == "adjoint":
+        return run_adjoint(args)
 
     import torch
     import torch.distributed as dist
@@ -339,11 +481,8 @@ def main():
         assert ppmg.sync_status(1, 1) == 0, ppmg.last_error()
         ms = ev0.elapsed_time(ev1) / args.steps
         if world > 1:
-            tt = torch.tensor([ms], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ms = float(tt.item())
-            if world > 1:
-                dist.barrier()
+            ms = max_over_ranks(ms, dist, dev)
+            dist.barrier()
         p2m = float(np.median([a for a, _ in p2m_ms]))
         m2p = float(np.median([b for _, b in p2m_ms]))
         return ms, p2m, m2p, launches, kparts
@@ -398,6 +537,60 @@ def main():
                      "p2m_frac": (bp / (a / 1e3) / 1e9) / peak,
                      "m2p_frac": (bm / (b / 1e3) / 1e9) / peak}
 
+    adj = None
+    if not args.no_adjoint:
+        # the adjoint pass of P2M at the same workload: dw = M2P(r), dx from the
+        # kernel derivative, r ~ N(0, 1) on the unique nodes (device pointers)
+        ppmg.set_precision(head)
+        gr = torch.Generator(device=dev)
+        gr.manual_seed(77)
+        R = torch.randn((1, nc, nc, nc, 3), generator=gr, device=dev,
+                        dtype=torch.float64).permute(4, 3, 2, 1, 0)
+        dw = torch.empty((n, 3), device=dev, dtype=torch.float64).t()
+        dx = torch.empty((n, 3), device=dev, dtype=torch.float64).t()
+
+        # one step = the forward P2M and its adjoint (the adjoint reuses the
+        # forward pass's cell order, as a training step would)
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+
+        def adj_step(timed=False):
+            if timed:
+                evs[0].record(stream)
+            if ppmg.ppm_interp_p2m(xp, n, up, 3, 1, 1, 2, g, field):
+                raise RuntimeError(f"library error {ppmg.last_error()}")
+            if timed:
+                evs[1].record(stream)
+            if ppmg.ppm_interp_p2m_adjoint(xp, n, up, 3, 1, 1, 2, R, dw, dx, field_lb=[1, 1, 1]):
+                raise RuntimeError(f"library error {ppmg.last_error()}")
+            if timed:
+                evs[2].record(stream)
+                evs[2].synchronize()
+                return evs[0].elapsed_time(evs[1]), evs[1].elapsed_time(evs[2])
+            return None
+
+        ksteps = min(args.steps, 5)
+        for _ in range(3):
+            adj_step()
+        torch.cuda.synchronize()
+        fw, bw = [], []
+        for _ in range(ksteps):
+            a, b = adj_step(True)
+            fw.append(a)
+            bw.append(b)
+        assert ppmg.sync_status(1, 1) == 0, ppmg.last_error()
+        red = dist if world > 1 else None
+        fms = max_over_ranks(float(np.median(fw)), red, dev)
+        bms = max_over_ranks(float(np.median(bw)), red, dev)
+        ab = n * (3 * 8 + 3 * 8 + 3 * 8 + 3 * 8) + nc ** 3 * 3 * 8
+        adj = {"forward_p2m_ms": fms, "adjoint_ms": bms, "steps": ksteps,
+               "particles_per_s": total / ((fms + bms) / 1e3),
+               "adjoint_alg_bytes": ab, "adjoint_frac_of_hbm_roofline": ab / (bms / 1e3) / 1e9 / peak,
+               "form": "mixed" if head == 1 else "fp64",
+               "what": "forward ppmg_interp_p2m_dv_3d_dev, then ppmg_interp_p2m_adjoint_dv_3d_dev "
+                       "(reuses the forward cell order; dw, dx gather with recomputed weights; "
+                       "xp, up, r read, dw, dx written); medians of CUDA-event times"}
+        del R, dw, dx
+
     e2e = None
     if not args.no_e2e:
         # host API with pinned host buffers: copies are inside the timed region
@@ -424,9 +617,7 @@ def main():
         t1 = time.perf_counter()
         el = t1 - t0
         if world > 1:
-            tt = torch.tensor([el], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            el = float(tt.item())
+            el = max_over_ranks(el, dist, dev)
         t1 = t0 + el
         fbytes = nf.nbytes
         h2d = nx.nbytes * 2 + nu.nbytes + fbytes
@@ -457,7 +648,7 @@ def main():
                        "l2": "inputs larger than L2 (xp/up/field each > 126 MB)",
                        "parallelism": f"{world} independent subdomain replicas"},
             "roofline": roof, "forms": parts, "clocks": clocks, "gpu_launches": launches,
-            "e2e": e2e, "cpu_baseline": cb,
+            "e2e": e2e, "cpu_baseline": cb, "adjoint": adj,
         }
         print(json.dumps(line))
     if world > 1:

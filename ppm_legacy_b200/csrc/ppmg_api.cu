@@ -62,6 +62,7 @@ struct Handle {
   // them (same key arithmetic: M2P's FP32 spacing equals P2M's spacing).
   bool sort_cached = false;
   int cache_prec = -1;        // record precision: 0 FP64 (double4), 1 FP32 (float4)
+  bool cache_quirk = false;   // the sort's keys used M2P's FP32 mesh spacing
   int64_t cache_np = -1, cache_ldxp = -1;
   bool dxi_same_d = false, dxi_same_f = false;
   std::mutex mu;
@@ -293,6 +294,7 @@ int p2m_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, const T* up, 
   if (e) return cuda_fail(info, e, caller);
   if (!remesh) {
     h.sort_cached = true;
+    h.cache_quirk = false;
     h.cache_prec = prec == P2M_FP64 ? 0 : 1;
     h.cache_np = Np;
     h.cache_ldxp = ldxp;
@@ -300,16 +302,18 @@ int p2m_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, const T* up, 
   return 0;
 }
 
-// Whether the cell order held in h.ws can serve an M2P of these positions:
-// same count, layout, record precision and key arithmetic, no invalid
-// particle in the sort, and an equal position fingerprint.  Synchronises the
-// stream once (a 24-byte read-back).
+// Whether the cell order held in h.ws can serve an M2P (quirk: keys from
+// M2P's FP32 mesh spacing) or a P2M adjoint (P2M's spacing) of these
+// positions: same count, layout, record precision and key arithmetic, no
+// invalid particle in the sort, and an equal position fingerprint.
+// Synchronises the stream once (a 24-byte read-back).
 template <class T>
-bool can_reuse_sort(Handle& h, const T* xp, int64_t ldxp, int64_t Np, int rec_prec,
+bool can_reuse_sort(Handle& h, const T* xp, int64_t ldxp, int64_t Np, int rec_prec, bool quirk,
                     cudaStream_t st) {
   if (!h.sort_cached || h.cache_np != Np || h.cache_ldxp != ldxp || h.cache_prec != rec_prec)
     return false;
-  if (!(is_f32<T>() ? h.dxi_same_f : h.dxi_same_d)) return false;
+  // keys and offsets agree when both sorts used the same mesh spacing
+  if (h.cache_quirk != quirk && !(is_f32<T>() ? h.dxi_same_f : h.dxi_same_d)) return false;
   if (position_hash<T>(xp, ldxp, Np, h.dim, h.d_hash + 1, st)) return false;
   if (cudaMemcpyAsync(h.h_small, h.d_hash, 2 * sizeof(unsigned long long),
                       cudaMemcpyDeviceToHost, st))
@@ -337,7 +341,7 @@ int m2p_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, T* up, int64_
                                    : (g_precision.load() == PPMG_PREC_MIXED ? M2P_MIXED
                                                                             : M2P_FP64);
   const int rec_prec = prec == M2P_FP64 ? 0 : 1;
-  const bool reuse = can_reuse_sort<T>(h, xp, ldxp, Np, rec_prec, st);
+  const bool reuse = can_reuse_sort<T>(h, xp, ldxp, Np, rec_prec, true, st);
   cudaError_t e = cudaSuccess;
   KeyParams kp = make_kp(h, KEY_INTERP_WRAP, true);
   if (!reuse) {
@@ -374,6 +378,7 @@ int m2p_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, T* up, int64_
   if (!reuse && h.dim == 3) {
     // the M2P sort (with its items) is now what ws holds
     h.sort_cached = true;
+    h.cache_quirk = true;
     h.cache_prec = rec_prec;
     h.cache_np = Np;
     h.cache_ldxp = ldxp;
@@ -553,12 +558,16 @@ int adjoint_pipeline(Handle& h, const double* xp, int64_t ldxp, int64_t Np, cons
   if (!make_fd(h, ldf, f_lb, f_ub, lo, hi, fd, caller, info)) return *info;
   if (Np == 0) return 0;
   const M2PPrec prec = g_precision.load() == PPMG_PREC_MIXED ? M2P_MIXED : M2P_FP64;
-  h.sort_cached = false;
-  // the transpose of P2M: P2M's stencil (FP64 mesh spacing), periodic wrap
-  KeyParams kp = make_kp(h, KEY_INTERP_WRAP, false);
-  cudaError_t e = sort_interp<double>(h, kp, xp, ldxp, nullptr, 0, 0, Np, prec == M2P_FP64,
-                                      h.d_status + 1, dw, lddw, lda, st);
-  if (e) return cuda_fail(info, e, caller);
+  // the transpose of P2M: P2M's stencil (FP64 mesh spacing), periodic wrap;
+  // the cell order of a P2M of the same positions serves as is
+  cudaError_t e = cudaSuccess;
+  if (!can_reuse_sort<double>(h, xp, ldxp, Np, prec == M2P_FP64 ? 0 : 1, false, st)) {
+    h.sort_cached = false;  // this sort builds no work items
+    KeyParams kp = make_kp(h, KEY_INTERP_WRAP, false);
+    e = sort_interp<double>(h, kp, xp, ldxp, nullptr, 0, 0, Np, prec == M2P_FP64,
+                            h.d_status + 1, dw, lddw, lda, st);
+    if (e) return cuda_fail(info, e, caller);
+  }
   const int* dnv = d_nvalid_of(h.ws, h.g.ncell);
   M2PParams P{};
   for (int a = 0; a < 3; ++a) P.N[a] = h.g.N[a];

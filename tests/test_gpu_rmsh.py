@@ -162,3 +162,37 @@ def test_adjoint_matches_oracle_and_finite_differences(kernel):
             xb[a, p] -= e
             fd = (loss(xa) - loss(xb)) / (2 * e)
             assert abs(fd - dx[a, p]) <= 1e-4 * max(1.0, abs(fd))
+
+
+def test_adjoint_reuses_p2m_order_only_for_identical_positions():
+    """The adjoint after a P2M of the same positions reuses its cell order; the
+    result equals the adjoint on a fresh sort (and the oracle) bit for bit."""
+    rng = np.random.default_rng(85)
+    nc = 16
+    t = registered(3, nc)
+    np_ = 4000
+    xp = random_particles(rng, 3, np_)
+    up = np.asfortranarray(rng.standard_normal((3, np_)))
+    R = np.asfortranarray(rng.standard_normal((3, nc, nc, nc, 1)))
+    g = [2, 2, 2]
+    lb, ub = box_bounds(t, g)
+    f = np.zeros((3,) + tuple(ub[a] - lb[a] + 1 for a in range(3)) + (1,), order="F")
+    for mode in (0, 1):
+        ppmg.set_precision(mode)
+        res = []
+        for warm in (False, True):
+            if warm:
+                assert ppmg.ppm_interp_p2m(xp, np_, up, 3, t.topo_id, t.mesh_id, 2, g, f) == 0
+            else:  # a different position set first: no order to reuse
+                xq = random_particles(rng, 3, np_)
+                assert ppmg.ppm_interp_p2m(xq, np_, up, 3, t.topo_id, t.mesh_id, 2, g, f) == 0
+            dw = np.zeros((3, np_), order="F")
+            dx = np.zeros((3, np_), order="F")
+            assert ppmg.ppm_interp_p2m_adjoint(xp, np_, up, 3, t.topo_id, t.mesh_id, 2, R, dw,
+                                               dx, field_lb=[1, 1, 1]) == 0
+            res.append((dw, dx))
+        assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
+        if mode == 0:
+            dwo, dxo = O.p2m_adjoint(t, xp, up, R, [1, 1, 1], [nc] * 3, 2)
+            assert max_rel(res[1][0], dwo) < 1e-13 and max_rel(res[1][1], dxo) < 1e-12
+    ppmg.set_precision(0)
