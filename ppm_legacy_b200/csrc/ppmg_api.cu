@@ -561,8 +561,9 @@ int adjoint_pipeline(Handle& h, const double* xp, int64_t ldxp, int64_t Np, cons
   // the transpose of P2M: P2M's stencil (FP64 mesh spacing), periodic wrap;
   // the cell order of a P2M of the same positions serves as is
   cudaError_t e = cudaSuccess;
-  if (!can_reuse_sort<double>(h, xp, ldxp, Np, prec == M2P_FP64 ? 0 : 1, false, st)) {
-    h.sort_cached = false;  // this sort builds no work items
+  const bool reuse = can_reuse_sort<double>(h, xp, ldxp, Np, prec == M2P_FP64 ? 0 : 1, false, st);
+  if (!reuse) {
+    h.sort_cached = false;  // the work items below describe this sort only
     KeyParams kp = make_kp(h, KEY_INTERP_WRAP, false);
     e = sort_interp<double>(h, kp, xp, ldxp, nullptr, 0, 0, Np, prec == M2P_FP64,
                             h.d_status + 1, dw, lddw, lda, st);
@@ -585,6 +586,19 @@ int adjoint_pipeline(Handle& h, const double* xp, int64_t ldxp, int64_t Np, cons
   P.dx = dx;
   P.lddx = lddx;
   for (int a = 0; a < 3; ++a) P.dxi[a] = h.g.dxi_d[a];
+  if (lda <= 4) {
+    TileItems ti;
+    if ((e = h.ws.tiles.ensure(tile_items_bytes(P.N)))) return cuda_fail(info, e, caller);
+    if (reuse) {
+      ti = tile_items_view(h.ws.tiles.p, P.N);
+    } else if ((e = make_tile_items(h.ws.start.as<int>(), P.N, Np, h.ws.tiles.p, ti, st))) {
+      return cuda_fail(info, e, caller);
+    }
+    P.start = h.ws.start.as<int>();
+    P.items = ti.items;
+    P.nitems = ti.nitems;
+    P.item_cap = ti.cap;
+  }
   e = launch_adjoint(P, kernel, prec, st);
   if (e) return cuda_fail(info, e, caller);
   return 0;

@@ -29,6 +29,19 @@ __device__ __forceinline__ void m2p_weights(CT f, CT w[S]) {
   }
 }
 
+// dW/dx of the 1D weights times the inverse mesh spacing (adjoint of P2M).
+template <int S, class CT>
+__device__ __forceinline__ void adj_dweights(CT f, CT dxi, CT d[S]) {
+  if constexpr (S == 4) {
+    mp4_dweights<CT>(f, d);
+  } else {
+    d[0] = CT(-1);
+    d[1] = CT(1);
+  }
+#pragma unroll
+  for (int i = 0; i < S; ++i) d[i] *= dxi;
+}
+
 // 2D M'4 in the reference's |x| branching form (ppm_interp_m2p.f:829-845):
 // w(ii) for ii = -1..2 at x = |f - ii|.
 template <class CT, bool EXACT>
@@ -230,8 +243,12 @@ __global__ void __launch_bounds__(256) k_adjoint3d(M2PParams P) {
 // per cell layer; particles of the layer are spread over all threads.
 // EXACT (FP64 form): the terms are summed per component in the reference's
 // order (x outer, z inner) with the reference's association, no contraction.
+// ADJ (adjoint of P2M): the ring holds the adjoint field r; every particle
+// gets dw(a) = sum_n W r(a) and dx(d) = sum_a u(a) sum_n d_d W r(a), the
+// derivative weights scaled by the inverse mesh spacing (all LC = lda
+// components in one launch).
 // --------------------------------------------------------------------------
-template <int S, class CT, bool EXACT, class FT, int LC>
+template <int S, class CT, bool EXACT, class FT, int LC, bool ADJ = false>
 __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
   using V = typename Vec4<CT>::type;
   constexpr int HL = S / 2;
@@ -375,7 +392,52 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
         m2p_weights<S, CT, EXACT>(rvcur.y, wy);
         m2p_weights<S, CT, EXACT>(rvcur.z, wz);
         FT* out = up + (int64_t)idcur * P.ldup + P.c0;
-        if constexpr (EXACT) {
+        if constexpr (ADJ) {
+          // strengths of the particle (needed once its gradient sums are done)
+          CT ua[LC];
+#pragma unroll
+          for (int a = 0; a < LC; ++a) ua[a] = (CT)__ldg(P.upin + (int64_t)idcur * P.ldupin + a);
+          CT dx[S], dy[S], dz[S];
+          adj_dweights<S, CT>(rvcur.x, (CT)P.dxi[0], dx);
+          adj_dweights<S, CT>(rvcur.y, (CT)P.dxi[1], dy);
+          adj_dweights<S, CT>(rvcur.z, (CT)P.dxi[2], dz);
+          CT acc[LC], ga[LC][3];
+#pragma unroll
+          for (int a = 0; a < LC; ++a) acc[a] = ga[a][0] = ga[a][1] = ga[a][2] = CT(0);
+#pragma unroll
+          for (int ii = 0; ii < S; ++ii)
+#pragma unroll
+            for (int jj = 0; jj < S; ++jj) {
+              const CT wij = wx[ii] * wy[jj];
+              const CT dxij = dx[ii] * wy[jj];
+              const CT dyij = wx[ii] * dy[jj];
+              const CT* col = ring + (size_t)((qy0 + jj) * WX + qx0 + ii) * CS;
+#pragma unroll
+              for (int a = 0; a < LC; ++a) {
+                CT part = CT(0), dpart = CT(0);
+#pragma unroll
+                for (int k = 0; k < S; ++k) {
+                  const CT v = col[slot_k[k] * LC + a];
+                  part = fma(wz[k], v, part);
+                  dpart = fma(dz[k], v, dpart);
+                }
+                acc[a] = fma(wij, part, acc[a]);
+                ga[a][0] = fma(dxij, part, ga[a][0]);
+                ga[a][1] = fma(dyij, part, ga[a][1]);
+                ga[a][2] = fma(wij, dpart, ga[a][2]);
+              }
+            }
+          CT g[3] = {CT(0), CT(0), CT(0)};
+#pragma unroll
+          for (int a = 0; a < LC; ++a) {
+            out[a] = (FT)acc[a];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) g[d] = fma(ua[a], ga[a][d], g[d]);
+          }
+          double* gx = P.dx + (int64_t)idcur * P.lddx;
+#pragma unroll
+          for (int d = 0; d < 3; ++d) gx[d] = (double)g[d];
+        } else if constexpr (EXACT) {
 #pragma unroll
           for (int a = 0; a < LC; ++a) {
             CT acc = CT(0);
@@ -508,8 +570,36 @@ cudaError_t launch_m2p(const M2PParams& P0, int dim, int kernel, M2PPrec prec, c
   return cudaGetLastError();
 }
 
+template <int S, class CT, int LC>
+cudaError_t launch_adjoint_tile(const M2PParams& P, cudaStream_t st) {
+  auto kern = k_m2p3d_tile<S, CT, false, double, LC, true>;
+  const size_t smem = (size_t)(kTileX + S - 1) * (kTileY + S - 1) * (S + 1) * LC * sizeof(CT);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e) return e;
+  kern<<<P.item_cap, 256, smem, st>>>(P);
+  count_launch();
+  return cudaGetLastError();
+}
+
+template <int S, class CT>
+cudaError_t adjoint_tile_lc(const M2PParams& P, cudaStream_t st) {
+  switch (P.lda) {
+    case 1: return launch_adjoint_tile<S, CT, 1>(P, st);
+    case 2: return launch_adjoint_tile<S, CT, 2>(P, st);
+    case 3: return launch_adjoint_tile<S, CT, 3>(P, st);
+    default: return launch_adjoint_tile<S, CT, 4>(P, st);
+  }
+}
+
 cudaError_t launch_adjoint(const M2PParams& P, int kernel, M2PPrec prec, cudaStream_t st) {
   if (P.nvalid <= 0) return cudaSuccess;
+  if (P.items && P.lda <= 4) {
+    // tiled gather over the work items of the cell order
+    if (kernel == kKernelMp4)
+      return prec == M2P_FP64 ? adjoint_tile_lc<4, double>(P, st) : adjoint_tile_lc<4, float>(P, st);
+    return prec == M2P_FP64 ? adjoint_tile_lc<2, double>(P, st) : adjoint_tile_lc<2, float>(P, st);
+  }
   const int nb = blocks_for(P.nvalid);
   if (kernel == kKernelMp4) {
     if (prec == M2P_FP64) k_adjoint3d<4, double><<<nb, 256, 0, st>>>(P);

@@ -197,28 +197,33 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
-constexpr size_t kMoveSmem = sizeof(uint4) * 2 * (size_t)kRSub + sizeof(int) * (size_t)kRSub +
-                             sizeof(int) * (size_t)(kRWarps * kRSlots + 3 * kRSlots + 64) +
-                             2 * sizeof(uint64_t);
+// Shared memory of k_radix_move: two key+id buffers (32 KB each), two plane
+// buffers (64 KB each), the 16-bit inverse map and per-warp digit counts,
+// the per-digit offsets and the mbarriers (~224 KB: one CTA per SM).
+constexpr size_t kMoveSmem = 2 * sizeof(int2) * (size_t)kRSub + 2 * sizeof(uint4) * (size_t)kRSub +
+                             sizeof(unsigned short) * (size_t)(kRSub + kRWarps * kRSlots) +
+                             sizeof(int) * (size_t)(3 * kRSlots + 64) + 4 * sizeof(uint64_t);
 
-// One stable pass.  Every tile walks its sub-tiles in order; the inputs of a
-// sub-tile arrive as 16-byte-unit planes (keys with ids, then every record and
-// strength plane), each by one TMA bulk copy into one of two buffers, two
-// planes ahead of the one being written.  The keys are ranked by digit (warp
-// w owns items [256w, 256w+256), ranked round by round with __match_any_sync);
-// inv[] maps every sorted position of the sub-tile to its item, so each plane
-// is written in digit runs straight from its buffer.
+// One stable pass.  Every tile walks its sub-tiles in order.  The inputs of
+// a sub-tile arrive by TMA bulk copies on two independent double-buffered
+// streams: keys with ids (one 32 KB unit per sub-tile, issued two sub-tiles
+// ahead) and the 16-byte planes of records and strengths (64 KB units, issued
+// two units ahead), each completing on its own mbarrier.  The keys are ranked
+// by digit (warp w owns items [256w, 256w+256), ranked round by round with
+// __match_any_sync); inv[] maps every sorted position of the sub-tile to its
+// item, so each plane is written in digit runs straight from its buffer.
 template <bool FIRST>
 __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
   extern __shared__ __align__(128) unsigned char smem[];
-  uint4* inb = reinterpret_cast<uint4*>(smem);                 // [2][kRSub]
-  int* inv = reinterpret_cast<int*>(inb + 2 * kRSub);          // [kRSub]
-  int* whist = inv + kRSub;                                    // [kRWarps][kRSlots]
-  int* run = whist + kRWarps * kRSlots;                        // next output slot per digit
-  int* dst = run + kRSlots;                                    // digit start in the sub-tile
-  int* tot = dst + kRSlots;                                    // digit count of the sub-tile
-  int* sw = tot + kRSlots;                                     // block scan scratch [33]
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sw + 64);        // [2]
+  int2* kb = reinterpret_cast<int2*>(smem);                           // [2][kRSub] (key, id)
+  uint4* pb = reinterpret_cast<uint4*>(kb + 2 * kRSub);               // [2][kRSub] planes
+  unsigned short* inv = reinterpret_cast<unsigned short*>(pb + 2 * kRSub);  // [kRSub]
+  unsigned short* whist = inv + kRSub;                                // [kRWarps][kRSlots]
+  int* run = reinterpret_cast<int*>(whist + kRWarps * kRSlots);       // next output slot per digit
+  int* dst = run + kRSlots;                                           // digit start in the sub-tile
+  int* tot = dst + kRSlots;                                           // digit count of the sub-tile
+  int* sw = tot + kRSlots;                                            // block scan scratch [33]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sw + 64);               // [0,1] keys, [2,3] planes
 
   const int nb = 1 << A.bits;
   const int nbk = FIRST ? nb + 1 : nb;
@@ -227,7 +232,7 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
   const int lane = tid & 31;
   const int w = tid >> 5;
   const unsigned lt = (1u << lane) - 1u;
-  int* wh = whist + w * kRSlots;
+  unsigned short* wh = whist + w * kRSlots;
 
   const int64_t n = FIRST ? A.np : (int64_t)*A.d_nvalid;
   if (FIRST && blockIdx.x == 0 && tid == 0)
@@ -235,58 +240,63 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
   const int64_t t0 = (int64_t)blockIdx.x * A.subs * kRSub;
   if (t0 >= n) return;
   const int nsc = (int)min((int64_t)A.subs, (n - t0 + kRSub - 1) / kRSub);
-  const int NU = 1 + A.nplanes;
-  const int total = nsc * NU;
+  const int NP = A.nplanes;
+  const int total_p = nsc * NP;
 
   for (int d = tid; d < nbk; d += kRThreads) run[d] = A.hist[(int64_t)d * A.ntiles + blockIdx.x];
   if (tid == 0) {
-    mbar_init(&bar[0]);
-    mbar_init(&bar[1]);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) mbar_init(&bar[i]);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
 
-  // unit k of this tile: sub-tile k / NU; 0 = keys (+ ids), then the planes
-  auto issue = [&](int k) {
-    if (k >= total) return;
-    const int sub = k / NU, kind = k - sub * NU;
-    const int64_t base = t0 + (int64_t)sub * kRSub;
-    const int subn = (int)min((int64_t)kRSub, n - base);
-    uint4* b = inb + (k & 1) * kRSub;
-    uint64_t* br = &bar[k & 1];
-    if (kind == 0) {
-      const uint32_t kb = (uint32_t)((subn * 4 + 15) & ~15);
-      mbar_expect_tx(br, FIRST ? kb : 2 * kb);
-      bulk_load(b, A.key_in + base, kb, br);
-      if (!FIRST) bulk_load(reinterpret_cast<int*>(b) + kRSub, A.id_in + base, kb, br);
-    } else {
-      const int pl = kind - 1;
-      const uint4* src = pl < A.rplanes ? A.rec_in + (int64_t)pl * A.np
-                                        : A.us_in + (int64_t)(pl - A.rplanes) * A.np;
-      mbar_expect_tx(br, (uint32_t)subn * 16u);
-      bulk_load(b, src + base, (uint32_t)subn * 16u, br);
-    }
+  auto sub_n = [&](int sub) { return (int)min((int64_t)kRSub, n - (t0 + (int64_t)sub * kRSub)); };
+  // keys (+ ids) of sub-tile s into kb[s & 1]
+  auto issue_keys = [&](int s) {
+    if (s >= nsc) return;
+    const int64_t base = t0 + (int64_t)s * kRSub;
+    const uint32_t bytes = (uint32_t)((sub_n(s) * 4 + 15) & ~15);
+    int* b = reinterpret_cast<int*>(kb + (s & 1) * kRSub);
+    uint64_t* br = &bar[s & 1];
+    mbar_expect_tx(br, FIRST ? bytes : 2 * bytes);
+    bulk_load(b, A.key_in + base, bytes, br);
+    if (!FIRST) bulk_load(b + kRSub, A.id_in + base, bytes, br);
   };
-  // every thread waits; all give up together (the outstanding copy is waited
-  // for once more, with the same bound, before the tile is abandoned)
-  auto wait_unit = [&](int k) -> bool {
-    const bool ok = mbar_wait(&bar[k & 1], (uint32_t)((k >> 1) & 1));
+  // plane unit u (sub-tile u / NP, plane u % NP) into pb[u & 1]
+  auto issue_plane = [&](int u) {
+    if (u >= total_p) return;
+    const int s = u / NP, pl = u - s * NP;
+    const int64_t base = t0 + (int64_t)s * kRSub;
+    const uint4* src = pl < A.rplanes ? A.rec_in + (int64_t)pl * A.np
+                                      : A.us_in + (int64_t)(pl - A.rplanes) * A.np;
+    const uint32_t bytes = (uint32_t)sub_n(s) * 16u;
+    uint64_t* br = &bar[2 + (u & 1)];
+    mbar_expect_tx(br, bytes);
+    bulk_load(pb + (u & 1) * kRSub, src + base, bytes, br);
+  };
+  // every thread waits; all give up together (copies still outstanding on
+  // either stream are waited for once more, with the same bound)
+  auto wait_on = [&](uint64_t* br, int use) -> bool {
+    const bool ok = mbar_wait(br, (uint32_t)((use >> 1) & 1));
     if (__syncthreads_and(ok)) return true;
     if (tid == 0) atomicExch(A.wait_flag, 1);
-    if (k + 1 < total) mbar_wait(&bar[(k + 1) & 1], (uint32_t)(((k + 1) >> 1) & 1));
+    for (int i = 0; i < 4; ++i) mbar_wait(&bar[i], 0u), mbar_wait(&bar[i], 1u);
     return false;
   };
 
   if (tid == 0) {
-    issue(0);
-    issue(1);
+    issue_keys(0);
+    issue_keys(1);
+    issue_plane(0);
+    issue_plane(1);
   }
-  int k = 0;
+  int u = 0;  // next plane unit
   for (int sub = 0; sub < nsc; ++sub) {
     const int64_t base = t0 + (int64_t)sub * kRSub;
-    const int subn = (int)min((int64_t)kRSub, n - base);
-    if (!wait_unit(k)) return;
-    const int* skeys = reinterpret_cast<const int*>(inb + (k & 1) * kRSub);
+    const int subn = sub_n(sub);
+    if (!wait_on(&bar[sub & 1], sub)) return;
+    const int* skeys = reinterpret_cast<const int*>(kb + (sub & 1) * kRSub);
     const int* sids = skeys + kRSub;
     for (int d = lane; d < nbk; d += 32) wh[d] = 0;
     __syncwarp();
@@ -300,7 +310,7 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
       const unsigned peers = __match_any_sync(0xffffffffu, d);
       const int before = valid ? wh[d] : 0;
       __syncwarp();
-      if (valid && lane == __ffs(peers) - 1) wh[d] = before + __popc(peers);
+      if (valid && lane == __ffs(peers) - 1) wh[d] = (unsigned short)(before + __popc(peers));
       __syncwarp();
       lpos[r] = valid ? before + __popc(peers & lt) : -1;
     }
@@ -311,7 +321,7 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
 #pragma unroll
       for (int ww = 0; ww < kRWarps; ++ww) {
         const int c = whist[ww * kRSlots + d];
-        whist[ww * kRSlots + d] = s;
+        whist[ww * kRSlots + d] = (unsigned short)s;
         s += c;
       }
       tot[d] = s;
@@ -340,7 +350,7 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
     for (int r = 0; r < kRItems; ++r)
       if (lpos[r] >= 0) {
         const int d = digit_of<FIRST>(key[r], A.shift, mask, nb, A.ncell);
-        inv[lpos[r] + dst[d] + wh[d]] = w * kRWarpItems + r * 32 + lane;
+        inv[lpos[r] + dst[d] + wh[d]] = (unsigned short)(w * kRWarpItems + r * 32 + lane);
       }
     __syncthreads();
     // keys and ids; each thread takes the sorted positions j = tid + 512 q
@@ -359,20 +369,18 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
       }
     }
     __syncthreads();
-    if (tid == 0) issue(k + 2);
-    ++k;
+    if (tid == 0) issue_keys(sub + 2);
     // record and strength planes
-    for (int pl = 0; pl < A.nplanes; ++pl) {
-      if (!wait_unit(k)) return;
-      const uint4* sb = inb + (k & 1) * kRSub;
+    for (int pl = 0; pl < NP; ++pl, ++u) {
+      if (!wait_on(&bar[2 + (u & 1)], u)) return;
+      const uint4* sb = pb + (u & 1) * kRSub;
       uint4* out = pl < A.rplanes ? A.rec_out + (int64_t)pl * A.np
                                   : A.us_out + (int64_t)(pl - A.rplanes) * A.np;
 #pragma unroll
       for (int q = 0; q < kRItems; ++q)
         if (gdst[q] >= 0) out[gdst[q]] = sb[inv[tid + q * kRThreads]];
       __syncthreads();
-      if (tid == 0) issue(k + 2);
-      ++k;
+      if (tid == 0) issue_plane(u + 2);
     }
     for (int d = tid; d < nbk; d += kRThreads) run[d] += tot[d];
   }
