@@ -190,6 +190,11 @@ void ppmg_map_field_ghost_d_dev(double* field_up, int64_t ldf, int lda, const in
 void ppmg_rmsh_comp_weights_d(const double* xp, int64_t ldxp, int64_t Np, int topo_id,
                               int mesh_id, int kernel, double* wx1, double* wx2,
                               double* wx3, int* info);
+/* Device twin: xp and the optional wx1/wx2/wx3 are device arrays, work is
+ * enqueued on `stream`; errors latch for ppmg_sync_status. */
+void ppmg_rmsh_comp_weights_d_dev(const double* xp, int64_t ldxp, int64_t Np, int topo_id,
+                                  int mesh_id, int kernel, double* wx1, double* wx2,
+                                  double* wx3, int* info, void* stream);
 
 /* ---- ppm_rmsh_remesh (ppm/src/ppm_rmsh_remesh.f:90-124) ------------------
  * Scatter with the weights of the last comp_weights call of this handle;
@@ -202,6 +207,9 @@ void ppmg_rmsh_remesh_dv_2d(const double* xp, int64_t ldxp, int64_t Np, const do
                             int64_t ldup, int lda, int topo_id, int mesh_id, int kernel,
                             const int* ghostsize, double* field_up, int64_t ldf,
                             const int64_t* f_lb, const int64_t* f_ub, int* info);
+/* Device twins (device xp, up, field_up; enqueued on `stream`). */
+void ppmg_rmsh_remesh_dv_3d_dev(PPMG_P2M_V_ARGS(double), void* stream);
+void ppmg_rmsh_remesh_dv_2d_dev(PPMG_P2M_V_ARGS(double), void* stream);
 
 /* ---- ppm_rmsh_create_part (ppm/src/ppm_rmsh_create_part.f:90-171) --------
  * Two calls: with up == NULL it only returns the new particle count in *np;
@@ -214,6 +222,15 @@ void ppmg_rmsh_create_part_d(const double* field_up, int64_t ldf, int lda,
                              int mesh_id, const double* cutoff, const double* cutoff_weights,
                              int resetpos, const double* field_wp, int64_t ldfw, int lda2,
                              int64_t* np, double* up, double* xp, double* wp, int* info);
+/* Device twin: field_up, field_wp and the outputs up/xp/wp are device
+ * arrays (cutoff and cutoff_weights stay host arrays); both calls run on
+ * `stream`, and the counting call synchronises it to return *np. */
+void ppmg_rmsh_create_part_d_dev(const double* field_up, int64_t ldf, int lda,
+                                 const int64_t* f_lb, const int64_t* f_ub, int topo_id,
+                                 int mesh_id, const double* cutoff, const double* cutoff_weights,
+                                 int resetpos, const double* field_wp, int64_t ldfw, int lda2,
+                                 int64_t* np, double* up, double* xp, double* wp, int* info,
+                                 void* stream);
 
 /* ---- ppm_neighlist_clist / ppm_util_rank3d (ppm/src/ppm_neighlist_clist.f:
  * 371-429, ppm/src/ppm_util_rank3d.f:353-533) ------------------------------

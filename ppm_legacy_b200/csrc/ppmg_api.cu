@@ -969,69 +969,117 @@ void ppmg_map_field_ghost_d_dev(double* field_up, int64_t ldf, int lda, const in
 }
 
 // ---- comp_weights / remesh ---------------------------------------------------
+}  // extern "C"
+
+namespace ppmg {
+namespace {
+// comp_weights on device positions dxp; the optional user weight arrays wx
+// (reference layout wx(1:2ks, 1, 1-ks:Np+ks)) are device arrays when
+// `user_dev`, else host arrays (copied back, synchronising the stream).
+// Returns 0 or the failing info.
+int comp_weights_core(Handle& h, const double* dxp, int64_t ldxp, int64_t Np, int kernel,
+                      double* const wx[3], bool user_dev, cudaStream_t st, int* info,
+                      const char* caller) {
+  const int dim = h.dim;
+  KeyParams kp = make_kp(h, KEY_INTERP_CHECKED, false);
+  cudaError_t e = bin_sort<double>(kp, dxp, ldxp, Np, h.g.ncell, h.ws_rmsh, h.d_status + 0, st);
+  if (e) return cuda_fail(info, e, caller);
+  const int S = kernel == kKernelMp4 ? 4 : 2;
+  e = h.ws_rmsh.w1d.ensure(sizeof(double) * (size_t)(Np > 0 ? Np : 1) * dim * S);
+  if (e) return cuda_fail(info, e, caller);
+  CWParams P{};
+  P.dim = dim;
+  P.S = S;
+  P.nvalid = Np;
+  P.d_nvalid = d_nvalid_of(h.ws_rmsh, h.g.ncell);
+  P.idx = h.ws_rmsh.idx.as<int>();
+  P.xp = dxp;
+  P.ldxp = ldxp;
+  for (int a = 0; a < 3; ++a) {
+    P.min_phys[a] = h.g.min_phys[a];
+    P.dxiq[a] = h.g.dxiq_d[a];
+    P.istart[a] = h.istart[a];
+  }
+  P.w = h.ws_rmsh.w1d.as<double>();
+  if ((e = launch_comp_weights(P, st))) return cuda_fail(info, e, caller);
+  const int ks = S / 2;
+  const int64_t nu = (int64_t)S * (Np + 2 * ks);
+  for (int a = 0; a < dim; ++a) {
+    if (!wx[a]) continue;
+    double* dst = wx[a];
+    if (!user_dev) {
+      dst = mirror<double>(h.ws_rmsh.h_aux, (const double*)nullptr, nu, st, e);
+      if (e) return cuda_fail(info, e, caller);
+    }
+    e = cudaMemsetAsync(dst, 0, sizeof(double) * (size_t)nu, st);
+    if (!e) e = launch_weights_to_user(P.w, P.idx, Np, P.d_nvalid, dim, S, a, dst, st);
+    if (!e && !user_dev)
+      e = cudaMemcpyAsync(wx[a], dst, sizeof(double) * (size_t)nu, cudaMemcpyDeviceToHost, st);
+    if (!e && !user_dev) e = cudaStreamSynchronize(st);
+    if (e) return cuda_fail(info, e, caller);
+  }
+  h.w_valid = true;
+  h.w_kernel = kernel;
+  h.w_np = Np;
+  return 0;
+}
+
+Handle* comp_weights_checks(const double* xp, int64_t ldxp, int64_t Np, int topo_id, int mesh_id,
+                            int kernel, int* info, const char* caller) {
+  (void)xp;
+  Handle* hh = find_handle(topo_id, mesh_id);
+  if (!hh) {
+    fail(info, kErrorError, kErrArgument, std::string(caller) + ": topo_id/mesh_id is invalid");
+    return nullptr;
+  }
+  const int dim = hh->dim;
+  if (Np < 0 || (Np > 0 && ldxp < dim) || Np >= (int64_t)1 << 31) {
+    fail(info, kErrorError, kErrArgument, std::string(caller) + ": invalid sizes");
+    return nullptr;
+  }
+  if (!check_kernel(kernel, caller, info)) return nullptr;
+  return get_checked(topo_id, mesh_id, dim, caller, info);
+}
+}  // namespace
+}  // namespace ppmg
+
+extern "C" {
+
 void ppmg_rmsh_comp_weights_d(const double* xp, int64_t ldxp, int64_t Np, int topo_id,
                               int mesh_id, int kernel, double* wx1, double* wx2,
                               double* wx3, int* info) {
   const char* caller = "ppmg_rmsh_comp_weights_d";
   clear_error();
   if (info) *info = 0;
-  Handle* hh = find_handle(topo_id, mesh_id);
-  if (!hh) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": topo_id/mesh_id is invalid"); return; }
-  const int dim = hh->dim;
-  if (Np < 0 || (Np > 0 && ldxp < dim) || Np >= (int64_t)1 << 31) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": invalid sizes"); return; }
-  if (!check_kernel(kernel, caller, info)) return;
-  Handle* h = get_checked(topo_id, mesh_id, dim, caller, info);
+  Handle* h = comp_weights_checks(xp, ldxp, Np, topo_id, mesh_id, kernel, info, caller);
   if (!h) return;
   std::lock_guard<std::mutex> lk(h->mu);
   cudaStream_t st = h->stream;
   cudaError_t e;
   const double* dxp = mirror<double>(h->ws_rmsh.h_xp, xp, ldxp * Np, st, e);
   if (e) { cuda_fail(info, e, caller); return; }
-  KeyParams kp = make_kp(*h, KEY_INTERP_CHECKED, false);
-  e = bin_sort<double>(kp, dxp, ldxp, Np, h->g.ncell, h->ws_rmsh, h->d_status + 0, st);
-  if (e) { cuda_fail(info, e, caller); return; }
-  const int S = kernel == kKernelMp4 ? 4 : 2;
-  e = h->ws_rmsh.w1d.ensure(sizeof(double) * (size_t)(Np > 0 ? Np : 1) * dim * S);
-  if (e) { cuda_fail(info, e, caller); return; }
-  CWParams P{};
-  P.dim = dim;
-  P.S = S;
-  P.nvalid = Np;
-  P.d_nvalid = d_nvalid_of(h->ws_rmsh, h->g.ncell);
-  P.idx = h->ws_rmsh.idx.as<int>();
-  P.xp = dxp;
-  P.ldxp = ldxp;
-  for (int a = 0; a < 3; ++a) {
-    P.min_phys[a] = h->g.min_phys[a];
-    P.dxiq[a] = h->g.dxiq_d[a];
-    P.istart[a] = h->istart[a];
-  }
-  P.w = h->ws_rmsh.w1d.as<double>();
-  if ((e = launch_comp_weights(P, st))) { cuda_fail(info, e, caller); return; }
-  double* user[3] = {wx1, wx2, wx3};
-  const int ks = S / 2;
-  const int64_t nu = (int64_t)S * (Np + 2 * ks);
-  for (int a = 0; a < dim; ++a) {
-    if (!user[a]) continue;
-    double* dtmp = mirror<double>(h->ws_rmsh.h_aux, (const double*)nullptr, nu, st, e);
-    if (!e) e = cudaMemsetAsync(dtmp, 0, sizeof(double) * (size_t)nu, st);
-    if (!e) e = launch_weights_to_user(P.w, P.idx, Np, P.d_nvalid, dim, S, a, dtmp, st);
-    if (!e) e = cudaMemcpyAsync(user[a], dtmp, sizeof(double) * (size_t)nu,
-                                cudaMemcpyDeviceToHost, st);
-    if (!e) e = cudaStreamSynchronize(st);
-    if (e) { cuda_fail(info, e, caller); return; }
-  }
-  h->w_valid = true;
-  h->w_kernel = kernel;
-  h->w_np = Np;
+  double* const wx[3] = {wx1, wx2, wx3};
+  if (comp_weights_core(*h, dxp, ldxp, Np, kernel, wx, false, st, info, caller)) return;
   read_status(*h, st, info, caller);
 }
 
+void ppmg_rmsh_comp_weights_d_dev(const double* xp, int64_t ldxp, int64_t Np, int topo_id,
+                                  int mesh_id, int kernel, double* wx1, double* wx2,
+                                  double* wx3, int* info, void* stream) {
+  const char* caller = "ppmg_rmsh_comp_weights_d_dev";
+  clear_error();
+  if (info) *info = 0;
+  Handle* h = comp_weights_checks(xp, ldxp, Np, topo_id, mesh_id, kernel, info, caller);
+  if (!h) return;
+  std::lock_guard<std::mutex> lk(h->mu);
+  double* const wx[3] = {wx1, wx2, wx3};
+  comp_weights_core(*h, xp, ldxp, Np, kernel, wx, true, (cudaStream_t)stream, info, caller);
+}
 static void remesh_common(const double* xp, int64_t ldxp, int64_t Np, const double* up,
                           int64_t ldup, int lda, int topo_id, int mesh_id, int kernel,
                           const int* ghostsize, double* field_up, int64_t ldf,
                           const int64_t* f_lb, const int64_t* f_ub, int* info, int dim,
-                          const char* caller) {
+                          const char* caller, bool dev = false, cudaStream_t dst = nullptr) {
   clear_error();
   if (info) *info = 0;
   if (Np < 0 || (Np > 0 && ldxp < dim) || lda < 1 || ldup < lda || ldf < lda) {
@@ -1050,6 +1098,12 @@ static void remesh_common(const double* xp, int64_t ldxp, int64_t Np, const doub
   std::lock_guard<std::mutex> lk(h->mu);
   if (!h->w_valid || h->w_kernel != kernel || h->w_np != Np) {
     fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": compute weights before remeshing");
+    return;
+  }
+  if (dev) {
+    // device arrays on the caller's stream; errors latch for ppmg_sync_status
+    p2m_pipeline<double>(*h, xp, ldxp, Np, up, ldup, lda, kernel, ghostsize, field_up, ldf, f_lb,
+                         f_ub, true, dst, info, caller);
     return;
   }
   cudaStream_t st = h->stream;
@@ -1083,14 +1137,30 @@ void ppmg_rmsh_remesh_dv_2d(const double* xp, int64_t ldxp, int64_t Np, const do
   remesh_common(xp, ldxp, Np, up, ldup, lda, topo_id, mesh_id, kernel, ghostsize, field_up, ldf,
                 f_lb, f_ub, info, 2, "ppmg_rmsh_remesh_dv_2d");
 }
+void ppmg_rmsh_remesh_dv_3d_dev(const double* xp, int64_t ldxp, int64_t Np, const double* up,
+                                int64_t ldup, int lda, int topo_id, int mesh_id, int kernel,
+                                const int* ghostsize, double* field_up, int64_t ldf,
+                                const int64_t* f_lb, const int64_t* f_ub, int* info,
+                                void* stream) {
+  remesh_common(xp, ldxp, Np, up, ldup, lda, topo_id, mesh_id, kernel, ghostsize, field_up, ldf,
+                f_lb, f_ub, info, 3, "ppmg_rmsh_remesh_dv_3d_dev", true, (cudaStream_t)stream);
+}
+void ppmg_rmsh_remesh_dv_2d_dev(const double* xp, int64_t ldxp, int64_t Np, const double* up,
+                                int64_t ldup, int lda, int topo_id, int mesh_id, int kernel,
+                                const int* ghostsize, double* field_up, int64_t ldf,
+                                const int64_t* f_lb, const int64_t* f_ub, int* info,
+                                void* stream) {
+  remesh_common(xp, ldxp, Np, up, ldup, lda, topo_id, mesh_id, kernel, ghostsize, field_up, ldf,
+                f_lb, f_ub, info, 2, "ppmg_rmsh_remesh_dv_2d_dev", true, (cudaStream_t)stream);
+}
 
 // ---- create_part ---------------------------------------------------------------
-void ppmg_rmsh_create_part_d(const double* field_up, int64_t ldf, int lda,
-                             const int64_t* f_lb, const int64_t* f_ub, int topo_id,
-                             int mesh_id, const double* cutoff, const double* cutoff_weights,
-                             int resetpos, const double* field_wp, int64_t ldfw, int lda2,
-                             int64_t* np, double* up, double* xp, double* wp, int* info) {
-  const char* caller = "ppmg_rmsh_create_part_d";
+static void create_part_common(const double* field_up, int64_t ldf, int lda,
+                               const int64_t* f_lb, const int64_t* f_ub, int topo_id,
+                               int mesh_id, const double* cutoff, const double* cutoff_weights,
+                               int resetpos, const double* field_wp, int64_t ldfw, int lda2,
+                               int64_t* np, double* up, double* xp, double* wp, int* info,
+                               bool dev, cudaStream_t dstream, const char* caller) {
   clear_error();
   if (info) *info = 0;
   Handle* hh = find_handle(topo_id, mesh_id);
@@ -1108,13 +1178,16 @@ void ppmg_rmsh_create_part_d(const double* field_up, int64_t ldf, int lda,
   FieldDesc fd, fdw;
   if (!make_fd(*h, ldf, f_lb, f_ub, lo, hi, fd, caller, info)) return;
   if (field_wp && !make_fd(*h, ldfw, f_lb, f_ub, lo, hi, fdw, caller, info)) return;
-  cudaStream_t st = h->stream;
-  cudaError_t e;
+  cudaStream_t st = dev ? dstream : h->stream;
+  cudaError_t e = cudaSuccess;
   const int64_t nf = field_elems(*h, ldf, f_lb, f_ub);
-  const double* dfield = mirror<double>(h->ws.h_field, field_up, nf, st, e);
-  if (e) { cuda_fail(info, e, caller); return; }
-  const double* dfw = nullptr;
-  if (field_wp) {
+  const double* dfield = field_up;
+  if (!dev) {
+    dfield = mirror<double>(h->ws.h_field, field_up, nf, st, e);
+    if (e) { cuda_fail(info, e, caller); return; }
+  }
+  const double* dfw = field_wp;
+  if (field_wp && !dev) {
     dfw = mirror<double>(h->ws.h_xp, field_wp, field_elems(*h, ldfw, f_lb, f_ub), st, e);
     if (e) { cuda_fail(info, e, caller); return; }
   }
@@ -1155,6 +1228,14 @@ void ppmg_rmsh_create_part_d(const double* field_up, int64_t ldf, int lda,
   if (e) { cuda_fail(info, e, caller); return; }
   if (np) *np = total;
   if (!up) return;  // counting call
+  if (dev) {
+    // device outputs up(lda, np) [, xp(dim, np), wp(lda2, np)]
+    P.up = up;
+    P.xp = resetpos ? xp : nullptr;
+    P.wp = field_wp ? wp : nullptr;
+    if ((e = launch_cp_fill(P, flag, pos, st))) cuda_fail(info, e, caller);
+    return;
+  }
   double* dout = mirror<double>(h->ws.h_aux, (const double*)nullptr,
                                 (int64_t)total * (lda + dim + (field_wp ? lda2 : 0)), st, e);
   if (e) { cuda_fail(info, e, caller); return; }
@@ -1171,6 +1252,26 @@ void ppmg_rmsh_create_part_d(const double* field_up, int64_t ldf, int lda,
   }
   if (!e) e = cudaStreamSynchronize(st);
   if (e) cuda_fail(info, e, caller);
+}
+
+void ppmg_rmsh_create_part_d(const double* field_up, int64_t ldf, int lda,
+                             const int64_t* f_lb, const int64_t* f_ub, int topo_id,
+                             int mesh_id, const double* cutoff, const double* cutoff_weights,
+                             int resetpos, const double* field_wp, int64_t ldfw, int lda2,
+                             int64_t* np, double* up, double* xp, double* wp, int* info) {
+  create_part_common(field_up, ldf, lda, f_lb, f_ub, topo_id, mesh_id, cutoff, cutoff_weights,
+                     resetpos, field_wp, ldfw, lda2, np, up, xp, wp, info, false, nullptr,
+                     "ppmg_rmsh_create_part_d");
+}
+void ppmg_rmsh_create_part_d_dev(const double* field_up, int64_t ldf, int lda,
+                                 const int64_t* f_lb, const int64_t* f_ub, int topo_id,
+                                 int mesh_id, const double* cutoff, const double* cutoff_weights,
+                                 int resetpos, const double* field_wp, int64_t ldfw, int lda2,
+                                 int64_t* np, double* up, double* xp, double* wp, int* info,
+                                 void* stream) {
+  create_part_common(field_up, ldf, lda, f_lb, f_ub, topo_id, mesh_id, cutoff, cutoff_weights,
+                     resetpos, field_wp, ldfw, lda2, np, up, xp, wp, info, true,
+                     (cudaStream_t)stream, "ppmg_rmsh_create_part_d_dev");
 }
 
 // ---- cell lists -------------------------------------------------------------------

@@ -203,8 +203,12 @@ def ppm_rmsh_comp_weights(xp, Np, topo_id, mesh_id, kernel, wx1_user=None, wx2_u
     _check(xp)
     info = C.c_int(0)
     w = [None if u is None else _addr(u) for u in (wx1_user, wx2_user, wx3_user)]
-    lib().ppmg_rmsh_comp_weights_d(_addr(xp), xp.shape[0], int(Np), topo_id, mesh_id, kernel,
-                                   w[0], w[1], w[2], C.byref(info))
+    a = (_addr(xp), xp.shape[0], int(Np), topo_id, mesh_id, kernel, w[0], w[1], w[2],
+         C.byref(info))
+    if _is_dev(xp):
+        lib().ppmg_rmsh_comp_weights_d_dev(*a, _stream())
+    else:
+        lib().ppmg_rmsh_comp_weights_d(*a)
     return info.value
 
 
@@ -222,9 +226,12 @@ def ppm_rmsh_remesh(xp, Np, up, *args, field_lb=None):
     info = C.c_int(0)
     ldup = up.shape[0] if vector else 1
     ldf = field_up.shape[0] if vector else 1
-    getattr(lib(), f"ppmg_rmsh_remesh_dv_{dim}d")(
-        _addr(xp), xp.shape[0], int(Np), _addr(up), ldup, lda, topo_id, mesh_id, kernel,
-        int_array(ghostsize), _addr(field_up), ldf, lb, ub, C.byref(info))
+    a = (_addr(xp), xp.shape[0], int(Np), _addr(up), ldup, lda, topo_id, mesh_id, kernel,
+         int_array(ghostsize), _addr(field_up), ldf, lb, ub, C.byref(info))
+    if _is_dev(xp):
+        getattr(lib(), f"ppmg_rmsh_remesh_dv_{dim}d_dev")(*a, _stream())
+    else:
+        getattr(lib(), f"ppmg_rmsh_remesh_dv_{dim}d")(*a)
     return info.value
 
 
@@ -253,7 +260,11 @@ def ppm_rmsh_create_part(field_up, topo_id, mesh_id, cutoff, lda=None, resetpos=
         ldfw = lda2
     n = C.c_int64(0)
     info = C.c_int(0)
-    fn = lib().ppmg_rmsh_create_part_d
+    dev = _is_dev(field_up)
+    if dev:
+        fn = lambda *a: lib().ppmg_rmsh_create_part_d_dev(*a, _stream())  # noqa: E731
+    else:
+        fn = lib().ppmg_rmsh_create_part_d
     common = (_addr(field_up), ldf, lda, lb, ub, topo_id, mesh_id, cut.ctypes.data,
               None if cw is None else cw.ctypes.data, int(bool(resetpos)),
               None if field_wp is None else _addr(field_wp), ldfw, lda2)
@@ -261,6 +272,20 @@ def ppm_rmsh_create_part(field_up, topo_id, mesh_id, cutoff, lda=None, resetpos=
     if info.value != 0:
         return info.value, 0, None, None, None
     npn = n.value
+    if dev:
+        # device outputs, column-major like the host arrays
+        def cm(rows):
+            return torch.empty((max(npn, 1), rows), dtype=torch.float64,
+                               device=field_up.device).t()[:, :npn]
+        up = cm(lda)
+        xp = cm(dim) if resetpos else None
+        wp = cm(max(lda2, 1)) if field_wp is not None else None
+        fn(*common, C.byref(n), _addr(up) if npn else None,
+           None if xp is None or not npn else _addr(xp),
+           None if wp is None or not npn else _addr(wp), C.byref(info))
+        if not vector:
+            up = up.reshape(-1)
+        return info.value, npn, up, xp, wp
     up = np.zeros((lda, npn), order="F")
     xp = np.zeros((dim, npn), order="F") if resetpos else None
     wp = np.zeros((max(lda2, 1), npn), order="F") if field_wp is not None else None

@@ -196,3 +196,50 @@ def test_adjoint_reuses_p2m_order_only_for_identical_positions():
             dwo, dxo = O.p2m_adjoint(t, xp, up, R, [1, 1, 1], [nc] * 3, 2)
             assert max_rel(res[1][0], dwo) < 1e-13 and max_rel(res[1][1], dxo) < 1e-12
     ppmg.set_precision(0)
+
+
+@pytest.mark.parametrize("dim,kernel", [(3, 2), (3, 1), (2, 2)])
+def test_remeshing_device_twins_match_host_entry_points(dim, kernel):
+    """comp_weights, remesh and create_part on device arrays (the `_dev`
+    twins, on the torch stream) equal the host-pointer entry points bit for bit."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(90 + dim + kernel)
+    nc = 12
+    t = registered(dim, nc)
+    g = [2] * dim
+    np_ = 3 * nc ** dim
+    xp = random_particles(rng, dim, np_)
+    up = np.asfortranarray(rng.standard_normal((3, np_)))
+    ks = 2 if kernel == 2 else 1
+    lb, ub = box_bounds(t, g)
+    shape = (3,) + tuple(ub[a] - lb[a] + 1 for a in range(dim)) + (1,)
+
+    def cm(a):
+        d = torch.from_numpy(np.ascontiguousarray(np.asarray(a).T)).cuda()
+        return d.permute(*reversed(range(d.dim())))
+
+    def host(a):
+        return a.permute(*reversed(range(a.dim()))).contiguous().cpu().numpy().T
+
+    wh = [np.zeros((2 * ks, 1, np_ + 2 * ks), order="F") for _ in range(dim)]
+    assert ppmg.ppm_rmsh_comp_weights(xp, np_, t.topo_id, t.mesh_id, kernel, *wh) == 0
+    fh = np.zeros(shape, order="F")
+    assert ppmg.ppm_rmsh_remesh(xp, np_, up, 3, t.topo_id, t.mesh_id, kernel, g, fh) == 0
+    cut = [0.05, 1e300]
+    ih, nh, uh, xh, _ = ppmg.ppm_rmsh_create_part(fh, t.topo_id, t.mesh_id, cut, lda=3,
+                                                  resetpos=True, ghostsize=g)
+    assert ih == 0 and nh > 0
+    dxp, dup = cm(xp), cm(up)
+    wd = [cm(np.zeros((2 * ks, 1, np_ + 2 * ks))) for _ in range(dim)]
+    assert ppmg.ppm_rmsh_comp_weights(dxp, np_, t.topo_id, t.mesh_id, kernel, *wd) == 0
+    fd = cm(np.full(shape, 3.0))
+    assert ppmg.ppm_rmsh_remesh(dxp, np_, dup, 3, t.topo_id, t.mesh_id, kernel, g, fd) == 0
+    assert ppmg.sync_status(t.topo_id, t.mesh_id) == 0
+    for a in range(dim):
+        assert np.array_equal(host(wd[a]), wh[a])
+    assert np.array_equal(host(fd), fh)
+    idv, nd, ud, xd, _ = ppmg.ppm_rmsh_create_part(fd, t.topo_id, t.mesh_id, cut, lda=3,
+                                                   resetpos=True, ghostsize=g)
+    assert idv == 0 and nd == nh
+    torch.cuda.synchronize()
+    assert np.array_equal(host(ud), uh) and np.array_equal(host(xd), xh)
