@@ -195,6 +195,14 @@ void ppmg_rmsh_comp_weights_d(const double* xp, int64_t ldxp, int64_t Np, int to
 void ppmg_rmsh_comp_weights_d_dev(const double* xp, int64_t ldxp, int64_t Np, int topo_id,
                                   int mesh_id, int kernel, double* wx1, double* wx2,
                                   double* wx3, int* info, void* stream);
+/* Single precision (ppm_rmsh_comp_weights_s): weights in FP32; a following
+ * remesh must be single precision too. */
+void ppmg_rmsh_comp_weights_s(const float* xp, int64_t ldxp, int64_t Np, int topo_id,
+                              int mesh_id, int kernel, float* wx1, float* wx2, float* wx3,
+                              int* info);
+void ppmg_rmsh_comp_weights_s_dev(const float* xp, int64_t ldxp, int64_t Np, int topo_id,
+                                  int mesh_id, int kernel, float* wx1, float* wx2, float* wx3,
+                                  int* info, void* stream);
 
 /* ---- ppm_rmsh_remesh (ppm/src/ppm_rmsh_remesh.f:90-124) ------------------
  * Scatter with the weights of the last comp_weights call of this handle;
@@ -210,6 +218,11 @@ void ppmg_rmsh_remesh_dv_2d(const double* xp, int64_t ldxp, int64_t Np, const do
 /* Device twins (device xp, up, field_up; enqueued on `stream`). */
 void ppmg_rmsh_remesh_dv_3d_dev(PPMG_P2M_V_ARGS(double), void* stream);
 void ppmg_rmsh_remesh_dv_2d_dev(PPMG_P2M_V_ARGS(double), void* stream);
+/* Single precision (ppm_rmsh_remesh.f:94-110 _sv/_ss: lda = 1 for scalars). */
+void ppmg_rmsh_remesh_sv_3d(PPMG_P2M_V_ARGS(float));
+void ppmg_rmsh_remesh_sv_2d(PPMG_P2M_V_ARGS(float));
+void ppmg_rmsh_remesh_sv_3d_dev(PPMG_P2M_V_ARGS(float), void* stream);
+void ppmg_rmsh_remesh_sv_2d_dev(PPMG_P2M_V_ARGS(float), void* stream);
 
 /* ---- ppm_rmsh_create_part (ppm/src/ppm_rmsh_create_part.f:90-171) --------
  * Two calls: with up == NULL it only returns the new particle count in *np;
@@ -230,6 +243,18 @@ void ppmg_rmsh_create_part_d_dev(const double* field_up, int64_t ldf, int lda,
                                  int mesh_id, const double* cutoff, const double* cutoff_weights,
                                  int resetpos, const double* field_wp, int64_t ldfw, int lda2,
                                  int64_t* np, double* up, double* xp, double* wp, int* info,
+                                 void* stream);
+/* Single precision (ppm_rmsh_create_part_s*): field, cutoffs and outputs FP32. */
+void ppmg_rmsh_create_part_s(const float* field_up, int64_t ldf, int lda,
+                             const int64_t* f_lb, const int64_t* f_ub, int topo_id,
+                             int mesh_id, const float* cutoff, const float* cutoff_weights,
+                             int resetpos, const float* field_wp, int64_t ldfw, int lda2,
+                             int64_t* np, float* up, float* xp, float* wp, int* info);
+void ppmg_rmsh_create_part_s_dev(const float* field_up, int64_t ldf, int lda,
+                                 const int64_t* f_lb, const int64_t* f_ub, int topo_id,
+                                 int mesh_id, const float* cutoff, const float* cutoff_weights,
+                                 int resetpos, const float* field_wp, int64_t ldfw, int lda2,
+                                 int64_t* np, float* up, float* xp, float* wp, int* info,
                                  void* stream);
 
 /* ---- ppm_neighlist_clist / ppm_util_rank3d (ppm/src/ppm_neighlist_clist.f:

@@ -205,32 +205,50 @@ def ghost_put(topo, field, lb, ub, ghost):
 
 
 def assign(topo, xp):
+    """Particle -> sub lists; float32 positions use the single-precision tests."""
     G = Geom(topo)
-    xp = _f64(xp)
+    k = "s" if np.asarray(xp).dtype == np.float32 else "d"
+    xp = np.asfortranarray(xp, dtype=np.float32 if k == "s" else np.float64)
     np_ = xp.shape[1]
     lst = np.zeros(max(np_, 1), dtype=np.int32)
     si = np.zeros(topo.nsubs, dtype=np.int32)
     err = C.c_int(0)
-    info = lib().orc_assign_d(G.ref(), _ptr(xp, C.c_double), xp.shape[0], np_,
-                              _ptr(lst, C.c_int), _ptr(si, C.c_int), C.byref(err))
+    info = getattr(lib(), f"orc_assign_{k}")(G.ref(), _ptr(xp, _ctk(k)), xp.shape[0], np_,
+                                             _ptr(lst, C.c_int), _ptr(si, C.c_int),
+                                             C.byref(err))
     if info != 0:
         raise OracleError(info, err.value)
     return lst[:np_], si
 
 
+def _kind(*arrays):
+    """'s' when the arrays are float32 (the reference's single variants), else 'd'."""
+    return "s" if any(a is not None and np.asarray(a).dtype == np.float32 for a in arrays) else "d"
+
+
+def _fk(a, k):
+    return np.asfortranarray(a, dtype=np.float32 if k == "s" else np.float64)
+
+
+def _ctk(k):
+    return C.c_float if k == "s" else C.c_double
+
+
 def comp_weights(topo, xp, kernel):
-    """Returns (wx list per axis shaped (2ks, nsubs, maxp+2ks) F-order, list, store_info)."""
+    """Returns (wx list per axis shaped (2ks, nsubs, maxp+2ks) F-order, list, store_info).
+    float32 positions run the single-precision routine (ppm_rmsh_comp_weights_s)."""
     G = Geom(topo)
-    xp = _f64(xp)
+    k = _kind(xp)
+    xp = _fk(xp, k)
     lst, si = assign(topo, xp)
     maxp = int(si.max()) if si.size else 0
     ks = 2 if kernel == 2 else 1
     shape = (2 * ks, topo.nsubs, maxp + 2 * ks)
-    wx = [np.zeros(shape, order="F") for _ in range(3)]
-    info = lib().orc_comp_weights_d(G.ref(), _ptr(xp, C.c_double), xp.shape[0], xp.shape[1],
-                                    kernel, _ptr(lst, C.c_int), _ptr(si, C.c_int), maxp,
-                                    _ptr(wx[0], C.c_double), _ptr(wx[1], C.c_double),
-                                    _ptr(wx[2], C.c_double))
+    ct = _ctk(k)
+    wx = [np.zeros(shape, order="F", dtype=xp.dtype) for _ in range(3)]
+    info = getattr(lib(), f"orc_comp_weights_{k}")(
+        G.ref(), _ptr(xp, ct), xp.shape[0], xp.shape[1], kernel, _ptr(lst, C.c_int),
+        _ptr(si, C.c_int), maxp, _ptr(wx[0], ct), _ptr(wx[1], ct), _ptr(wx[2], ct))
     if info != 0:
         raise OracleError(info, 0)
     return wx, lst, si
@@ -238,20 +256,22 @@ def comp_weights(topo, xp, kernel):
 
 def remesh(topo, xp, up, kernel, ghost, wx, lst, si):
     G = Geom(topo)
-    xp = _f64(xp)
-    up = _f64(up if up.ndim == 2 else up.reshape(1, -1))
+    k = _kind(xp)
+    xp = _fk(xp, k)
+    up = _fk(up if up.ndim == 2 else up.reshape(1, -1), k)
     lda = up.shape[0]
     field, lb, ub = new_field(topo, lda, ghost)
+    field = _fk(field, k)
     fd = field_desc(lda, lb, ub)
     gh = _ghost(ghost)
     err = C.c_int(0)
     maxp = int(si.max()) if si.size else 0
-    info = lib().orc_remesh_d(G.ref(), _ptr(xp, C.c_double), xp.shape[0], xp.shape[1],
-                              _ptr(up, C.c_double), lda, kernel, _ptr(gh, C.c_int),
-                              _ptr(lst, C.c_int), _ptr(si, C.c_int), maxp,
-                              _ptr(wx[0], C.c_double), _ptr(wx[1], C.c_double),
-                              _ptr(wx[2], C.c_double), _ptr(field, C.c_double),
-                              C.byref(fd), C.byref(err))
+    ct = _ctk(k)
+    wx = [_fk(w, k) for w in wx]
+    info = getattr(lib(), f"orc_remesh_{k}")(
+        G.ref(), _ptr(xp, ct), xp.shape[0], xp.shape[1], _ptr(up, ct), lda, kernel,
+        _ptr(gh, C.c_int), _ptr(lst, C.c_int), _ptr(si, C.c_int), maxp, _ptr(wx[0], ct),
+        _ptr(wx[1], ct), _ptr(wx[2], ct), _ptr(field, ct), C.byref(fd), C.byref(err))
     if info != 0:
         raise OracleError(info, err.value)
     return field, lb, ub
@@ -260,25 +280,28 @@ def remesh(topo, xp, up, kernel, ghost, wx, lst, si):
 def create_part(topo, field, lb, ub, cutoff, cutoff_weights=None, resetpos=True,
                 field_wp=None):
     G = Geom(topo)
-    field = _f64(field)
+    k = _kind(field)
+    ct = _ctk(k)
+    dt = np.float32 if k == "s" else np.float64
+    field = _fk(field, k)
     lda = field.shape[0]
     fd = field_desc(lda, lb, ub)
-    cut = np.asarray(cutoff, dtype=np.float64)
-    cw = None if cutoff_weights is None else np.ascontiguousarray(cutoff_weights, dtype=np.float64)
-    fw = None if field_wp is None else _f64(field_wp)
+    cut = np.asarray(cutoff, dtype=dt)
+    cw = None if cutoff_weights is None else np.ascontiguousarray(cutoff_weights, dtype=dt)
+    fw = None if field_wp is None else _fk(field_wp, k)
     lda2 = 0 if fw is None else fw.shape[0]
     npo = C.c_int(0)
-    cwp = _ptr(cw, C.c_double) if cw is not None else None
-    fwp = _ptr(fw, C.c_double) if fw is not None else None
-    lib().orc_create_part_d(G.ref(), _ptr(field, C.c_double), C.byref(fd), _ptr(cut, C.c_double),
-                            cwp, int(resetpos), fwp, lda2, C.byref(npo), None, None, None)
+    cwp = _ptr(cw, ct) if cw is not None else None
+    fwp = _ptr(fw, ct) if fw is not None else None
+    fn = getattr(lib(), f"orc_create_part_{k}")
+    fn(G.ref(), _ptr(field, ct), C.byref(fd), _ptr(cut, ct), cwp, int(resetpos), fwp, lda2,
+       C.byref(npo), None, None, None)
     n = npo.value
-    up = np.zeros((lda, n), order="F")
-    xp = np.zeros((topo.dim, n), order="F")
-    wp = np.zeros((max(lda2, 1), n), order="F") if fw is not None else None
-    lib().orc_create_part_d(G.ref(), _ptr(field, C.c_double), C.byref(fd), _ptr(cut, C.c_double),
-                            cwp, int(resetpos), fwp, lda2, C.byref(npo), _ptr(up, C.c_double),
-                            _ptr(xp, C.c_double), _ptr(wp, C.c_double) if wp is not None else None)
+    up = np.zeros((lda, n), order="F", dtype=dt)
+    xp = np.zeros((topo.dim, n), order="F", dtype=dt)
+    wp = np.zeros((max(lda2, 1), n), order="F", dtype=dt) if fw is not None else None
+    fn(G.ref(), _ptr(field, ct), C.byref(fd), _ptr(cut, ct), cwp, int(resetpos), fwp, lda2,
+       C.byref(npo), _ptr(up, ct), _ptr(xp, ct), _ptr(wp, ct) if wp is not None else None)
     return n, up, (xp if resetpos else None), wp
 
 

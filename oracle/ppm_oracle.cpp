@@ -653,39 +653,43 @@ int orc_ghost_put_s(const orc_geom* g, float* field, const orc_field* fl, const 
   return 0;
 }
 
+}  // extern "C"
+
 // ppm_rmsh_comp_weights.f:851-996.  wx(iidec, isub, ip) with bounds
 // (1:2ks, 1:nsubs, 1-ks:maxp+ks); ip is the position in the sub's list.
-int orc_comp_weights_d(const orc_geom* g, const double* xp, int ldxp, int np, int kernel,
-                       const int* list, const int* store_info, int maxp, double* wx1,
-                       double* wx2, double* wx3) {
+template <class T>
+static int comp_weights_impl(const orc_geom* g, const T* xp, int ldxp, int np, int kernel,
+                             const int* list, const int* store_info, int maxp, T* wx1, T* wx2,
+                             T* wx3) {
   (void)np;
   const int d = g->dim;
   int ks = kernel == ORC_KERNEL_MP4 ? 2 : (kernel == ORC_KERNEL_BSP2 ? 1 : 0);
   if (ks == 0) return ORC_ERROR_ERROR;
   const int nw = 2 * ks;
   const int64_t n3 = (int64_t)maxp + 2 * ks;
-  double* wx[3] = {wx1, wx2, wx3};
+  T* wx[3] = {wx1, wx2, wx3};
   for (int a = 0; a < d; ++a)
-    std::fill(wx[a], wx[a] + (int64_t)nw * g->nsubs * n3, 0.0);
-  double dxi[3];
-  for (int a = 0; a < d; ++a) dxi[a] = dxi_real<double>(g, a);
+    std::fill(wx[a], wx[a] + (int64_t)nw * g->nsubs * n3, T(0));
+  T dxi[3];
+  for (int a = 0; a < d; ++a) dxi[a] = dxi_real<T>(g, a);
   int q = 0;
   for (int s = 0; s < g->nsubs; ++s) {
     const int* is = g->istart + s * 3;
     for (int ip = 1; ip <= store_info[s]; ++ip) {
-      const double* x = xp + (int64_t)list[q + ip - 1] * ldxp;
+      const T* x = xp + (int64_t)list[q + ip - 1] * ldxp;
       for (int a = 0; a < d; ++a) {
-        double xi = (x[a] - g->min_phys[a]) * dxi[a];
+        const T mn = (T)g->min_phys[a];
+        T xi = (x[a] - mn) * dxi[a];
         int ipa = fint(xi) + 2 - is[a];
         int lo = kernel == ORC_KERNEL_MP4 ? ipa - 1 : ipa;
         for (int t = 0; t < nw; ++t) {
           int ii = lo + t;
-          double xd = std::fabs((double)(ii - 2 + is[a]) - (x[a] - g->min_phys[a]) * dxi[a]);
-          double w = 0.0;
+          T xd = std::fabs((T)(ii - 2 + is[a]) - (x[a] - mn) * dxi[a]);
+          T w = T(0);
           if (kernel == ORC_KERNEL_MP4) {
-            w = mp4_abs_le<double>(xd);
-          } else if (xd <= 1.0) {
-            w = 1.0 - xd;
+            w = mp4_abs_le<T>(xd);
+          } else if (xd <= T(1)) {
+            w = T(1) - xd;
           }
           int64_t idx = (int64_t)t + nw * ((int64_t)s + (int64_t)g->nsubs * ((int64_t)ip - (1 - ks)));
           wx[a][idx] = w;
@@ -699,10 +703,11 @@ int orc_comp_weights_d(const orc_geom* g, const double* xp, int ldxp, int np, in
 
 // ppm_rmsh_remesh.f:508-924: zero the whole field, scatter with the stored
 // weights over nodes ip-1..ip+2 (M'4) or ip..ip+1 (bsp2), then ghost put.
-int orc_remesh_d(const orc_geom* g, const double* xp, int ldxp, int np, const double* up,
-                 int lda, int kernel, const int* ghost, const int* list,
-                 const int* store_info, int maxp, const double* wx1, const double* wx2,
-                 const double* wx3, double* field, const orc_field* fl, int* err) {
+template <class T>
+static int remesh_impl(const orc_geom* g, const T* xp, int ldxp, int np, const T* up, int lda,
+                       int kernel, const int* ghost, const int* list, const int* store_info,
+                       int maxp, const T* wx1, const T* wx2, const T* wx3, T* field,
+                       const orc_field* fl, int* err) {
   (void)np;
   (void)maxp;
   if (err) *err = 0;
@@ -712,22 +717,22 @@ int orc_remesh_d(const orc_geom* g, const double* xp, int ldxp, int np, const do
   for (int a = 0; a < d; ++a)
     if (ghost[a] < ks - 1) { if (err) *err = ORC_ERR_ARGUMENT; return ORC_ERROR_ERROR; }
   const int nw = 2 * ks;
-  FieldView<double> F(field, fl, d);
+  FieldView<T> F(field, fl, d);
   int64_t total = (int64_t)F.lda * F.ext[0] * F.ext[1] * F.ext[2] * g->nsubs;
-  std::fill(field, field + total, 0.0);
-  double dxi[3];
-  for (int a = 0; a < d; ++a) dxi[a] = dxi_mk<double>(g, a);
-  const double* wx[3] = {wx1, wx2, wx3};
+  std::fill(field, field + total, T(0));
+  T dxi[3];
+  for (int a = 0; a < d; ++a) dxi[a] = dxi_mk<T>(g, a);
+  const T* wx[3] = {wx1, wx2, wx3};
   bool ok = true;
   int q = 0;
   for (int s = 0; s < g->nsubs; ++s) {
     const int* is = g->istart + s * 3;
     for (int ip = 1; ip <= store_info[s]; ++ip) {
       int iq = list[q + ip - 1];
-      const double* x = xp + (int64_t)iq * ldxp;
-      const double* u = up + (int64_t)iq * lda;
+      const T* x = xp + (int64_t)iq * ldxp;
+      const T* u = up + (int64_t)iq * lda;
       int ipa[3] = {0, 0, 0};
-      for (int a = 0; a < d; ++a) ipa[a] = fint((x[a] - g->min_phys[a]) * dxi[a]) + 2 - is[a];
+      for (int a = 0; a < d; ++a) ipa[a] = fint((x[a] - (T)g->min_phys[a]) * dxi[a]) + 2 - is[a];
       int lo[3];
       for (int a = 0; a < 3; ++a) lo[a] = kernel == ORC_KERNEL_MP4 ? ipa[a] - 1 : ipa[a];
       auto W = [&](int a, int t) {
@@ -740,9 +745,9 @@ int orc_remesh_d(const orc_geom* g, const double* xp, int ldxp, int np, const do
           for (int id = 0; id < nw; ++id) {
             int i = lo[0] + id, j = lo[1] + jd, k = d == 3 ? lo[2] + kd : 0;
             if (!F.inside(i, j, k)) { ok = false; continue; }
-            double w = d == 3 ? W(0, id) * W(1, jd) * W(2, kd) : W(0, id) * W(1, jd);
+            T w = d == 3 ? W(0, id) * W(1, jd) * W(2, kd) : W(0, id) * W(1, jd);
             for (int c = 0; c < lda; ++c) {
-              double& f = F.at(c, i, j, k, s);
+              T& f = F.at(c, i, j, k, s);
               f = f + w * u[c];
             }
           }
@@ -750,24 +755,26 @@ int orc_remesh_d(const orc_geom* g, const double* xp, int ldxp, int np, const do
     q += store_info[s];
   }
   if (!ok) { if (err) *err = ORC_ERR_OUT_OF_FIELD; return ORC_ERROR_ERROR; }
-  ghost_put<double>(g, F, ghost);
+  ghost_put<T>(g, F, ghost);
   return 0;
 }
 
 // ppm_rmsh_create_part.f:427-681: nodes i=1..nnx (nnx = nnodes-1 on periodic
 // or interior upper faces), visited k,j,i with i fastest; a node becomes a
 // particle when cutoff(1) < strength < cutoff(2).
-int orc_create_part_d(const orc_geom* g, const double* field, const orc_field* fl,
-                      const double* cutoff, const double* cutoff_weights, int resetpos,
-                      const double* field_wp, int lda2, int* np_out, double* up_out,
-                      double* xp_out, double* wp_out) {
+template <class T>
+static int create_part_impl(const orc_geom* g, const T* field, const orc_field* fl,
+                            const T* cutoff, const T* cutoff_weights, int resetpos,
+                            const T* field_wp, int lda2, int* np_out, T* up_out, T* xp_out,
+                            T* wp_out) {
   const int d = g->dim;
-  FieldView<double> F(const_cast<double*>(field), fl, d);
+  FieldView<T> F(const_cast<T*>(field), fl, d);
   orc_field fl2 = *fl;
   fl2.lda = lda2 > 0 ? lda2 : 1;
-  FieldView<double> FW(const_cast<double*>(field_wp), &fl2, d);
-  double h[3];
-  for (int a = 0; a < d; ++a) h[a] = (g->max_phys[a] - g->min_phys[a]) / (double)(g->Nm[a] - 1);
+  FieldView<T> FW(const_cast<T*>(field_wp), &fl2, d);
+  T h[3];
+  for (int a = 0; a < d; ++a)
+    h[a] = ((T)g->max_phys[a] - (T)g->min_phys[a]) / (T)(g->Nm[a] - 1);
   int inp = 0;
   for (int s = 0; s < g->nsubs; ++s) {
     int nnl[3] = {1, 1, 1};
@@ -779,13 +786,13 @@ int orc_create_part_d(const orc_geom* g, const double* field, const orc_field* f
       for (int j = 1; j <= nnl[1]; ++j)
         for (int i = 1; i <= nnl[0]; ++i) {
           int kk = d == 3 ? k : 0;
-          double str;
+          T str;
           if (F.lda == 1 && cutoff_weights == nullptr) {
             str = std::fabs(F.at(0, i, j, kk, s));
           } else {
-            double sum = 0.0;
+            T sum = T(0);
             for (int c = 0; c < F.lda; ++c) {
-              double v = F.at(c, i, j, kk, s);
+              T v = F.at(c, i, j, kk, s);
               if (cutoff_weights) v = v * cutoff_weights[c];
               sum = sum + v * v;
             }
@@ -800,7 +807,7 @@ int orc_create_part_d(const orc_geom* g, const double* field, const orc_field* f
               if (resetpos && xp_out) {
                 int idx[3] = {i, j, k};
                 for (int a = 0; a < d; ++a)
-                  xp_out[(int64_t)inp * d + a] = (double)(idx[a] - 1) * h[a] + g->min_sub[s * 3 + a];
+                  xp_out[(int64_t)inp * d + a] = (T)(idx[a] - 1) * h[a] + (T)g->min_sub[s * 3 + a];
               }
             }
             ++inp;
@@ -809,6 +816,48 @@ int orc_create_part_d(const orc_geom* g, const double* field, const orc_field* f
   }
   *np_out = inp;
   return 0;
+}
+
+extern "C" {
+
+// Single- and double-precision instantiations (ppm_kind_single / _double).
+int orc_comp_weights_d(const orc_geom* g, const double* xp, int ldxp, int np, int kernel,
+                       const int* list, const int* store_info, int maxp, double* wx1,
+                       double* wx2, double* wx3) {
+  return comp_weights_impl<double>(g, xp, ldxp, np, kernel, list, store_info, maxp, wx1, wx2, wx3);
+}
+int orc_comp_weights_s(const orc_geom* g, const float* xp, int ldxp, int np, int kernel,
+                       const int* list, const int* store_info, int maxp, float* wx1,
+                       float* wx2, float* wx3) {
+  return comp_weights_impl<float>(g, xp, ldxp, np, kernel, list, store_info, maxp, wx1, wx2, wx3);
+}
+int orc_remesh_d(const orc_geom* g, const double* xp, int ldxp, int np, const double* up,
+                 int lda, int kernel, const int* ghost, const int* list,
+                 const int* store_info, int maxp, const double* wx1, const double* wx2,
+                 const double* wx3, double* field, const orc_field* fl, int* err) {
+  return remesh_impl<double>(g, xp, ldxp, np, up, lda, kernel, ghost, list, store_info, maxp, wx1,
+                             wx2, wx3, field, fl, err);
+}
+int orc_remesh_s(const orc_geom* g, const float* xp, int ldxp, int np, const float* up,
+                 int lda, int kernel, const int* ghost, const int* list,
+                 const int* store_info, int maxp, const float* wx1, const float* wx2,
+                 const float* wx3, float* field, const orc_field* fl, int* err) {
+  return remesh_impl<float>(g, xp, ldxp, np, up, lda, kernel, ghost, list, store_info, maxp, wx1,
+                            wx2, wx3, field, fl, err);
+}
+int orc_create_part_d(const orc_geom* g, const double* field, const orc_field* fl,
+                      const double* cutoff, const double* cutoff_weights, int resetpos,
+                      const double* field_wp, int lda2, int* np_out, double* up_out,
+                      double* xp_out, double* wp_out) {
+  return create_part_impl<double>(g, field, fl, cutoff, cutoff_weights, resetpos, field_wp, lda2,
+                                  np_out, up_out, xp_out, wp_out);
+}
+int orc_create_part_s(const orc_geom* g, const float* field, const orc_field* fl,
+                      const float* cutoff, const float* cutoff_weights, int resetpos,
+                      const float* field_wp, int lda2, int* np_out, float* up_out,
+                      float* xp_out, float* wp_out) {
+  return create_part_impl<float>(g, field, fl, cutoff, cutoff_weights, resetpos, field_wp, lda2,
+                                 np_out, up_out, xp_out, wp_out);
 }
 
 // ppm_util_rank3d.f:353-533 and ppm_util_rank2d.f (same structure in 2D).

@@ -106,11 +106,18 @@ int orc_ghost_put_s(const orc_geom* g, float* field, const orc_field* fl, const 
 int orc_comp_weights_d(const orc_geom* g, const double* xp, int ldxp, int np, int kernel,
                        const int* list, const int* store_info, int maxp, double* wx1,
                        double* wx2, double* wx3);
+int orc_comp_weights_s(const orc_geom* g, const float* xp, int ldxp, int np, int kernel,
+                       const int* list, const int* store_info, int maxp, float* wx1,
+                       float* wx2, float* wx3);
 /* ppm_rmsh_remesh with stored weights (zero field, scatter, ghost put). */
 int orc_remesh_d(const orc_geom* g, const double* xp, int ldxp, int np, const double* up,
                  int lda, int kernel, const int* ghost, const int* list,
                  const int* store_info, int maxp, const double* wx1, const double* wx2,
                  const double* wx3, double* field, const orc_field* fl, int* err);
+int orc_remesh_s(const orc_geom* g, const float* xp, int ldxp, int np, const float* up,
+                 int lda, int kernel, const int* ghost, const int* list,
+                 const int* store_info, int maxp, const float* wx1, const float* wx2,
+                 const float* wx3, float* field, const orc_field* fl, int* err);
 
 /* ppm_rmsh_create_part.  Pass 1 (count) when up_out == NULL.
  * cutoff_weights may be NULL; field_wp/wp_out/lda2 optional (NULL / 0). */
@@ -118,6 +125,10 @@ int orc_create_part_d(const orc_geom* g, const double* field, const orc_field* f
                       const double* cutoff, const double* cutoff_weights, int resetpos,
                       const double* field_wp, int lda2, int* np_out, double* up_out,
                       double* xp_out, double* wp_out);
+int orc_create_part_s(const orc_geom* g, const float* field, const orc_field* fl,
+                      const float* cutoff, const float* cutoff_weights, int resetpos,
+                      const float* field_wp, int lda2, int* np_out, float* up_out,
+                      float* xp_out, float* wp_out);
 
 /* ppm_util_rank3d / ppm_util_rank2d: stable cell ranking.
  * lpdx: 1-based particle ids (size >= np), lhbx: nbox+1 1-based pointers.

@@ -44,6 +44,13 @@ SIGNATURES = {
     "ppmg_rmsh_comp_weights_d": ([_pd, _i64, _i64, _i, _i, _i, _pd, _pd, _pd, _pi], None),
     "ppmg_rmsh_comp_weights_d_dev": ([_pd, _i64, _i64, _i, _i, _i, _pd, _pd, _pd, _pi, _vp],
                                      None),
+    "ppmg_rmsh_comp_weights_s": ([_pd, _i64, _i64, _i, _i, _i, _pd, _pd, _pd, _pi], None),
+    "ppmg_rmsh_comp_weights_s_dev": ([_pd, _i64, _i64, _i, _i, _i, _pd, _pd, _pd, _pi, _vp],
+                                     None),
+    "ppmg_rmsh_remesh_sv_3d": (_P2M_V, None),
+    "ppmg_rmsh_remesh_sv_2d": (_P2M_V, None),
+    "ppmg_rmsh_remesh_sv_3d_dev": (_P2M_V + [_vp], None),
+    "ppmg_rmsh_remesh_sv_2d_dev": (_P2M_V + [_vp], None),
     "ppmg_rmsh_remesh_dv_3d": (_P2M_V, None),
     "ppmg_rmsh_remesh_dv_2d": (_P2M_V, None),
     "ppmg_rmsh_remesh_dv_3d_dev": (_P2M_V + [_vp], None),
@@ -51,6 +58,10 @@ SIGNATURES = {
     "ppmg_rmsh_create_part_d": ([_pd, _i64, _i, _pi64, _pi64, _i, _i, _pd, _pd, _i, _pd, _i64, _i,
                                  _pi64, _pd, _pd, _pd, _pi], None),
     "ppmg_rmsh_create_part_d_dev": ([_pd, _i64, _i, _pi64, _pi64, _i, _i, _pd, _pd, _i, _pd, _i64,
+                                     _i, _pi64, _pd, _pd, _pd, _pi, _vp], None),
+    "ppmg_rmsh_create_part_s": ([_pd, _i64, _i, _pi64, _pi64, _i, _i, _pd, _pd, _i, _pd, _i64, _i,
+                                 _pi64, _pd, _pd, _pd, _pi], None),
+    "ppmg_rmsh_create_part_s_dev": ([_pd, _i64, _i, _pi64, _pi64, _i, _i, _pd, _pd, _i, _pd, _i64,
                                      _i, _pi64, _pd, _pd, _pd, _pi, _vp], None),
     "ppmg_util_rank3d_d": (_RANK, None),
     "ppmg_util_rank2d_d": (_RANK, None),

@@ -68,6 +68,7 @@ struct Handle {
   std::mutex mu;
   // comp_weights state
   bool w_valid = false;
+  bool w_single = false;  // the stored weights are FP32 (comp_weights_s)
   int w_kernel = 0;
   int64_t w_np = 0;
   ~Handle() {
@@ -977,56 +978,59 @@ namespace {
 // (reference layout wx(1:2ks, 1, 1-ks:Np+ks)) are device arrays when
 // `user_dev`, else host arrays (copied back, synchronising the stream).
 // Returns 0 or the failing info.
-int comp_weights_core(Handle& h, const double* dxp, int64_t ldxp, int64_t Np, int kernel,
-                      double* const wx[3], bool user_dev, cudaStream_t st, int* info,
+template <class T>
+int comp_weights_core(Handle& h, const T* dxp, int64_t ldxp, int64_t Np, int kernel,
+                      T* const wx[3], bool user_dev, cudaStream_t st, int* info,
                       const char* caller) {
   const int dim = h.dim;
   KeyParams kp = make_kp(h, KEY_INTERP_CHECKED, false);
-  cudaError_t e = bin_sort<double>(kp, dxp, ldxp, Np, h.g.ncell, h.ws_rmsh, h.d_status + 0, st);
+  cudaError_t e = bin_sort<T>(kp, dxp, ldxp, Np, h.g.ncell, h.ws_rmsh, h.d_status + 0, st);
   if (e) return cuda_fail(info, e, caller);
   const int S = kernel == kKernelMp4 ? 4 : 2;
-  e = h.ws_rmsh.w1d.ensure(sizeof(double) * (size_t)(Np > 0 ? Np : 1) * dim * S);
+  const int wstride = weight_stride(dim, S, (int)sizeof(T));
+  e = h.ws_rmsh.w1d.ensure(sizeof(T) * (size_t)(Np > 0 ? Np : 1) * wstride);
   if (e) return cuda_fail(info, e, caller);
-  CWParams P{};
+  CWParams<T> P{};
   P.dim = dim;
   P.S = S;
+  P.wstride = wstride;
   P.nvalid = Np;
   P.d_nvalid = d_nvalid_of(h.ws_rmsh, h.g.ncell);
   P.idx = h.ws_rmsh.idx.as<int>();
   P.xp = dxp;
   P.ldxp = ldxp;
   for (int a = 0; a < 3; ++a) {
-    P.min_phys[a] = h.g.min_phys[a];
-    P.dxiq[a] = h.g.dxiq_d[a];
+    P.min_phys[a] = (T)h.g.min_phys[a];
+    P.dxiq[a] = is_f32<T>() ? (T)h.g.dxiq_f[a] : (T)h.g.dxiq_d[a];
     P.istart[a] = h.istart[a];
   }
-  P.w = h.ws_rmsh.w1d.as<double>();
-  if ((e = launch_comp_weights(P, st))) return cuda_fail(info, e, caller);
+  P.w = h.ws_rmsh.w1d.as<T>();
+  if ((e = launch_comp_weights<T>(P, st))) return cuda_fail(info, e, caller);
   const int ks = S / 2;
   const int64_t nu = (int64_t)S * (Np + 2 * ks);
   for (int a = 0; a < dim; ++a) {
     if (!wx[a]) continue;
-    double* dst = wx[a];
+    T* dst = wx[a];
     if (!user_dev) {
-      dst = mirror<double>(h.ws_rmsh.h_aux, (const double*)nullptr, nu, st, e);
+      dst = mirror<T>(h.ws_rmsh.h_aux, (const T*)nullptr, nu, st, e);
       if (e) return cuda_fail(info, e, caller);
     }
-    e = cudaMemsetAsync(dst, 0, sizeof(double) * (size_t)nu, st);
-    if (!e) e = launch_weights_to_user(P.w, P.idx, Np, P.d_nvalid, dim, S, a, dst, st);
+    e = cudaMemsetAsync(dst, 0, sizeof(T) * (size_t)nu, st);
+    if (!e) e = launch_weights_to_user<T>(P.w, P.idx, Np, P.d_nvalid, wstride, S, a, dst, st);
     if (!e && !user_dev)
-      e = cudaMemcpyAsync(wx[a], dst, sizeof(double) * (size_t)nu, cudaMemcpyDeviceToHost, st);
+      e = cudaMemcpyAsync(wx[a], dst, sizeof(T) * (size_t)nu, cudaMemcpyDeviceToHost, st);
     if (!e && !user_dev) e = cudaStreamSynchronize(st);
     if (e) return cuda_fail(info, e, caller);
   }
   h.w_valid = true;
+  h.w_single = is_f32<T>();
   h.w_kernel = kernel;
   h.w_np = Np;
   return 0;
 }
 
-Handle* comp_weights_checks(const double* xp, int64_t ldxp, int64_t Np, int topo_id, int mesh_id,
-                            int kernel, int* info, const char* caller) {
-  (void)xp;
+Handle* comp_weights_checks(int64_t ldxp, int64_t Np, int topo_id, int mesh_id, int kernel,
+                            int* info, const char* caller) {
   Handle* hh = find_handle(topo_id, mesh_id);
   if (!hh) {
     fail(info, kErrorError, kErrArgument, std::string(caller) + ": topo_id/mesh_id is invalid");
@@ -1045,39 +1049,59 @@ Handle* comp_weights_checks(const double* xp, int64_t ldxp, int64_t Np, int topo
 
 extern "C" {
 
+extern "C++" {
+template <class T>
+static void comp_weights_entry(const T* xp, int64_t ldxp, int64_t Np, int topo_id, int mesh_id,
+                               int kernel, T* wx1, T* wx2, T* wx3, int* info, bool dev,
+                               cudaStream_t dstream, const char* caller) {
+  clear_error();
+  if (info) *info = 0;
+  Handle* h = comp_weights_checks(ldxp, Np, topo_id, mesh_id, kernel, info, caller);
+  if (!h) return;
+  std::lock_guard<std::mutex> lk(h->mu);
+  T* const wx[3] = {wx1, wx2, wx3};
+  if (dev) {
+    comp_weights_core<T>(*h, xp, ldxp, Np, kernel, wx, true, dstream, info, caller);
+    return;
+  }
+  cudaStream_t st = h->stream;
+  cudaError_t e;
+  const T* dxp = mirror<T>(h->ws_rmsh.h_xp, xp, ldxp * Np, st, e);
+  if (e) { cuda_fail(info, e, caller); return; }
+  if (comp_weights_core<T>(*h, dxp, ldxp, Np, kernel, wx, false, st, info, caller)) return;
+  read_status(*h, st, info, caller);
+}
+}  // extern "C++"
+
 void ppmg_rmsh_comp_weights_d(const double* xp, int64_t ldxp, int64_t Np, int topo_id,
                               int mesh_id, int kernel, double* wx1, double* wx2,
                               double* wx3, int* info) {
-  const char* caller = "ppmg_rmsh_comp_weights_d";
-  clear_error();
-  if (info) *info = 0;
-  Handle* h = comp_weights_checks(xp, ldxp, Np, topo_id, mesh_id, kernel, info, caller);
-  if (!h) return;
-  std::lock_guard<std::mutex> lk(h->mu);
-  cudaStream_t st = h->stream;
-  cudaError_t e;
-  const double* dxp = mirror<double>(h->ws_rmsh.h_xp, xp, ldxp * Np, st, e);
-  if (e) { cuda_fail(info, e, caller); return; }
-  double* const wx[3] = {wx1, wx2, wx3};
-  if (comp_weights_core(*h, dxp, ldxp, Np, kernel, wx, false, st, info, caller)) return;
-  read_status(*h, st, info, caller);
+  comp_weights_entry<double>(xp, ldxp, Np, topo_id, mesh_id, kernel, wx1, wx2, wx3, info, false,
+                             nullptr, "ppmg_rmsh_comp_weights_d");
 }
-
+void ppmg_rmsh_comp_weights_s(const float* xp, int64_t ldxp, int64_t Np, int topo_id,
+                              int mesh_id, int kernel, float* wx1, float* wx2, float* wx3,
+                              int* info) {
+  comp_weights_entry<float>(xp, ldxp, Np, topo_id, mesh_id, kernel, wx1, wx2, wx3, info, false,
+                            nullptr, "ppmg_rmsh_comp_weights_s");
+}
 void ppmg_rmsh_comp_weights_d_dev(const double* xp, int64_t ldxp, int64_t Np, int topo_id,
                                   int mesh_id, int kernel, double* wx1, double* wx2,
                                   double* wx3, int* info, void* stream) {
-  const char* caller = "ppmg_rmsh_comp_weights_d_dev";
-  clear_error();
-  if (info) *info = 0;
-  Handle* h = comp_weights_checks(xp, ldxp, Np, topo_id, mesh_id, kernel, info, caller);
-  if (!h) return;
-  std::lock_guard<std::mutex> lk(h->mu);
-  double* const wx[3] = {wx1, wx2, wx3};
-  comp_weights_core(*h, xp, ldxp, Np, kernel, wx, true, (cudaStream_t)stream, info, caller);
+  comp_weights_entry<double>(xp, ldxp, Np, topo_id, mesh_id, kernel, wx1, wx2, wx3, info, true,
+                             (cudaStream_t)stream, "ppmg_rmsh_comp_weights_d_dev");
 }
-static void remesh_common(const double* xp, int64_t ldxp, int64_t Np, const double* up,
+void ppmg_rmsh_comp_weights_s_dev(const float* xp, int64_t ldxp, int64_t Np, int topo_id,
+                                  int mesh_id, int kernel, float* wx1, float* wx2, float* wx3,
+                                  int* info, void* stream) {
+  comp_weights_entry<float>(xp, ldxp, Np, topo_id, mesh_id, kernel, wx1, wx2, wx3, info, true,
+                            (cudaStream_t)stream, "ppmg_rmsh_comp_weights_s_dev");
+}
+extern "C++" {
+template <class T>
+static void remesh_common(const T* xp, int64_t ldxp, int64_t Np, const T* up,
                           int64_t ldup, int lda, int topo_id, int mesh_id, int kernel,
-                          const int* ghostsize, double* field_up, int64_t ldf,
+                          const int* ghostsize, T* field_up, int64_t ldf,
                           const int64_t* f_lb, const int64_t* f_ub, int* info, int dim,
                           const char* caller, bool dev = false, cudaStream_t dst = nullptr) {
   clear_error();
@@ -1096,32 +1120,33 @@ static void remesh_common(const double* xp, int64_t ldxp, int64_t Np, const doub
   Handle* h = get_checked(topo_id, mesh_id, dim, caller, info);
   if (!h) return;
   std::lock_guard<std::mutex> lk(h->mu);
-  if (!h->w_valid || h->w_kernel != kernel || h->w_np != Np) {
+  if (!h->w_valid || h->w_kernel != kernel || h->w_np != Np || h->w_single != is_f32<T>()) {
     fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": compute weights before remeshing");
     return;
   }
   if (dev) {
     // device arrays on the caller's stream; errors latch for ppmg_sync_status
-    p2m_pipeline<double>(*h, xp, ldxp, Np, up, ldup, lda, kernel, ghostsize, field_up, ldf, f_lb,
+    p2m_pipeline<T>(*h, xp, ldxp, Np, up, ldup, lda, kernel, ghostsize, field_up, ldf, f_lb,
                          f_ub, true, dst, info, caller);
     return;
   }
   cudaStream_t st = h->stream;
   cudaError_t e;
-  const double* dxp = mirror<double>(h->ws_rmsh.h_xp, xp, ldxp * Np, st, e);
+  const T* dxp = mirror<T>(h->ws_rmsh.h_xp, xp, ldxp * Np, st, e);
   if (e) { cuda_fail(info, e, caller); return; }
-  const double* dup = mirror<double>(h->ws_rmsh.h_up, up, ldup * Np, st, e);
+  const T* dup = mirror<T>(h->ws_rmsh.h_up, up, ldup * Np, st, e);
   if (e) { cuda_fail(info, e, caller); return; }
   const int64_t nf = field_elems(*h, ldf, f_lb, f_ub);
-  double* dfield = mirror<double>(h->ws_rmsh.h_field, (const double*)nullptr, nf, st, e);
+  T* dfield = mirror<T>(h->ws_rmsh.h_field, (const T*)nullptr, nf, st, e);
   if (e) { cuda_fail(info, e, caller); return; }
-  if (p2m_pipeline<double>(*h, dxp, ldxp, Np, dup, ldup, lda, kernel, ghostsize, dfield, ldf,
+  if (p2m_pipeline<T>(*h, dxp, ldxp, Np, dup, ldup, lda, kernel, ghostsize, dfield, ldf,
                            f_lb, f_ub, true, st, info, caller))
     return;
-  e = cudaMemcpyAsync(field_up, dfield, sizeof(double) * (size_t)nf, cudaMemcpyDeviceToHost, st);
+  e = cudaMemcpyAsync(field_up, dfield, sizeof(T) * (size_t)nf, cudaMemcpyDeviceToHost, st);
   if (e) { cuda_fail(info, e, caller); return; }
   read_status(*h, st, info, caller);
 }
+}  // extern "C++"
 
 void ppmg_rmsh_remesh_dv_3d(const double* xp, int64_t ldxp, int64_t Np, const double* up,
                             int64_t ldup, int lda, int topo_id, int mesh_id, int kernel,
@@ -1153,13 +1178,47 @@ void ppmg_rmsh_remesh_dv_2d_dev(const double* xp, int64_t ldxp, int64_t Np, cons
   remesh_common(xp, ldxp, Np, up, ldup, lda, topo_id, mesh_id, kernel, ghostsize, field_up, ldf,
                 f_lb, f_ub, info, 2, "ppmg_rmsh_remesh_dv_2d_dev", true, (cudaStream_t)stream);
 }
+void ppmg_rmsh_remesh_sv_3d(const float* xp, int64_t ldxp, int64_t Np, const float* up,
+                            int64_t ldup, int lda, int topo_id, int mesh_id, int kernel,
+                            const int* ghostsize, float* field_up, int64_t ldf,
+                            const int64_t* f_lb, const int64_t* f_ub, int* info) {
+  remesh_common<float>(xp, ldxp, Np, up, ldup, lda, topo_id, mesh_id, kernel, ghostsize, field_up,
+                       ldf, f_lb, f_ub, info, 3, "ppmg_rmsh_remesh_sv_3d");
+}
+void ppmg_rmsh_remesh_sv_3d_dev(const float* xp, int64_t ldxp, int64_t Np, const float* up,
+                                int64_t ldup, int lda, int topo_id, int mesh_id, int kernel,
+                                const int* ghostsize, float* field_up, int64_t ldf,
+                                const int64_t* f_lb, const int64_t* f_ub, int* info,
+                                void* stream) {
+  remesh_common<float>(xp, ldxp, Np, up, ldup, lda, topo_id, mesh_id, kernel, ghostsize, field_up,
+                       ldf, f_lb, f_ub, info, 3, "ppmg_rmsh_remesh_sv_3d_dev", true,
+                       (cudaStream_t)stream);
+}
+void ppmg_rmsh_remesh_sv_2d(const float* xp, int64_t ldxp, int64_t Np, const float* up,
+                            int64_t ldup, int lda, int topo_id, int mesh_id, int kernel,
+                            const int* ghostsize, float* field_up, int64_t ldf,
+                            const int64_t* f_lb, const int64_t* f_ub, int* info) {
+  remesh_common<float>(xp, ldxp, Np, up, ldup, lda, topo_id, mesh_id, kernel, ghostsize, field_up,
+                       ldf, f_lb, f_ub, info, 2, "ppmg_rmsh_remesh_sv_2d");
+}
+void ppmg_rmsh_remesh_sv_2d_dev(const float* xp, int64_t ldxp, int64_t Np, const float* up,
+                                int64_t ldup, int lda, int topo_id, int mesh_id, int kernel,
+                                const int* ghostsize, float* field_up, int64_t ldf,
+                                const int64_t* f_lb, const int64_t* f_ub, int* info,
+                                void* stream) {
+  remesh_common<float>(xp, ldxp, Np, up, ldup, lda, topo_id, mesh_id, kernel, ghostsize, field_up,
+                       ldf, f_lb, f_ub, info, 2, "ppmg_rmsh_remesh_sv_2d_dev", true,
+                       (cudaStream_t)stream);
+}
 
 // ---- create_part ---------------------------------------------------------------
-static void create_part_common(const double* field_up, int64_t ldf, int lda,
+extern "C++" {
+template <class T>
+static void create_part_common(const T* field_up, int64_t ldf, int lda,
                                const int64_t* f_lb, const int64_t* f_ub, int topo_id,
-                               int mesh_id, const double* cutoff, const double* cutoff_weights,
-                               int resetpos, const double* field_wp, int64_t ldfw, int lda2,
-                               int64_t* np, double* up, double* xp, double* wp, int* info,
+                               int mesh_id, const T* cutoff, const T* cutoff_weights,
+                               int resetpos, const T* field_wp, int64_t ldfw, int lda2,
+                               int64_t* np, T* up, T* xp, T* wp, int* info,
                                bool dev, cudaStream_t dstream, const char* caller) {
   clear_error();
   if (info) *info = 0;
@@ -1181,30 +1240,30 @@ static void create_part_common(const double* field_up, int64_t ldf, int lda,
   cudaStream_t st = dev ? dstream : h->stream;
   cudaError_t e = cudaSuccess;
   const int64_t nf = field_elems(*h, ldf, f_lb, f_ub);
-  const double* dfield = field_up;
+  const T* dfield = field_up;
   if (!dev) {
-    dfield = mirror<double>(h->ws.h_field, field_up, nf, st, e);
+    dfield = mirror<T>(h->ws.h_field, field_up, nf, st, e);
     if (e) { cuda_fail(info, e, caller); return; }
   }
-  const double* dfw = field_wp;
+  const T* dfw = field_wp;
   if (field_wp && !dev) {
-    dfw = mirror<double>(h->ws.h_xp, field_wp, field_elems(*h, ldfw, f_lb, f_ub), st, e);
+    dfw = mirror<T>(h->ws.h_xp, field_wp, field_elems(*h, ldfw, f_lb, f_ub), st, e);
     if (e) { cuda_fail(info, e, caller); return; }
   }
-  const double* dcw = nullptr;
+  const T* dcw = nullptr;
   if (cutoff_weights) {
-    dcw = mirror<double>(h->ws.w1d, cutoff_weights, lda, st, e);
+    dcw = mirror<T>(h->ws.w1d, cutoff_weights, lda, st, e);
     if (e) { cuda_fail(info, e, caller); return; }
   }
-  CPParams P{};
+  CPParams<T> P{};
   P.dim = dim;
   P.lda = lda;
   P.lda2 = lda2;
   for (int a = 0; a < 3; ++a) {
     // periodic axes visit nodes 1..Nm-1 (ppm_rmsh_create_part.f:433-453)
     P.nn[a] = a < dim ? h->g.N[a] : 1;
-    P.h[a] = h->g.h_d[a];
-    P.min_sub[a] = h->g.min_sub[a];
+    P.h[a] = (T)h->g.h_d[a];
+    P.min_sub[a] = (T)h->g.min_sub[a];
   }
   P.field = dfield;
   P.fd = fd;
@@ -1236,7 +1295,7 @@ static void create_part_common(const double* field_up, int64_t ldf, int lda,
     if ((e = launch_cp_fill(P, flag, pos, st))) cuda_fail(info, e, caller);
     return;
   }
-  double* dout = mirror<double>(h->ws.h_aux, (const double*)nullptr,
+  T* dout = mirror<T>(h->ws.h_aux, (const T*)nullptr,
                                 (int64_t)total * (lda + dim + (field_wp ? lda2 : 0)), st, e);
   if (e) { cuda_fail(info, e, caller); return; }
   P.up = dout;
@@ -1244,15 +1303,16 @@ static void create_part_common(const double* field_up, int64_t ldf, int lda,
   P.wp = field_wp ? dout + (int64_t)total * (lda + dim) : nullptr;
   if ((e = launch_cp_fill(P, flag, pos, st))) { cuda_fail(info, e, caller); return; }
   if (total > 0) {
-    e = cudaMemcpyAsync(up, P.up, sizeof(double) * (size_t)total * lda, cudaMemcpyDeviceToHost, st);
+    e = cudaMemcpyAsync(up, P.up, sizeof(T) * (size_t)total * lda, cudaMemcpyDeviceToHost, st);
     if (!e && resetpos && xp)
-      e = cudaMemcpyAsync(xp, P.xp, sizeof(double) * (size_t)total * dim, cudaMemcpyDeviceToHost, st);
+      e = cudaMemcpyAsync(xp, P.xp, sizeof(T) * (size_t)total * dim, cudaMemcpyDeviceToHost, st);
     if (!e && field_wp && wp)
-      e = cudaMemcpyAsync(wp, P.wp, sizeof(double) * (size_t)total * lda2, cudaMemcpyDeviceToHost, st);
+      e = cudaMemcpyAsync(wp, P.wp, sizeof(T) * (size_t)total * lda2, cudaMemcpyDeviceToHost, st);
   }
   if (!e) e = cudaStreamSynchronize(st);
   if (e) cuda_fail(info, e, caller);
 }
+}  // extern "C++"
 
 void ppmg_rmsh_create_part_d(const double* field_up, int64_t ldf, int lda,
                              const int64_t* f_lb, const int64_t* f_ub, int topo_id,
@@ -1272,6 +1332,25 @@ void ppmg_rmsh_create_part_d_dev(const double* field_up, int64_t ldf, int lda,
   create_part_common(field_up, ldf, lda, f_lb, f_ub, topo_id, mesh_id, cutoff, cutoff_weights,
                      resetpos, field_wp, ldfw, lda2, np, up, xp, wp, info, true,
                      (cudaStream_t)stream, "ppmg_rmsh_create_part_d_dev");
+}
+void ppmg_rmsh_create_part_s(const float* field_up, int64_t ldf, int lda,
+                             const int64_t* f_lb, const int64_t* f_ub, int topo_id,
+                             int mesh_id, const float* cutoff, const float* cutoff_weights,
+                             int resetpos, const float* field_wp, int64_t ldfw, int lda2,
+                             int64_t* np, float* up, float* xp, float* wp, int* info) {
+  create_part_common<float>(field_up, ldf, lda, f_lb, f_ub, topo_id, mesh_id, cutoff,
+                            cutoff_weights, resetpos, field_wp, ldfw, lda2, np, up, xp, wp, info,
+                            false, nullptr, "ppmg_rmsh_create_part_s");
+}
+void ppmg_rmsh_create_part_s_dev(const float* field_up, int64_t ldf, int lda,
+                                 const int64_t* f_lb, const int64_t* f_ub, int topo_id,
+                                 int mesh_id, const float* cutoff, const float* cutoff_weights,
+                                 int resetpos, const float* field_wp, int64_t ldfw, int lda2,
+                                 int64_t* np, float* up, float* xp, float* wp, int* info,
+                                 void* stream) {
+  create_part_common<float>(field_up, ldf, lda, f_lb, f_ub, topo_id, mesh_id, cutoff,
+                            cutoff_weights, resetpos, field_wp, ldfw, lda2, np, up, xp, wp, info,
+                            true, (cudaStream_t)stream, "ppmg_rmsh_create_part_s_dev");
 }
 
 // ---- cell lists -------------------------------------------------------------------

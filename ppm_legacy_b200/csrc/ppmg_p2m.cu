@@ -169,11 +169,18 @@ __device__ __forceinline__ void scan_cells(int n, F val, int* out, int* wsum, in
 }
 
 // Shared memory of k_p2m3d for `cap` staging slots.
-template <int S, class CT, bool WST>
+// 16-byte units of one staged particle's record part: its packed record, or
+// (stored weights) 3 x S weights of the field's type padded to 16 bytes
+template <int S, class CT, class OT, bool WST>
+constexpr int p2m_rec_units() {
+  return WST ? (3 * S * (int)sizeof(OT) + 15) / 16 : (int)sizeof(typename Vec4<CT>::type) / 16;
+}
+
+template <int S, class CT, class OT, bool WST>
 constexpr size_t p2m3d_smem(int cap) {
   using V = typename Vec4<CT>::type;
   constexpr int NSC = (kTileX + S - 1) * (kTileY + S - 1);
-  constexpr int IU = (WST ? 3 * S * 8 / 16 : (int)sizeof(V) / 16) + (int)sizeof(V) / 16;
+  constexpr int IU = p2m_rec_units<S, CT, OT, WST>() + (int)sizeof(V) / 16;
   return (size_t)cap * (3 * sizeof(V) + (S + 2) * sizeof(CT) + 16 * IU + 2) +
          sizeof(int) * (size_t)(6 * NSC + 2);
 }
@@ -188,7 +195,7 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
   constexpr int NSC = WX * WY;
   constexpr int NT = kTX * kTY;
   constexpr int PERC = (NSC + NT - 1) / NT;  // staged cells per thread (count loads)
-  constexpr int RU = WST ? 3 * S * 8 / 16 : (int)sizeof(V) / 16;  // 16-byte units: record part
+  constexpr int RU = p2m_rec_units<S, CT, OT, WST>();  // 16-byte units: record part
   constexpr int UU = (int)sizeof(V) / 16;                          // strengths part
   constexpr int IU = RU + UU;
   static_assert(NSC <= 3 * NT, "staged cells exceed the scan width");
@@ -363,7 +370,7 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
       const uint4* r = raw + (size_t)i * IU;
       CT w[3][S];
       if constexpr (WST) {
-        const double* wsrc = reinterpret_cast<const double*>(r);
+        const OT* wsrc = reinterpret_cast<const OT*>(r);
 #pragma unroll
         for (int k = 0; k < S; ++k) {
           w[0][k] = (CT)wsrc[k];
@@ -631,7 +638,9 @@ __global__ void __launch_bounds__(kTile2) k_p2m2d(P2MParams P) {
         const V u = load_vec(us, s, P.ps);
         CT w[2][S];
         if constexpr (WST) {
-          const double* ws = static_cast<const double*>(P.rec) + s * (2 * S);
+          // stored weights: 2 x S values of the field's type, padded to 16 bytes
+          constexpr int WS2 = (2 * S * (int)sizeof(OT) + 15) / 16 * 16 / (int)sizeof(OT);
+          const OT* ws = static_cast<const OT*>(P.rec) + s * WS2;
 #pragma unroll
           for (int k = 0; k < S; ++k) {
             w[0][k] = (CT)ws[k];
@@ -718,9 +727,9 @@ cudaError_t launch_lc(const P2MParams& P, int dim, cudaStream_t st) {
     // staging slots: as many as fit in ~110 KB (2 CTAs / SM)
     P2MParams Q = P;
     int cap = 2048;
-    while (cap > 64 && p2m3d_smem<S, CT, WST>(cap) > (size_t)110 * 1024) cap -= 16;
+    while (cap > 64 && p2m3d_smem<S, CT, OT, WST>(cap) > (size_t)110 * 1024) cap -= 16;
     Q.cap = cap;
-    const size_t smem = p2m3d_smem<S, CT, WST>(cap);
+    const size_t smem = p2m3d_smem<S, CT, OT, WST>(cap);
     auto kern = k_p2m3d<S, CT, COMP, OT, LC, WST>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);

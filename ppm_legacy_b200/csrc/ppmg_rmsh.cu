@@ -22,34 +22,36 @@ int nblocks(int64_t n, int t = 256) {
 // (bsp2) at distances |ii - 2 + istart - xi|, tested with <= as the reference.
 // Stored as (w_axis0[S], w_axis1[S], [w_axis2[S]]) per sorted particle.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double mp4_le(double x) {
-  if (x <= 2.0) {
-    if (x <= 1.0) return rsub(1.0, rmul(rmul(x, x), rsub(2.5, rmul(1.5, x))));
-    return radd(2.0, rmul(radd(-4.0, rmul(rsub(2.5, rmul(0.5, x)), x)), x));
+template <class T>
+__device__ __forceinline__ T mp4_le(T x) {
+  if (x <= T(2)) {
+    if (x <= T(1)) return rsub(T(1), rmul(rmul(x, x), rsub(T(2.5), rmul(T(1.5), x))));
+    return radd(T(2), rmul(radd(T(-4), rmul(rsub(T(2.5), rmul(T(0.5), x)), x)), x));
   }
-  return 0.0;
+  return T(0);
 }
 
-__global__ void k_comp_weights(CWParams P) {
+template <class T>
+__global__ void k_comp_weights(CWParams<T> P) {
   const int S = P.S;
   const int64_t nv = min(P.nvalid, (int64_t)*P.d_nvalid);
   for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nv;
        s += (int64_t)gridDim.x * blockDim.x) {
     const int64_t p = P.idx[s];
-    const double* x = P.xp + p * P.ldxp;
-    double* w = P.w + s * (int64_t)(P.dim * S);
+    const T* x = P.xp + p * P.ldxp;
+    T* w = P.w + s * (int64_t)P.wstride;
     for (int a = 0; a < P.dim; ++a) {
-      const double xi = rmul(rsub(x[a], P.min_phys[a]), P.dxiq[a]);
+      const T xi = rmul(rsub(x[a], P.min_phys[a]), P.dxiq[a]);
       const int ip = (int)xi + 2 - P.istart[a];
       const int lo = S == 4 ? ip - 1 : ip;
       for (int t = 0; t < S; ++t) {
         const int ii = lo + t;
-        const double xd = fabs(rsub((double)(ii - 2 + P.istart[a]), xi));
-        double v;
+        const T xd = fabs(rsub((T)(ii - 2 + P.istart[a]), xi));
+        T v;
         if (S == 4) {
-          v = mp4_le(xd);
+          v = mp4_le<T>(xd);
         } else {
-          v = xd <= 1.0 ? rsub(1.0, xd) : 0.0;
+          v = xd <= T(1) ? rsub(T(1), xd) : T(0);
         }
         w[a * S + t] = v;
       }
@@ -59,16 +61,17 @@ __global__ void k_comp_weights(CWParams P) {
 
 // Sorted weights -> the reference's user layout wx(1:2ks, 1:1, 1-ks:Np+ks)
 // for one axis, indexed by the particle's list position (= id + 1).
-__global__ void k_weights_to_user(const double* __restrict__ w, const int* __restrict__ idx,
-                                  int64_t nvalid, const int* __restrict__ d_nvalid, int dim,
-                                  int S, int axis, double* __restrict__ out) {
+template <class T>
+__global__ void k_weights_to_user(const T* __restrict__ w, const int* __restrict__ idx,
+                                  int64_t nvalid, const int* __restrict__ d_nvalid, int wstride,
+                                  int S, int axis, T* __restrict__ out) {
   const int ks = S / 2;
   const int64_t nv = min(nvalid, (int64_t)*d_nvalid);
   for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nv;
        s += (int64_t)gridDim.x * blockDim.x) {
     const int64_t p = idx[s];
     for (int t = 0; t < S; ++t)
-      out[(int64_t)t + (int64_t)S * (p + ks)] = w[s * (dim * S) + axis * S + t];
+      out[(int64_t)t + (int64_t)S * (p + ks)] = w[s * wstride + axis * S + t];
   }
 }
 
@@ -84,21 +87,22 @@ __device__ __forceinline__ int64_t node_off(const FieldDesc& fd, int dim, int i,
   return o;
 }
 
-__global__ void k_cp_flag(CPParams P, int* __restrict__ flag) {
+template <class T>
+__global__ void k_cp_flag(CPParams<T> P, int* __restrict__ flag) {
   const int64_t nq = (int64_t)P.nn[0] * P.nn[1] * P.nn[2];
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq;
        q += (int64_t)gridDim.x * blockDim.x) {
     const int i = (int)(q % P.nn[0]) + 1;
     const int j = (int)((q / P.nn[0]) % P.nn[1]) + 1;
     const int k = (int)(q / ((int64_t)P.nn[0] * P.nn[1])) + 1;
-    const double* f = P.field + node_off(P.fd, P.dim, i, j, k);
-    double str;
+    const T* f = P.field + node_off(P.fd, P.dim, i, j, k);
+    T str;
     if (P.lda == 1 && P.cw == nullptr) {
       str = fabs(f[0]);
     } else {
-      double sum = 0.0;
+      T sum = T(0);
       for (int a = 0; a < P.lda; ++a) {
-        double v = f[a];
+        T v = f[a];
         if (P.cw) v = rmul(v, P.cw[a]);
         sum = radd(sum, rmul(v, v));
       }
@@ -108,7 +112,8 @@ __global__ void k_cp_flag(CPParams P, int* __restrict__ flag) {
   }
 }
 
-__global__ void k_cp_fill(CPParams P, const int* __restrict__ flag,
+template <class T>
+__global__ void k_cp_fill(CPParams<T> P, const int* __restrict__ flag,
                           const int* __restrict__ pos) {
   const int64_t nq = (int64_t)P.nn[0] * P.nn[1] * P.nn[2];
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq;
@@ -127,7 +132,7 @@ __global__ void k_cp_fill(CPParams P, const int* __restrict__ flag,
     if (P.xp) {
       const int idx[3] = {i, j, k};
       for (int a = 0; a < P.dim; ++a)
-        P.xp[o * P.dim + a] = radd(rmul((double)(idx[a] - 1), P.h[a]), P.min_sub[a]);
+        P.xp[o * P.dim + a] = radd(rmul((T)(idx[a] - 1), P.h[a]), P.min_sub[a]);
     }
   }
 }
@@ -208,37 +213,52 @@ __global__ void k_plus_one(const int* __restrict__ in, int* __restrict__ out, in
 
 }  // namespace
 
-cudaError_t launch_comp_weights(const CWParams& P, cudaStream_t st) {
+template <class T>
+cudaError_t launch_comp_weights(const CWParams<T>& P, cudaStream_t st) {
   if (P.nvalid <= 0) return cudaSuccess;
-  k_comp_weights<<<nblocks(P.nvalid), 256, 0, st>>>(P);
+  k_comp_weights<T><<<nblocks(P.nvalid), 256, 0, st>>>(P);
   count_launch();
   return cudaGetLastError();
 }
 
-cudaError_t launch_weights_to_user(const double* w, const int* idx, int64_t nvalid,
-                                   const int* d_nvalid, int dim, int S, int axis, double* out,
+template <class T>
+cudaError_t launch_weights_to_user(const T* w, const int* idx, int64_t nvalid,
+                                   const int* d_nvalid, int wstride, int S, int axis, T* out,
                                    cudaStream_t st) {
   if (nvalid <= 0) return cudaSuccess;
-  k_weights_to_user<<<nblocks(nvalid), 256, 0, st>>>(w, idx, nvalid, d_nvalid, dim, S, axis,
-                                                     out);
+  k_weights_to_user<T><<<nblocks(nvalid), 256, 0, st>>>(w, idx, nvalid, d_nvalid, wstride, S,
+                                                        axis, out);
   count_launch();
   return cudaGetLastError();
 }
 
-cudaError_t launch_cp_flag(const CPParams& P, int* flag, cudaStream_t st) {
+template <class T>
+cudaError_t launch_cp_flag(const CPParams<T>& P, int* flag, cudaStream_t st) {
   const int64_t nq = (int64_t)P.nn[0] * P.nn[1] * P.nn[2];
-  k_cp_flag<<<nblocks(nq), 256, 0, st>>>(P, flag);
+  k_cp_flag<T><<<nblocks(nq), 256, 0, st>>>(P, flag);
   count_launch();
   return cudaGetLastError();
 }
 
-cudaError_t launch_cp_fill(const CPParams& P, const int* flag, const int* pos,
+template <class T>
+cudaError_t launch_cp_fill(const CPParams<T>& P, const int* flag, const int* pos,
                            cudaStream_t st) {
   const int64_t nq = (int64_t)P.nn[0] * P.nn[1] * P.nn[2];
-  k_cp_fill<<<nblocks(nq), 256, 0, st>>>(P, flag, pos);
+  k_cp_fill<T><<<nblocks(nq), 256, 0, st>>>(P, flag, pos);
   count_launch();
   return cudaGetLastError();
 }
+
+#define PPMG_RMSH_INST(T)                                                                     \
+  template cudaError_t launch_comp_weights<T>(const CWParams<T>&, cudaStream_t);              \
+  template cudaError_t launch_weights_to_user<T>(const T*, const int*, int64_t, const int*,   \
+                                                 int, int, int, T*, cudaStream_t);            \
+  template cudaError_t launch_cp_flag<T>(const CPParams<T>&, int*, cudaStream_t);             \
+  template cudaError_t launch_cp_fill<T>(const CPParams<T>&, const int*, const int*,          \
+                                         cudaStream_t);
+PPMG_RMSH_INST(double)
+PPMG_RMSH_INST(float)
+#undef PPMG_RMSH_INST
 
 template <class T>
 cudaError_t launch_ghost(const GhostParams& P, int maptype, T* field, T* tmp,

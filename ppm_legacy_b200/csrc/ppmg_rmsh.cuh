@@ -5,34 +5,43 @@
 
 namespace ppmg {
 
-// ppm_rmsh_comp_weights: 1D weights per sorted particle.
+// Stored 1D weights per sorted particle: dim x S values of the routine's
+// kind, padded to a multiple of 16 bytes (one or more whole 16-byte units).
+inline int weight_stride(int dim, int S, int tsize) {
+  return (dim * S * tsize + 15) / 16 * 16 / tsize;
+}
+
+// ppm_rmsh_comp_weights (T = double: _d, float: _s): 1D weights per sorted particle.
+template <class T>
 struct CWParams {
   int dim, S;
+  int wstride;          // weight_stride(dim, S, sizeof(T))
   int64_t nvalid;       // grid bound (Np); sorted count is *d_nvalid
   const int* d_nvalid;
   const int* idx;
-  const double* xp;
+  const T* xp;
   int64_t ldxp;
-  double min_phys[3];
-  double dxiq[3];  // FP32 mesh spacing widened (ppm_rmsh_comp_weights.f:146-147)
+  T min_phys[3];
+  T dxiq[3];  // FP32 mesh spacing (ppm_rmsh_comp_weights.f:146-147)
   int istart[3];
-  double* w;       // out: nvalid x dim x S
+  T* w;       // out: nvalid x wstride
 };
 
-// ppm_rmsh_create_part.
+// ppm_rmsh_create_part (T = double: _d, float: _s).
+template <class T>
 struct CPParams {
   int dim, lda, lda2;
   int nn[3];        // nodes visited per axis
-  const double* field;
+  const T* field;
   FieldDesc fd;
-  const double* field_wp;
+  const T* field_wp;
   FieldDesc fdw;
-  const double* cw;  // cutoff weights or nullptr
-  double cut0, cut1;
-  double h[3], min_sub[3];
-  double* up;
-  double* xp;
-  double* wp;
+  const T* cw;  // cutoff weights or nullptr
+  T cut0, cut1;
+  T h[3], min_sub[3];
+  T* up;
+  T* xp;
+  T* wp;
 };
 
 struct GhostParams {
@@ -42,12 +51,16 @@ struct GhostParams {
   FieldDesc fd;
 };
 
-cudaError_t launch_comp_weights(const CWParams& P, cudaStream_t st);
-cudaError_t launch_weights_to_user(const double* w, const int* idx, int64_t nvalid,
-                                   const int* d_nvalid, int dim, int S, int axis, double* out,
+template <class T>
+cudaError_t launch_comp_weights(const CWParams<T>& P, cudaStream_t st);
+template <class T>
+cudaError_t launch_weights_to_user(const T* w, const int* idx, int64_t nvalid,
+                                   const int* d_nvalid, int wstride, int S, int axis, T* out,
                                    cudaStream_t st);
-cudaError_t launch_cp_flag(const CPParams& P, int* flag, cudaStream_t st);
-cudaError_t launch_cp_fill(const CPParams& P, const int* flag, const int* pos,
+template <class T>
+cudaError_t launch_cp_flag(const CPParams<T>& P, int* flag, cudaStream_t st);
+template <class T>
+cudaError_t launch_cp_fill(const CPParams<T>& P, const int* flag, const int* pos,
                            cudaStream_t st);
 template <class T>
 cudaError_t launch_ghost(const GhostParams& P, int maptype, T* field, T* tmp,

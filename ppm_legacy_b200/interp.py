@@ -198,17 +198,22 @@ def ppm_rmsh_comp_weights(xp, Np, topo_id, mesh_id, kernel, wx1_user=None, wx2_u
     """ppm_rmsh_comp_weights(xp, Np, topo_id, mesh_id, kernel[, wx1, wx2, wx3]).
 
     The weights stay in the library (like the reference's module state); user
-    arrays, when given, must be float64 (2ks, 1, Np+2ks) column-major.
+    arrays, when given, have xp's dtype and shape (2ks, 1, Np+2ks), column-major.
+    float32 positions select ppm_rmsh_comp_weights_s (FP32 weights).
     """
     _check(xp)
+    k = _kind(xp)
+    for u in (wx1_user, wx2_user, wx3_user):
+        if u is not None and _kind(u) != k:
+            raise TypeError("ppm_rmsh_comp_weights: wx arrays must have the dtype of xp")
     info = C.c_int(0)
     w = [None if u is None else _addr(u) for u in (wx1_user, wx2_user, wx3_user)]
     a = (_addr(xp), xp.shape[0], int(Np), topo_id, mesh_id, kernel, w[0], w[1], w[2],
          C.byref(info))
     if _is_dev(xp):
-        lib().ppmg_rmsh_comp_weights_d_dev(*a, _stream())
+        getattr(lib(), f"ppmg_rmsh_comp_weights_{k}_dev")(*a, _stream())
     else:
-        lib().ppmg_rmsh_comp_weights_d(*a)
+        getattr(lib(), f"ppmg_rmsh_comp_weights_{k}")(*a)
     return info.value
 
 
@@ -217,10 +222,15 @@ def ppm_rmsh_remesh(xp, Np, up, *args, field_lb=None):
 
     The reference puts ``info`` before ``field_up``; here ``field_up`` must be
     preallocated by the caller (the reference's ppm_alloc grow step) and is
-    overwritten entirely (zeroed, then the remeshed field).
+    overwritten entirely (zeroed, then the remeshed field).  float32 arrays
+    select the single-precision variants (_ss/_sv), which need weights from
+    a single-precision ppm_rmsh_comp_weights.
     """
     vector, lda, topo_id, mesh_id, kernel, ghostsize, field_up = _split(up, args, "ppm_rmsh_remesh")
     _check(xp, up, field_up)
+    k = _kind(xp)
+    if _kind(up) != k or _kind(field_up) != k:
+        raise TypeError("ppm_rmsh_remesh: xp, up and field_up must share one dtype")
     dim = field_up.ndim - (2 if vector else 1)
     lb, ub = _bounds(field_up, dim, vector, ghostsize, field_lb)
     info = C.c_int(0)
@@ -229,9 +239,9 @@ def ppm_rmsh_remesh(xp, Np, up, *args, field_lb=None):
     a = (_addr(xp), xp.shape[0], int(Np), _addr(up), ldup, lda, topo_id, mesh_id, kernel,
          int_array(ghostsize), _addr(field_up), ldf, lb, ub, C.byref(info))
     if _is_dev(xp):
-        getattr(lib(), f"ppmg_rmsh_remesh_dv_{dim}d_dev")(*a, _stream())
+        getattr(lib(), f"ppmg_rmsh_remesh_{k}v_{dim}d_dev")(*a, _stream())
     else:
-        getattr(lib(), f"ppmg_rmsh_remesh_dv_{dim}d")(*a)
+        getattr(lib(), f"ppmg_rmsh_remesh_{k}v_{dim}d")(*a)
     return info.value
 
 
@@ -242,29 +252,34 @@ def ppm_rmsh_create_part(field_up, topo_id, mesh_id, cutoff, lda=None, resetpos=
 
     The reference reallocates xp/up/wp in place (POINTER arguments); this
     mirror returns the new arrays: up (lda, np), xp (dim, np) when resetpos,
-    wp (lda2, np) when field_wp is given.
+    wp (lda2, np) when field_wp is given.  A float32 field selects
+    ppm_rmsh_create_part_s* (FP32 cutoffs and outputs).
     """
     vector = lda is not None
     lda = int(lda) if vector else 1
     _check(field_up)
+    k = _kind(field_up)
+    ft = np.float64 if k == "d" else np.float32
     dim = field_up.ndim - (2 if vector else 1)
     lb, ub = _bounds(field_up, dim, vector, ghostsize, field_lb)
     ldf = field_up.shape[0] if vector else 1
-    cut = np.asarray(cutoff, dtype=np.float64)
-    cw = None if cutoff_weights is None else np.ascontiguousarray(cutoff_weights, dtype=np.float64)
+    cut = np.ascontiguousarray(cutoff, dtype=ft)
+    cw = None if cutoff_weights is None else np.ascontiguousarray(cutoff_weights, dtype=ft)
     lda2 = 0
     ldfw = 0
     if field_wp is not None:
         _check(field_wp)
+        if _kind(field_wp) != k:
+            raise TypeError("ppm_rmsh_create_part: field_wp must have the dtype of field_up")
         lda2 = field_wp.shape[0] if field_wp.ndim == dim + 2 else 1
         ldfw = lda2
     n = C.c_int64(0)
     info = C.c_int(0)
     dev = _is_dev(field_up)
     if dev:
-        fn = lambda *a: lib().ppmg_rmsh_create_part_d_dev(*a, _stream())  # noqa: E731
+        fn = lambda *a: getattr(lib(), f"ppmg_rmsh_create_part_{k}_dev")(*a, _stream())  # noqa: E731
     else:
-        fn = lib().ppmg_rmsh_create_part_d
+        fn = getattr(lib(), f"ppmg_rmsh_create_part_{k}")
     common = (_addr(field_up), ldf, lda, lb, ub, topo_id, mesh_id, cut.ctypes.data,
               None if cw is None else cw.ctypes.data, int(bool(resetpos)),
               None if field_wp is None else _addr(field_wp), ldfw, lda2)
@@ -275,7 +290,7 @@ def ppm_rmsh_create_part(field_up, topo_id, mesh_id, cutoff, lda=None, resetpos=
     if dev:
         # device outputs, column-major like the host arrays
         def cm(rows):
-            return torch.empty((max(npn, 1), rows), dtype=torch.float64,
+            return torch.empty((max(npn, 1), rows), dtype=field_up.dtype,
                                device=field_up.device).t()[:, :npn]
         up = cm(lda)
         xp = cm(dim) if resetpos else None
@@ -286,9 +301,9 @@ def ppm_rmsh_create_part(field_up, topo_id, mesh_id, cutoff, lda=None, resetpos=
         if not vector:
             up = up.reshape(-1)
         return info.value, npn, up, xp, wp
-    up = np.zeros((lda, npn), order="F")
-    xp = np.zeros((dim, npn), order="F") if resetpos else None
-    wp = np.zeros((max(lda2, 1), npn), order="F") if field_wp is not None else None
+    up = np.zeros((lda, npn), dtype=ft, order="F")
+    xp = np.zeros((dim, npn), dtype=ft, order="F") if resetpos else None
+    wp = np.zeros((max(lda2, 1), npn), dtype=ft, order="F") if field_wp is not None else None
     fn(*common, C.byref(n), up.ctypes.data, None if xp is None else xp.ctypes.data,
        None if wp is None else wp.ctypes.data, C.byref(info))
     if not vector:

@@ -243,3 +243,84 @@ def test_remeshing_device_twins_match_host_entry_points(dim, kernel):
     assert idv == 0 and nd == nh
     torch.cuda.synchronize()
     assert np.array_equal(host(ud), uh) and np.array_equal(host(xd), xh)
+
+
+@pytest.mark.parametrize("dim,kernel", [(3, 2), (3, 1), (2, 2)])
+def test_single_precision_remeshing_matches_oracle(dim, kernel):
+    """comp_weights_s, remesh_sv and create_part_s against the oracle's single
+    routines: weights bit for bit, the field to FP32 summation order (1e-5
+    normwise), and create_part's particles from a field both sides share."""
+    rng = np.random.default_rng(110 + dim + kernel)
+    nc = 12
+    t = registered(dim, nc)
+    g = [2] * dim
+    np_ = 2 * nc ** dim
+    xp = random_particles(rng, dim, np_).astype(np.float32, order="F")
+    up = rng.standard_normal((3, np_)).astype(np.float32, order="F")
+    ks = 2 if kernel == 2 else 1
+    wx = [np.zeros((2 * ks, 1, np_ + 2 * ks), dtype=np.float32, order="F") for _ in range(dim)]
+    assert ppmg.ppm_rmsh_comp_weights(xp, np_, t.topo_id, t.mesh_id, kernel, *wx) == 0
+    wo, lst, si = O.comp_weights(t, xp, kernel)
+    for a in range(dim):
+        assert np.array_equal(wx[a], wo[a])
+    lb, ub = box_bounds(t, g)
+    f = np.full((3,) + tuple(ub[a] - lb[a] + 1 for a in range(dim)) + (1,), 5.0,
+                dtype=np.float32, order="F")
+    assert ppmg.ppm_rmsh_remesh(xp, np_, up, 3, t.topo_id, t.mesh_id, kernel, g, f) == 0, \
+        ppmg.last_error()
+    fo, _, _ = O.remesh(t, xp, up, kernel, g, wo, lst, si)
+    real = (slice(None),) + tuple(slice(1 - lb[a], t.Nm[a] + 1 - lb[a]) for a in range(dim)) + (0,)
+    assert max_rel(f[real].astype(np.float64), fo[real].astype(np.float64)) < 1e-5
+    # create_part on the GPU's field: same count, order, strengths and positions
+    cut = [0.2, 1e30]
+    info, n, upn, xpn, _ = ppmg.ppm_rmsh_create_part(f, t.topo_id, t.mesh_id, cut, lda=3,
+                                                     resetpos=True, ghostsize=g)
+    assert info == 0, ppmg.last_error()
+    no, upo, xpo, _ = O.create_part(t, f, lb, ub, cut)
+    assert n == no and n > 0 and upn.dtype == np.float32
+    assert np.array_equal(upn, upo) and np.array_equal(xpn, xpo)
+    # single weights do not feed a double remesh
+    fd = np.zeros(f.shape, order="F")
+    info = ppmg.ppm_rmsh_remesh(xp.astype(np.float64), np_, up.astype(np.float64), 3, t.topo_id,
+                                t.mesh_id, kernel, g, fd)
+    assert info == -2 and "weights" in ppmg.last_error()[2]
+
+
+def test_single_precision_remeshing_device_twins():
+    """float32 torch arrays take the single `_dev` twins and equal the host calls."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(120)
+    nc = 10
+    t = registered(3, nc)
+    g = [2, 2, 2]
+    np_ = 3 * nc ** 3
+    xp = random_particles(rng, 3, np_).astype(np.float32, order="F")
+    up = rng.standard_normal((2, np_)).astype(np.float32, order="F")
+    lb, ub = box_bounds(t, g)
+    shape = (2,) + tuple(ub[a] - lb[a] + 1 for a in range(3)) + (1,)
+
+    def cm(a):
+        d = torch.from_numpy(np.ascontiguousarray(np.asarray(a).T)).cuda()
+        return d.permute(*reversed(range(d.dim())))
+
+    def host(a):
+        return a.permute(*reversed(range(a.dim()))).contiguous().cpu().numpy().T
+
+    assert ppmg.ppm_rmsh_comp_weights(xp, np_, t.topo_id, t.mesh_id, 2) == 0
+    fh = np.zeros(shape, dtype=np.float32, order="F")
+    assert ppmg.ppm_rmsh_remesh(xp, np_, up, 2, t.topo_id, t.mesh_id, 2, g, fh) == 0
+    ih, nh, uh, xh, _ = ppmg.ppm_rmsh_create_part(fh, t.topo_id, t.mesh_id, [0.1, 1e30], lda=2,
+                                                  resetpos=True, ghostsize=g)
+    assert ih == 0 and nh > 0
+    dxp, dup = cm(xp), cm(up)
+    assert ppmg.ppm_rmsh_comp_weights(dxp, np_, t.topo_id, t.mesh_id, 2) == 0
+    fd = cm(np.full(shape, 3.0, dtype=np.float32))
+    assert ppmg.ppm_rmsh_remesh(dxp, np_, dup, 2, t.topo_id, t.mesh_id, 2, g, fd) == 0
+    assert ppmg.sync_status(t.topo_id, t.mesh_id) == 0
+    assert fd.dtype == torch.float32 and np.array_equal(host(fd), fh)
+    idv, nd, ud, xd, _ = ppmg.ppm_rmsh_create_part(fd, t.topo_id, t.mesh_id, [0.1, 1e30], lda=2,
+                                                   resetpos=True, ghostsize=g)
+    assert idv == 0 and nd == nh
+    torch.cuda.synchronize()
+    assert ud.dtype == torch.float32
+    assert np.array_equal(host(ud), uh) and np.array_equal(host(xd), xh)

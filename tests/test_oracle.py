@@ -179,3 +179,32 @@ def test_create_part_order_and_band():
     # (k, j, i) order with i fastest: (3,0,0) comes before (1,2,3)
     np.testing.assert_array_equal(up.T, [[0.0, 0.5], [3.0, 0.0]])
     np.testing.assert_allclose(xp.T, [[0.75, 0.0, 0.0], [0.25, 0.5, 0.75]])
+
+
+def test_single_precision_remeshing_tracks_double():
+    """The single variants (comp_weights_s, remesh_sv, create_part_s) compute in
+    FP32 and agree with the double routines to FP32 rounding on the same inputs."""
+    rng = np.random.default_rng(9)
+    for dim, kernel in ((3, 2), (2, 1)):
+        t = topo_for(dim, 10)
+        g = [2] * dim
+        x32 = random_particles(rng, dim, 400).astype(np.float32, order="F")
+        u32 = rng.standard_normal((2, 400)).astype(np.float32, order="F")
+        w32, lst, si = O.comp_weights(t, x32, kernel)
+        w64, lst64, _ = O.comp_weights(t, x32.astype(np.float64), kernel)
+        assert w32[0].dtype == np.float32 and np.array_equal(lst, lst64)
+        for a in range(dim):
+            assert np.abs(w32[a] - w64[a]).max() < 2e-6
+        f32, lb, _ = O.remesh(t, x32, u32, kernel, g, w32, lst, si)
+        f64, _, _ = O.remesh(t, x32.astype(np.float64), u32.astype(np.float64), kernel, g, w64,
+                             lst, si)
+        assert f32.dtype == np.float32
+        assert max_rel(f32.astype(np.float64), f64) < 1e-5
+        n32, up32, xp32, _ = O.create_part(t, f32, lb, [lb[a] + f32.shape[1 + a] - 1
+                                                       for a in range(dim)], [0.5, 1e30])
+        n64, up64, xp64, _ = O.create_part(t, f32.astype(np.float64), lb,
+                                           [lb[a] + f32.shape[1 + a] - 1 for a in range(dim)],
+                                           [0.5, 1e30])
+        assert n32 == n64 and up32.dtype == np.float32
+        assert np.array_equal(up32.astype(np.float64), up64)
+        assert np.abs(xp32 - xp64).max() < 1e-6
