@@ -20,11 +20,11 @@ namespace ppmg {
 namespace {
 
 constexpr int kCThreads = 256;                  // count kernel
-constexpr int kRThreads = 512;                  // move kernel
+constexpr int kRThreads = 1024;                 // move kernel
 constexpr int kRWarps = kRThreads / 32;
-constexpr int kRItems = 8;                      // items per thread and sub-tile
+constexpr int kRItems = 4;                      // items per thread and sub-tile
 constexpr int kRSub = kRThreads * kRItems;      // 4096 items per sub-tile
-constexpr int kRWarpItems = kRSub / kRWarps;    // 256 consecutive items per warp
+constexpr int kRWarpItems = kRSub / kRWarps;    // 128 consecutive items per warp
 constexpr int kRMaxBits = 9;                    // >= 8 items per digit and sub-tile
 constexpr int kRMaxBuckets = 1 << kRMaxBits;
 constexpr int kRSlots = kRMaxBuckets + 32;      // + the invalid bucket of the first pass
@@ -197,25 +197,28 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
-// Shared memory of k_radix_move: two key+id buffers (32 KB each), two plane
+// Shared memory of k_radix_move: two key buffers (16 KB each), two plane
 // buffers (64 KB each), the 16-bit inverse map and per-warp digit counts,
-// the per-digit offsets and the mbarriers (~224 KB: one CTA per SM).
-constexpr size_t kMoveSmem = 2 * sizeof(int2) * (size_t)kRSub + 2 * sizeof(uint4) * (size_t)kRSub +
+// the per-digit offsets and the mbarriers (~209 KB: one CTA of 32 warps per
+// SM, enough warps to cover the shared-memory latency of the ranking).
+constexpr size_t kMoveSmem = 2 * sizeof(int) * (size_t)kRSub + 2 * sizeof(uint4) * (size_t)kRSub +
                              sizeof(unsigned short) * (size_t)(kRSub + kRWarps * kRSlots) +
                              sizeof(int) * (size_t)(3 * kRSlots + 64) + 4 * sizeof(uint64_t);
 
 // One stable pass.  Every tile walks its sub-tiles in order.  The inputs of
 // a sub-tile arrive by TMA bulk copies on two independent double-buffered
-// streams: keys with ids (one 32 KB unit per sub-tile, issued two sub-tiles
-// ahead) and the 16-byte planes of records and strengths (64 KB units, issued
-// two units ahead), each completing on its own mbarrier.  The keys are ranked
-// by digit (warp w owns items [256w, 256w+256), ranked round by round with
-// __match_any_sync); inv[] maps every sorted position of the sub-tile to its
-// item, so each plane is written in digit runs straight from its buffer.
+// streams: keys (one 16 KB unit per sub-tile, issued two sub-tiles ahead)
+// and the units of ids (16 KB; not in the first pass, whose ids are the
+// item positions) and 16-byte planes of records and strengths (64 KB),
+// issued two units ahead, each stream completing on its own mbarriers.  The
+// keys are ranked by digit (warp w owns items [128w, 128w+128), ranked round
+// by round with one ballot per digit bit); inv[] maps every sorted position of the
+// sub-tile to its item, so the ids and each plane are written in digit runs
+// straight from their buffer.
 template <bool FIRST>
 __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
   extern __shared__ __align__(128) unsigned char smem[];
-  int2* kb = reinterpret_cast<int2*>(smem);                           // [2][kRSub] (key, id)
+  int* kb = reinterpret_cast<int*>(smem);                             // [2][kRSub] keys
   uint4* pb = reinterpret_cast<uint4*>(kb + 2 * kRSub);               // [2][kRSub] planes
   unsigned short* inv = reinterpret_cast<unsigned short*>(pb + 2 * kRSub);  // [kRSub]
   unsigned short* whist = inv + kRSub;                                // [kRWarps][kRSlots]
@@ -233,6 +236,7 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
   const int w = tid >> 5;
   const unsigned lt = (1u << lane) - 1u;
   unsigned short* wh = whist + w * kRSlots;
+  const int dbits = A.bits + (FIRST ? 1 : 0);  // the first pass has the invalid bucket nb
 
   const int64_t n = FIRST ? A.np : (int64_t)*A.d_nvalid;
   if (FIRST && blockIdx.x == 0 && tid == 0)
@@ -240,8 +244,8 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
   const int64_t t0 = (int64_t)blockIdx.x * A.subs * kRSub;
   if (t0 >= n) return;
   const int nsc = (int)min((int64_t)A.subs, (n - t0 + kRSub - 1) / kRSub);
-  const int NP = A.nplanes;
-  const int total_p = nsc * NP;
+  const int NU = A.nplanes + (FIRST ? 0 : 1);  // stream units per sub-tile: [ids,] planes
+  const int total_p = nsc * NU;
 
   for (int d = tid; d < nbk; d += kRThreads) run[d] = A.hist[(int64_t)d * A.ntiles + blockIdx.x];
   if (tid == 0) {
@@ -252,26 +256,32 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
   __syncthreads();
 
   auto sub_n = [&](int sub) { return (int)min((int64_t)kRSub, n - (t0 + (int64_t)sub * kRSub)); };
-  // keys (+ ids) of sub-tile s into kb[s & 1]
+  // keys of sub-tile s into kb[s & 1] (rounded up to 16 bytes: the key
+  // arrays are allocated 16 entries long)
   auto issue_keys = [&](int s) {
     if (s >= nsc) return;
     const int64_t base = t0 + (int64_t)s * kRSub;
     const uint32_t bytes = (uint32_t)((sub_n(s) * 4 + 15) & ~15);
-    int* b = reinterpret_cast<int*>(kb + (s & 1) * kRSub);
     uint64_t* br = &bar[s & 1];
-    mbar_expect_tx(br, FIRST ? bytes : 2 * bytes);
-    bulk_load(b, A.key_in + base, bytes, br);
-    if (!FIRST) bulk_load(b + kRSub, A.id_in + base, bytes, br);
+    mbar_expect_tx(br, bytes);
+    bulk_load(kb + (s & 1) * kRSub, A.key_in + base, bytes, br);
   };
-  // plane unit u (sub-tile u / NP, plane u % NP) into pb[u & 1]
+  // stream unit u (sub-tile u / NU; unit u % NU: the ids unless FIRST, then
+  // the planes) into pb[u & 1]
   auto issue_plane = [&](int u) {
     if (u >= total_p) return;
-    const int s = u / NP, pl = u - s * NP;
+    const int s = u / NU, pl = u - s * NU - (FIRST ? 0 : 1);
     const int64_t base = t0 + (int64_t)s * kRSub;
+    uint64_t* br = &bar[2 + (u & 1)];
+    if (pl < 0) {  // ids (rounded up to 16 bytes like the keys)
+      const uint32_t bytes = (uint32_t)((sub_n(s) * 4 + 15) & ~15);
+      mbar_expect_tx(br, bytes);
+      bulk_load(pb + (u & 1) * kRSub, A.id_in + base, bytes, br);
+      return;
+    }
     const uint4* src = pl < A.rplanes ? A.rec_in + (int64_t)pl * A.np
                                       : A.us_in + (int64_t)(pl - A.rplanes) * A.np;
     const uint32_t bytes = (uint32_t)sub_n(s) * 16u;
-    uint64_t* br = &bar[2 + (u & 1)];
     mbar_expect_tx(br, bytes);
     bulk_load(pb + (u & 1) * kRSub, src + base, bytes, br);
   };
@@ -296,8 +306,7 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
     const int64_t base = t0 + (int64_t)sub * kRSub;
     const int subn = sub_n(sub);
     if (!wait_on(&bar[sub & 1], sub)) return;
-    const int* skeys = reinterpret_cast<const int*>(kb + (sub & 1) * kRSub);
-    const int* sids = skeys + kRSub;
+    const int* skeys = kb + (sub & 1) * kRSub;
     for (int d = lane; d < nbk; d += 32) wh[d] = 0;
     __syncwarp();
     int key[kRItems], lpos[kRItems];
@@ -307,7 +316,16 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
       const bool valid = li < subn;
       key[r] = valid ? skeys[li] : 0;
       const int d = valid ? digit_of<FIRST>(key[r], A.shift, mask, nb, A.ncell) : -1;
-      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      // lanes holding the same digit, one ballot per digit bit (a match
+      // instruction serialises over the distinct values of the warp)
+      unsigned peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+      for (int b = 0; b <= kRMaxBits; ++b)
+        if (b < dbits) {
+          const bool bit = (d >> b) & 1;
+          const unsigned m = __ballot_sync(0xffffffffu, bit);
+          peers &= bit ? m : ~m;
+        }
       const int before = valid ? wh[d] : 0;
       __syncwarp();
       if (valid && lane == __ffs(peers) - 1) wh[d] = (unsigned short)(before + __popc(peers));
@@ -353,7 +371,8 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
         inv[lpos[r] + dst[d] + wh[d]] = (unsigned short)(w * kRWarpItems + r * 32 + lane);
       }
     __syncthreads();
-    // keys and ids; each thread takes the sorted positions j = tid + 512 q
+    // keys (first pass: and ids); thread t takes the sorted positions
+    // j = t + 1024 q
     int gdst[kRItems];
 #pragma unroll
     for (int q = 0; q < kRItems; ++q) {
@@ -365,20 +384,27 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
         const int d = digit_of<FIRST>(kk, A.shift, mask, nb, A.ncell);
         gdst[q] = run[d] + (j - dst[d]);
         A.key_out[gdst[q]] = kk;
-        A.id_out[gdst[q]] = FIRST ? (int)(base + li) : sids[li];
+        if (FIRST) A.id_out[gdst[q]] = (int)(base + li);
       }
     }
     __syncthreads();
     if (tid == 0) issue_keys(sub + 2);
-    // record and strength planes
-    for (int pl = 0; pl < NP; ++pl, ++u) {
+    // ids, then the record and strength planes
+    for (int pl = FIRST ? 0 : -1; pl < A.nplanes; ++pl, ++u) {
       if (!wait_on(&bar[2 + (u & 1)], u)) return;
       const uint4* sb = pb + (u & 1) * kRSub;
-      uint4* out = pl < A.rplanes ? A.rec_out + (int64_t)pl * A.np
-                                  : A.us_out + (int64_t)(pl - A.rplanes) * A.np;
+      if (pl < 0) {
+        const int* sid = reinterpret_cast<const int*>(sb);
 #pragma unroll
-      for (int q = 0; q < kRItems; ++q)
-        if (gdst[q] >= 0) out[gdst[q]] = sb[inv[tid + q * kRThreads]];
+        for (int q = 0; q < kRItems; ++q)
+          if (gdst[q] >= 0) A.id_out[gdst[q]] = sid[inv[tid + q * kRThreads]];
+      } else {
+        uint4* out = pl < A.rplanes ? A.rec_out + (int64_t)pl * A.np
+                                    : A.us_out + (int64_t)(pl - A.rplanes) * A.np;
+#pragma unroll
+        for (int q = 0; q < kRItems; ++q)
+          if (gdst[q] >= 0) out[gdst[q]] = sb[inv[tid + q * kRThreads]];
+      }
       __syncthreads();
       if (tid == 0) issue_plane(u + 2);
     }
