@@ -269,6 +269,14 @@ void ppmg_util_rank3d_d(const double* xp, int64_t ldxp, int64_t Np, const double
 void ppmg_util_rank2d_d(const double* xp, int64_t ldxp, int64_t Np, const double* xmin,
                         const double* xmax, const int* Nm, const int* Ngl, int* lpdx,
                         int* lhbx, int64_t* icount, int* info);
+/* Single precision (ppm_util_rank3d_s / ppm_util_rank2d_s): positions, bounds
+ * and the cell spacing in FP32, as the reference's REAL(4) build. */
+void ppmg_util_rank3d_s(const float* xp, int64_t ldxp, int64_t Np, const float* xmin,
+                        const float* xmax, const int* Nm, const int* Ngl, int* lpdx,
+                        int* lhbx, int64_t* icount, int* info);
+void ppmg_util_rank2d_s(const float* xp, int64_t ldxp, int64_t Np, const float* xmin,
+                        const float* xmax, const int* Nm, const int* Ngl, int* lpdx,
+                        int* lhbx, int64_t* icount, int* info);
 
 /* ---- Instrumentation (no counterpart in the reference) -------------------
  * ppmg_kernel_timing(1) makes the library bracket, on the launching stream,

@@ -306,8 +306,11 @@ def create_part(topo, field, lb, ub, cutoff, cutoff_weights=None, resetpos=True,
 
 
 def rank(xp, xmin, xmax, Nm, Ngl):
-    """ppm_util_rank{2,3}d: returns (lpdx 1-based, lhbx 1-based, icount)."""
-    xp = _f64(xp)
+    """ppm_util_rank{2,3}d: returns (lpdx 1-based, lhbx 1-based, icount).
+    float32 positions run ppm_util_rank{2,3}d_s (bounds and spacing in FP32)."""
+    k = _kind(xp)
+    ct = _ctk(k)
+    xp = _fk(xp, k)
     dim = len(Nm)
     Ngl = np.asarray(Ngl, dtype=np.int32)
     Nm = np.asarray(Nm, dtype=np.int32)
@@ -315,11 +318,11 @@ def rank(xp, xmin, xmax, Nm, Ngl):
     lpdx = np.zeros(max(xp.shape[1], 1), dtype=np.int32)
     lhbx = np.zeros(nbox + 1, dtype=np.int32)
     ic = C.c_int(0)
-    xmin = np.asarray(xmin, dtype=np.float64)
-    xmax = np.asarray(xmax, dtype=np.float64)
-    fn = lib().orc_rank3d_d if dim == 3 else lib().orc_rank2d_d
-    fn(_ptr(xp, C.c_double), xp.shape[0], xp.shape[1], _ptr(xmin, C.c_double),
-       _ptr(xmax, C.c_double), _ptr(Nm, C.c_int), _ptr(Ngl, C.c_int), _ptr(lpdx, C.c_int),
+    xmin = np.ascontiguousarray(xmin, dtype=xp.dtype)
+    xmax = np.ascontiguousarray(xmax, dtype=xp.dtype)
+    fn = getattr(lib(), f"orc_rank{dim}d_{k}")
+    fn(_ptr(xp, ct), xp.shape[0], xp.shape[1], _ptr(xmin, ct),
+       _ptr(xmax, ct), _ptr(Nm, C.c_int), _ptr(Ngl, C.c_int), _ptr(lpdx, C.c_int),
        _ptr(lhbx, C.c_int), C.byref(ic))
     return lpdx[: ic.value], lhbx, ic.value
 

@@ -861,23 +861,27 @@ int orc_create_part_s(const orc_geom* g, const float* field, const orc_field* fl
 }
 
 // ppm_util_rank3d.f:353-533 and ppm_util_rank2d.f (same structure in 2D).
-static int rank_impl(int dim, const double* xp, int ldxp, int np, const double* xmin,
-                     const double* xmax, const int* Nm, const int* Ngl, int* lpdx, int* lhbx,
+extern "C++" {
+// T: the precision of ppm_util_rank3d_s/_d (positions, bounds and spacing in
+// REAL(MK), ppm_util_rank3d.f:353-425).
+template <class T>
+static int rank_impl(int dim, const T* xp, int ldxp, int np, const T* xmin,
+                     const T* xmax, const int* Nm, const int* Ngl, int* lpdx, int* lhbx,
                      int* icount_out) {
   int Nmtot[3] = {1, 1, 1};
   for (int a = 0; a < dim; ++a) Nmtot[a] = Nm[a] + Ngl[a] + Ngl[dim + a];
   int64_t nbox = (int64_t)Nmtot[0] * Nmtot[1] * Nmtot[2];
-  double rd[3];
-  for (int a = 0; a < dim; ++a) rd[a] = (double)Nm[a] / (xmax[a] - xmin[a]);
+  T rd[3];
+  for (int a = 0; a < dim; ++a) rd[a] = (T)Nm[a] / (xmax[a] - xmin[a]);
   std::vector<int64_t> pbox(np);
   std::vector<int> npbx(nbox, 0);
   int icount = 0;
   int64_t n2 = (int64_t)Nmtot[0] * Nmtot[1];
   for (int ip = 0; ip < np; ++ip) {
-    const double* x = xp + (int64_t)ip * ldxp;
+    const T* x = xp + (int64_t)ip * ldxp;
     int c[3] = {0, 0, 0};
     for (int a = 0; a < dim; ++a) {
-      c[a] = (int)std::floor((x[a] - xmin[a]) * rd[a]) + Ngl[a];
+      c[a] = (int)std::floor((T)((x[a] - xmin[a]) * rd[a])) + Ngl[a];
       if (x[a] >= xmax[a] && c[a] < Nm[a] + Ngl[a]) c[a] = Nm[a] + Ngl[a];
     }
     for (int a = 0; a < dim; ++a)
@@ -909,6 +913,7 @@ static int rank_impl(int dim, const double* xp, int ldxp, int np, const double* 
   *icount_out = icount;
   return 0;
 }
+}  // extern "C++"
 
 int orc_rank3d_d(const double* xp, int ldxp, int np, const double* xmin,
                  const double* xmax, const int* Nm, const int* Ngl, int* lpdx, int* lhbx,
@@ -918,6 +923,14 @@ int orc_rank3d_d(const double* xp, int ldxp, int np, const double* xmin,
 int orc_rank2d_d(const double* xp, int ldxp, int np, const double* xmin,
                  const double* xmax, const int* Nm, const int* Ngl, int* lpdx, int* lhbx,
                  int* icount) {
+  return rank_impl(2, xp, ldxp, np, xmin, xmax, Nm, Ngl, lpdx, lhbx, icount);
+}
+int orc_rank3d_s(const float* xp, int ldxp, int np, const float* xmin, const float* xmax,
+                 const int* Nm, const int* Ngl, int* lpdx, int* lhbx, int* icount) {
+  return rank_impl(3, xp, ldxp, np, xmin, xmax, Nm, Ngl, lpdx, lhbx, icount);
+}
+int orc_rank2d_s(const float* xp, int ldxp, int np, const float* xmin, const float* xmax,
+                 const int* Nm, const int* Ngl, int* lpdx, int* lhbx, int* icount) {
   return rank_impl(2, xp, ldxp, np, xmin, xmax, Nm, Ngl, lpdx, lhbx, icount);
 }
 

@@ -139,6 +139,12 @@ int orc_rank3d_d(const double* xp, int ldxp, int np, const double* xmin,
 int orc_rank2d_d(const double* xp, int ldxp, int np, const double* xmin,
                  const double* xmax, const int* Nm, const int* Ngl, int* lpdx, int* lhbx,
                  int* icount);
+/* Single precision (ppm_util_rank3d_s / rank2d_s): positions, bounds and the
+ * cell spacing in FP32. */
+int orc_rank3d_s(const float* xp, int ldxp, int np, const float* xmin, const float* xmax,
+                 const int* Nm, const int* Ngl, int* lpdx, int* lhbx, int* icount);
+int orc_rank2d_s(const float* xp, int ldxp, int np, const float* xmin, const float* xmax,
+                 const int* Nm, const int* Ngl, int* lpdx, int* lhbx, int* icount);
 
 /* Adjoint of P2M on one periodic sub (no reference counterpart): given the
  * adjoint field r on real nodes, dw(a,p) = sum_n W(xi_p - n) r(a,n) and

@@ -1354,8 +1354,12 @@ void ppmg_rmsh_create_part_s_dev(const float* field_up, int64_t ldf, int lda,
 }
 
 // ---- cell lists -------------------------------------------------------------------
-static void rank_common(int dim, const double* xp, int64_t ldxp, int64_t Np, const double* xmin,
-                        const double* xmax, const int* Nm, const int* Ngl, int* lpdx, int* lhbx,
+extern "C++" {
+// T: the precision of ppm_util_rank{2,3}d_{s,d} (positions, bounds and the
+// cell spacing rdx = REAL(Nm)/(xmax - xmin) in REAL(MK), ppm_util_rank3d.f:353).
+template <class T>
+static void rank_common(int dim, const T* xp, int64_t ldxp, int64_t Np, const T* xmin,
+                        const T* xmax, const int* Nm, const int* Ngl, int* lpdx, int* lhbx,
                         int64_t* icount, int* info, const char* caller) {
   clear_error();
   if (info) *info = 0;
@@ -1366,9 +1370,12 @@ static void rank_common(int dim, const double* xp, int64_t ldxp, int64_t Np, con
   for (int a = 0; a < 3; ++a) {
     cp.Nm[a] = a < dim ? Nm[a] : 1;
     cp.Nt[a] = a < dim ? Nm[a] + Ngl[a] + Ngl[dim + a] : 1;
-    cp.xmin[a] = a < dim ? xmin[a] : 0.0;
-    cp.xmax[a] = a < dim ? xmax[a] : 1.0;
-    cp.rd[a] = a < dim ? (double)Nm[a] / (xmax[a] - xmin[a]) : 1.0;
+    cp.xmin[a] = a < dim ? (double)xmin[a] : 0.0;
+    cp.xmax[a] = a < dim ? (double)xmax[a] : 1.0;
+    cp.rd[a] = a < dim ? (double)Nm[a] / ((double)xmax[a] - (double)xmin[a]) : 1.0;
+    cp.xminf[a] = a < dim ? (float)xmin[a] : 0.0f;
+    cp.xmaxf[a] = a < dim ? (float)xmax[a] : 1.0f;
+    cp.rdf[a] = a < dim ? (float)Nm[a] / ((float)xmax[a] - (float)xmin[a]) : 1.0f;
     nbox *= cp.Nt[a];
   }
   for (int a = 0; a < dim; ++a) {
@@ -1384,9 +1391,9 @@ static void rank_common(int dim, const double* xp, int64_t ldxp, int64_t Np, con
   cudaError_t e = cudaSuccess;
   if (!st) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
   if (e) { cuda_fail(info, e, caller); return; }
-  const double* dxp = mirror<double>(ws.h_xp, xp, ldxp * Np, st, e);
+  const T* dxp = mirror<T>(ws.h_xp, xp, ldxp * Np, st, e);
   if (e) { cuda_fail(info, e, caller); return; }
-  if ((e = clist_sort(cp, dxp, ldxp, Np, nbox, ws, st))) { cuda_fail(info, e, caller); return; }
+  if ((e = clist_sort<T>(cp, dxp, ldxp, Np, nbox, ws, st))) { cuda_fail(info, e, caller); return; }
   int nin = 0;
   e = cudaMemcpyAsync(&nin, ws.err.p, sizeof(int), cudaMemcpyDeviceToHost, st);
   if (!e) e = ws.h_aux.ensure(sizeof(int) * (size_t)(Np + nbox + 2));
@@ -1401,6 +1408,7 @@ static void rank_common(int dim, const double* xp, int64_t ldxp, int64_t Np, con
   if (e) { cuda_fail(info, e, caller); return; }
   if (icount) *icount = nin;
 }
+}  // extern "C++"
 
 void ppmg_util_rank3d_d(const double* xp, int64_t ldxp, int64_t Np, const double* xmin,
                         const double* xmax, const int* Nm, const int* Ngl, int* lpdx,
@@ -1413,6 +1421,18 @@ void ppmg_util_rank2d_d(const double* xp, int64_t ldxp, int64_t Np, const double
                         int* lhbx, int64_t* icount, int* info) {
   rank_common(2, xp, ldxp, Np, xmin, xmax, Nm, Ngl, lpdx, lhbx, icount, info,
               "ppmg_util_rank2d_d");
+}
+void ppmg_util_rank3d_s(const float* xp, int64_t ldxp, int64_t Np, const float* xmin,
+                        const float* xmax, const int* Nm, const int* Ngl, int* lpdx,
+                        int* lhbx, int64_t* icount, int* info) {
+  rank_common(3, xp, ldxp, Np, xmin, xmax, Nm, Ngl, lpdx, lhbx, icount, info,
+              "ppmg_util_rank3d_s");
+}
+void ppmg_util_rank2d_s(const float* xp, int64_t ldxp, int64_t Np, const float* xmin,
+                        const float* xmax, const int* Nm, const int* Ngl, int* lpdx,
+                        int* lhbx, int64_t* icount, int* info) {
+  rank_common(2, xp, ldxp, Np, xmin, xmax, Nm, Ngl, lpdx, lhbx, icount, info,
+              "ppmg_util_rank2d_s");
 }
 
 }  // extern "C"

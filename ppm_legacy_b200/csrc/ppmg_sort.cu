@@ -359,20 +359,28 @@ template cudaError_t pack_records<float, float>(const KeyParams&, const float*, 
 // ---------------------------------------------------------------------------
 namespace {
 
-__global__ void k_clist_bin(ClistParams cp, const double* __restrict__ xp, int64_t ldxp,
+template <class T>
+__global__ void k_clist_bin(ClistParams cp, const T* __restrict__ xp, int64_t ldxp,
                             int64_t np, int* __restrict__ key, int* __restrict__ slot,
                             int* __restrict__ count, int* __restrict__ nin) {
+  constexpr bool F = sizeof(T) == 4;
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np;
        p += (int64_t)gridDim.x * blockDim.x) {
-    const double* x = xp + p * ldxp;
+    const T* x = xp + p * ldxp;
     int c[3] = {0, 0, 0};
     for (int a = 0; a < cp.dim; ++a) {
-      // FLOOR((x - x0) * rdx) + Ngl: the subtraction first (ppm_util_rank3d.f:415-425)
-      c[a] = (int)floor(rmul(rsub(x[a], cp.xmin[a]), cp.rd[a])) + cp.Ngl[a];
-      if (x[a] >= cp.xmax[a] && c[a] < cp.Nm[a] + cp.Ngl[a]) c[a] = cp.Nm[a] + cp.Ngl[a];
+      // FLOOR((x - x0) * rdx) + Ngl in REAL(MK): the subtraction first
+      // (ppm_util_rank3d.f:353-425)
+      const T x0 = F ? (T)cp.xminf[a] : (T)cp.xmin[a];
+      const T rd = F ? (T)cp.rdf[a] : (T)cp.rd[a];
+      const T xm = F ? (T)cp.xmaxf[a] : (T)cp.xmax[a];
+      c[a] = (int)floor(rmul(rsub(x[a], x0), rd)) + cp.Ngl[a];
+      if (x[a] >= xm && c[a] < cp.Nm[a] + cp.Ngl[a]) c[a] = cp.Nm[a] + cp.Ngl[a];
     }
-    for (int a = 0; a < cp.dim; ++a)
-      if (x[a] < cp.xmax[a] && c[a] >= cp.Nm[a] + cp.Ngl[a]) c[a] = cp.Nm[a] + cp.Ngl[a] - 1;
+    for (int a = 0; a < cp.dim; ++a) {
+      const T xm = F ? (T)cp.xmaxf[a] : (T)cp.xmax[a];
+      if (x[a] < xm && c[a] >= cp.Nm[a] + cp.Ngl[a]) c[a] = cp.Nm[a] + cp.Ngl[a] - 1;
+    }
     bool in = true;
     for (int a = 0; a < cp.dim; ++a) in = in && c[a] >= 0 && c[a] < cp.Nt[a];
     int k = -1;
@@ -387,7 +395,8 @@ __global__ void k_clist_bin(ClistParams cp, const double* __restrict__ xp, int64
 
 }  // namespace
 
-cudaError_t clist_sort(const ClistParams& cp, const double* xp, int64_t ldxp, int64_t np,
+template <class T>
+cudaError_t clist_sort(const ClistParams& cp, const T* xp, int64_t ldxp, int64_t np,
                        int64_t nbox, Workspace& ws, cudaStream_t st) {
   cudaError_t e;
   const size_t pn = sizeof(int) * (size_t)(np > 0 ? np : 1);
@@ -400,12 +409,16 @@ cudaError_t clist_sort(const ClistParams& cp, const double* xp, int64_t ldxp, in
   if ((e = cudaMemsetAsync(ws.count.p, 0, sizeof(int) * (size_t)(nbox + 1), st))) return e;
   if ((e = cudaMemsetAsync(ws.err.p, 0, sizeof(int) * 4, st))) return e;
   if (np > 0) {
-    k_clist_bin<<<grid_for(np, 256), 256, 0, st>>>(cp, xp, ldxp, np, ws.key.as<int>(),
-                                                   ws.slot.as<int>(), ws.count.as<int>(),
-                                                   ws.err.as<int>());
+    k_clist_bin<T><<<grid_for(np, 256), 256, 0, st>>>(cp, xp, ldxp, np, ws.key.as<int>(),
+                                                      ws.slot.as<int>(), ws.count.as<int>(),
+                                                      ws.err.as<int>());
     count_launch();
   }
   return sort_tail(np, nbox, ws, st);
 }
+template cudaError_t clist_sort<double>(const ClistParams&, const double*, int64_t, int64_t,
+                                        int64_t, Workspace&, cudaStream_t);
+template cudaError_t clist_sort<float>(const ClistParams&, const float*, int64_t, int64_t,
+                                       int64_t, Workspace&, cudaStream_t);
 
 }  // namespace ppmg

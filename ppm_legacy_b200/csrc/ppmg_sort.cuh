@@ -111,9 +111,11 @@ struct ClistParams {
   int Nm[3];
   int Ngl[6];
   int Nt[3];
-  double xmin[3], xmax[3], rd[3];
+  double xmin[3], xmax[3], rd[3];  // double positions
+  float xminf[3], xmaxf[3], rdf[3];  // float positions (ppm_util_rank3d_s)
 };
-cudaError_t clist_sort(const ClistParams& cp, const double* xp, int64_t ldxp, int64_t np,
+template <class T>
+cudaError_t clist_sort(const ClistParams& cp, const T* xp, int64_t ldxp, int64_t np,
                        int64_t nbox, Workspace& ws, cudaStream_t st);
 
 }  // namespace ppmg

@@ -312,8 +312,10 @@ def ppm_rmsh_create_part(field_up, topo_id, mesh_id, cutoff, lda=None, resetpos=
 
 
 def ppm_util_rank(xp, Np, xmin, xmax, Nm, Ngl):
-    """ppm_util_rank{2,3}d: returns (info, lpdx, lhbx) with 1-based entries."""
+    """ppm_util_rank{2,3}d: returns (info, lpdx, lhbx) with 1-based entries.
+    float32 positions select ppm_util_rank{2,3}d_s (bounds and spacing in FP32)."""
     _check(xp)
+    k = _kind(xp)
     dim = len(Nm)
     nbox = 1
     for a in range(dim):
@@ -322,9 +324,10 @@ def ppm_util_rank(xp, Np, xmin, xmax, Nm, Ngl):
     lhbx = np.zeros(nbox + 1, dtype=np.int32)
     ic = C.c_int64(0)
     info = C.c_int(0)
-    xmin = np.ascontiguousarray(xmin, dtype=np.float64)
-    xmax = np.ascontiguousarray(xmax, dtype=np.float64)
-    getattr(lib(), f"ppmg_util_rank{dim}d_d")(
+    ft = np.float64 if k == "d" else np.float32
+    xmin = np.ascontiguousarray(xmin, dtype=ft)
+    xmax = np.ascontiguousarray(xmax, dtype=ft)
+    getattr(lib(), f"ppmg_util_rank{dim}d_{k}")(
         _addr(xp), xp.shape[0], int(Np), xmin.ctypes.data, xmax.ctypes.data, int_array(Nm),
         int_array(Ngl), lpdx.ctypes.data, lhbx.ctypes.data, C.byref(ic), C.byref(info))
     return info.value, lpdx[: ic.value], lhbx

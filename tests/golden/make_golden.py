@@ -108,12 +108,20 @@ def m2p_exact(xp, F, lo, hi, nc, kernel, quirk=True):
     return out
 
 
-def rank_py(xp, xmin, xmax, Nm, Ngl):
-    """Plain restatement of ppm_util_rank{2,3}d (1-based lpdx, lhbx)."""
+def rank_py(xp, xmin, xmax, Nm, Ngl, single=False):
+    """Plain restatement of ppm_util_rank{2,3}d (1-based lpdx, lhbx); single:
+    the _s variant, every operation rounded to FP32 (numpy float32 scalars)."""
     dim, npart = xp.shape
     Nt = [Nm[a] + Ngl[a] + Ngl[dim + a] for a in range(dim)]
     nbox = int(np.prod(Nt))
-    rd = [Nm[a] / (xmax[a] - xmin[a]) for a in range(dim)]
+    if single:
+        f = np.float32
+        xp = xp.astype(np.float32)
+        xmin = [f(v) for v in xmin]
+        xmax = [f(v) for v in xmax]
+        rd = [f(Nm[a]) / (xmax[a] - xmin[a]) for a in range(dim)]
+    else:
+        rd = [Nm[a] / (xmax[a] - xmin[a]) for a in range(dim)]
     pbox = []
     for p in range(npart):
         c = []
@@ -206,6 +214,33 @@ def main():
         lpdx, lhbx = rank_py(xp, xmin, xmax, Nm, Ngl)
         cases.append(dict(kind="rank", name=f"rank{dim}d", dim=dim, xmin=xmin, xmax=xmax, Nm=Nm,
                           Ngl=Ngl, xp=xp.T.tolist(), lpdx=lpdx, lhbx=lhbx))
+
+    # single-precision ranking (ppm_util_rank{2,3}d_s) on a box whose FP32
+    # cell spacing rounds: particles on the FP32 cell faces, one ulp either
+    # side of them, on and beyond the upper face, in the lower ghost layer
+    for dim in (2, 3):
+        npart = 240
+        xmin = [0.1, -0.3, 0.25][:dim]
+        xmax = [0.7, 0.9, 1.0][:dim]
+        Nm = [7, 9, 6][:dim]
+        Ngl = [1] * (2 * dim)
+        f32 = np.float32
+        xp = (np.array(xmin)[:, None] + rng.random((dim, npart)) *
+              (np.array(xmax) - np.array(xmin))[:, None]).astype(np.float32)
+        for a in range(dim):
+            h = (f32(xmax[a]) - f32(xmin[a])) / f32(Nm[a])
+            faces = np.array([f32(xmin[a]) + f32(k) * h for k in range(Nm[a] + 1)], np.float32)
+            sel = faces[rng.integers(0, Nm[a] + 1, 60)]
+            xp[a, :60] = sel
+            xp[a, 60:90] = np.nextafter(sel[:30], np.float32(np.inf))
+            xp[a, 90:120] = np.nextafter(sel[30:], np.float32(-np.inf))
+        xp[:, 120:125] = np.array(xmax, np.float32)[:, None]
+        xp[0, 125:130] = np.float32(xmax[0] + 0.5)
+        xp[:, 130:135] = (np.array(xmin) - 0.01).astype(np.float32)[:, None]
+        lpdx, lhbx = rank_py(xp, xmin, xmax, Nm, Ngl, single=True)
+        cases.append(dict(kind="rank", name=f"rank{dim}d_s", prec="s", dim=dim, xmin=xmin,
+                          xmax=xmax, Nm=Nm, Ngl=Ngl, xp=xp.astype(np.float64).T.tolist(),
+                          lpdx=lpdx, lhbx=lhbx))
 
     with open(OUT, "w") as fh:
         json.dump(dict(generator="tests/golden/make_golden.py", seed=1234, cases=cases), fh,

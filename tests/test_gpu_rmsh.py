@@ -107,7 +107,8 @@ def test_ghost_get_put_match_oracle(dim, lda):
 
 @pytest.mark.parametrize("case", golden_cases("rank"), ids=lambda c: c["name"])
 def test_util_rank_bit_exact(case):
-    xp = np.asfortranarray(np.array(case["xp"]).T)
+    xp = np.asfortranarray(np.array(case["xp"]).T,
+                           dtype=np.float32 if case.get("prec") == "s" else np.float64)
     info, lpdx, lhbx = ppmg.ppm_util_rank(xp, xp.shape[1], case["xmin"], case["xmax"],
                                           case["Nm"], case["Ngl"])
     assert info == 0, ppmg.last_error()
@@ -324,3 +325,21 @@ def test_single_precision_remeshing_device_twins():
     torch.cuda.synchronize()
     assert ud.dtype == torch.float32
     assert np.array_equal(host(ud), uh) and np.array_equal(host(xd), xh)
+
+
+@pytest.mark.parametrize("dim", [3, 2])
+def test_util_rank_single_large_bit_exact(dim):
+    """ppm_util_rank{2,3}d_s on 200k FP32 positions over a box whose FP32 cell
+    spacing rounds (crowded cell included) equals the oracle's single routine."""
+    rng = np.random.default_rng(75 + dim)
+    xmin = np.array([0.1, -0.3, 0.25][:dim], dtype=np.float32)
+    xmax = np.array([0.7, 0.9, 1.0][:dim], dtype=np.float32)
+    Nm = [37, 41, 29][:dim]
+    Ngl = [1] * (2 * dim)
+    xp = (xmin[:, None] + rng.random((dim, 200000)) * (xmax - xmin)[:, None]).astype(np.float32)
+    xp[:, :2000] = ((xmin + xmax) / 2)[:, None]
+    xp = np.asfortranarray(xp)
+    info, lpdx, lhbx = ppmg.ppm_util_rank(xp, xp.shape[1], xmin, xmax, Nm, Ngl)
+    assert info == 0, ppmg.last_error()
+    ref_l, ref_h, _ = O.rank(xp, xmin, xmax, Nm, Ngl)
+    assert np.array_equal(lpdx, ref_l) and np.array_equal(lhbx, ref_h)
