@@ -179,6 +179,9 @@ void ppmg_map_field_ghost_s(float* field_up, int64_t ldf, int lda, const int64_t
 void ppmg_map_field_ghost_d_dev(double* field_up, int64_t ldf, int lda, const int64_t* f_lb,
                                 const int64_t* f_ub, int topo_id, int mesh_id,
                                 const int* ghostsize, int maptype, int* info, void* stream);
+void ppmg_map_field_ghost_s_dev(float* field_up, int64_t ldf, int lda, const int64_t* f_lb,
+                                const int64_t* f_ub, int topo_id, int mesh_id,
+                                const int* ghostsize, int maptype, int* info, void* stream);
 
 /* ---- ppm_rmsh_comp_weights (ppm/src/ppm_rmsh_comp_weights.f:96-103) ------
  * Computes the per-particle 1D weights and keeps them (with the particle

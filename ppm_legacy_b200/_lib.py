@@ -41,6 +41,7 @@ SIGNATURES = {
     "ppmg_map_field_ghost_d": (_GHOST, None),
     "ppmg_map_field_ghost_s": (_GHOST, None),
     "ppmg_map_field_ghost_d_dev": (_GHOST + [_vp], None),
+    "ppmg_map_field_ghost_s_dev": (_GHOST + [_vp], None),
     "ppmg_rmsh_comp_weights_d": ([_pd, _i64, _i64, _i, _i, _i, _pd, _pd, _pd, _pi], None),
     "ppmg_rmsh_comp_weights_d_dev": ([_pd, _i64, _i64, _i, _i, _i, _pd, _pd, _pd, _pi, _vp],
                                      None),

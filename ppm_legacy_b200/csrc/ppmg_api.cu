@@ -953,10 +953,11 @@ void ppmg_map_field_ghost_s(float* field_up, int64_t ldf, int lda, const int64_t
   ghost_host<float>(field_up, ldf, lda, f_lb, f_ub, topo_id, mesh_id, ghostsize, maptype, info,
                     "ppmg_map_field_ghost_s");
 }
-void ppmg_map_field_ghost_d_dev(double* field_up, int64_t ldf, int lda, const int64_t* f_lb,
-                                const int64_t* f_ub, int topo_id, int mesh_id,
-                                const int* ghostsize, int maptype, int* info, void* stream) {
-  const char* caller = "ppmg_map_field_ghost_d_dev";
+extern "C++" {
+template <class T>
+static void ghost_dev(T* field_up, int64_t ldf, int lda, const int64_t* f_lb, const int64_t* f_ub,
+                      int topo_id, int mesh_id, const int* ghostsize, int maptype, int* info,
+                      cudaStream_t stream, const char* caller) {
   clear_error();
   if (info) *info = 0;
   Handle* hh = find_handle(topo_id, mesh_id);
@@ -965,8 +966,21 @@ void ppmg_map_field_ghost_d_dev(double* field_up, int64_t ldf, int lda, const in
   if (!h) return;
   if (lda < 1 || ldf < lda) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": lda inconsistent"); return; }
   std::lock_guard<std::mutex> lk(h->mu);
-  ghost_pipeline<double>(*h, field_up, ldf, lda, f_lb, f_ub, ghostsize, maptype,
-                         (cudaStream_t)stream, info, caller);
+  ghost_pipeline<T>(*h, field_up, ldf, lda, f_lb, f_ub, ghostsize, maptype, stream, info, caller);
+}
+}  // extern "C++"
+
+void ppmg_map_field_ghost_d_dev(double* field_up, int64_t ldf, int lda, const int64_t* f_lb,
+                                const int64_t* f_ub, int topo_id, int mesh_id,
+                                const int* ghostsize, int maptype, int* info, void* stream) {
+  ghost_dev<double>(field_up, ldf, lda, f_lb, f_ub, topo_id, mesh_id, ghostsize, maptype, info,
+                    (cudaStream_t)stream, "ppmg_map_field_ghost_d_dev");
+}
+void ppmg_map_field_ghost_s_dev(float* field_up, int64_t ldf, int lda, const int64_t* f_lb,
+                                const int64_t* f_ub, int topo_id, int mesh_id,
+                                const int* ghostsize, int maptype, int* info, void* stream) {
+  ghost_dev<float>(field_up, ldf, lda, f_lb, f_ub, topo_id, mesh_id, ghostsize, maptype, info,
+                   (cudaStream_t)stream, "ppmg_map_field_ghost_s_dev");
 }
 
 // ---- comp_weights / remesh ---------------------------------------------------

@@ -185,9 +185,7 @@ def ppm_map_field_ghost(field_up, *args, field_lb=None):
          int(maptype), C.byref(info))
     k = _kind(field_up)
     if _is_dev(field_up):
-        if k != "d":
-            raise TypeError("device ghost mapping supports float64 fields")
-        lib().ppmg_map_field_ghost_d_dev(*a, _stream())
+        getattr(lib(), f"ppmg_map_field_ghost_{k}_dev")(*a, _stream())
     else:
         getattr(lib(), f"ppmg_map_field_ghost_{k}")(*a)
     return info.value

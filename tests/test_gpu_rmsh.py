@@ -343,3 +343,30 @@ def test_util_rank_single_large_bit_exact(dim):
     assert info == 0, ppmg.last_error()
     ref_l, ref_h, _ = O.rank(xp, xmin, xmax, Nm, Ngl)
     assert np.array_equal(lpdx, ref_l) and np.array_equal(lhbx, ref_h)
+
+
+@pytest.mark.parametrize("maptype", ["put", "get"])
+def test_ghost_single_device_twin_matches_host(maptype):
+    """ppmg_map_field_ghost_s_dev on a float32 torch field equals the host
+    ppmg_map_field_ghost_s bit for bit (and the oracle within FP32 rounding)."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(130)
+    nc = 9
+    t = registered(3, nc)
+    g = [2, 1, 3]
+    lb, ub = box_bounds(t, g)
+    F = rng.standard_normal((2,) + tuple(ub[a] - lb[a] + 1 for a in range(3)) + (1,))
+    F = np.asfortranarray(F.astype(np.float32))
+    mt = getattr(ppmg.params, f"ppm_param_map_ghost_{maptype}")
+    Fh = F.copy(order="F")
+    assert ppmg.ppm_map_field_ghost(Fh, 2, t.topo_id, t.mesh_id, g, mt) == 0, ppmg.last_error()
+    d = torch.from_numpy(np.ascontiguousarray(F.T)).cuda()
+    Fd = d.permute(*reversed(range(d.dim())))
+    assert ppmg.ppm_map_field_ghost(Fd, 2, t.topo_id, t.mesh_id, g, mt) == 0, ppmg.last_error()
+    assert ppmg.sync_status(t.topo_id, t.mesh_id) == 0
+    got = Fd.permute(*reversed(range(Fd.dim()))).contiguous().cpu().numpy().T
+    assert got.dtype == np.float32 and np.array_equal(got, Fh)
+    if maptype == "put":
+        Fo = F.astype(np.float64, order="F")
+        O.ghost_put(t, Fo, lb, ub, g)
+        assert max_rel(Fh.astype(np.float64), Fo) < 1e-6
