@@ -248,6 +248,26 @@ __global__ void __launch_bounds__(256) k_adjoint3d(M2PParams P) {
 // derivative weights scaled by the inverse mesh spacing (all LC = lda
 // components in one launch).
 // --------------------------------------------------------------------------
+// One particle's LC results to up(c0:c0+LC-1, p).  Rows land at random
+// addresses, so every store is a separate L2 request: three FP64 values go
+// as one 16-byte and one 8-byte store (the row starts 8 or 16 bytes past a
+// 16-byte boundary; which of the two pairs is aligned follows from it).
+template <class FT, class CT, int LC>
+__device__ __forceinline__ void store_row(FT* out, const CT* acc) {
+  if constexpr (sizeof(FT) == 8 && LC == 3) {
+    if ((reinterpret_cast<uintptr_t>(out) & 15) == 0) {
+      *reinterpret_cast<double2*>(out) = make_double2((double)acc[0], (double)acc[1]);
+      out[2] = (FT)acc[2];
+    } else {
+      out[0] = (FT)acc[0];
+      *reinterpret_cast<double2*>(out + 1) = make_double2((double)acc[1], (double)acc[2]);
+    }
+  } else {
+#pragma unroll
+    for (int a = 0; a < LC; ++a) out[a] = (FT)acc[a];
+  }
+}
+
 template <int S, class CT, bool EXACT, class FT, int LC, bool ADJ = false>
 __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
   using V = typename Vec4<CT>::type;
@@ -430,14 +450,13 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
           CT g[3] = {CT(0), CT(0), CT(0)};
 #pragma unroll
           for (int a = 0; a < LC; ++a) {
-            out[a] = (FT)acc[a];
 #pragma unroll
             for (int d = 0; d < 3; ++d) g[d] = fma(ua[a], ga[a][d], g[d]);
           }
-          double* gx = P.dx + (int64_t)idcur * P.lddx;
-#pragma unroll
-          for (int d = 0; d < 3; ++d) gx[d] = (double)g[d];
+          store_row<FT, CT, LC>(out, acc);
+          store_row<double, CT, 3>(P.dx + (int64_t)idcur * P.lddx, g);
         } else if constexpr (EXACT) {
+          CT res[LC];
 #pragma unroll
           for (int a = 0; a < LC; ++a) {
             CT acc = CT(0);
@@ -451,8 +470,9 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
                 for (int kk = 0; kk < S; ++kk)
                   acc = radd(acc, rmul(rmul(wij, wz[kk]), col[slot_k[kk] * LC]));
               }
-            out[a] = (FT)acc;
+            res[a] = acc;
           }
+          store_row<FT, CT, LC>(out, res);
         } else {
           CT acc[LC];
 #pragma unroll
@@ -471,8 +491,7 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
                 acc[a] = fma(wij, part, acc[a]);
               }
             }
-#pragma unroll
-          for (int a = 0; a < LC; ++a) out[a] = (FT)acc[a];
+          store_row<FT, CT, LC>(out, acc);
         }
       }
       rcur = rnext;
