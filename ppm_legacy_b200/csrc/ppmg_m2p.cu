@@ -255,12 +255,13 @@ __global__ void __launch_bounds__(256) k_adjoint3d(M2PParams P) {
 template <class FT, class CT, int LC>
 __device__ __forceinline__ void store_row(FT* out, const CT* acc) {
   if constexpr (sizeof(FT) == 8 && LC == 3) {
+    double* o = reinterpret_cast<double*>(out);
     if ((reinterpret_cast<uintptr_t>(out) & 15) == 0) {
-      *reinterpret_cast<double2*>(out) = make_double2((double)acc[0], (double)acc[1]);
-      out[2] = (FT)acc[2];
+      __stcs(reinterpret_cast<double2*>(o), make_double2((double)acc[0], (double)acc[1]));
+      __stcs(o + 2, (double)acc[2]);
     } else {
-      out[0] = (FT)acc[0];
-      *reinterpret_cast<double2*>(out + 1) = make_double2((double)acc[1], (double)acc[2]);
+      __stcs(o, (double)acc[0]);
+      __stcs(reinterpret_cast<double2*>(o + 1), make_double2((double)acc[1], (double)acc[2]));
     }
   } else {
 #pragma unroll

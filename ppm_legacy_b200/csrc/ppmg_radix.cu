@@ -383,8 +383,8 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
         const int kk = skeys[li];
         const int d = digit_of<FIRST>(kk, A.shift, mask, nb, A.ncell);
         gdst[q] = run[d] + (j - dst[d]);
-        A.key_out[gdst[q]] = kk;
-        if (FIRST) A.id_out[gdst[q]] = (int)(base + li);
+        __stcs(A.key_out + gdst[q], kk);
+        if (FIRST) __stcs(A.id_out + gdst[q], (int)(base + li));
       }
     }
     __syncthreads();
@@ -397,13 +397,13 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
         const int* sid = reinterpret_cast<const int*>(sb);
 #pragma unroll
         for (int q = 0; q < kRItems; ++q)
-          if (gdst[q] >= 0) A.id_out[gdst[q]] = sid[inv[tid + q * kRThreads]];
+          if (gdst[q] >= 0) __stcs(A.id_out + gdst[q], sid[inv[tid + q * kRThreads]]);
       } else {
         uint4* out = pl < A.rplanes ? A.rec_out + (int64_t)pl * A.np
                                     : A.us_out + (int64_t)(pl - A.rplanes) * A.np;
 #pragma unroll
         for (int q = 0; q < kRItems; ++q)
-          if (gdst[q] >= 0) out[gdst[q]] = sb[inv[tid + q * kRThreads]];
+          if (gdst[q] >= 0) __stcs(out + gdst[q], sb[inv[tid + q * kRThreads]]);
       }
       __syncthreads();
       if (tid == 0) issue_plane(u + 2);
