@@ -19,7 +19,7 @@
 namespace ppmg {
 namespace {
 
-constexpr int kCThreads = 256;                  // count kernel
+constexpr int kCThreads = 512;                  // count kernel (full occupancy in one wave)
 constexpr int kRThreads = 1024;                 // move kernel
 constexpr int kRWarps = kRThreads / 32;
 constexpr int kRItems = 4;                      // items per thread and sub-tile

@@ -123,6 +123,8 @@ template <class T>
 __global__ void k_hash(const T* __restrict__ xp, int64_t ldxp, int64_t np, int dim,
                        unsigned long long* __restrict__ hash) {
   unsigned long long hacc = 0;
+  // unrolled: the loads of several particles are in flight at once
+#pragma unroll 4
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np;
        p += (int64_t)gridDim.x * blockDim.x)
     hacc += particle_hash<T>(xp + p * ldxp, dim, p);
