@@ -269,17 +269,35 @@ __device__ __forceinline__ void store_row(FT* out, const CT* acc) {
   }
 }
 
+// Cell layers gathered per step of the z sweep (one barrier per step) and
+// the node-plane ring that takes: the S + LPS - 1 planes the step reads and
+// the LPS planes being filled for the next step.  Two layers per step for
+// FP32 rings (at ~1 particle per cell a layer gives each thread only ~2
+// particles between barriers); one for FP64 rings, whose gather is
+// arithmetic-bound.
+template <int S, class CT, int LC>
+constexpr int m2p_layers() {
+  return sizeof(CT) == 4 ? 2 : 1;
+}
+
+template <int S, class CT, int LC>
+constexpr size_t m2p_ring_bytes() {
+  return (size_t)(kTileX + S - 1) * (kTileY + S - 1) * (S + 2 * m2p_layers<S, CT, LC>() - 1) *
+         LC * sizeof(CT);
+}
+
 template <int S, class CT, bool EXACT, class FT, int LC, bool ADJ = false>
 __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
   using V = typename Vec4<CT>::type;
   constexpr int HL = S / 2;
-  constexpr int HH = S / 2 - 1;
   constexpr int WX = kTileX + S - 1;
   constexpr int WY = kTileY + S - 1;
   constexpr int NCOL = WX * WY;
-  constexpr int R = S + 1;                     // ring slots: S in use + 1 being filled
+  constexpr int LPS = m2p_layers<S, CT, LC>();  // cell layers per step
+  constexpr int R = S + 2 * LPS - 1;           // ring slots
   constexpr int CS = R * LC;                   // CT values per node column
   constexpr int PER = (NCOL + 255) / 256;      // columns per thread when loading a plane
+  static_assert(16 * LPS <= 32, "row tables are loaded by the first warp");
 
   if ((int)blockIdx.x >= *P.nitems) return;
   const int4 it = P.items[blockIdx.x];
@@ -292,7 +310,8 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
 
   extern __shared__ __align__(16) unsigned char smem[];
   CT* ring = reinterpret_cast<CT*>(smem);  // [NCOL][R][LC]
-  __shared__ int rbeg[2][kTileY], rpre[2][kTileY + 1];
+  // row tables of the step's LPS layers and of the next step's (double buffered)
+  __shared__ int rbeg[2 * LPS][kTileY], rpre[2 * LPS][kTileY + 1];
 
   const int tid = threadIdx.x;
   const FT* F = static_cast<const FT*>(P.field);
@@ -308,32 +327,41 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
   auto plane_oz = [&](int z) {
     return (int64_t)(wrap_index(z, P.N[2]) + 1 - P.fd.lb[2]) * P.fd.s[2];
   };
-  // row ranges of cell layer cz: thread t < 16 loads row t
+  // row ranges of cell layers cz .. cz+LPS-1: thread 16 l + r loads row r of
+  // layer cz + l
   auto row_load = [&](int cz, int& b, int& n) {
     b = 0;
     n = 0;
-    if (tid < YW && cz < Z1) {
-      const int64_t c0 = (int64_t)X0 + (int64_t)P.N[0] * (Y0 + tid + (int64_t)P.N[1] * cz);
+    const int l = tid >> 4, r = tid & 15;
+    if (tid < 16 * LPS && r < YW && cz + l < Z1) {
+      const int64_t c0 =
+          (int64_t)X0 + (int64_t)P.N[0] * (Y0 + r + (int64_t)P.N[1] * (cz + l));
       b = P.start[c0];
       n = P.start[c0 + XW] - b;
     }
   };
-  auto row_store = [&](int buf, int b, int n) {
-    if (tid < kTileY) {
-      rbeg[buf][tid] = b;
+  // row tables base .. base+LPS-1 from the loaded ranges (inclusive scan per
+  // group of 16 lanes)
+  auto row_store = [&](int base, int b, int n) {
+    if (tid < 32) {
+      const int l = tid >> 4, r = tid & 15;
       int inc = n;
 #pragma unroll
       for (int o = 1; o < kTileY; o <<= 1) {
-        const int t = __shfl_up_sync(0x0000ffffu, inc, o);
-        if (tid >= o) inc += t;
+        const int t = __shfl_up_sync(0xffffffffu, inc, o, 16);
+        if (r >= o) inc += t;
       }
-      rpre[buf][tid + 1] = inc;
-      if (tid == 0) rpre[buf][0] = 0;
+      if (l < LPS) {
+        rbeg[base + l][r] = b;
+        rpre[base + l][r + 1] = inc;
+        if (r == 0) rpre[base + l][0] = 0;
+      }
     }
   };
 
-  // prologue: planes Z0-(HL-1) .. Z0+HH+1 (the S planes of layer Z0) and its rows
-  for (int z = Z0 - (HL - 1); z <= Z0 + HH + 1; ++z) {
+  // prologue: planes Z0-(HL-1) .. Z0+LPS-1+HL (the planes of the first
+  // step's layers) and their rows
+  for (int z = Z0 - (HL - 1); z <= Z0 + LPS - 1 + HL; ++z) {
     const int slot = wrap_index(z, R);
     const int64_t oz = plane_oz(z);
     for (int q = tid; q < NCOL; q += 256) {
@@ -346,64 +374,75 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
   {
     int b, n;
     row_load(Z0, b, n);
-    row_store(Z0 & 1, b, n);
+    row_store(0, b, n);
   }
   __syncthreads();
 
   FT* up = static_cast<FT*>(P.up);
   const V* rec = static_cast<const V*>(P.rec);
 
-  for (int cz = Z0; cz < Z1; ++cz) {
-    const int buf = cz & 1;
-    // prefetch the next layer's new plane and rows into registers
-    const bool more = cz + 1 < Z1;
-    const int zn = cz + HH + 2;
-    CT pre[PER][LC];
+  for (int cz = Z0, step = 0; cz < Z1; cz += LPS, ++step) {
+    const int cb = (step & 1) * LPS;  // row tables of this step's layers
+    // prefetch the next step's new planes and rows into registers
+    const bool more = cz + LPS < Z1;
+    CT pre[LPS][PER][LC];
     if (more) {
-      const int64_t oz = plane_oz(zn);
 #pragma unroll
-      for (int k = 0; k < PER; ++k) {
-        const int q = tid + 256 * k;
-        if (q < NCOL) {
-          const int64_t o = col_off(q, oz);
+      for (int l = 0; l < LPS; ++l) {
+        const int64_t oz = plane_oz(cz + LPS + HL + l);
 #pragma unroll
-          for (int a = 0; a < LC; ++a) pre[k][a] = (CT)__ldg(F + o + a);
+        for (int k = 0; k < PER; ++k) {
+          const int q = tid + 256 * k;
+          if (q < NCOL) {
+            const int64_t o = col_off(q, oz);
+#pragma unroll
+            for (int a = 0; a < LC; ++a) pre[l][k][a] = (CT)__ldg(F + o + a);
+          }
         }
       }
     }
     int nb, nn;
-    row_load(cz + 1, nb, nn);
+    row_load(cz + LPS, nb, nn);
 
-    const int ntot = rpre[buf][kTileY];
-    int slot_k[S];
-#pragma unroll
-    for (int k = 0; k < S; ++k) slot_k[k] = wrap_index(cz - (HL - 1) + k, R);
+    // the step's particles: layer 0's rows, then layer 1's
+    const int n0 = rpre[cb][kTileY];
+    const int ntot = n0 + (LPS > 1 ? rpre[cb + LPS - 1][kTileY] : 0);
     // software-pipelined particle loop: the next record is loaded while the
     // current particle is gathered
-    auto locate = [&](int i, int& r) {
+    auto locate = [&](int i, int& r, int& l) {
+      l = (LPS > 1 && i >= n0) ? 1 : 0;
+      const int j = i - (l ? n0 : 0);
+      const int tb = cb + l;
       r = 0;
 #pragma unroll
-      for (int t = 1; t < kTileY; ++t) r += (i >= rpre[buf][t]) ? 1 : 0;
-      return (int64_t)rbeg[buf][r] + (i - rpre[buf][r]);
+      for (int t = 1; t < kTileY; ++t) r += (j >= rpre[tb][t]) ? 1 : 0;
+      return (int64_t)rbeg[tb][r] + (j - rpre[tb][r]);
     };
-    int rcur = 0, idcur = 0;
+    int rcur = 0, idcur = 0, lcur = 0;
     int64_t scur = 0;
     V rvcur;
     if (tid < ntot) {
-      scur = locate(tid, rcur);
+      scur = locate(tid, rcur, lcur);
       rvcur = load_vec(rec, scur, P.nvalid);
       idcur = P.idx[scur];
     }
     for (int i = tid; i < ntot; i += 256) {
-      int rnext = 0, idnext = 0;
+      int rnext = 0, idnext = 0, lnext = 0;
       int64_t snext = 0;
       V rvnext;
       if (i + 256 < ntot) {
-        snext = locate(i + 256, rnext);
+        snext = locate(i + 256, rnext, lnext);
         rvnext = load_vec(rec, snext, P.nvalid);
         idnext = P.idx[snext];
       }
       {
+        // ring slots of the S planes of this particle's layer
+        int slot_k[S];
+        {
+          const int s0 = wrap_index(cz + lcur - (HL - 1), R);
+#pragma unroll
+          for (int k = 0; k < S; ++k) slot_k[k] = s0 + k < R ? s0 + k : s0 + k - R;
+        }
         int cell;
         if constexpr (sizeof(CT) == 4) cell = __float_as_int(rvcur.w); else cell = (int)rvcur.w;
         const int qx0 = cell % P.N[0] - X0;  // local column of the first stencil node
@@ -499,29 +538,33 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
       scur = snext;
       rvcur = rvnext;
       idcur = idnext;
+      lcur = lnext;
     }
-    // publish the prefetched plane (its slot is not read by this layer) and rows
+    // publish the prefetched planes (their slots are not read by this step)
+    // and rows
     if (more) {
-      const int slot = wrap_index(zn, R);
 #pragma unroll
-      for (int k = 0; k < PER; ++k) {
-        const int q = tid + 256 * k;
-        if (q < NCOL) {
-          CT* d = ring + (size_t)q * CS + slot * LC;
+      for (int l = 0; l < LPS; ++l) {
+        const int slot = wrap_index(cz + LPS + HL + l, R);
 #pragma unroll
-          for (int a = 0; a < LC; ++a) d[a] = pre[k][a];
+        for (int k = 0; k < PER; ++k) {
+          const int q = tid + 256 * k;
+          if (q < NCOL) {
+            CT* d = ring + (size_t)q * CS + slot * LC;
+#pragma unroll
+            for (int a = 0; a < LC; ++a) d[a] = pre[l][k][a];
+          }
         }
       }
     }
-    row_store(buf ^ 1, nb, nn);
+    row_store(cb ^ LPS, nb, nn);
     __syncthreads();
   }
 }
 
 template <int S, class CT, bool EXACT, class FT>
 cudaError_t launch_tile_lc(const M2PParams& P, int lc, cudaStream_t st) {
-  auto go = [&](auto kern, int LCv) {
-    const size_t smem = (size_t)(kTileX + S - 1) * (kTileY + S - 1) * (S + 1) * LCv * sizeof(CT);
+  auto go = [&](auto kern, size_t smem) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e) return e;
@@ -529,10 +572,10 @@ cudaError_t launch_tile_lc(const M2PParams& P, int lc, cudaStream_t st) {
     return cudaGetLastError();
   };
   switch (lc) {
-    case 1: return go(k_m2p3d_tile<S, CT, EXACT, FT, 1>, 1);
-    case 2: return go(k_m2p3d_tile<S, CT, EXACT, FT, 2>, 2);
-    case 3: return go(k_m2p3d_tile<S, CT, EXACT, FT, 3>, 3);
-    default: return go(k_m2p3d_tile<S, CT, EXACT, FT, 4>, 4);
+    case 1: return go(k_m2p3d_tile<S, CT, EXACT, FT, 1>, m2p_ring_bytes<S, CT, 1>());
+    case 2: return go(k_m2p3d_tile<S, CT, EXACT, FT, 2>, m2p_ring_bytes<S, CT, 2>());
+    case 3: return go(k_m2p3d_tile<S, CT, EXACT, FT, 3>, m2p_ring_bytes<S, CT, 3>());
+    default: return go(k_m2p3d_tile<S, CT, EXACT, FT, 4>, m2p_ring_bytes<S, CT, 4>());
   }
 }
 
@@ -593,7 +636,7 @@ cudaError_t launch_m2p(const M2PParams& P0, int dim, int kernel, M2PPrec prec, c
 template <int S, class CT, int LC>
 cudaError_t launch_adjoint_tile(const M2PParams& P, cudaStream_t st) {
   auto kern = k_m2p3d_tile<S, CT, false, double, LC, true>;
-  const size_t smem = (size_t)(kTileX + S - 1) * (kTileY + S - 1) * (S + 1) * LC * sizeof(CT);
+  const size_t smem = m2p_ring_bytes<S, CT, LC>();
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e) return e;
