@@ -71,6 +71,17 @@ void ppmg_mesh_register(int topo_id, int mesh_id, int dim, const double* min_phy
                         const double* min_sub, const double* max_sub, const int* subs_bc,
                         const int* istart, const int* nnodes, int* info);
 void ppmg_mesh_unregister(int topo_id, int mesh_id, int* info);
+/* The subdomain (0-based isub) this GPU computes on: the one-entry
+ * ppm_isublist of the process (ppm/src/ppm_topo_mkfield.f:311-319 builds the
+ * reference's per-process sub list).  Required when nsubs > 1.  Supported
+ * decomposition: slabs along z, every subdomain spanning x and y.  On a
+ * slab the 3D P2M and M2P compute on the local sub with z not periodic:
+ * P2M leaves in its z ghost planes the contributions owed to the
+ * neighbouring slabs, M2P reads its z ghost planes; the exchange between the
+ * slabs (the ghost put / get of ppm_map_field_ghost, ppm_map_field_send.f)
+ * is the caller's, e.g. ppm_legacy_b200.halo over torch.distributed.  Other
+ * routines return info = -2 (errno 503) on a slab. */
+void ppmg_mesh_set_local_sub(int topo_id, int mesh_id, int isub, int* info);
 
 /* Wait for all work of the handle's `_dev` calls on `stream` and return the
  * data-dependent status latched since the last call (info/errno as above). */

@@ -35,6 +35,7 @@ SIGNATURES = {
     "ppmg_mesh_register": ([_i, _i, _i, _pd, _pd, _pi, _pi, _i, _pd, _pd, _pi, _pi, _pi, _pi],
                            None),
     "ppmg_mesh_unregister": ([_i, _i, _pi], None),
+    "ppmg_mesh_set_local_sub": ([_i, _i, _i, _pi], None),
     "ppmg_sync_status": ([_i, _i, _vp, _pi], None),
     "ppmg_interp_p2m_adjoint_dv_3d": (_ADJ, None),
     "ppmg_interp_p2m_adjoint_dv_3d_dev": (_ADJ + [_vp], None),

@@ -49,6 +49,12 @@ struct Handle {
   int bcdef[6] = {0, 0, 0, 0, 0, 0};
   std::vector<double> min_sub, max_sub;
   std::vector<int> subs_bc, istart, nnodes;
+  // the subdomain this GPU computes on (ppm_isublist of one entry): -1 until
+  // ppmg_mesh_set_local_sub when nsubs > 1
+  int local_sub = 0;
+  // the local subdomain is one z-slab of the domain: z is not periodic
+  // within it, its neighbours' slabs hold the ghost nodes' owners
+  bool open_z = false;
   Geom g{};
   Workspace ws;       // P2M / M2P / adjoint / ghost / clist scratch
   Workspace ws_rmsh;  // comp_weights -> remesh state (ppm_module_data_rmsh)
@@ -108,7 +114,8 @@ Handle* find_handle(int topo_id, int mesh_id) {
 
 // Checks shared by every hot-path entry point (the ppm_debug > 0 checks of
 // ppm_interp_p2m.f:338-410, always on here).
-Handle* get_checked(int topo_id, int mesh_id, int dim, const char* caller, int* info) {
+Handle* get_checked(int topo_id, int mesh_id, int dim, const char* caller, int* info,
+                    bool slab_ok = false) {
   Handle* h = find_handle(topo_id, mesh_id);
   if (!h) {
     fail(info, kErrorError, kErrArgument, std::string(caller) + ": topo_id/mesh_id is invalid");
@@ -119,9 +126,17 @@ Handle* get_checked(int topo_id, int mesh_id, int dim, const char* caller, int* 
          std::string(caller) + ": routine dimension does not match the registered mesh");
     return nullptr;
   }
-  if (h->nsubs != 1) {
+  if (h->local_sub < 0) {
     fail(info, kErrorError, kErrArgument,
-         std::string(caller) + ": one subdomain per GPU is supported (nsubs must be 1)");
+         std::string(caller) +
+             ": nsubs > 1: select this GPU's subdomain with ppmg_mesh_set_local_sub");
+    return nullptr;
+  }
+  if (h->open_z && !slab_ok) {
+    fail(info, kErrorError, kErrArgument,
+         std::string(caller) +
+             ": a z-slab subdomain is supported by the 3D P2M and M2P; this routine needs one "
+             "periodic subdomain per GPU");
     return nullptr;
   }
   for (int f = 0; f < 2 * dim; ++f)
@@ -193,6 +208,7 @@ KeyParams make_kp(const Handle& h, int mode, bool quirk) {
     kp.minf[a] = (float)kp.min[a];
     kp.maxf[a] = (float)kp.max[a];
     kp.dxif[a] = a < h.dim ? (quirk ? h.g.dxiq_f[a] : h.g.dxi_f[a]) : 1.0f;
+    kp.open[a] = a == 2 && h.open_z ? 1 : 0;
   }
   return kp;
 }
@@ -290,7 +306,14 @@ int p2m_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, const T* up, 
   P.us = ws.us.p;
   P.field = field;
   P.fd = fd;
-  if ((e = ws.tiles.ensure(p2m_scratch_bytes(h.dim, P.N)))) return cuda_fail(info, e, caller);
+  if (h.open_z) {
+    // a z-slab: every node plane of the written box 1-g:Nm+g is produced
+    // (ghost planes hold the contributions owed to the neighbouring slabs)
+    P.open_z = 1;
+    P.zlo = lo[2] - 1;
+    P.ze = hi[2] - lo[2] + 1;
+  }
+  if ((e = ws.tiles.ensure(p2m_scratch_bytes(h.dim, P.N, P.ze)))) return cuda_fail(info, e, caller);
   e = launch_p2m(P, h.dim, kernel, prec, lda, Np > 0 ? Np : 1, remesh, ws.tiles.p, st);
   if (e) return cuda_fail(info, e, caller);
   if (!remesh) {
@@ -335,6 +358,13 @@ int m2p_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, T* up, int64_
     lo[a] = 1;
     hi[a] = h.g.N[a];
   }
+  if (h.open_z) {
+    // a z-slab reads the node planes its stencils reach, ghost planes
+    // included (filled from the neighbouring slabs by a ghost get)
+    const int HL = kernel == kKernelMp4 ? 2 : 1;
+    lo[2] = 2 - HL;
+    hi[2] = h.g.N[2] + HL;
+  }
   FieldDesc fd;
   if (!make_fd(h, ldf, f_lb, f_ub, lo, hi, fd, caller, info)) return *info;
   if (Np == 0) return 0;
@@ -347,8 +377,9 @@ int m2p_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, T* up, int64_
   KeyParams kp = make_kp(h, KEY_INTERP_WRAP, true);
   if (!reuse) {
     h.sort_cached = false;
+    // outside a z-slab: unassigned (405); else only non-finite positions fail
     e = sort_interp<T>(h, kp, xp, ldxp, (const T*)nullptr, 0, 0, Np, prec == M2P_FP64,
-                       h.d_status + 1, up, ldup, lda, st);
+                       h.d_status + (h.open_z ? 0 : 1), up, ldup, lda, st);
     if (e) return cuda_fail(info, e, caller);
   }
   const int* dnv = d_nvalid_of(h.ws, h.g.ncell);
@@ -363,10 +394,13 @@ int m2p_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, T* up, int64_
   P.up = up;
   P.ldup = ldup;
   P.lda = lda;
+  P.open_z = h.open_z ? 1 : 0;
   if (h.dim == 3) {
     TileItems ti;
     if ((e = h.ws.tiles.ensure(tile_items_bytes(P.N)))) return cuda_fail(info, e, caller);
-    if (reuse) {
+    // a z-slab's P2M items cover its node planes -g .. nz+g, not M2P's cell
+    // layers: M2P builds its own (the cell order itself is reused)
+    if (reuse && !h.open_z) {
       ti = tile_items_view(h.ws.tiles.p, P.N);
     } else if ((e = make_tile_items(h.ws.start.as<int>(), P.N, Np, h.ws.tiles.p, ti, st))) {
       return cuda_fail(info, e, caller);
@@ -445,7 +479,7 @@ void p2m_host(const T* xp, int64_t ldxp, int64_t Np, const T* up, int64_t ldup, 
   if (Np >= (int64_t)1 << 31) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": Np must be < 2^31"); return; }
   if (!check_kernel(kernel, caller, info)) return;
   if (dim == 2 && kernel != kKernelMp4) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": Only Mp4 is available in 2D"); return; }
-  Handle* h = get_checked(topo_id, mesh_id, dim, caller, info);
+  Handle* h = get_checked(topo_id, mesh_id, dim, caller, info, dim == 3);
   if (!h) return;
   std::lock_guard<std::mutex> lk(h->mu);
   cudaStream_t st = h->stream;
@@ -482,7 +516,7 @@ void p2m_dev(const T* xp, int64_t ldxp, int64_t Np, const T* up, int64_t ldup, i
   }
   if (!check_kernel(kernel, caller, info)) return;
   if (dim == 2 && kernel != kKernelMp4) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": Only Mp4 is available in 2D"); return; }
-  Handle* h = get_checked(topo_id, mesh_id, dim, caller, info);
+  Handle* h = get_checked(topo_id, mesh_id, dim, caller, info, dim == 3);
   if (!h) return;
   std::lock_guard<std::mutex> lk(h->mu);
   p2m_pipeline<T>(*h, xp, ldxp, Np, up, ldup, lda, kernel, ghostsize, field_up, ldf, f_lb,
@@ -502,7 +536,7 @@ void m2p_host(const T* xp, int64_t ldxp, int64_t Np, T* up, int64_t ldup, int ld
   if (lda < 1 || ldup < lda || ldf < lda) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": lda / leading dimensions inconsistent"); return; }
   if (Np >= (int64_t)1 << 31) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": Np must be < 2^31"); return; }
   if (!check_kernel(kernel, caller, info)) return;
-  Handle* h = get_checked(topo_id, mesh_id, dim, caller, info);
+  Handle* h = get_checked(topo_id, mesh_id, dim, caller, info, dim == 3);
   if (!h) return;
   std::lock_guard<std::mutex> lk(h->mu);
   cudaStream_t st = h->stream;
@@ -539,7 +573,7 @@ void m2p_dev(const T* xp, int64_t ldxp, int64_t Np, T* up, int64_t ldup, int lda
     return;
   }
   if (!check_kernel(kernel, caller, info)) return;
-  Handle* h = get_checked(topo_id, mesh_id, dim, caller, info);
+  Handle* h = get_checked(topo_id, mesh_id, dim, caller, info, dim == 3);
   if (!h) return;
   std::lock_guard<std::mutex> lk(h->mu);
   m2p_pipeline<T>(*h, xp, ldxp, Np, up, ldup, lda, kernel, field_up, ldf, f_lb, f_ub, st, info,
@@ -737,6 +771,7 @@ void ppmg_mesh_register(int topo_id, int mesh_id, int dim, const double* min_phy
   h->subs_bc.assign(subs_bc, subs_bc + 6 * nsubs);
   h->istart.assign(istart, istart + 3 * nsubs);
   h->nnodes.assign(nnodes, nnodes + 3 * nsubs);
+  h->local_sub = nsubs == 1 ? 0 : -1;
   Geom& g = h->g;
   g.dim = dim;
   g.ncell = ncell;
@@ -773,6 +808,43 @@ void ppmg_mesh_register(int topo_id, int mesh_id, int dim, const double* min_phy
   if (e) { cuda_fail(info, e, "ppmg_mesh_register"); return; }
   std::lock_guard<std::mutex> lk(g_mu);
   handles()[{topo_id, mesh_id}] = std::move(h);
+}
+
+void ppmg_mesh_set_local_sub(int topo_id, int mesh_id, int isub, int* info) {
+  const char* caller = "ppmg_mesh_set_local_sub";
+  clear_error();
+  if (info) *info = 0;
+  Handle* h = find_handle(topo_id, mesh_id);
+  if (!h) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": topo_id/mesh_id is invalid"); return; }
+  std::lock_guard<std::mutex> lk(h->mu);
+  if (isub < 0 || isub >= h->nsubs) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": isub out of range"); return; }
+  if (h->nsubs > 1) {
+    // supported decomposition: slabs along z, every subdomain spanning the
+    // whole domain in x and y (ppm_param_decomp_zpencil cut along z only)
+    if (h->dim != 3) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": several subdomains are supported in 3D only"); return; }
+    for (int s = 0; s < h->nsubs; ++s)
+      for (int a = 0; a < 2; ++a)
+        if (h->istart[3 * s + a] != 1 || h->nnodes[3 * s + a] != h->Nm[a]) {
+          fail(info, kErrorError, ppmg::kErrArgument,
+               std::string(caller) + ": only a decomposition into z-slabs (each subdomain "
+                                     "spanning x and y) is supported");
+          return;
+        }
+    const int nz = h->nnodes[3 * isub + 2] - 1;
+    if (nz < 1) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": the subdomain has no cell layer"); return; }
+    Geom& g = h->g;
+    g.N[2] = nz;
+    for (int a = 0; a < 3; ++a) {
+      g.min_sub[a] = h->min_sub[3 * isub + a];
+      g.max_sub[a] = h->max_sub[3 * isub + a];
+    }
+    g.ncell = (int64_t)g.N[0] * g.N[1] * g.N[2];
+    h->Nm[2] = nz + 1;
+    h->open_z = true;
+  }
+  h->local_sub = isub;
+  h->sort_cached = false;
+  h->w_valid = false;
 }
 
 void ppmg_mesh_unregister(int topo_id, int mesh_id, int* info) {

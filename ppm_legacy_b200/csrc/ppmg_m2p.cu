@@ -17,6 +17,12 @@ namespace ppmg {
 
 namespace {
 
+// 0-based node plane of stencil plane z: periodic wrap, or (a z-slab) the
+// plane itself, ghost planes included
+__device__ __forceinline__ int zplane(const M2PParams& P, int z) {
+  return P.open_z ? z : wrap_index(z, P.N[2]);
+}
+
 template <int S, class CT, bool EXACT>
 __device__ __forceinline__ void m2p_weights(CT f, CT w[S]) {
   if constexpr (S == 4) {
@@ -90,7 +96,7 @@ __global__ void __launch_bounds__(256) k_m2p3d(M2PParams P) {
   for (int i = 0; i < S; ++i) {
     ox[i] = (int64_t)(wrap_index(cx - (HL - 1) + i, P.N[0]) + 1 - P.fd.lb[0]) * P.fd.s[0];
     oy[i] = (int64_t)(wrap_index(cy - (HL - 1) + i, P.N[1]) + 1 - P.fd.lb[1]) * P.fd.s[1];
-    oz[i] = (int64_t)(wrap_index(cz - (HL - 1) + i, P.N[2]) + 1 - P.fd.lb[2]) * P.fd.s[2];
+    oz[i] = (int64_t)(zplane(P, cz - (HL - 1) + i) + 1 - P.fd.lb[2]) * P.fd.s[2];
   }
   const FT* F = static_cast<const FT*>(P.field);
   FT* up = static_cast<FT*>(P.up) + (int64_t)P.idx[s] * P.ldup;
@@ -196,7 +202,7 @@ __global__ void __launch_bounds__(256) k_adjoint3d(M2PParams P) {
   for (int i = 0; i < S; ++i) {
     ox[i] = (int64_t)(wrap_index(cx - (HL - 1) + i, P.N[0]) + 1 - P.fd.lb[0]) * P.fd.s[0];
     oy[i] = (int64_t)(wrap_index(cy - (HL - 1) + i, P.N[1]) + 1 - P.fd.lb[1]) * P.fd.s[1];
-    oz[i] = (int64_t)(wrap_index(cz - (HL - 1) + i, P.N[2]) + 1 - P.fd.lb[2]) * P.fd.s[2];
+    oz[i] = (int64_t)(zplane(P, cz - (HL - 1) + i) + 1 - P.fd.lb[2]) * P.fd.s[2];
   }
   const double* F = static_cast<const double*>(P.field);
   const int64_t p = P.idx[s];
@@ -325,7 +331,12 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
            (int64_t)(yw + 1 - P.fd.lb[1]) * P.fd.s[1] + oz + P.c0;
   };
   auto plane_oz = [&](int z) {
-    return (int64_t)(wrap_index(z, P.N[2]) + 1 - P.fd.lb[2]) * P.fd.s[2];
+    return (int64_t)(zplane(P, z) + 1 - P.fd.lb[2]) * P.fd.s[2];
+  };
+  // a z-slab loads only the planes its cell layers 0 .. N2-1 read (a step
+  // past the last layer would reach one plane beyond the required box)
+  auto plane_ok = [&](int z) {
+    return !P.open_z || (z >= -(HL - 1) && z <= P.N[2] - 1 + HL);
   };
   // row ranges of cell layers cz .. cz+LPS-1: thread 16 l + r loads row r of
   // layer cz + l
@@ -362,6 +373,7 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
   // prologue: planes Z0-(HL-1) .. Z0+LPS-1+HL (the planes of the first
   // step's layers) and their rows
   for (int z = Z0 - (HL - 1); z <= Z0 + LPS - 1 + HL; ++z) {
+    if (!plane_ok(z)) continue;
     const int slot = wrap_index(z, R);
     const int64_t oz = plane_oz(z);
     for (int q = tid; q < NCOL; q += 256) {
@@ -390,10 +402,13 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
 #pragma unroll
       for (int l = 0; l < LPS; ++l) {
         const int64_t oz = plane_oz(cz + LPS + HL + l);
+        const bool ok = plane_ok(cz + LPS + HL + l);
 #pragma unroll
         for (int k = 0; k < PER; ++k) {
           const int q = tid + 256 * k;
-          if (q < NCOL) {
+#pragma unroll
+          for (int a = 0; a < LC; ++a) pre[l][k][a] = CT(0);
+          if (q < NCOL && ok) {
             const int64_t o = col_off(q, oz);
 #pragma unroll
             for (int a = 0; a < LC; ++a) pre[l][k][a] = (CT)__ldg(F + o + a);

@@ -54,7 +54,10 @@ __device__ __forceinline__ void emit_node(const P2MParams& P, int x, int y, int 
   for (int a = 0; a < DIM; ++a) {
     // 1-based images n+1+t*N within [box_lo, box_hi]
     const int N = P.N[a];
-    if (P.fd.box_lo[a] > 1 - N && P.fd.box_hi[a] < 2 * N + 1) {
+    if (a == 2 && P.open_z) {
+      // no periodic images along an open axis: the node itself
+      lo[a] = hi[a] = 0;
+    } else if (P.fd.box_lo[a] > 1 - N && P.fd.box_hi[a] < 2 * N + 1) {
       // ghost layers narrower than the mesh: t in {-1, 0, 1}
       lo[a] = n[a] + 1 - N >= P.fd.box_lo[a] ? -1 : 0;
       hi[a] = n[a] + 1 + N <= P.fd.box_hi[a] ? 1 : 0;
@@ -244,12 +247,14 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
   // cell offsets of the staged cells of layer cz, kept in registers until published
   int pb[PERC], pe[PERC];
   auto load_counts = [&](int cz) {
-    const int czw = wrap_index(cz, P.N[2]);
+    // open z: the layers outside the slab hold no particles of this subdomain
+    const bool empty = P.open_z && (cz < 0 || cz >= P.N[2]);
+    const int czw = empty ? 0 : wrap_index(cz, P.N[2]);
 #pragma unroll
     for (int k = 0; k < PERC; ++k) {
       const int q = tid + NT * k;
       pb[k] = pe[k] = 0;
-      if (q < NSC) {
+      if (q < NSC && !empty) {
         const int r = q / WX, qx = q - r * WX;
         const int cx = wrap_index(X0 - HL + qx, P.N[0]);
         const int cy = wrap_index(Y0 - HL + r, P.N[1]);
@@ -521,21 +526,24 @@ __global__ void k_layer_counts(const int* __restrict__ start, int N0, int N1, in
 
 // Split every xy tile's z range into work items of about `target` particles
 // (at least min_tz and at most max_tz layers; the halo makes short items dear).
-__global__ void k_make_items(const int* __restrict__ lc, int N2, int ntiles, int target,
-                             int min_tz, int max_tz, int4* __restrict__ items,
+// The z planes are zlo .. zlo+ze-1; plane z counts the particles of cell
+// layer z (none outside 0 .. N2-1).
+__global__ void k_make_items(const int* __restrict__ lc, int N2, int zlo, int ze, int ntiles,
+                             int target, int min_tz, int max_tz, int4* __restrict__ items,
                              int* __restrict__ nitems) {
   const int tile = blockIdx.x * blockDim.x + threadIdx.x;
   if (tile >= ntiles) return;
   int z0 = 0, acc = 0;
-  for (int cz = 0; cz < N2; ++cz) {
-    acc += lc[(int64_t)tile * N2 + cz];
-    const int len = cz + 1 - z0;
+  for (int ez = 0; ez < ze; ++ez) {
+    const int cz = zlo + ez;
+    if (cz >= 0 && cz < N2) acc += lc[(int64_t)tile * N2 + cz];
+    const int len = ez + 1 - z0;
     const bool want = (acc >= target && len >= min_tz) || len >= max_tz;
-    if (cz == N2 - 1 || (want && N2 - (cz + 1) >= min_tz)) {
+    if (ez == ze - 1 || (want && ze - (ez + 1) >= min_tz)) {
       const int q = atomicAdd(nitems, 1);
       // weight: particles of the item's own cells + a per-layer cost
-      items[q] = make_int4(tile, z0, cz + 1, acc + 32 * len);
-      z0 = cz + 1;
+      items[q] = make_int4(tile, zlo + z0, zlo + ez + 1, acc + 32 * len);
+      z0 = ez + 1;
       acc = 0;
     }
   }
@@ -782,33 +790,38 @@ constexpr int kMinTZ = 8, kMaxTZ = 64;
 int tiles_xy(const int N[3]) {
   return ((N[0] + kTileX - 1) / kTileX) * ((N[1] + kTileY - 1) / kTileY);
 }
-int item_capacity(const int N[3]) {
-  return tiles_xy(N) * ((N[2] + kMinTZ - 1) / kMinTZ) + 1;
+int item_capacity(const int N[3], int ze) {
+  if (ze <= 0) ze = N[2];
+  return tiles_xy(N) * ((ze + kMinTZ - 1) / kMinTZ) + 1;
 }
 }  // namespace
 
 // Layout: items[cap] | nitems (64 bytes) | unordered items[cap] | layer counts
-size_t tile_items_bytes(const int N[3]) {
-  return 2 * sizeof(int4) * (size_t)item_capacity(N) +
+size_t tile_items_bytes(const int N[3], int ze) {
+  return 2 * sizeof(int4) * (size_t)item_capacity(N, ze) +
          sizeof(int) * (size_t)tiles_xy(N) * N[2] + 64;
 }
 
-size_t p2m_scratch_bytes(int dim, const int N[3]) {
-  return dim == 3 ? tile_items_bytes(N) : 16;
+size_t p2m_scratch_bytes(int dim, const int N[3], int ze) {
+  return dim == 3 ? tile_items_bytes(N, ze) : 16;
 }
 
-TileItems tile_items_view(void* scratch, const int N[3]) {
+TileItems tile_items_view(void* scratch, const int N[3], int ze) {
   TileItems t;
-  t.cap = item_capacity(N);
+  t.cap = item_capacity(N, ze);
   t.items = static_cast<const int4*>(scratch);
   t.nitems = reinterpret_cast<const int*>(t.items + t.cap);
   return t;
 }
 
 cudaError_t make_tile_items(const int* start, const int N[3], int64_t nvalid, void* scratch,
-                            TileItems& out, cudaStream_t st) {
+                            TileItems& out, cudaStream_t st, int zlo, int ze) {
+  if (ze <= 0) {
+    zlo = 0;
+    ze = N[2];
+  }
   const int nt = tiles_xy(N);
-  const int cap_items = item_capacity(N);
+  const int cap_items = item_capacity(N, ze);
   int4* items = static_cast<int4*>(scratch);
   int* nitems = reinterpret_cast<int*>(items + cap_items);
   int4* unordered = reinterpret_cast<int4*>(nitems + 16);
@@ -821,7 +834,7 @@ cudaError_t make_tile_items(const int* start, const int N[3], int64_t nvalid, vo
                                      lc);
   const int64_t tgt64 = nvalid / (148 * 2 * 8);
   const int target = (int)(tgt64 < 4096 ? 4096 : (tgt64 > (1 << 30) ? (1 << 30) : tgt64));
-  k_make_items<<<(nt + 127) / 128, 128, 0, st>>>(lc, N[2], nt, target, kMinTZ, kMaxTZ,
+  k_make_items<<<(nt + 127) / 128, 128, 0, st>>>(lc, N[2], zlo, ze, nt, target, kMinTZ, kMaxTZ,
                                                  unordered, nitems);
   k_order_items<<<1, 1024, 0, st>>>(unordered, nitems, items);
   count_launch(3);
@@ -839,7 +852,9 @@ cudaError_t launch_p2m(const P2MParams& P0, int dim, int kernel, P2MPrec prec, i
   if (dim == 3) {
     // work items: xy tiles split along z into segments of similar particle count
     TileItems ti;
-    if ((e = make_tile_items(P0.start, P0.N, nvalid, scratch, ti, st))) return e;
+    if ((e = make_tile_items(P0.start, P0.N, nvalid, scratch, ti, st, P0.open_z ? P0.zlo : 0,
+                             P0.open_z ? P0.ze : 0)))
+      return e;
     Pw.items = ti.items;
     Pw.nitems = ti.nitems;
     Pw.item_cap = ti.cap;

@@ -26,10 +26,15 @@ struct P2MParams {
   const int4* items;
   const int* nitems;
   int item_cap;
+  // open z (a z-slab subdomain): cell layers outside [0, N[2]) are empty,
+  // nodes have no periodic images along z, and the work items cover the
+  // ze node planes zlo .. zlo+ze-1 (0-based) of the written box
+  int open_z, zlo, ze;
 };
 
-// Device scratch launch_p2m needs (work items, per-layer counts).
-size_t p2m_scratch_bytes(int dim, const int N[3]);
+// Device scratch launch_p2m needs (work items, per-layer counts); ze: node
+// planes the items cover (<= 0: N[2]).
+size_t p2m_scratch_bytes(int dim, const int N[3], int ze = 0);
 
 // Work items of the 3D tile kernels: (xy tile of kTileX x kTileY cells,
 // z0, z1) with z ranges split so every item holds a similar particle count.
@@ -38,11 +43,13 @@ struct TileItems {
   const int* nitems;  // device count
   int cap;            // grid size to launch (items beyond *nitems exit)
 };
-size_t tile_items_bytes(const int N[3]);
+size_t tile_items_bytes(const int N[3], int ze = 0);
 // The items a previous make_tile_items left in `scratch`.
-TileItems tile_items_view(void* scratch, const int N[3]);
+TileItems tile_items_view(void* scratch, const int N[3], int ze = 0);
+// Items over the z planes zlo .. zlo+ze-1 (ze <= 0: the cell layers 0 .. N[2]-1);
+// planes outside the cell layers count no particles.
 cudaError_t make_tile_items(const int* start, const int N[3], int64_t nvalid, void* scratch,
-                            TileItems& out, cudaStream_t st);
+                            TileItems& out, cudaStream_t st, int zlo = 0, int ze = 0);
 
 // Tile depth (nodes along the sweep axis per CTA) of the 2D gather.
 int p2m_tile_depth(int dim, const int N[3]);

@@ -40,7 +40,10 @@ enum KeyMode {
   KEY_INTERP_WRAP = 1,     // M2P / adjoint: any finite x, periodic wrap
 };
 
-// Key computation parameters (one subdomain, periodic).
+// Key computation parameters (one subdomain).  An axis is periodic within the
+// subdomain unless open[a]: the subdomain is then one slab of a larger
+// domain along a, its neighbours hold the rest, and positions outside it
+// are invalid in every mode.
 struct KeyParams {
   int dim;
   int N[3];
@@ -48,6 +51,7 @@ struct KeyParams {
   double dxi[3];
   float minf[3], maxf[3], dxif[3];
   int mode;
+  int open[3];
 };
 
 // Counting sort of Np particles into the Nx*Ny*Nz cells.  On return

@@ -30,12 +30,16 @@ __device__ __forceinline__ bool cell_axis(const KeyParams& kp, int a, T x, int& 
   using A = KeyArith<T>;
   const T xi = rmul(rsub(x, A::mn(kp, a)), A::di(kp, a));
   const int n = kp.N[a];
-  if (kp.mode == KEY_INTERP_CHECKED) {
+  if (kp.mode == KEY_INTERP_CHECKED || kp.open[a]) {
     // closed-lower / open-upper containment (periodic upper face)
     if (!(x >= A::mn(kp, a) && x < A::mx(kp, a))) return false;
     int i0 = (int)xi;  // xi >= 0 here: INT == FLOOR
+    // xi may round up to exactly Nc: on a periodic axis that is cell 0 at
+    // offset 0, on an open axis the last cell at offset 1 (the same node
+    // weights: only the node at the upper face gets 1)
+    if (kp.open[a] && i0 >= n) i0 = n - 1;
     f = rsub(xi, (T)i0);
-    cell = i0 >= n ? i0 - n : i0;  // xi may round up to exactly Nc
+    cell = i0 >= n ? i0 - n : i0;
     return true;
   }
   // periodic wrap of any finite position

@@ -23,7 +23,9 @@ import ctypes as C
 
 import numpy as np
 
+from . import halo
 from . import params as P
+from . import topo as _topo
 from ._lib import int_array, last_error, lib  # noqa: F401
 
 try:  # torch is optional: only the device-pointer path needs it
@@ -96,8 +98,21 @@ def _split(up, args, name):
     raise TypeError(f"{name}: wrong number of arguments")
 
 
-def ppm_interp_p2m(xp, Np, up, *args, field_lb=None):
-    """ppm_interp_p2m(xp, Np, up, [lda,] topo_id, mesh_id, kernel, ghostsize, field_up)."""
+def _slab_exchange(field_up, topo_id, mesh_id, ghostsize, lb, put):
+    """The z ghost exchange of a slab handle (every rank takes it, also after
+    a local error, so that no neighbour waits for a message never sent)."""
+    t, isub = _topo.local_sub(topo_id, mesh_id)
+    fn = halo.put if put else halo.get
+    fn({isub: field_up}, t, list(ghostsize), [int(v) for v in lb], halo.comm_for(topo_id, mesh_id))
+
+
+def ppm_interp_p2m(xp, Np, up, *args, field_lb=None, exchange=True):
+    """ppm_interp_p2m(xp, Np, up, [lda,] topo_id, mesh_id, kernel, ghostsize, field_up).
+
+    On a z-slab handle the ghost put with the neighbouring slabs follows the
+    local deposit (as the reference's P2M ends with ppm_map_field_ghost put);
+    exchange=False leaves it to the caller (halo.put).
+    """
     vector, lda, topo_id, mesh_id, kernel, ghostsize, field_up = _split(up, args, "ppm_interp_p2m")
     _check(xp, up, field_up)
     dim = field_up.ndim - (2 if vector else 1)
@@ -119,6 +134,8 @@ def ppm_interp_p2m(xp, Np, up, *args, field_lb=None):
             raise TypeError("device (torch) arrays use the vector variant (pass lda)")
         getattr(lib(), name)(_addr(xp), xp.shape[0], int(Np), _addr(up), topo_id, mesh_id,
                              kernel, g, _addr(field_up), lb, ub, C.byref(info))
+    if exchange and _topo.is_slab(topo_id, mesh_id):
+        _slab_exchange(field_up, topo_id, mesh_id, ghostsize, lb, True)
     return info.value
 
 
@@ -168,7 +185,9 @@ def ppm_map_field_ghost(field_up, *args, field_lb=None):
     """ppm_map_field_ghost(field_up, [lda,] topo_id, mesh_id, ghostsize, maptype).
 
     maptype ppm_param_map_ghost_get or ppm_param_map_ghost_put; the
-    init/push/send/pop steps of the reference happen inside the call.
+    init/push/send/pop steps of the reference happen inside the call.  On a
+    z-slab handle this is the exchange with the neighbouring slabs
+    (ppm_legacy_b200.halo); x and y are periodic within the slab.
     """
     if len(args) == 5:
         lda, topo_id, mesh_id, ghostsize, maptype = args
@@ -179,6 +198,12 @@ def ppm_map_field_ghost(field_up, *args, field_lb=None):
     _check(field_up)
     dim = field_up.ndim - (2 if vector else 1)
     lb, ub = _bounds(field_up, dim, vector, ghostsize, field_lb)
+    if _topo.is_slab(topo_id, mesh_id):
+        if int(maptype) not in (P.ppm_param_map_ghost_get, P.ppm_param_map_ghost_put):
+            return -2
+        _slab_exchange(field_up, topo_id, mesh_id, ghostsize, lb,
+                       int(maptype) == P.ppm_param_map_ghost_put)
+        return 0
     info = C.c_int(0)
     ldf = field_up.shape[0] if vector else 1
     a = (_addr(field_up), ldf, int(lda), lb, ub, topo_id, mesh_id, int_array(ghostsize),

@@ -111,8 +111,27 @@ def cartesian(dim: int, Nc, decomp=None, min_phys=None, max_phys=None, bcdef=Non
                     decomp=tuple(decomp) + (1,) * (3 - len(decomp)))
 
 
-def register(topo: Topology) -> int:
-    """Hand the geometry to libppmg (ppmg_mesh_register); returns info."""
+# (topo_id, mesh_id) -> (Topology, local sub) of every registered handle
+_registered: dict = {}
+
+
+def local_sub(topo_id: int, mesh_id: int):
+    """(Topology, isub) registered under (topo_id, mesh_id), or None."""
+    return _registered.get((int(topo_id), int(mesh_id)))
+
+
+def is_slab(topo_id: int, mesh_id: int) -> bool:
+    """Whether the handle computes on one z-slab of a decomposed domain."""
+    r = local_sub(topo_id, mesh_id)
+    return r is not None and r[0].nsubs > 1
+
+
+def register(topo: Topology, isub=None) -> int:
+    """Hand the geometry to libppmg (ppmg_mesh_register); returns info.
+
+    isub: the subdomain this process's GPU computes on (needed when the
+    topology has several subdomains: a decomposition into z-slabs).
+    """
     import ctypes as C
 
     from ._lib import int_array, lib
@@ -127,6 +146,12 @@ def register(topo: Topology) -> int:
         int_array(topo.Nm), int_array(topo.bcdef), int(topo.nsubs), ms.ctypes.data,
         Ms.ctypes.data, int_array(topo.subs_bc.reshape(-1)), int_array(topo.istart.reshape(-1)),
         int_array(topo.nnodes.reshape(-1)), C.byref(info))
+    if info.value == 0 and isub is not None:
+        lib().ppmg_mesh_set_local_sub(int(topo.topo_id), int(topo.mesh_id), int(isub),
+                                      C.byref(info))
+    if info.value == 0:
+        _registered[(int(topo.topo_id), int(topo.mesh_id))] = (
+            topo, 0 if isub is None else int(isub))
     return info.value
 
 
@@ -137,4 +162,5 @@ def unregister(topo: Topology) -> int:
 
     info = C.c_int(0)
     lib().ppmg_mesh_unregister(int(topo.topo_id), int(topo.mesh_id), C.byref(info))
+    _registered.pop((int(topo.topo_id), int(topo.mesh_id)), None)
     return info.value

@@ -1,0 +1,166 @@
+"""3D P2M and M2P on z-slab subdomains (ppmg_mesh_set_local_sub) against the
+oracle's multi-subdomain routines, on one GPU: every slab is a handle of its
+own in this process and the ghost exchange between them runs in-process
+(halo.LocalComm, the same block arithmetic that DistComm sends between
+ranks)."""
+import copy
+
+import numpy as np
+import pytest
+
+import ppm_legacy_b200 as ppmg
+from ppm_legacy_b200 import halo
+from _util import max_rel, random_particles, topo_for
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+_next_id = [7000]
+
+
+def slab_handles(t):
+    """One handle per slab (topo ids of their own), local sub = the slab."""
+    out = []
+    for s in range(t.nsubs):
+        _next_id[0] += 1
+        ts = copy.deepcopy(t)
+        ts.topo_id = _next_id[0]
+        assert ppmg.register(ts, isub=s) == 0, ppmg.last_error()
+        out.append(ts)
+    return out
+
+
+def dev_f(a):
+    d = torch.from_numpy(np.ascontiguousarray(np.asarray(a).T)).cuda()
+    return d.permute(*reversed(range(d.dim())))
+
+
+def host(a):
+    return a.permute(*reversed(range(a.dim()))).contiguous().cpu().numpy().T
+
+
+def run(nc, nslab, kernel, g, lda, mode, seed, n=None):
+    rng = np.random.default_rng(seed)
+    t = topo_for(3, nc, decomp=(1, 1, nslab))
+    n = n or 2 * nc ** 3
+    xp = random_particles(rng, 3, n)
+    up = np.asfortranarray(rng.standard_normal((lda, n)))
+    gg = [g] * 3
+    lst, si = O.assign(t, xp)
+    ids = np.split(lst, np.cumsum(si)[:-1])
+    hs = slab_handles(t)
+    ppmg.set_precision(mode)
+    lb = [1 - g] * 3
+    fields = {}
+    for s, ts in enumerate(hs):
+        nz = int(t.nnodes[s, 2]) - 1
+        shape = (lda, nc + 1 + 2 * g, nc + 1 + 2 * g, nz + 1 + 2 * g, 1)
+        f = dev_f(np.full(shape, 9.0))
+        xs = dev_f(xp[:, ids[s]])
+        us = dev_f(up[:, ids[s]])
+        assert ppmg.ppm_interp_p2m(xs, len(ids[s]), us, lda, ts.topo_id, 1, kernel, gg, f,
+                                   exchange=False) == 0, ppmg.last_error()
+        fields[s] = f
+    halo.put(fields, t, gg, lb, halo.LocalComm())
+    fo, lbo, ubo = O.p2m(t, xp, up, kernel, gg)
+    tol = 1e-13 if mode == 0 else 1e-6
+    for s in range(nslab):
+        nz = int(t.nnodes[s, 2]) - 1
+        got = host(fields[s])
+        real = (slice(None),) + tuple(slice(g, g + nc + 1) for _ in range(2)) + (slice(g, g + nz + 1), 0)
+        ref = fo[(slice(None),) + tuple(slice(1 - lbo[a], 1 - lbo[a] + nc + 1) for a in range(2))
+                 + (slice(1 - lbo[2], 1 - lbo[2] + nz + 1), s)]
+        assert max_rel(got[real], ref) < tol, (s, max_rel(got[real], ref))
+    # M2P: ghost get between the slabs, then every slab gathers its particles
+    halo.get(fields, t, gg, lb, halo.LocalComm())
+    O.ghost_get(t, fo, lbo, ubo, gg)
+    ref = O.m2p(t, xp, fo, lbo, ubo, lda, kernel, gg)
+    for s, ts in enumerate(hs):
+        out = dev_f(np.zeros((lda, len(ids[s]))))
+        assert ppmg.ppm_interp_m2p(dev_f(xp[:, ids[s]]), len(ids[s]), out, lda, ts.topo_id, 1,
+                                   kernel, gg, fields[s]) == 0, ppmg.last_error()
+        assert ppmg.sync_status(ts.topo_id, 1) == 0, ppmg.last_error()
+        got = host(out)
+        mt = 1e-14 if mode == 0 else 1e-6
+        assert max_rel(got, ref[:, ids[s]]) <= mt, (s, max_rel(got, ref[:, ids[s]]))
+    ppmg.set_precision(0)
+    for ts in hs:
+        ppmg.unregister(ts)
+
+
+@pytest.mark.parametrize("nc,nslab,kernel,g,lda", [
+    (16, 2, 2, 2, 3), (12, 3, 2, 2, 1), (16, 4, 1, 1, 2), (12, 2, 2, 3, 5)])
+def test_slab_p2m_put_get_m2p_match_oracle(nc, nslab, kernel, g, lda):
+    run(nc, nslab, kernel, g, lda, 0, seed=nc * nslab + kernel)
+
+
+def test_slab_mixed_precision_within_tolerance():
+    run(24, 3, 2, 2, 3, 1, seed=5)
+
+
+def test_slab_particles_on_the_slab_faces():
+    """Particles on the planes between slabs and one ulp below them (the
+    stencil origin may round up to the slab's top face)."""
+    rng = np.random.default_rng(11)
+    nc, nslab = 12, 3
+    t = topo_for(3, nc, decomp=(1, 1, nslab))
+    faces = np.unique(np.concatenate([t.min_sub[:, 2], t.max_sub[:, 2]]))
+    faces = faces[faces < 1.0]
+    below = np.nextafter(faces[1:], 0.0)
+    z = np.concatenate([faces, below])
+    n = z.size * 20
+    xp = random_particles(rng, 3, n)
+    xp[2] = np.repeat(z, 20)
+    up = np.asfortranarray(rng.standard_normal((2, n)))
+    gg = [2, 2, 2]
+    lst, si = O.assign(t, xp)
+    ids = np.split(lst, np.cumsum(si)[:-1])
+    hs = slab_handles(t)
+    fields = {}
+    for s, ts in enumerate(hs):
+        nz = int(t.nnodes[s, 2]) - 1
+        f = dev_f(np.zeros((2, nc + 5, nc + 5, nz + 5, 1)))
+        assert ppmg.ppm_interp_p2m(dev_f(xp[:, ids[s]]), len(ids[s]), dev_f(up[:, ids[s]]), 2,
+                                   ts.topo_id, 1, 2, gg, f, exchange=False) == 0
+        fields[s] = f
+    halo.put(fields, t, gg, [-1, -1, -1], halo.LocalComm())
+    fo, lbo, _ = O.p2m(t, xp, up, 2, gg)
+    for s in range(nslab):
+        nz = int(t.nnodes[s, 2]) - 1
+        got = host(fields[s])[:, 2:nc + 3, 2:nc + 3, 2:nz + 3, 0]
+        ref = fo[:, 1 - lbo[0]:2 - lbo[0] + nc, 1 - lbo[1]:2 - lbo[1] + nc,
+                 1 - lbo[2]:2 - lbo[2] + nz, s]
+        assert max_rel(got, ref) < 1e-13
+    for ts in hs:
+        ppmg.unregister(ts)
+
+
+def test_slab_particle_outside_its_slab_is_unassigned():
+    t = topo_for(3, 12, decomp=(1, 1, 2))
+    hs = slab_handles(t)
+    xp = dev_f(np.array([[0.5], [0.5], [0.75]]))  # in slab 1, given to slab 0
+    f = dev_f(np.zeros((1, 17, 17, 11, 1)))
+    ppmg.ppm_interp_p2m(xp, 1, dev_f(np.ones((1, 1))), 1, hs[0].topo_id, 1, 2, [2, 2, 2], f,
+                        exchange=False)
+    info = ppmg.sync_status(hs[0].topo_id, 1)
+    assert info == -1 and ppmg.last_error()[1] == 405
+    for ts in hs:
+        ppmg.unregister(ts)
+
+
+def test_slab_handle_refuses_other_routines():
+    """Remeshing, the adjoint and 2D keep one periodic subdomain per GPU."""
+    t = topo_for(3, 12, decomp=(1, 1, 2))
+    hs = slab_handles(t)
+    xp = np.asfortranarray(np.array([[0.5], [0.5], [0.25]]))
+    assert ppmg.ppm_rmsh_comp_weights(xp, 1, hs[0].topo_id, 1, 2) == -2
+    assert "slab" in ppmg.last_error()[2]
+    t2 = topo_for(3, 12, decomp=(2, 1, 1), topo_id=7900)
+    ppmg.register(t2)
+    import ctypes as C
+    info = C.c_int(0)
+    ppmg.lib().ppmg_mesh_set_local_sub(7900, 1, 0, C.byref(info))
+    assert info.value == -2 and "z-slabs" in ppmg.last_error()[2]
+    for ts in hs + [t2]:
+        ppmg.unregister(ts)
