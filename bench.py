@@ -13,8 +13,11 @@ form is measured on the same data and reported beside it.
 restatement of the Fortran loops, one thread per subdomain as `mpirun -np P`
 would run it) on a bounded sample of the same workload.
 
-Multi-GPU (torchrun): weak scaling, every rank runs its own subdomain-sized
-problem (independent replicas, no data-path collective); time = max over ranks.
+Multi-GPU (torchrun): weak scaling by domain decomposition.  N ranks own the
+N z-slabs of a 512 x 512 x 512N periodic mesh (one 512^3 slab and its own
+134M particles per GPU); a step is the local P2M with the ghost put between
+neighbouring slabs (NCCL point-to-point, ppm_legacy_b200.halo), the ghost
+get, and the local M2P; time = max over ranks.
 """
 from __future__ import annotations
 
@@ -98,6 +101,24 @@ def measured_traffic(kernel, np_):
         return d["bytes_per_launch"] * np_ / d["particles"]
     except Exception:
         return None
+
+
+def slab_topology(ppmg, nc, world, topo_id=1, mesh_id=1):
+    """The weak-scaling domain: world z-slabs of nc^3 cells, cubic cells of
+    size 1/nc, periodic; slab r covers z in [r, r+1)."""
+    return ppmg.cartesian(3, [nc, nc, nc * world], decomp=(1, 1, world),
+                          min_phys=[0.0, 0.0, 0.0], max_phys=[1.0, 1.0, float(world)],
+                          topo_id=topo_id, mesh_id=mesh_id)
+
+
+def shift_to_slab(torch, xp, rank):
+    """Move positions from [0,1)^3 into slab `rank` (z in [rank, rank+1)); a
+    z that rounds up to the slab's top face goes to its bottom face."""
+    if rank == 0:
+        return xp
+    z = xp[2] + float(rank)
+    xp[2] = torch.where(z >= float(rank + 1), torch.full_like(z, float(rank)), z)
+    return xp
 
 
 def gen_particles(torch, cfg, device, seed):
@@ -449,8 +470,14 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=dev)
     xp, up, nc, n = gen_particles(torch, args.config, dev, seed=1000 + rank)
-    t = ppmg.cartesian(3, nc, topo_id=1, mesh_id=1)
-    assert ppmg.register(t) == 0, ppmg.last_error()
+    if world > 1:
+        # one z-slab per rank; P2M ends with the ghost put between the slabs
+        t = slab_topology(ppmg, nc, world)
+        xp = shift_to_slab(torch, xp, rank)
+        assert ppmg.register(t, isub=rank) == 0, ppmg.last_error()
+    else:
+        t = ppmg.cartesian(3, nc, topo_id=1, mesh_id=1)
+        assert ppmg.register(t) == 0, ppmg.last_error()
     g = [2, 2, 2]
     ext = nc + 1 + 2 * g[0]
     field = torch.empty((ext, ext, ext, 3), device=dev, dtype=torch.float64).permute(3, 2, 1, 0)
@@ -466,8 +493,16 @@ def main():
         ppmg.lib().ppmg_kernel_timing_read(part, C.byref(tot), C.byref(cnt))
         return float(tot.value), int(cnt.value)
 
+    get = ppmg.params.ppm_param_map_ghost_get
+
+    def ghost_get(f):
+        # the slabs' z ghost planes from the neighbours (M2P reads them)
+        if world > 1 and ppmg.ppm_map_field_ghost(f, 3, 1, 1, g, get):
+            raise RuntimeError(f"library error {ppmg.last_error()}")
+
     def step():
         i1 = ppmg.ppm_interp_p2m(xp, n, up, 3, 1, 1, 2, g, field)
+        ghost_get(field)
         i2 = ppmg.ppm_interp_m2p(xp, n, out, 3, 1, 1, 2, g, field)
         if i1 or i2:
             raise RuntimeError(f"library error {ppmg.last_error()}")
@@ -493,6 +528,7 @@ def main():
             evp[0].record(stream)
             ppmg.ppm_interp_p2m(xp, n, up, 3, 1, 1, 2, g, field)
             evp[1].record(stream)
+            ghost_get(field)
             ppmg.ppm_interp_m2p(xp, n, out, 3, 1, 1, 2, g, field)
             evp[2].record(stream)
             evp[2].synchronize()
@@ -562,7 +598,8 @@ def main():
                      "m2p_frac": (bm / (b / 1e3) / 1e9) / peak}
 
     adj = None
-    if not args.no_adjoint:
+    # the adjoint keeps one periodic subdomain per GPU: single-GPU runs only
+    if not args.no_adjoint and world == 1:
         # the adjoint pass of P2M at the same workload: dw = M2P(r), dx from the
         # kernel derivative, r ~ N(0, 1) on the unique nodes (device pointers)
         ppmg.set_precision(head)
@@ -628,6 +665,7 @@ def main():
 
         def e2e_step():
             i1 = ppmg.ppm_interp_p2m(nx, n, nu, 3, 1, 1, 2, g, nf)
+            ghost_get(nf)
             i2 = ppmg.ppm_interp_m2p(nx, n, no, 3, 1, 1, 2, g, nf)
             if i1 or i2:
                 raise RuntimeError(f"library error {ppmg.last_error()}")
@@ -670,7 +708,9 @@ def main():
                                    f"particles per GPU ({CONFIGS[args.config][2]}), lda 3, "
                                    f"ghostsize 2",
                        "l2": "inputs larger than L2 (xp/up/field each > 126 MB)",
-                       "parallelism": f"{world} independent subdomain replicas"},
+                       "parallelism": "1 periodic subdomain" if world == 1 else
+                       f"{world} z-slab subdomains of a 512x512x{512 * world} mesh, ghost put/get "
+                       "between neighbouring slabs over NCCL"},
             "roofline": roof, "forms": parts, "clocks": clocks, "gpu_launches": launches,
             "e2e": e2e, "cpu_baseline": cb, "adjoint": adj,
         }

@@ -292,7 +292,9 @@ constexpr size_t m2p_ring_bytes() {
          LC * sizeof(CT);
 }
 
-template <int S, class CT, bool EXACT, class FT, int LC, bool ADJ = false>
+// OZ: a z-slab subdomain (P.open_z), compiled apart so that the periodic
+// gather keeps its plane loads unconditional.
+template <int S, class CT, bool EXACT, class FT, int LC, bool ADJ = false, bool OZ = false>
 __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
   using V = typename Vec4<CT>::type;
   constexpr int HL = S / 2;
@@ -331,12 +333,12 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
            (int64_t)(yw + 1 - P.fd.lb[1]) * P.fd.s[1] + oz + P.c0;
   };
   auto plane_oz = [&](int z) {
-    return (int64_t)(zplane(P, z) + 1 - P.fd.lb[2]) * P.fd.s[2];
+    return (int64_t)((OZ ? z : wrap_index(z, P.N[2])) + 1 - P.fd.lb[2]) * P.fd.s[2];
   };
   // a z-slab loads only the planes its cell layers 0 .. N2-1 read (a step
   // past the last layer would reach one plane beyond the required box)
   auto plane_ok = [&](int z) {
-    return !P.open_z || (z >= -(HL - 1) && z <= P.N[2] - 1 + HL);
+    return !OZ || (z >= -(HL - 1) && z <= P.N[2] - 1 + HL);
   };
   // row ranges of cell layers cz .. cz+LPS-1: thread 16 l + r loads row r of
   // layer cz + l
@@ -406,8 +408,10 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
 #pragma unroll
         for (int k = 0; k < PER; ++k) {
           const int q = tid + 256 * k;
+          if constexpr (OZ) {
 #pragma unroll
-          for (int a = 0; a < LC; ++a) pre[l][k][a] = CT(0);
+            for (int a = 0; a < LC; ++a) pre[l][k][a] = CT(0);
+          }
           if (q < NCOL && ok) {
             const int64_t o = col_off(q, oz);
 #pragma unroll
@@ -579,18 +583,23 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
 
 template <int S, class CT, bool EXACT, class FT>
 cudaError_t launch_tile_lc(const M2PParams& P, int lc, cudaStream_t st) {
-  auto go = [&](auto kern, size_t smem) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  auto go = [&](auto kern, auto kern_oz, size_t smem) {
+    auto k = P.open_z ? kern_oz : kern;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e) return e;
-    kern<<<P.item_cap, 256, smem, st>>>(P);
+    k<<<P.item_cap, 256, smem, st>>>(P);
     return cudaGetLastError();
   };
   switch (lc) {
-    case 1: return go(k_m2p3d_tile<S, CT, EXACT, FT, 1>, m2p_ring_bytes<S, CT, 1>());
-    case 2: return go(k_m2p3d_tile<S, CT, EXACT, FT, 2>, m2p_ring_bytes<S, CT, 2>());
-    case 3: return go(k_m2p3d_tile<S, CT, EXACT, FT, 3>, m2p_ring_bytes<S, CT, 3>());
-    default: return go(k_m2p3d_tile<S, CT, EXACT, FT, 4>, m2p_ring_bytes<S, CT, 4>());
+    case 1: return go(k_m2p3d_tile<S, CT, EXACT, FT, 1>, k_m2p3d_tile<S, CT, EXACT, FT, 1, false, true>,
+                      m2p_ring_bytes<S, CT, 1>());
+    case 2: return go(k_m2p3d_tile<S, CT, EXACT, FT, 2>, k_m2p3d_tile<S, CT, EXACT, FT, 2, false, true>,
+                      m2p_ring_bytes<S, CT, 2>());
+    case 3: return go(k_m2p3d_tile<S, CT, EXACT, FT, 3>, k_m2p3d_tile<S, CT, EXACT, FT, 3, false, true>,
+                      m2p_ring_bytes<S, CT, 3>());
+    default: return go(k_m2p3d_tile<S, CT, EXACT, FT, 4>, k_m2p3d_tile<S, CT, EXACT, FT, 4, false, true>,
+                       m2p_ring_bytes<S, CT, 4>());
   }
 }
 

@@ -167,25 +167,36 @@ class DistComm:
         import torch
         import torch.distributed as dist
         me = dist.get_rank(self.group)
+        # NCCL moves device memory only: host blocks (the host-pointer API)
+        # travel through device copies
+        dev = None
+        if dist.get_backend(self.group) == "nccl":
+            dev = torch.device("cuda", torch.cuda.current_device())
+
+        def wire(t):
+            return t.to(dev) if dev is not None and t.device.type == "cpu" else t.contiguous()
+
         ops, bufs, local = [], [], {}
         for src, dst, tag, t in sends:
             if self._rank(dst) == me:
                 local[(src, dst, tag)] = t
             else:
-                ops.append(dist.P2POp(dist.isend, t.contiguous(), self._peer(dst), self.group,
-                                      tag))
+                ops.append(dist.P2POp(dist.isend, wire(t), self._peer(dst), self.group, tag))
         for dst, src, tag, like in recvs:
-            buf = torch.empty_like(like, memory_format=torch.contiguous_format)
+            buf = torch.empty_like(like, memory_format=torch.contiguous_format,
+                                   device=dev if dev is not None else like.device)
             bufs.append(buf)
             if self._rank(src) != me:
                 ops.append(dist.P2POp(dist.irecv, buf, self._peer(src), self.group, tag))
         if ops:
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
+        out = []
         for (dst, src, tag, like), buf in zip(recvs, bufs):
             if self._rank(src) == me:
                 buf.copy_(local[(src, dst, tag)])
-        return bufs
+            out.append(buf.to(like.device) if buf.device != like.device else buf)
+        return out
 
     def _peer(self, s):
         # global rank of the subdomain's owner (group ranks -> global ranks)

@@ -75,3 +75,25 @@ def test_weak_scaling_units_and_bytes():
     kb = bench.kernel_bytes(np_, nc, 3, 2, True)
     assert kb["p2m_gather"] == np_ * 32 + (nc + 5) ** 3 * 24
     assert kb["m2p_gather"] == nc ** 3 * 24 + np_ * 44
+
+
+def test_weak_scaling_slab_topology_and_particle_shift():
+    """The N-GPU benchmark domain: slab r is z in [r, r+1) with cubic cells of
+    1/nc, and every particle shifted into slab r stays inside it (a z that
+    would round up to the slab's top face moves to its bottom face)."""
+    import numpy as np
+
+    import ppm_legacy_b200 as ppmg
+    from ppm_legacy_b200 import halo
+    world, nc = 3, 8
+    t = bench.slab_topology(ppmg, nc, world)
+    assert t.nsubs == world and list(t.Nm) == [nc + 1, nc + 1, nc * world + 1]
+    assert np.allclose(t.h, 1.0 / nc)
+    for r in range(world):
+        assert t.min_sub[r, 2] == r and t.max_sub[r, 2] == r + 1
+        assert halo.neighbours(t, r) == ((r - 1) % world, (r + 1) % world)
+        xp = torch.rand((3, 1000), dtype=torch.float64)
+        xp[2, :3] = torch.tensor([0.0, np.nextafter(1.0, 0.0), 0.5])
+        xp = bench.shift_to_slab(torch, xp.t().contiguous().t(), r)
+        z = xp[2].numpy()
+        assert (z >= t.min_sub[r, 2]).all() and (z < t.max_sub[r, 2]).all()
