@@ -130,8 +130,8 @@ __device__ __forceinline__ void cp_async_wait_all() {
 }
 
 // Exclusive scan over n <= 3*256 cell values v(q) (thread t owns cells 3t ..
-// 3t+2); writes out[0..n] (out[n] = total) and returns the total and the
-// maximum through the smem scalars red[0], red[1].
+// 3t+2) by a CTA of 8 warps; writes out[0..n] (out[n] = total) and returns
+// the total through the smem scalar red[0].
 template <class F>
 __device__ __forceinline__ void scan_cells(int n, F val, int* out, int* wsum, int* red) {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -140,27 +140,25 @@ __device__ __forceinline__ void scan_cells(int n, F val, int* out, int* wsum, in
   const int v1 = q0 + 1 < n ? val(q0 + 1) : 0;
   const int v2 = q0 + 2 < n ? val(q0 + 2) : 0;
   const int s = v0 + v1 + v2;
-  int m = max(v0, max(v1, v2));
   int inc = s;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     const int t = __shfl_up_sync(0xffffffffu, inc, o);
     if (lane >= o) inc += t;
-    m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
   }
   if (lane == 31) wsum[wid] = inc;
-  if (lane == 0) wsum[8 + wid] = m;
   __syncthreads();
-  if (tid == 0) {
-    int run = 0, mx = 0;
-    for (int w = 0; w < 8; ++w) {
-      const int t = wsum[w];
-      wsum[w] = run;
-      run += t;
-      mx = max(mx, wsum[8 + w]);
+  if (wid == 0) {
+    // the 8 warp totals: exclusive offsets by a shuffle scan in warp 0
+    const int w = lane < 8 ? wsum[lane] : 0;
+    int wi = w;
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += t;
     }
-    red[0] = run;
-    red[1] = mx;
+    if (lane < 8) wsum[lane] = wi - w;
+    if (lane == 7) red[0] = wi;
   }
   __syncthreads();
   const int ex = inc - s + wsum[wid];
