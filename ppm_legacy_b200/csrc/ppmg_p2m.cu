@@ -131,7 +131,9 @@ __device__ __forceinline__ void cp_async_wait_all() {
 
 // Exclusive scan over n <= 3*256 cell values v(q) (thread t owns cells 3t ..
 // 3t+2) by a CTA of 8 warps; writes out[0..n] (out[n] = total) and returns
-// the total through the smem scalar red[0].
+// the total through the smem scalar red[0] (visible to all on return).  A
+// thread may read its own cells' out[] at once; the others', and the next
+// scan, only after a barrier of the caller.
 template <class F>
 __device__ __forceinline__ void scan_cells(int n, F val, int* out, int* wsum, int* red) {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -166,7 +168,6 @@ __device__ __forceinline__ void scan_cells(int n, F val, int* out, int* wsum, in
   if (q0 + 1 < n) out[q0 + 1] = ex + v0;
   if (q0 + 2 < n) out[q0 + 2] = ex + v0 + v1;
   if (tid == 0) out[n] = red[0];
-  __syncthreads();
 }
 
 // Shared memory of k_p2m3d for `cap` staging slots.
