@@ -1088,7 +1088,7 @@ int comp_weights_core(Handle& h, const T* dxp, int64_t ldxp, int64_t Np, int ker
   for (int a = 0; a < 3; ++a) {
     P.min_phys[a] = (T)h.g.min_phys[a];
     P.dxiq[a] = is_f32<T>() ? (T)h.g.dxiq_f[a] : (T)h.g.dxiq_d[a];
-    P.istart[a] = h.istart[a];
+    P.istart[a] = h.istart[3 * h.local_sub + a];  // the local subdomain's first node
   }
   P.w = h.ws_rmsh.w1d.as<T>();
   if ((e = launch_comp_weights<T>(P, st))) return cuda_fail(info, e, caller);
@@ -1128,7 +1128,7 @@ Handle* comp_weights_checks(int64_t ldxp, int64_t Np, int topo_id, int mesh_id, 
     return nullptr;
   }
   if (!check_kernel(kernel, caller, info)) return nullptr;
-  return get_checked(topo_id, mesh_id, dim, caller, info);
+  return get_checked(topo_id, mesh_id, dim, caller, info, dim == 3);
 }
 }  // namespace
 }  // namespace ppmg
@@ -1203,7 +1203,7 @@ static void remesh_common(const T* xp, int64_t ldxp, int64_t Np, const T* up,
       fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": ghostsize too small for this kernel");
       return;
     }
-  Handle* h = get_checked(topo_id, mesh_id, dim, caller, info);
+  Handle* h = get_checked(topo_id, mesh_id, dim, caller, info, dim == 3);
   if (!h) return;
   std::lock_guard<std::mutex> lk(h->mu);
   if (!h->w_valid || h->w_kernel != kernel || h->w_np != Np || h->w_single != is_f32<T>()) {
@@ -1310,7 +1310,7 @@ static void create_part_common(const T* field_up, int64_t ldf, int lda,
   if (info) *info = 0;
   Handle* hh = find_handle(topo_id, mesh_id);
   if (!hh) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": topo_id/mesh_id is invalid"); return; }
-  Handle* h = get_checked(topo_id, mesh_id, hh->dim, caller, info);
+  Handle* h = get_checked(topo_id, mesh_id, hh->dim, caller, info, hh->dim == 3);
   if (!h) return;
   if (lda < 1 || ldf < lda || (field_wp && (lda2 < 1 || ldfw < lda2))) {
     fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": lda / lda2 inconsistent");
@@ -1346,7 +1346,8 @@ static void create_part_common(const T* field_up, int64_t ldf, int lda,
   P.lda = lda;
   P.lda2 = lda2;
   for (int a = 0; a < 3; ++a) {
-    // periodic axes visit nodes 1..Nm-1 (ppm_rmsh_create_part.f:433-453)
+    // periodic axes, and a z-slab's internal upper face, visit nodes 1..Nm-1
+    // (ppm_rmsh_create_part.f:433-453)
     P.nn[a] = a < dim ? h->g.N[a] : 1;
     P.h[a] = (T)h->g.h_d[a];
     P.min_sub[a] = (T)h->g.min_sub[a];

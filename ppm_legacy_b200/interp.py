@@ -240,14 +240,15 @@ def ppm_rmsh_comp_weights(xp, Np, topo_id, mesh_id, kernel, wx1_user=None, wx2_u
     return info.value
 
 
-def ppm_rmsh_remesh(xp, Np, up, *args, field_lb=None):
+def ppm_rmsh_remesh(xp, Np, up, *args, field_lb=None, exchange=True):
     """ppm_rmsh_remesh(xp, Np, up, [lda,] topo_id, mesh_id, kernel, ghostsize, field_up).
 
     The reference puts ``info`` before ``field_up``; here ``field_up`` must be
     preallocated by the caller (the reference's ppm_alloc grow step) and is
     overwritten entirely (zeroed, then the remeshed field).  float32 arrays
     select the single-precision variants (_ss/_sv), which need weights from
-    a single-precision ppm_rmsh_comp_weights.
+    a single-precision ppm_rmsh_comp_weights.  On a z-slab handle the ghost
+    put with the neighbouring slabs follows (exchange=False: the caller's).
     """
     vector, lda, topo_id, mesh_id, kernel, ghostsize, field_up = _split(up, args, "ppm_rmsh_remesh")
     _check(xp, up, field_up)
@@ -265,6 +266,8 @@ def ppm_rmsh_remesh(xp, Np, up, *args, field_lb=None):
         getattr(lib(), f"ppmg_rmsh_remesh_{k}v_{dim}d_dev")(*a, _stream())
     else:
         getattr(lib(), f"ppmg_rmsh_remesh_{k}v_{dim}d")(*a)
+    if exchange and _topo.is_slab(topo_id, mesh_id):
+        _slab_exchange(field_up, topo_id, mesh_id, ghostsize, lb, True)
     return info.value
 
 

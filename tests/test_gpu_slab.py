@@ -150,12 +150,16 @@ def test_slab_particle_outside_its_slab_is_unassigned():
 
 
 def test_slab_handle_refuses_other_routines():
-    """Remeshing, the adjoint and 2D keep one periodic subdomain per GPU."""
+    """The adjoint keeps one periodic subdomain per GPU; only z-slabs split."""
     t = topo_for(3, 12, decomp=(1, 1, 2))
     hs = slab_handles(t)
     xp = np.asfortranarray(np.array([[0.5], [0.5], [0.25]]))
-    assert ppmg.ppm_rmsh_comp_weights(xp, 1, hs[0].topo_id, 1, 2) == -2
-    assert "slab" in ppmg.last_error()[2]
+    up = np.ones((1, 1), order="F")
+    R = np.zeros((1, 12, 12, 6, 1), order="F")
+    info = ppmg.ppm_interp_p2m_adjoint(xp, 1, up, 1, hs[0].topo_id, 1, 2, R,
+                                       np.zeros((1, 1), order="F"), np.zeros((3, 1), order="F"),
+                                       field_lb=[1, 1, 1])
+    assert info == -2 and "slab" in ppmg.last_error()[2]
     t2 = topo_for(3, 12, decomp=(2, 1, 1), topo_id=7900)
     ppmg.register(t2)
     import ctypes as C
@@ -163,4 +167,61 @@ def test_slab_handle_refuses_other_routines():
     ppmg.lib().ppmg_mesh_set_local_sub(7900, 1, 0, C.byref(info))
     assert info.value == -2 and "z-slabs" in ppmg.last_error()[2]
     for ts in hs + [t2]:
+        ppmg.unregister(ts)
+
+
+@pytest.mark.parametrize("nslab,kernel,lda", [(2, 2, 3), (3, 1, 1)])
+def test_slab_remeshing_chain_matches_oracle(nslab, kernel, lda):
+    """comp_weights, remesh (+ ghost put between the slabs) and create_part on
+    every slab against the oracle's multi-subdomain remeshing: weights bit for
+    bit, the field to summation order, the new particles slab by slab in the
+    reference's order (the shared upper plane of a slab creates none)."""
+    rng = np.random.default_rng(200 + nslab)
+    nc = 12
+    t = topo_for(3, nc, decomp=(1, 1, nslab))
+    n = 2 * nc ** 3
+    xp = random_particles(rng, 3, n)
+    up = np.asfortranarray(rng.standard_normal((lda, n)))
+    g = [2, 2, 2] if kernel == 2 else [1, 1, 1]
+    ks = 2 if kernel == 2 else 1
+    lst, si = O.assign(t, xp)
+    ids = np.split(lst, np.cumsum(si)[:-1])
+    wo, lsto, sio = O.comp_weights(t, xp, kernel)
+    fo, lbo, ubo = O.remesh(t, xp, up, kernel, g, wo, lsto, sio)
+    cut = [0.2, 1e300]
+    no, upo, xpo, _ = O.create_part(t, fo, lbo, ubo, cut)
+    hs = slab_handles(t)
+    fields, wxs = {}, {}
+    lb = [1 - g[0]] * 3
+    for s, ts in enumerate(hs):
+        ns = len(ids[s])
+        xs = np.asfortranarray(xp[:, ids[s]])
+        wx = [np.zeros((2 * ks, 1, ns + 2 * ks), order="F") for _ in range(3)]
+        assert ppmg.ppm_rmsh_comp_weights(xs, ns, ts.topo_id, 1, kernel, *wx) == 0, \
+            ppmg.last_error()
+        for a in range(3):
+            assert np.array_equal(wx[a][:, 0, :], wo[a][:, s, :ns + 2 * ks])
+        nz = int(t.nnodes[s, 2]) - 1
+        f = dev_f(np.full((lda, nc + 1 + 2 * g[0], nc + 1 + 2 * g[0], nz + 1 + 2 * g[0], 1), 5.0))
+        assert ppmg.ppm_rmsh_remesh(dev_f(xs), ns, dev_f(up[:, ids[s]]), lda, ts.topo_id, 1,
+                                    kernel, g, f, exchange=False) == 0, ppmg.last_error()
+        fields[s] = f
+    halo.put(fields, t, g, lb, halo.LocalComm())
+    ups, xps = [], []
+    for s, ts in enumerate(hs):
+        nz = int(t.nnodes[s, 2]) - 1
+        got = host(fields[s])[(slice(None),) + (slice(g[0], g[0] + nc + 1),) * 2 +
+                              (slice(g[0], g[0] + nz + 1), 0)]
+        ref = fo[(slice(None),) + tuple(slice(1 - lbo[a], 2 - lbo[a] + nc) for a in range(2)) +
+                 (slice(1 - lbo[2], 2 - lbo[2] + nz), s)]
+        assert max_rel(got, ref) < 1e-13
+        info, ns, upn, xpn, _ = ppmg.ppm_rmsh_create_part(fields[s], ts.topo_id, 1, cut, lda=lda,
+                                                          resetpos=True, ghostsize=g)
+        assert info == 0, ppmg.last_error()
+        ups.append(host(upn).reshape(lda, -1))
+        xps.append(host(xpn))
+    upg, xpg = np.concatenate(ups, axis=1), np.concatenate(xps, axis=1)
+    assert upg.shape[1] == no
+    assert max_rel(upg, upo) < 1e-13 and np.array_equal(xpg, xpo)
+    for ts in hs:
         ppmg.unregister(ts)
