@@ -293,6 +293,22 @@ void ppmg_util_rank3d_s(const float* xp, int64_t ldxp, int64_t Np, const float* 
 void ppmg_util_rank2d_s(const float* xp, int64_t ldxp, int64_t Np, const float* xmin,
                         const float* xmax, const int* Nm, const int* Ngl, int* lpdx,
                         int* lhbx, int64_t* icount, int* info);
+/* Device twins: xp, lpdx (Np entries, the first icount valid) and lhbx
+ * (nbox+1) are device arrays, the work runs on `stream`; the bounds, Nm and
+ * Ngl are host arrays.  The call returns once the lists are complete (the
+ * ranking's scratch is shared by all calls), with icount set when given. */
+void ppmg_util_rank3d_d_dev(const double* xp, int64_t ldxp, int64_t Np, const double* xmin,
+                            const double* xmax, const int* Nm, const int* Ngl, int* lpdx,
+                            int* lhbx, int64_t* icount, int* info, void* stream);
+void ppmg_util_rank2d_d_dev(const double* xp, int64_t ldxp, int64_t Np, const double* xmin,
+                            const double* xmax, const int* Nm, const int* Ngl, int* lpdx,
+                            int* lhbx, int64_t* icount, int* info, void* stream);
+void ppmg_util_rank3d_s_dev(const float* xp, int64_t ldxp, int64_t Np, const float* xmin,
+                            const float* xmax, const int* Nm, const int* Ngl, int* lpdx,
+                            int* lhbx, int64_t* icount, int* info, void* stream);
+void ppmg_util_rank2d_s_dev(const float* xp, int64_t ldxp, int64_t Np, const float* xmin,
+                            const float* xmax, const int* Nm, const int* Ngl, int* lpdx,
+                            int* lhbx, int64_t* icount, int* info, void* stream);
 
 /* ---- Instrumentation (no counterpart in the reference) -------------------
  * ppmg_kernel_timing(1) makes the library bracket, on the launching stream,

@@ -69,6 +69,10 @@ SIGNATURES = {
     "ppmg_util_rank2d_d": (_RANK, None),
     "ppmg_util_rank3d_s": (_RANK, None),
     "ppmg_util_rank2d_s": (_RANK, None),
+    "ppmg_util_rank3d_d_dev": (_RANK + [_vp], None),
+    "ppmg_util_rank2d_d_dev": (_RANK + [_vp], None),
+    "ppmg_util_rank3d_s_dev": (_RANK + [_vp], None),
+    "ppmg_util_rank2d_s_dev": (_RANK + [_vp], None),
     "ppmg_interp_p2m_dv_3d_noalloc": (_P2M_V + [_vp], None),
     "ppmg_kernel_timing": ([_i], None),
     "ppmg_kernel_timing_read": ([_i, C.POINTER(C.c_double), _pi64], _i),

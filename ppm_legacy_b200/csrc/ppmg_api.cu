@@ -1447,7 +1447,8 @@ extern "C++" {
 template <class T>
 static void rank_common(int dim, const T* xp, int64_t ldxp, int64_t Np, const T* xmin,
                         const T* xmax, const int* Nm, const int* Ngl, int* lpdx, int* lhbx,
-                        int64_t* icount, int* info, const char* caller) {
+                        int64_t* icount, int* info, const char* caller, bool dev = false,
+                        cudaStream_t dstream = nullptr) {
   clear_error();
   if (info) *info = 0;
   if (Np < 0 || (Np > 0 && ldxp < dim) || Np >= (int64_t)1 << 31) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": invalid sizes"); return; }
@@ -1478,6 +1479,22 @@ static void rank_common(int dim, const T* xp, int64_t ldxp, int64_t Np, const T*
   cudaError_t e = cudaSuccess;
   if (!st) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
   if (e) { cuda_fail(info, e, caller); return; }
+  if (dev) {
+    // device positions and lists on the caller's stream; the workspace is
+    // shared by every call, so the call returns once its lists are written
+    if ((e = clist_sort<T>(cp, xp, ldxp, Np, nbox, ws, dstream)) ||
+        (e = launch_plus_one(ws.idx.as<int>(), lpdx, Np, dstream)) ||
+        (e = launch_plus_one(ws.start.as<int>(), lhbx, nbox + 1, dstream))) {
+      cuda_fail(info, e, caller);
+      return;
+    }
+    int nd = 0;
+    e = cudaMemcpyAsync(&nd, ws.err.p, sizeof(int), cudaMemcpyDeviceToHost, dstream);
+    if (!e) e = cudaStreamSynchronize(dstream);
+    if (e) { cuda_fail(info, e, caller); return; }
+    if (icount) *icount = nd;
+    return;
+  }
   const T* dxp = mirror<T>(ws.h_xp, xp, ldxp * Np, st, e);
   if (e) { cuda_fail(info, e, caller); return; }
   if ((e = clist_sort<T>(cp, dxp, ldxp, Np, nbox, ws, st))) { cuda_fail(info, e, caller); return; }
@@ -1508,6 +1525,30 @@ void ppmg_util_rank2d_d(const double* xp, int64_t ldxp, int64_t Np, const double
                         int* lhbx, int64_t* icount, int* info) {
   rank_common(2, xp, ldxp, Np, xmin, xmax, Nm, Ngl, lpdx, lhbx, icount, info,
               "ppmg_util_rank2d_d");
+}
+void ppmg_util_rank3d_d_dev(const double* xp, int64_t ldxp, int64_t Np, const double* xmin,
+                            const double* xmax, const int* Nm, const int* Ngl, int* lpdx,
+                            int* lhbx, int64_t* icount, int* info, void* stream) {
+  rank_common(3, xp, ldxp, Np, xmin, xmax, Nm, Ngl, lpdx, lhbx, icount, info,
+              "ppmg_util_rank3d_d_dev", true, (cudaStream_t)stream);
+}
+void ppmg_util_rank2d_d_dev(const double* xp, int64_t ldxp, int64_t Np, const double* xmin,
+                            const double* xmax, const int* Nm, const int* Ngl, int* lpdx,
+                            int* lhbx, int64_t* icount, int* info, void* stream) {
+  rank_common(2, xp, ldxp, Np, xmin, xmax, Nm, Ngl, lpdx, lhbx, icount, info,
+              "ppmg_util_rank2d_d_dev", true, (cudaStream_t)stream);
+}
+void ppmg_util_rank3d_s_dev(const float* xp, int64_t ldxp, int64_t Np, const float* xmin,
+                            const float* xmax, const int* Nm, const int* Ngl, int* lpdx,
+                            int* lhbx, int64_t* icount, int* info, void* stream) {
+  rank_common(3, xp, ldxp, Np, xmin, xmax, Nm, Ngl, lpdx, lhbx, icount, info,
+              "ppmg_util_rank3d_s_dev", true, (cudaStream_t)stream);
+}
+void ppmg_util_rank2d_s_dev(const float* xp, int64_t ldxp, int64_t Np, const float* xmin,
+                            const float* xmax, const int* Nm, const int* Ngl, int* lpdx,
+                            int* lhbx, int64_t* icount, int* info, void* stream) {
+  rank_common(2, xp, ldxp, Np, xmin, xmax, Nm, Ngl, lpdx, lhbx, icount, info,
+              "ppmg_util_rank2d_s_dev", true, (cudaStream_t)stream);
 }
 void ppmg_util_rank3d_s(const float* xp, int64_t ldxp, int64_t Np, const float* xmin,
                         const float* xmax, const int* Nm, const int* Ngl, int* lpdx,

@@ -339,23 +339,32 @@ def ppm_rmsh_create_part(field_up, topo_id, mesh_id, cutoff, lda=None, resetpos=
 
 def ppm_util_rank(xp, Np, xmin, xmax, Nm, Ngl):
     """ppm_util_rank{2,3}d: returns (info, lpdx, lhbx) with 1-based entries.
-    float32 positions select ppm_util_rank{2,3}d_s (bounds and spacing in FP32)."""
+    float32 positions select ppm_util_rank{2,3}d_s (bounds and spacing in FP32);
+    torch CUDA positions the device twins (lpdx, lhbx as device int32 tensors)."""
     _check(xp)
     k = _kind(xp)
     dim = len(Nm)
     nbox = 1
     for a in range(dim):
         nbox *= int(Nm[a]) + int(Ngl[a]) + int(Ngl[dim + a])
-    lpdx = np.zeros(max(int(Np), 1), dtype=np.int32)
-    lhbx = np.zeros(nbox + 1, dtype=np.int32)
+    dev = _is_dev(xp)
+    if dev:
+        lpdx = torch.zeros(max(int(Np), 1), dtype=torch.int32, device=xp.device)
+        lhbx = torch.zeros(nbox + 1, dtype=torch.int32, device=xp.device)
+    else:
+        lpdx = np.zeros(max(int(Np), 1), dtype=np.int32)
+        lhbx = np.zeros(nbox + 1, dtype=np.int32)
     ic = C.c_int64(0)
     info = C.c_int(0)
     ft = np.float64 if k == "d" else np.float32
     xmin = np.ascontiguousarray(xmin, dtype=ft)
     xmax = np.ascontiguousarray(xmax, dtype=ft)
-    getattr(lib(), f"ppmg_util_rank{dim}d_{k}")(
-        _addr(xp), xp.shape[0], int(Np), xmin.ctypes.data, xmax.ctypes.data, int_array(Nm),
-        int_array(Ngl), lpdx.ctypes.data, lhbx.ctypes.data, C.byref(ic), C.byref(info))
+    a = (_addr(xp), xp.shape[0], int(Np), xmin.ctypes.data, xmax.ctypes.data, int_array(Nm),
+         int_array(Ngl), _addr(lpdx), _addr(lhbx), C.byref(ic), C.byref(info))
+    if dev:
+        getattr(lib(), f"ppmg_util_rank{dim}d_{k}_dev")(*a, _stream())
+    else:
+        getattr(lib(), f"ppmg_util_rank{dim}d_{k}")(*a)
     return info.value, lpdx[: ic.value], lhbx
 
 

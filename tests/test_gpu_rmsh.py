@@ -370,3 +370,24 @@ def test_ghost_single_device_twin_matches_host(maptype):
         Fo = F.astype(np.float64, order="F")
         O.ghost_put(t, Fo, lb, ub, g)
         assert max_rel(Fh.astype(np.float64), Fo) < 1e-6
+
+
+@pytest.mark.parametrize("dim,dtype", [(3, np.float64), (2, np.float64), (3, np.float32),
+                                       (2, np.float32)])
+def test_util_rank_device_twins_match_host(dim, dtype):
+    """ppm_util_rank on torch CUDA positions (the `_dev` twins, lists left on
+    the device) equals the host entry points bit for bit."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(140 + dim)
+    xmin = np.array([0.1, -0.3, 0.25][:dim])
+    xmax = np.array([0.7, 0.9, 1.0][:dim])
+    Nm = [23, 17, 11][:dim]
+    Ngl = [1] * (2 * dim)
+    xp = (xmin[:, None] - 0.05 + rng.random((dim, 50000)) * (xmax - xmin + 0.1)[:, None])
+    xp = np.asfortranarray(xp.astype(dtype))
+    ih, lh, hh = ppmg.ppm_util_rank(xp, xp.shape[1], xmin, xmax, Nm, Ngl)
+    xd = torch.from_numpy(np.ascontiguousarray(xp.T)).cuda().t()
+    idv, ld, hd = ppmg.ppm_util_rank(xd, xp.shape[1], xmin, xmax, Nm, Ngl)
+    assert ih == 0 and idv == 0, ppmg.last_error()
+    assert ld.is_cuda and hd.is_cuda
+    assert np.array_equal(ld.cpu().numpy(), lh) and np.array_equal(hd.cpu().numpy(), hh)
