@@ -293,6 +293,27 @@ void ppmg_util_rank3d_s(const float* xp, int64_t ldxp, int64_t Np, const float* 
 void ppmg_util_rank2d_s(const float* xp, int64_t ldxp, int64_t Np, const float* xmin,
                         const float* xmax, const int* Nm, const int* Ngl, int* lpdx,
                         int* lhbx, int64_t* icount, int* info);
+/* ---- particle redistribution between z-slab subdomains (the routing of
+ * ppm_map_part_partial, ppm/src/ppm_map_part_partial.f:288-420) ------------
+ * route: every particle of the device array xp goes to the subdomain that
+ * contains it among the local slab and its two z neighbours (closed-lower /
+ * open-upper boxes; positions are expected inside the domain, the client
+ * imposing the periodic bounds first as in PPM).  perm (device, Np ints)
+ * receives the particle ids grouped by class: kept, to the slab below, to the
+ * slab above, in no neighbour; each class in ascending id.  counts (host, 4)
+ * receives the class sizes; the call returns once they are known.  Particles
+ * in no neighbour give info = -2, errno 405.
+ * gather: dst(0:lda-1, j) = src(0:lda-1, perm[j]) for j < n (device arrays;
+ * positions or any particle property). */
+void ppmg_map_part_route_d_dev(const double* xp, int64_t ldxp, int64_t Np, int topo_id,
+                               int mesh_id, int* perm, int64_t* counts, int* info, void* stream);
+void ppmg_map_part_route_s_dev(const float* xp, int64_t ldxp, int64_t Np, int topo_id,
+                               int mesh_id, int* perm, int64_t* counts, int* info, void* stream);
+void ppmg_map_part_gather_d_dev(const double* src, int64_t lds, int lda, const int* perm,
+                                int64_t n, double* dst, int64_t ldd, int* info, void* stream);
+void ppmg_map_part_gather_s_dev(const float* src, int64_t lds, int lda, const int* perm,
+                                int64_t n, float* dst, int64_t ldd, int* info, void* stream);
+
 /* Device twins: xp, lpdx (Np entries, the first icount valid) and lhbx
  * (nbox+1) are device arrays, the work runs on `stream`; the bounds, Nm and
  * Ngl are host arrays.  The call returns once the lists are complete (the

@@ -19,6 +19,7 @@
 #include "ppmg_m2p.cuh"
 #include "ppmg_p2m.cuh"
 #include "ppmg_rmsh.cuh"
+#include "ppmg_map.cuh"
 #include "ppmg_sort.cuh"
 
 namespace ppmg {
@@ -58,6 +59,7 @@ struct Handle {
   Geom g{};
   Workspace ws;       // P2M / M2P / adjoint / ghost / clist scratch
   Workspace ws_rmsh;  // comp_weights -> remesh state (ppm_module_data_rmsh)
+  Workspace ws_map;   // particle routing between slabs
   cudaStream_t stream = nullptr;
   int* d_status = nullptr;  // [0] particles outside the sub, [1] non-finite
   // position fingerprints: [0] of the sort held in ws, [1] of an M2P's xp
@@ -1438,6 +1440,112 @@ void ppmg_rmsh_create_part_s_dev(const float* field_up, int64_t ldf, int lda,
   create_part_common<float>(field_up, ldf, lda, f_lb, f_ub, topo_id, mesh_id, cutoff,
                             cutoff_weights, resetpos, field_wp, ldfw, lda2, np, up, xp, wp, info,
                             true, (cudaStream_t)stream, "ppmg_rmsh_create_part_s_dev");
+}
+
+// ---- particle routing between z-slab subdomains -------------------------------------
+extern "C++" {
+template <class T>
+static void route_common(const T* xp, int64_t ldxp, int64_t Np, int topo_id, int mesh_id,
+                         int* perm, int64_t* counts, int* info, cudaStream_t st,
+                         const char* caller) {
+  clear_error();
+  if (info) *info = 0;
+  Handle* hh = find_handle(topo_id, mesh_id);
+  if (!hh) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": topo_id/mesh_id is invalid"); return; }
+  Handle* h = get_checked(topo_id, mesh_id, 3, caller, info, true);
+  if (!h) return;
+  if (Np < 0 || (Np > 0 && ldxp < 3) || Np >= (int64_t)1 << 31) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": invalid sizes"); return; }
+  std::lock_guard<std::mutex> lk(h->mu);
+  // the local slab and its z neighbours (periodic across the domain's z faces)
+  RouteParams R{};
+  const int s = h->local_sub;
+  const double zmin = h->g.min_phys[2], zmax = h->g.max_phys[2];
+  auto box = [&](int c, int sub) {
+    R.zlo[c] = h->min_sub[3 * sub + 2];
+    R.zhi[c] = h->max_sub[3 * sub + 2];
+    R.zlof[c] = (float)R.zlo[c];
+    R.zhif[c] = (float)R.zhi[c];
+  };
+  for (int c = 0; c < 3; ++c) R.zlo[c] = R.zhi[c] = 0.0, R.zlof[c] = R.zhif[c] = 0.0f;
+  box(0, s);
+  if (h->open_z) {
+    const double lo = h->min_sub[3 * s + 2], hi = h->max_sub[3 * s + 2];
+    for (int q = 0; q < h->nsubs; ++q) {
+      if (q == s) continue;
+      if (h->max_sub[3 * q + 2] == (lo > zmin ? lo : zmax)) box(1, q);
+      if (h->min_sub[3 * q + 2] == (hi < zmax ? hi : zmin)) box(2, q);
+    }
+  }
+  for (int a = 0; a < 2; ++a) {
+    R.lo[a] = h->g.min_sub[a];
+    R.hi[a] = h->g.max_sub[a];
+    R.lof[a] = (float)R.lo[a];
+    R.hif[a] = (float)R.hi[a];
+  }
+  if (counts)
+    for (int c = 0; c < 4; ++c) counts[c] = 0;
+  if (Np == 0) return;
+  const int nblk = route_blocks(Np);
+  Workspace& ws = h->ws_map;
+  cudaError_t e;
+  if ((e = ws.key.ensure((size_t)Np)) || (e = ws.count.ensure(sizeof(int) * 4 * (size_t)nblk)) ||
+      (e = ws.start.ensure(sizeof(int) * 4 * (size_t)nblk))) { cuda_fail(info, e, caller); return; }
+  if ((e = launch_route<T>(R, xp, ldxp, Np, static_cast<unsigned char*>(ws.key.p),
+                           ws.count.as<int>(), ws.start.as<int>(), perm, ws, st))) {
+    cuda_fail(info, e, caller);
+    return;
+  }
+  // class starts: off[c * nblk] (c = 1..3); the call returns once they are read
+  int st4[4] = {0, 0, 0, 0};
+  for (int c = 1; c < 4 && !e; ++c)
+    e = cudaMemcpyAsync(st4 + c, ws.start.as<int>() + (size_t)c * nblk, sizeof(int),
+                        cudaMemcpyDeviceToHost, st);
+  if (!e) e = cudaStreamSynchronize(st);
+  if (e) { cuda_fail(info, e, caller); return; }
+  if (counts) {
+    counts[0] = st4[1];
+    counts[1] = st4[2] - st4[1];
+    counts[2] = st4[3] - st4[2];
+    counts[3] = Np - st4[3];
+  }
+  if (Np - st4[3] > 0)
+    fail(info, kErrorError, kErrPartUnass,
+         std::string(caller) + ": " + std::to_string(Np - st4[3]) +
+             " particles lie in no neighbouring subdomain");
+}
+
+template <class T>
+static void gather_common(const T* src, int64_t lds, int lda, const int* perm, int64_t n, T* dst,
+                          int64_t ldd, int* info, cudaStream_t st, const char* caller) {
+  clear_error();
+  if (info) *info = 0;
+  if (n < 0 || lda < 1 || lds < lda || ldd < lda) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": invalid sizes"); return; }
+  cudaError_t e = launch_gather_cols<T>(src, lds, lda, perm, n, dst, ldd, st);
+  if (e) cuda_fail(info, e, caller);
+}
+}  // extern "C++"
+
+void ppmg_map_part_route_d_dev(const double* xp, int64_t ldxp, int64_t Np, int topo_id,
+                               int mesh_id, int* perm, int64_t* counts, int* info,
+                               void* stream) {
+  route_common<double>(xp, ldxp, Np, topo_id, mesh_id, perm, counts, info, (cudaStream_t)stream,
+                       "ppmg_map_part_route_d_dev");
+}
+void ppmg_map_part_route_s_dev(const float* xp, int64_t ldxp, int64_t Np, int topo_id,
+                               int mesh_id, int* perm, int64_t* counts, int* info,
+                               void* stream) {
+  route_common<float>(xp, ldxp, Np, topo_id, mesh_id, perm, counts, info, (cudaStream_t)stream,
+                      "ppmg_map_part_route_s_dev");
+}
+void ppmg_map_part_gather_d_dev(const double* src, int64_t lds, int lda, const int* perm,
+                                int64_t n, double* dst, int64_t ldd, int* info, void* stream) {
+  gather_common<double>(src, lds, lda, perm, n, dst, ldd, info, (cudaStream_t)stream,
+                        "ppmg_map_part_gather_d_dev");
+}
+void ppmg_map_part_gather_s_dev(const float* src, int64_t lds, int lda, const int* perm,
+                                int64_t n, float* dst, int64_t ldd, int* info, void* stream) {
+  gather_common<float>(src, lds, lda, perm, n, dst, ldd, info, (cudaStream_t)stream,
+                       "ppmg_map_part_gather_s_dev");
 }
 
 // ---- cell lists -------------------------------------------------------------------

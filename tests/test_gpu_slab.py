@@ -225,3 +225,38 @@ def test_slab_remeshing_chain_matches_oracle(nslab, kernel, lda):
     assert max_rel(upg, upo) < 1e-13 and np.array_equal(xpg, xpo)
     for ts in hs:
         ppmg.unregister(ts)
+
+
+@pytest.mark.parametrize("nslab,far", [(3, 0), (2, 0), (4, 5)])
+def test_particle_redistribution_on_gpu(nslab, far):
+    """ppm_map_part_partial's routing and packing kernels on every slab, the
+    blocks exchanged in-process: each slab ends with exactly the particles it
+    contains (kept ones first, then arrivals from below, then from above),
+    their properties intact; particles two slabs away are reported (405) and
+    dropped."""
+    from ppm_legacy_b200 import mapping
+    from test_slab_exchange import check_mapping, moved_particles, route_rule
+    t = topo_for(3, 12, decomp=(1, 1, nslab))
+    hs = slab_handles(t)
+    before, parts = {}, {}
+    for s, ts in enumerate(hs):
+        rng = np.random.default_rng(600 + s)
+        x = moved_particles(t, s, 5000, rng, far=far)
+        ids = np.arange(s * 100000, s * 100000 + 5000, dtype=np.int64)[None, :]
+        u = np.asfortranarray(rng.standard_normal((3, 5000)))
+        before[s] = (x, ids, u)
+        parts[s] = (ts.topo_id, 1, dev_f(x), [dev_f(ids), dev_f(u)])
+    info, res = mapping.map_subs(parts, t, halo.LocalComm())
+    after = {s: (host(x2), host(p2[0]), host(p2[1])) for s, (x2, p2) in res.items()}
+    if far:
+        assert info == -2
+        for s in before:  # the far particles are dropped before the check
+            keep = route_rule(t, s, before[s][0]) < 3
+            before[s] = tuple(np.asfortranarray(a[:, keep]) for a in before[s])
+    else:
+        assert info == 0, ppmg.last_error()
+    check_mapping(t, before, after)
+    assert sum(a[0].shape[1] for a in after.values()) == sum(b[0].shape[1]
+                                                             for b in before.values())
+    for ts in hs:
+        ppmg.unregister(ts)

@@ -150,3 +150,118 @@ def test_put_then_get_over_gloo(world):
         p.join(timeout=60)
         assert p.exitcode == 0
     assert all(v == "ok" for v in res.values()), res
+
+
+# ---- particle redistribution between slabs (ppm_legacy_b200.mapping) --------
+
+def route_rule(topo, s, x):
+    """Class of every particle of slab s (0 kept, 1 below, 2 above, 3 none):
+    closed-lower / open-upper boxes, the first match in that order."""
+    below, above = halo.neighbours(topo, s)
+    inxy = np.ones(x.shape[1], bool)
+    for a in range(2):
+        inxy &= (x[a] >= topo.min_phys[a]) & (x[a] < topo.max_phys[a])
+    cls = np.full(x.shape[1], 3)
+    for c, q in reversed(list(enumerate([s, below, above]))):
+        cls[inxy & (x[2] >= topo.min_sub[q, 2]) & (x[2] < topo.max_sub[q, 2])] = c
+    return cls
+
+
+def moved_particles(topo, s, n, rng, far=0):
+    """n particles of slab s displaced by up to 0.4 of a slab in z (periodic);
+    `far` of them moved two slabs away."""
+    lo, hi = topo.min_sub[s, 2], topo.max_sub[s, 2]
+    L = topo.max_phys[2] - topo.min_phys[2]
+    x = rng.random((3, n))
+    x[2] = lo + x[2] * (hi - lo) + rng.uniform(-0.4, 0.4, n) * (hi - lo)
+    x[2, :far] += 2 * (hi - lo)
+    x[2] = np.mod(x[2] - topo.min_phys[2], L) + topo.min_phys[2]
+    return np.asfortranarray(x)
+
+
+def check_mapping(topo, before, after):
+    """before/after {s: (xp, ids, u)} numpy; every particle ends in the slab
+    that contains it, kept ones first in their order, then arrivals from
+    below, then from above, each in the sender's order."""
+    for s, (x, ids, u) in after.items():
+        cls = route_rule(topo, s, x)
+        assert (cls == 0).all()
+        below, above = halo.neighbours(topo, s)
+        xb, ib, ub = before[s]
+        cb = route_rule(topo, s, xb)
+        exp = [ib[0][cb == 0]]
+        for q, c in ((below, 2), (above, 1)):
+            xq, iq, _ = before[q]
+            exp.append(iq[0][route_rule(topo, q, xq) == c])
+        if below == above:  # two slabs: the neighbour's both groups come from one rank
+            xq, iq, _ = before[below]
+            cq = route_rule(topo, below, xq)
+            exp = [ib[0][cb == 0], iq[0][cq == 1]]
+        assert np.array_equal(ids[0], np.concatenate(exp)), s
+        # positions and properties travel with their particle
+        allx = np.concatenate([before[q][0] for q in before], axis=1)
+        allu = np.concatenate([before[q][2] for q in before], axis=1)
+        alli = np.concatenate([before[q][1] for q in before], axis=1)[0]
+        pos = {int(i): k for k, i in enumerate(alli)}
+        idx = [pos[int(i)] for i in ids[0]]
+        assert np.array_equal(x, allx[:, idx]) and np.array_equal(u, allu[:, idx])
+
+
+def _cpu_route(topo, s):
+    def route(tid, mid, xp):
+        cls = route_rule(topo, s, xp.numpy())
+        perm = np.concatenate([np.nonzero(cls == c)[0] for c in range(4)]).astype(np.int32)
+        return (-2 if (cls == 3).any() else 0), torch.from_numpy(perm), \
+            [int((cls == c).sum()) for c in range(4)]
+    return route
+
+
+def _cpu_gather(src, perm, n):
+    return src.t()[perm[:n].long()].t()
+
+
+def _map_main(rank, world, port, out):
+    from ppm_legacy_b200 import mapping
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        t = topo_for(3, 12, decomp=(1, 1, world))
+        before = {}
+        for s in range(world):
+            rng = np.random.default_rng(500 + s)
+            x = moved_particles(t, s, 300, rng)
+            before[s] = (x, np.arange(s * 1000, s * 1000 + 300)[None, :],
+                         np.asfortranarray(rng.standard_normal((2, 300))))
+        x, i, u = before[rank]
+        parts = {rank: (1, 1, torch.from_numpy(x), [torch.from_numpy(np.asfortranarray(i)),
+                                                    torch.from_numpy(u)])}
+        info, res = mapping.map_subs(parts, t, halo.DistComm(), route=_cpu_route(t, rank),
+                                     gather=_cpu_gather)
+        x2, (i2, u2) = res[rank]
+        check_mapping(t, before, {rank: (x2.numpy(), i2.numpy(), u2.numpy())})
+        assert info == 0
+        dist.barrier()
+        out.put((rank, "ok"))
+    except Exception as e:  # reported to the parent, which fails the test
+        import traceback
+        out.put((rank, traceback.format_exc()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_particle_redistribution_over_gloo(world):
+    """The size and particle-block exchange of ppm_map_part_partial over gloo
+    (routing by a restatement of the rule on CPU; the device kernels are
+    tested on the GPU)."""
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_map_main, args=(r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(out.get(timeout=180) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert all(v == "ok" for v in res.values()), res
