@@ -75,14 +75,15 @@ void ppmg_mesh_unregister(int topo_id, int mesh_id, int* info);
  * ppm_isublist of the process (ppm/src/ppm_topo_mkfield.f:311-319 builds the
  * reference's per-process sub list).  Required when nsubs > 1.  Supported
  * decomposition: slabs along z, every subdomain spanning x and y.  On a
- * slab the 3D P2M, M2P and remeshing (comp_weights, remesh, create_part)
- * compute on the local sub with z not periodic: P2M and remesh leave in
- * their z ghost planes the contributions owed to the neighbouring slabs, M2P
- * reads its z ghost planes, create_part skips the slab's shared upper node
- * plane; the exchange between the slabs (the ghost put / get of
- * ppm_map_field_ghost, ppm_map_field_send.f) is the caller's, e.g.
- * ppm_legacy_b200.halo over torch.distributed.  The adjoint, the 2D routines
- * and the standalone ghost mapping return info = -2 (errno 503) on a slab. */
+ * slab the 3D P2M, M2P, P2M adjoint and remeshing (comp_weights, remesh,
+ * create_part) compute on the local sub with z not periodic: P2M and remesh
+ * leave in their z ghost planes the contributions owed to the neighbouring
+ * slabs, M2P and the adjoint read their field's z ghost planes, create_part
+ * skips the slab's shared upper node plane; the exchange between the slabs
+ * (the ghost put / get of ppm_map_field_ghost, ppm_map_field_send.f) is the
+ * caller's, e.g. ppm_legacy_b200.halo over torch.distributed.  The
+ * standalone ghost mapping and the allocation-free P2M return info = -2
+ * (errno 503) on a slab. */
 void ppmg_mesh_set_local_sub(int topo_id, int mesh_id, int isub, int* info);
 
 /* Wait for all work of the handle's `_dev` calls on `stream` and return the

@@ -591,6 +591,12 @@ int adjoint_pipeline(Handle& h, const double* xp, int64_t ldxp, int64_t Np, cons
     lo[a] = 1;
     hi[a] = h.g.N[a];
   }
+  if (h.open_z) {
+    // a z-slab reads r's z ghost planes (the adjoint of the put is a get)
+    const int HL = kernel == kKernelMp4 ? 2 : 1;
+    lo[2] = 2 - HL;
+    hi[2] = h.g.N[2] + HL;
+  }
   FieldDesc fd;
   if (!make_fd(h, ldf, f_lb, f_ub, lo, hi, fd, caller, info)) return *info;
   if (Np == 0) return 0;
@@ -603,7 +609,7 @@ int adjoint_pipeline(Handle& h, const double* xp, int64_t ldxp, int64_t Np, cons
     h.sort_cached = false;  // the work items below describe this sort only
     KeyParams kp = make_kp(h, KEY_INTERP_WRAP, false);
     e = sort_interp<double>(h, kp, xp, ldxp, nullptr, 0, 0, Np, prec == M2P_FP64,
-                            h.d_status + 1, dw, lddw, lda, st);
+                            h.d_status + (h.open_z ? 0 : 1), dw, lddw, lda, st);
     if (e) return cuda_fail(info, e, caller);
   }
   const int* dnv = d_nvalid_of(h.ws, h.g.ncell);
@@ -622,11 +628,13 @@ int adjoint_pipeline(Handle& h, const double* xp, int64_t ldxp, int64_t Np, cons
   P.ldupin = ldup;
   P.dx = dx;
   P.lddx = lddx;
+  P.open_z = h.open_z ? 1 : 0;
   for (int a = 0; a < 3; ++a) P.dxi[a] = h.g.dxi_d[a];
   if (lda <= 4) {
     TileItems ti;
     if ((e = h.ws.tiles.ensure(tile_items_bytes(P.N)))) return cuda_fail(info, e, caller);
-    if (reuse) {
+    // a z-slab's P2M items cover node planes, not cell layers: own items
+    if (reuse && !h.open_z) {
       ti = tile_items_view(h.ws.tiles.p, P.N);
     } else if ((e = make_tile_items(h.ws.start.as<int>(), P.N, Np, h.ws.tiles.p, ti, st))) {
       return cuda_fail(info, e, caller);
@@ -963,7 +971,7 @@ static void adjoint_common(const double* xp, int64_t ldxp, int64_t Np, const dou
     return;
   }
   if (!check_kernel(kernel, caller, info)) return;
-  Handle* h = get_checked(topo_id, mesh_id, 3, caller, info);
+  Handle* h = get_checked(topo_id, mesh_id, 3, caller, info, true);
   if (!h) return;
   std::lock_guard<std::mutex> lk(h->mu);
   if (dev) {

@@ -659,7 +659,8 @@ cudaError_t launch_m2p(const M2PParams& P0, int dim, int kernel, M2PPrec prec, c
 
 template <int S, class CT, int LC>
 cudaError_t launch_adjoint_tile(const M2PParams& P, cudaStream_t st) {
-  auto kern = k_m2p3d_tile<S, CT, false, double, LC, true>;
+  auto kern = P.open_z ? k_m2p3d_tile<S, CT, false, double, LC, true, true>
+                       : k_m2p3d_tile<S, CT, false, double, LC, true>;
   const size_t smem = m2p_ring_bytes<S, CT, LC>();
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);

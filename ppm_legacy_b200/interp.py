@@ -166,10 +166,17 @@ def ppm_interp_m2p(xp, Np, up, *args, field_lb=None):
 
 
 def ppm_interp_p2m_adjoint(xp, Np, up, lda, topo_id, mesh_id, kernel, r_field, dw, dx,
-                           ghostsize=(0, 0, 0), field_lb=None):
-    """Adjoint of P2M (3D, FP64): dw = M2P(r), dx = sum_a up(a) grad_x W . r(a)."""
+                           ghostsize=(0, 0, 0), field_lb=None, exchange=True):
+    """Adjoint of P2M (3D, FP64): dw = M2P(r), dx = sum_a up(a) grad_x W . r(a).
+
+    On a z-slab handle the adjoint of P2M's ghost put is a ghost get: r's z
+    ghost planes are filled from the neighbouring slabs first (exchange=False:
+    the caller's); r then needs z ghost layers (ghostsize / field_lb).
+    """
     _check(xp, up, r_field, dw, dx)
     lb, ub = _bounds(r_field, 3, True, ghostsize, field_lb)
+    if exchange and _topo.is_slab(topo_id, mesh_id):
+        _slab_exchange(r_field, topo_id, mesh_id, ghostsize, lb, False)
     info = C.c_int(0)
     a = (_addr(xp), xp.shape[0], int(Np), _addr(up), up.shape[0], int(lda), topo_id, mesh_id,
          kernel, _addr(r_field), r_field.shape[0], lb, ub, _addr(dw), dw.shape[0], _addr(dx),

@@ -150,16 +150,18 @@ def test_slab_particle_outside_its_slab_is_unassigned():
 
 
 def test_slab_handle_refuses_other_routines():
-    """The adjoint keeps one periodic subdomain per GPU; only z-slabs split."""
+    """The C-ABI ghost mapping leaves the exchange between slabs to the host;
+    only z-slab decompositions are accepted."""
+    import ctypes as C
+    from ppm_legacy_b200._lib import int_array
     t = topo_for(3, 12, decomp=(1, 1, 2))
     hs = slab_handles(t)
-    xp = np.asfortranarray(np.array([[0.5], [0.5], [0.25]]))
-    up = np.ones((1, 1), order="F")
-    R = np.zeros((1, 12, 12, 6, 1), order="F")
-    info = ppmg.ppm_interp_p2m_adjoint(xp, 1, up, 1, hs[0].topo_id, 1, 2, R,
-                                       np.zeros((1, 1), order="F"), np.zeros((3, 1), order="F"),
-                                       field_lb=[1, 1, 1])
-    assert info == -2 and "slab" in ppmg.last_error()[2]
+    F = np.zeros((1, 17, 17, 11, 1), order="F")
+    info = C.c_int(0)
+    ppmg.lib().ppmg_map_field_ghost_d(F.ctypes.data, 1, 1, int_array([-1] * 3, C.c_int64),
+                                      int_array([15, 15, 9], C.c_int64), hs[0].topo_id, 1,
+                                      int_array([2, 2, 2]), 5, C.byref(info))
+    assert info.value == -2 and "slab" in ppmg.last_error()[2]
     t2 = topo_for(3, 12, decomp=(2, 1, 1), topo_id=7900)
     ppmg.register(t2)
     import ctypes as C
@@ -258,5 +260,47 @@ def test_particle_redistribution_on_gpu(nslab, far):
     check_mapping(t, before, after)
     assert sum(a[0].shape[1] for a in after.values()) == sum(b[0].shape[1]
                                                              for b in before.values())
+    for ts in hs:
+        ppmg.unregister(ts)
+
+
+@pytest.mark.parametrize("nslab,kernel", [(3, 2), (2, 1)])
+def test_slab_adjoint_matches_global_oracle(nslab, kernel):
+    """The P2M adjoint on every slab (r's z ghost planes by the ghost get
+    between the slabs) equals the oracle's adjoint over the whole domain."""
+    rng = np.random.default_rng(700 + nslab)
+    nc, lda = 12, 2
+    t = topo_for(3, nc, decomp=(1, 1, nslab))
+    t1 = topo_for(3, nc)
+    n = 3000
+    xp = random_particles(rng, 3, n)
+    up = np.asfortranarray(rng.standard_normal((lda, n)))
+    R = rng.standard_normal((lda, nc, nc, nc))
+    dwo, dxo = O.p2m_adjoint(t1, xp, up, np.asfortranarray(R[..., None]), [1, 1, 1], [nc] * 3,
+                             kernel)
+    lst, si = O.assign(t, xp)
+    ids = np.split(lst, np.cumsum(si)[:-1])
+    hs = slab_handles(t)
+    g = 2
+    rs = {}
+    for s in range(nslab):
+        z0 = int(t.istart[s, 2]) - 1
+        nz = int(t.nnodes[s, 2]) - 1
+        zi = (z0 + np.arange(1 - g, nz + 2 + g) - 1) % nc
+        loc = np.array(R[:, :, :, zi])
+        loc[:, :, :, :g] = 0.0          # ghost planes: from the neighbours
+        loc[:, :, :, nz + 1 + g:] = 0.0
+        rs[s] = dev_f(loc[..., None])
+    halo.get(rs, t, [0, 0, g], [1, 1, 1 - g], halo.LocalComm())
+    for s, ts in enumerate(hs):
+        m = len(ids[s])
+        dw = dev_f(np.zeros((lda, m)))
+        dx = dev_f(np.zeros((3, m)))
+        assert ppmg.ppm_interp_p2m_adjoint(dev_f(xp[:, ids[s]]), m, dev_f(up[:, ids[s]]), lda,
+                                           ts.topo_id, 1, kernel, rs[s], dw, dx,
+                                           field_lb=[1, 1, 1 - g], exchange=False) == 0
+        assert ppmg.sync_status(ts.topo_id, 1) == 0, ppmg.last_error()
+        assert max_rel(host(dw), dwo[:, ids[s]]) < 1e-12
+        assert max_rel(host(dx), dxo[:, ids[s]]) < 1e-11
     for ts in hs:
         ppmg.unregister(ts)
