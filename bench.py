@@ -67,6 +67,8 @@ def max_over_ranks(x, dist=None, device=None):
     if dist is None or not dist.is_available() or not dist.is_initialized():
         return float(x)
     import torch
+    if dist.get_backend() != "nccl":
+        device = "cpu"
     t = torch.tensor([float(x)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
@@ -444,6 +446,9 @@ def main():
     ap.add_argument("--cpu-warmup", type=int, default=0)
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--dist-backend", default="nccl", choices=["nccl", "gloo"],
+                    help="N > 1: the process-group backend (gloo stages the slab exchange "
+                         "through host memory)")
     ap.add_argument("--workload", default="roundtrip", choices=["roundtrip", "remesh", "adjoint"],
                     help="roundtrip: the metric (default); remesh / adjoint: the 256^3 remesh "
                          "and 128^3 adjoint workloads, one JSON line each")
@@ -462,13 +467,16 @@ def main():
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0")) % max(torch.cuda.device_count(), 1)
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     if world > 1:
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=dev)
+        if args.dist_backend == "nccl":
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=dev)
+        else:  # host-staged transport (validation of the multi-rank flow)
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
     xp, up, nc, n = gen_particles(torch, args.config, dev, seed=1000 + rank)
     if world > 1:
         # one z-slab per rank; P2M ends with the ghost put between the slabs
@@ -704,13 +712,17 @@ def main():
             "dtype": "f32+f64 (mixed: FP64 offsets, FP32 weights, compensated FP32 sums)"
             if head == 1 else "f64",
             "data": "synthetic (seeded, generated on device)",
-            "config": {"workload": f"3D M'4 P2M+M2P round trip, {nc}^3 periodic mesh, {n} "
-                                   f"particles per GPU ({CONFIGS[args.config][2]}), lda 3, "
+            "config": {"workload": (f"3D M'4 P2M+M2P round trip, {nc}^3 periodic mesh"
+                                    if world == 1 else
+                                    f"3D M'4 P2M+M2P round trip, one {nc}^3 slab per GPU of a "
+                                    f"{nc}x{nc}x{nc * world} periodic mesh") +
+                                   f", {n} particles per GPU ({CONFIGS[args.config][2]}), lda 3, "
                                    f"ghostsize 2",
                        "l2": "inputs larger than L2 (xp/up/field each > 126 MB)",
                        "parallelism": "1 periodic subdomain" if world == 1 else
-                       f"{world} z-slab subdomains of a 512x512x{512 * world} mesh, ghost put/get "
-                       "between neighbouring slabs over NCCL"},
+                       f"{world} z-slab subdomains of a {nc}x{nc}x{nc * world} periodic mesh, "
+                       f"ghost put/get between neighbouring slabs over "
+                       f"{args.dist_backend.upper()}"},
             "roofline": roof, "forms": parts, "clocks": clocks, "gpu_launches": launches,
             "e2e": e2e, "cpu_baseline": cb, "adjoint": adj,
         }

@@ -167,14 +167,15 @@ class DistComm:
         import torch
         import torch.distributed as dist
         me = dist.get_rank(self.group)
-        # NCCL moves device memory only: host blocks (the host-pointer API)
-        # travel through device copies
-        dev = None
+        # NCCL moves device memory only, gloo host memory only: blocks on the
+        # other side travel through copies
         if dist.get_backend(self.group) == "nccl":
             dev = torch.device("cuda", torch.cuda.current_device())
+        else:
+            dev = torch.device("cpu")
 
         def wire(t):
-            return t.to(dev) if dev is not None and t.device.type == "cpu" else t.contiguous()
+            return t.to(dev) if t.device != dev else t.contiguous()
 
         ops, bufs, local = [], [], {}
         for src, dst, tag, t in sends:
@@ -183,8 +184,7 @@ class DistComm:
             else:
                 ops.append(dist.P2POp(dist.isend, wire(t), self._peer(dst), self.group, tag))
         for dst, src, tag, like in recvs:
-            buf = torch.empty_like(like, memory_format=torch.contiguous_format,
-                                   device=dev if dev is not None else like.device)
+            buf = torch.empty_like(like, memory_format=torch.contiguous_format, device=dev)
             bufs.append(buf)
             if self._rank(src) != me:
                 ops.append(dist.P2POp(dist.irecv, buf, self._peer(src), self.group, tag))
