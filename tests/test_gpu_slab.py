@@ -90,7 +90,7 @@ def run(nc, nslab, kernel, g, lda, mode, seed, n=None):
 
 
 @pytest.mark.parametrize("nc,nslab,kernel,g,lda", [
-    (16, 2, 2, 2, 3), (12, 3, 2, 2, 1), (16, 4, 1, 1, 2), (12, 2, 2, 3, 5)])
+    (16, 2, 2, 2, 3), (12, 3, 2, 2, 1), (16, 4, 1, 1, 2), (12, 2, 2, 3, 5), (13, 3, 2, 2, 3)])
 def test_slab_p2m_put_get_m2p_match_oracle(nc, nslab, kernel, g, lda):
     run(nc, nslab, kernel, g, lda, 0, seed=nc * nslab + kernel)
 
@@ -172,14 +172,13 @@ def test_slab_handle_refuses_other_routines():
         ppmg.unregister(ts)
 
 
-@pytest.mark.parametrize("nslab,kernel,lda", [(2, 2, 3), (3, 1, 1)])
-def test_slab_remeshing_chain_matches_oracle(nslab, kernel, lda):
+@pytest.mark.parametrize("nslab,kernel,lda,nc", [(2, 2, 3, 12), (3, 1, 1, 12), (3, 2, 2, 13)])
+def test_slab_remeshing_chain_matches_oracle(nslab, kernel, lda, nc):
     """comp_weights, remesh (+ ghost put between the slabs) and create_part on
     every slab against the oracle's multi-subdomain remeshing: weights bit for
     bit, the field to summation order, the new particles slab by slab in the
     reference's order (the shared upper plane of a slab creates none)."""
-    rng = np.random.default_rng(200 + nslab)
-    nc = 12
+    rng = np.random.default_rng(200 + nslab + nc)
     t = topo_for(3, nc, decomp=(1, 1, nslab))
     n = 2 * nc ** 3
     xp = random_particles(rng, 3, n)
