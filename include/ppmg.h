@@ -294,6 +294,28 @@ void ppmg_util_rank3d_s(const float* xp, int64_t ldxp, int64_t Np, const float* 
 void ppmg_util_rank2d_s(const float* xp, int64_t ldxp, int64_t Np, const float* xmin,
                         const float* xmax, const int* Nm, const int* Ngl, int* lpdx,
                         int* lhbx, int64_t* icount, int* info);
+/* ---- FFT Poisson solver (ppm_fdsolver_solve_3d with the spectral step of
+ * ppm/src/ppm_fdsolver_poisson_3d.f:60-82) ----------------------------------
+ * Solves lap(phi) = omega on the periodic mesh of one subdomain, component
+ * by component, in place: omega is read at the unique nodes 1..Nm-1 of
+ * field_up(ldf, f_lb:f_ub), every mode of its transform is multiplied by
+ * -1/|k|^2 (k_a = 2 pi / L_a times the wave number folded to |.| <= N_a/2,
+ * the zero mode set to 0), and phi is written to every node of the box
+ * 1-g:Nm+g (real nodes and their periodic images).  FFTs by cuFFT (the
+ * reference uses FFTW); a z-slab handle returns info = -2. */
+void ppmg_fdsolver_poisson_3d_d(double* field_up, int64_t ldf, int lda, const int64_t* f_lb,
+                                const int64_t* f_ub, int topo_id, int mesh_id,
+                                const int* ghostsize, int* info);
+void ppmg_fdsolver_poisson_3d_s(float* field_up, int64_t ldf, int lda, const int64_t* f_lb,
+                                const int64_t* f_ub, int topo_id, int mesh_id,
+                                const int* ghostsize, int* info);
+void ppmg_fdsolver_poisson_3d_d_dev(double* field_up, int64_t ldf, int lda, const int64_t* f_lb,
+                                    const int64_t* f_ub, int topo_id, int mesh_id,
+                                    const int* ghostsize, int* info, void* stream);
+void ppmg_fdsolver_poisson_3d_s_dev(float* field_up, int64_t ldf, int lda, const int64_t* f_lb,
+                                    const int64_t* f_ub, int topo_id, int mesh_id,
+                                    const int* ghostsize, int* info, void* stream);
+
 /* ---- particle redistribution between z-slab subdomains (the routing of
  * ppm_map_part_partial, ppm/src/ppm_map_part_partial.f:288-420) ------------
  * route: every particle of the device array xp goes to the subdomain that

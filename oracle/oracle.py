@@ -360,3 +360,27 @@ def roundtrip_owned(topo, xp, owner, up, kernel, ghost, nthreads=0):
     if info != 0:
         raise OracleError(info, 0)
     return field, lb, ub, out
+
+
+def poisson(U, lengths):
+    """lap(phi) = omega on a periodic mesh, restated from the spectral step of
+    ppm_fdsolver_poisson_3d.f:60-82 (every mode times -1/|k|^2, k_a = 2 pi /
+    L_a times the wave number folded to |.| <= N_a/2, zero mode 0) between a
+    forward and a backward FFT normalised by 1/(Nx Ny Nz).  U(lda, Nx, Ny, Nz)
+    holds omega at the unique nodes; returns phi there (numpy FFTs)."""
+    U = np.asarray(U, dtype=np.float64)
+    nx, ny, nz = U.shape[1:]
+    k = [2.0 * np.pi / float(lengths[a]) *
+         np.minimum(np.arange(n), n - np.arange(n)).astype(np.float64)
+         for a, n in enumerate((nx, ny, nz))]
+    kx = k[0][: nx // 2 + 1]  # the real-to-complex axis: 0 .. nx/2
+    k2 = kx[:, None, None] ** 2 + k[1][None, :, None] ** 2 + k[2][None, None, :] ** 2
+    k2[0, 0, 0] = 1.0
+    out = np.empty_like(U)
+    for a in range(U.shape[0]):
+        spec = np.fft.rfftn(U[a], axes=(2, 1, 0))
+        spec = -spec / k2
+        spec[0, 0, 0] = 0.0
+        out[a] = np.fft.irfftn(spec, s=(nz, ny, nx), axes=(2, 1, 0))
+    return out
+

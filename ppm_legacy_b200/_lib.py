@@ -70,6 +70,10 @@ SIGNATURES = {
     "ppmg_util_rank3d_s": (_RANK, None),
     "ppmg_util_rank2d_s": (_RANK, None),
     "ppmg_util_rank3d_d_dev": (_RANK + [_vp], None),
+    "ppmg_fdsolver_poisson_3d_d": ([_pd, _i64, _i, _pi64, _pi64, _i, _i, _pi, _pi], None),
+    "ppmg_fdsolver_poisson_3d_s": ([_pd, _i64, _i, _pi64, _pi64, _i, _i, _pi, _pi], None),
+    "ppmg_fdsolver_poisson_3d_d_dev": ([_pd, _i64, _i, _pi64, _pi64, _i, _i, _pi, _pi, _vp], None),
+    "ppmg_fdsolver_poisson_3d_s_dev": ([_pd, _i64, _i, _pi64, _pi64, _i, _i, _pi, _pi, _vp], None),
     "ppmg_map_part_route_d_dev": ([_pd, _i64, _i64, _i, _i, _pd, _pi64, _pi, _vp], None),
     "ppmg_map_part_route_s_dev": ([_pd, _i64, _i64, _i, _i, _pd, _pi64, _pi, _vp], None),
     "ppmg_map_part_gather_d_dev": ([_pd, _i64, _i, _pd, _i64, _pd, _i64, _pi, _vp], None),

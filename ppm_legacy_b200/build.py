@@ -14,7 +14,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libppmg.so")
 BUILD_DIR = os.path.join(HERE, "_build")
 SOURCES = ["ppmg_sort.cu", "ppmg_radix.cu", "ppmg_p2m.cu", "ppmg_m2p.cu", "ppmg_rmsh.cu", "ppmg_map.cu",
-           "ppmg_api.cu"]
+           "ppmg_fd.cu", "ppmg_api.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
          "--expt-relaxed-constexpr"]
@@ -61,7 +61,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         msg = "\n".join(f"--- {s}\n{o}" for s, o in failed)
         raise RuntimeError(f"nvcc failed:\n{msg}")
     tmp = OUT + ".tmp"
-    cmd = [cc, *ARCH, "-shared", "--cudart", "static", "-o", tmp, *objs]
+    cmd = [cc, *ARCH, "-shared", "--cudart", "static", "-o", tmp, *objs, "-lcufft"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, OUT)
     return OUT

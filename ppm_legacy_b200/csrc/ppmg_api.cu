@@ -20,6 +20,7 @@
 #include "ppmg_p2m.cuh"
 #include "ppmg_rmsh.cuh"
 #include "ppmg_map.cuh"
+#include "ppmg_fd.cuh"
 #include "ppmg_sort.cuh"
 
 namespace ppmg {
@@ -60,6 +61,8 @@ struct Handle {
   Workspace ws;       // P2M / M2P / adjoint / ghost / clist scratch
   Workspace ws_rmsh;  // comp_weights -> remesh state (ppm_module_data_rmsh)
   Workspace ws_map;   // particle routing between slabs
+  Workspace ws_fd;    // Poisson solver buffers
+  FFTPlans fft;       // its cuFFT plans
   cudaStream_t stream = nullptr;
   int* d_status = nullptr;  // [0] particles outside the sub, [1] non-finite
   // position fingerprints: [0] of the sort held in ws, [1] of an M2P's xp
@@ -80,6 +83,7 @@ struct Handle {
   int w_kernel = 0;
   int64_t w_np = 0;
   ~Handle() {
+    fft.release();
     if (stream) cudaStreamDestroy(stream);
     if (d_status) cudaFree(d_status);
     if (d_hash) cudaFree(d_hash);
@@ -1448,6 +1452,77 @@ void ppmg_rmsh_create_part_s_dev(const float* field_up, int64_t ldf, int lda,
   create_part_common<float>(field_up, ldf, lda, f_lb, f_ub, topo_id, mesh_id, cutoff,
                             cutoff_weights, resetpos, field_wp, ldfw, lda2, np, up, xp, wp, info,
                             true, (cudaStream_t)stream, "ppmg_rmsh_create_part_s_dev");
+}
+
+// ---- FFT Poisson solver ------------------------------------------------------------
+extern "C++" {
+template <class T>
+static void poisson_common(T* field_up, int64_t ldf, int lda, const int64_t* f_lb,
+                           const int64_t* f_ub, int topo_id, int mesh_id, const int* ghostsize,
+                           int* info, bool dev, cudaStream_t dstream, const char* caller) {
+  clear_error();
+  if (info) *info = 0;
+  Handle* hh = find_handle(topo_id, mesh_id);
+  if (!hh) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": topo_id/mesh_id is invalid"); return; }
+  Handle* h = get_checked(topo_id, mesh_id, 3, caller, info);
+  if (!h) return;
+  if (lda < 1 || ldf < lda) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": lda inconsistent"); return; }
+  if (!check_ghost(*h, ghostsize, caller, info)) return;
+  std::lock_guard<std::mutex> lk(h->mu);
+  int lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = 1 - ghostsize[a];
+    hi[a] = h->Nm[a] + ghostsize[a];
+  }
+  FieldDesc fd;
+  if (!make_fd(*h, ldf, f_lb, f_ub, lo, hi, fd, caller, info)) return;
+  cudaStream_t st = dev ? dstream : h->stream;
+  cudaError_t e = cudaSuccess;
+  const int64_t nf = field_elems(*h, ldf, f_lb, f_ub);
+  T* dfield = field_up;
+  if (!dev) {
+    dfield = mirror<T>(h->ws.h_field, field_up, nf, st, e);
+    if (e) { cuda_fail(info, e, caller); return; }
+  }
+  double len[3];
+  for (int a = 0; a < 3; ++a) len[a] = h->g.max_phys[a] - h->g.min_phys[a];
+  const int bad = fd_poisson<T>(h->fft, h->ws_fd, h->g.N, len, dfield, fd, lda, st, e);
+  if (bad) {
+    fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": cuFFT plan or transform failed");
+    return;
+  }
+  if (e) { cuda_fail(info, e, caller); return; }
+  if (!dev) {
+    e = cudaMemcpyAsync(field_up, dfield, sizeof(T) * (size_t)nf, cudaMemcpyDeviceToHost, st);
+    if (!e) e = cudaStreamSynchronize(st);
+    if (e) cuda_fail(info, e, caller);
+  }
+}
+}  // extern "C++"
+
+void ppmg_fdsolver_poisson_3d_d(double* field_up, int64_t ldf, int lda, const int64_t* f_lb,
+                                const int64_t* f_ub, int topo_id, int mesh_id,
+                                const int* ghostsize, int* info) {
+  poisson_common<double>(field_up, ldf, lda, f_lb, f_ub, topo_id, mesh_id, ghostsize, info, false,
+                         nullptr, "ppmg_fdsolver_poisson_3d_d");
+}
+void ppmg_fdsolver_poisson_3d_s(float* field_up, int64_t ldf, int lda, const int64_t* f_lb,
+                                const int64_t* f_ub, int topo_id, int mesh_id,
+                                const int* ghostsize, int* info) {
+  poisson_common<float>(field_up, ldf, lda, f_lb, f_ub, topo_id, mesh_id, ghostsize, info, false,
+                        nullptr, "ppmg_fdsolver_poisson_3d_s");
+}
+void ppmg_fdsolver_poisson_3d_d_dev(double* field_up, int64_t ldf, int lda, const int64_t* f_lb,
+                                    const int64_t* f_ub, int topo_id, int mesh_id,
+                                    const int* ghostsize, int* info, void* stream) {
+  poisson_common<double>(field_up, ldf, lda, f_lb, f_ub, topo_id, mesh_id, ghostsize, info, true,
+                         (cudaStream_t)stream, "ppmg_fdsolver_poisson_3d_d_dev");
+}
+void ppmg_fdsolver_poisson_3d_s_dev(float* field_up, int64_t ldf, int lda, const int64_t* f_lb,
+                                    const int64_t* f_ub, int topo_id, int mesh_id,
+                                    const int* ghostsize, int* info, void* stream) {
+  poisson_common<float>(field_up, ldf, lda, f_lb, f_ub, topo_id, mesh_id, ghostsize, info, true,
+                        (cudaStream_t)stream, "ppmg_fdsolver_poisson_3d_s_dev");
 }
 
 // ---- particle routing between z-slab subdomains -------------------------------------

@@ -223,6 +223,25 @@ def ppm_map_field_ghost(field_up, *args, field_lb=None):
     return info.value
 
 
+def ppm_fdsolver_poisson(field_up, lda, topo_id, mesh_id, ghostsize, field_lb=None):
+    """Solve lap(phi) = omega in place on the periodic 3D mesh
+    (ppm_fdsolver_solve_3d with ppm_fdsolver_poisson_3d): field_up(lda, ...)
+    holds omega at the unique nodes on entry and phi, with its periodic
+    images in the ghost layers, on return.  float32 arrays: the single
+    variant; torch CUDA arrays: the device twin."""
+    _check(field_up)
+    lb, ub = _bounds(field_up, 3, True, ghostsize, field_lb)
+    k = _kind(field_up)
+    info = C.c_int(0)
+    a = (_addr(field_up), field_up.shape[0], int(lda), lb, ub, topo_id, mesh_id,
+         int_array(ghostsize), C.byref(info))
+    if _is_dev(field_up):
+        getattr(lib(), f"ppmg_fdsolver_poisson_3d_{k}_dev")(*a, _stream())
+    else:
+        getattr(lib(), f"ppmg_fdsolver_poisson_3d_{k}")(*a)
+    return info.value
+
+
 def ppm_rmsh_comp_weights(xp, Np, topo_id, mesh_id, kernel, wx1_user=None, wx2_user=None,
                           wx3_user=None):
     """ppm_rmsh_comp_weights(xp, Np, topo_id, mesh_id, kernel[, wx1, wx2, wx3]).

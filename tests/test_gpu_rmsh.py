@@ -391,3 +391,40 @@ def test_util_rank_device_twins_match_host(dim, dtype):
     assert ih == 0 and idv == 0, ppmg.last_error()
     assert ld.is_cuda and hd.is_cuda
     assert np.array_equal(ld.cpu().numpy(), lh) and np.array_equal(hd.cpu().numpy(), hh)
+
+
+@pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-12), (np.float32, 1e-5)])
+def test_fdsolver_poisson_matches_oracle(dtype, tol):
+    """ppm_fdsolver_poisson on a non-cubic periodic mesh against the oracle's
+    spectral restatement: phi at the real nodes and every periodic image of
+    the ghost layers; the device twin equals the host entry point."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(150)
+    nc = (24, 16, 20)
+    lo, hi = [0.0, -1.0, 0.5], [1.5, 0.0, 2.5]
+    t = registered(3, list(nc), lo, hi)
+    g = [2, 1, 2]
+    lb, ub = box_bounds(t, g)
+    U = rng.standard_normal((3,) + nc)
+    F = periodic_fill(U, lb, ub, 3).astype(dtype)
+    Fh = F.copy(order="F")
+    assert ppmg.ppm_fdsolver_poisson(Fh, 3, t.topo_id, t.mesh_id, g) == 0, ppmg.last_error()
+    phi = O.poisson(U.astype(dtype).astype(np.float64),
+                    [hi[a] - lo[a] for a in range(3)])
+    ref = periodic_fill(phi, lb, ub, 3)
+    assert max_rel(Fh.astype(np.float64), ref) < tol
+    d = torch.from_numpy(np.ascontiguousarray(F.T)).cuda()
+    Fd = d.permute(*reversed(range(d.dim())))
+    assert ppmg.ppm_fdsolver_poisson(Fd, 3, t.topo_id, t.mesh_id, g) == 0, ppmg.last_error()
+    torch.cuda.synchronize()
+    got = Fd.permute(*reversed(range(Fd.dim()))).contiguous().cpu().numpy().T
+    assert np.array_equal(got, Fh)
+
+
+def test_fdsolver_poisson_refuses_a_slab():
+    import copy
+    t = topo_for(3, 12, decomp=(1, 1, 2), topo_id=7950)
+    assert ppmg.register(copy.deepcopy(t), isub=0) == 0
+    F = np.zeros((1, 13, 13, 7, 1), order="F")
+    assert ppmg.ppm_fdsolver_poisson(F, 1, 7950, 1, [0, 0, 0]) == -2
+    ppmg.unregister(t)
