@@ -432,9 +432,13 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
       l = (LPS > 1 && i >= n0) ? 1 : 0;
       const int j = i - (l ? n0 : 0);
       const int tb = cb + l;
+      // the last row starting at or before j (row starts are non-decreasing):
+      // binary lifting over rows 0 .. kTileY-1
+      static_assert(kTileY == 16, "four lifting steps");
       r = 0;
 #pragma unroll
-      for (int t = 1; t < kTileY; ++t) r += (j >= rpre[tb][t]) ? 1 : 0;
+      for (int step = kTileY / 2; step > 0; step >>= 1)
+        if (rpre[tb][r + step] <= j) r += step;
       return (int64_t)rbeg[tb][r] + (j - rpre[tb][r]);
     };
     int rcur = 0, idcur = 0, lcur = 0;

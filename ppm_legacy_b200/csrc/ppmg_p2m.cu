@@ -363,6 +363,7 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
   __syncthreads();
   int n_cur = plan(0, true);
   bool last_cur = left == 0;  // the unit in flight completes its layer
+  bool first_cur = true;      // the unit in flight opens its layer
   issue(0);
 
   for (int u = 0;; ++u) {
@@ -404,6 +405,8 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
     //    completes its layer); its loads fly while unit u is accumulated
     const int cz_u = cz;
     const bool last_u = last_cur;
+    const bool first_u = first_cur;
+    first_cur = last_u;
     const int n_u = n_cur;
     bool more = true;
     if (last_u) {
@@ -457,13 +460,20 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
     if constexpr (COMP) {
       // fold the unit's partial sums (every unit: total strength stays
       // conserved to ~1e-11 of sum |u|)
+      // Two slots skip the TwoSum: the newest slot on the layer's first unit
+      // still holds (0, 0), so the fold is a move; slot 0 on the layer's last
+      // unit keeps its partial, which step 4 adds to (hi, lo) in FP64.
 #pragma unroll
       for (int e = 0; e < 2; ++e)
 #pragma unroll
         for (int k = 0; k < S; ++k)
 #pragma unroll
           for (int a = 0; a < LC; ++a) {
-            two_sum_fold<CT>(hi[e][k][a], lo[e][k][a], acc[e][k][a]);
+            if (k == 0 && last_u) continue;
+            if (k == S - 1 && first_u)
+              hi[e][k][a] = acc[e][k][a];
+            else
+              two_sum_fold<CT>(hi[e][k][a], lo[e][k][a], acc[e][k][a]);
             acc[e][k][a] = CT(0);
           }
     }
@@ -476,8 +486,13 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
           double v[LC];
 #pragma unroll
           for (int a = 0; a < LC; ++a)
-            v[a] = COMP ? (double)hi[e][0][a] + (double)lo[e][0][a] : (double)acc[e][0][a];
+            v[a] = COMP ? ((double)hi[e][0][a] + (double)lo[e][0][a]) + (double)acc[e][0][a]
+                        : (double)acc[e][0][a];
           emit_node<3, OT, LC>(P, x0 + e, y, zc, v);
+        }
+        if constexpr (COMP) {
+#pragma unroll
+          for (int a = 0; a < LC; ++a) acc[e][0][a] = CT(0);
         }
 #pragma unroll
         for (int k = 0; k < S - 1; ++k)

@@ -169,6 +169,13 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) {
 __device__ __forceinline__ void mbar_init(uint64_t* bar) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
 }
+__device__ __forceinline__ void mbar_init_count(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
                "r"(bytes)
@@ -203,7 +210,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 // SM, enough warps to cover the shared-memory latency of the ranking).
 constexpr size_t kMoveSmem = 2 * sizeof(int) * (size_t)kRSub + 2 * sizeof(uint4) * (size_t)kRSub +
                              sizeof(unsigned short) * (size_t)(kRSub + kRWarps * kRSlots) +
-                             sizeof(int) * (size_t)(3 * kRSlots + 64) + 4 * sizeof(uint64_t);
+                             sizeof(int) * (size_t)(3 * kRSlots + 64) + 6 * sizeof(uint64_t);
 
 // One stable pass.  Every tile walks its sub-tiles in order.  The inputs of
 // a sub-tile arrive by TMA bulk copies on two independent double-buffered
@@ -226,7 +233,9 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
   int* dst = run + kRSlots;                                           // digit start in the sub-tile
   int* tot = dst + kRSlots;                                           // digit count of the sub-tile
   int* sw = tot + kRSlots;                                            // block scan scratch [33]
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sw + 64);               // [0,1] keys, [2,3] planes
+  // [0,1] keys full, [2,3] plane buffers full, [4,5] plane buffers released
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sw + 64);
+  __shared__ int s_fail;  // a bulk copy never completed: the tile gives up
 
   const int nb = 1 << A.bits;
   const int nbk = FIRST ? nb + 1 : nb;
@@ -251,6 +260,10 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
   if (tid == 0) {
 #pragma unroll
     for (int i = 0; i < 4; ++i) mbar_init(&bar[i]);
+    // a plane buffer is released once every warp has read it
+    mbar_init_count(&bar[4], kRWarps);
+    mbar_init_count(&bar[5], kRWarps);
+    s_fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
@@ -373,13 +386,15 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
     __syncthreads();
     // keys (first pass: and ids); thread t takes the sorted positions
     // j = t + 1024 q
-    int gdst[kRItems];
+    int gdst[kRItems], lix[kRItems];
 #pragma unroll
     for (int q = 0; q < kRItems; ++q) {
       const int j = tid + q * kRThreads;
       gdst[q] = -1;
+      lix[q] = 0;
       if (j < subn) {
         const int li = inv[j];
+        lix[q] = li;
         const int kk = skeys[li];
         const int d = digit_of<FIRST>(kk, A.shift, mask, nb, A.ncell);
         gdst[q] = run[d] + (j - dst[d]);
@@ -389,26 +404,47 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
     }
     __syncthreads();
     if (tid == 0) issue_keys(sub + 2);
-    // ids, then the record and strength planes
+    // ids, then the record and strength planes.  No block barrier per
+    // unit: every thread waits for the unit's copy itself, each warp
+    // releases the buffer on bar[4 + b] once it has read its items, and
+    // thread 0 refills the buffer when all warps have released it.
     for (int pl = FIRST ? 0 : -1; pl < A.nplanes; ++pl, ++u) {
-      if (!wait_on(&bar[2 + (u & 1)], u)) return;
-      const uint4* sb = pb + (u & 1) * kRSub;
-      if (pl < 0) {
-        const int* sid = reinterpret_cast<const int*>(sb);
+      const int b = u & 1;
+      const uint32_t par = (uint32_t)((u >> 1) & 1);
+      const bool ok = *(volatile int*)&s_fail == 0 && mbar_wait(&bar[2 + b], par);
+      if (ok) {
+        const uint4* sb = pb + b * kRSub;
+        if (pl < 0) {
+          const int* sid = reinterpret_cast<const int*>(sb);
 #pragma unroll
-        for (int q = 0; q < kRItems; ++q)
-          if (gdst[q] >= 0) __stcs(A.id_out + gdst[q], sid[inv[tid + q * kRThreads]]);
+          for (int q = 0; q < kRItems; ++q)
+            if (gdst[q] >= 0) __stcs(A.id_out + gdst[q], sid[lix[q]]);
+        } else {
+          uint4* out = pl < A.rplanes ? A.rec_out + (int64_t)pl * A.np
+                                      : A.us_out + (int64_t)(pl - A.rplanes) * A.np;
+#pragma unroll
+          for (int q = 0; q < kRItems; ++q)
+            if (gdst[q] >= 0) __stcs(out + gdst[q], sb[lix[q]]);
+        }
       } else {
-        uint4* out = pl < A.rplanes ? A.rec_out + (int64_t)pl * A.np
-                                    : A.us_out + (int64_t)(pl - A.rplanes) * A.np;
-#pragma unroll
-        for (int q = 0; q < kRItems; ++q)
-          if (gdst[q] >= 0) __stcs(out + gdst[q], sb[inv[tid + q * kRThreads]]);
+        s_fail = 1;
       }
-      __syncthreads();
-      if (tid == 0) issue_plane(u + 2);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&bar[4 + b]);
+      if (tid == 0) {
+        if (*(volatile int*)&s_fail == 0 && mbar_wait(&bar[4 + b], par))
+          issue_plane(u + 2);
+        else
+          s_fail = 1;
+      }
     }
     for (int d = tid; d < nbk; d += kRThreads) run[d] += tot[d];
+    // a give-up ends the tile together, once the copies in flight are done
+    if (__syncthreads_or(*(volatile int*)&s_fail != 0)) {
+      if (tid == 0) atomicExch(A.wait_flag, 1);
+      for (int i = 0; i < 4; ++i) mbar_wait(&bar[i], 0u), mbar_wait(&bar[i], 1u);
+      return;
+    }
   }
 }
 
