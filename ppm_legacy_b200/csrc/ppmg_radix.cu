@@ -5,9 +5,9 @@
 // slots and then gathers every particle's position and strengths from random
 // addresses; on large unordered particle sets those random accesses, not the
 // arithmetic, set its time.  Here every pass reads its input in order and
-// writes it grouped by one digit of the cell key: a tile of 2048 particles is
-// ranked in shared memory and leaves as runs of equal digit, so both the
-// reads and the writes are coalesced.  The first pass builds the keys and the
+// writes it grouped by one digit of the cell key: a sub-tile of 4096
+// particles is ranked in shared memory and leaves as runs of equal digit, so
+// both the reads and the writes are coalesced.  The first pass builds the keys and the
 // records from xp / up; the later passes move (key, id, record, strengths).
 // The sort is stable and starts from particle-id order, so particles of one
 // cell end in ascending id -- the fill order of ppm_util_rank3d.f:525-533.

@@ -131,6 +131,25 @@ __global__ void k_hash(const T* __restrict__ xp, int64_t ldxp, int64_t np, int d
   block_add_hash(hacc, hash);
 }
 
+// The same fingerprint for 3D FP64 positions packed three to a row (ldxp 3)
+// at a 16-byte aligned base: each thread reads particles 2q and 2q+1 as
+// three 16-byte streaming loads; a last odd particle is read alone.
+__global__ void k_hash_xyz_pairs(const double* __restrict__ xp, int64_t np,
+                                 unsigned long long* __restrict__ hash) {
+  unsigned long long hacc = 0;
+  const int64_t npair = np / 2;
+  const double2* v = reinterpret_cast<const double2*>(xp);
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < npair;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const double2 a = __ldcs(v + 3 * q), b = __ldcs(v + 3 * q + 1), c = __ldcs(v + 3 * q + 2);
+    const double x0[3] = {a.x, a.y, b.x}, x1[3] = {b.y, c.x, c.y};
+    hacc += particle_hash<double>(x0, 3, 2 * q) + particle_hash<double>(x1, 3, 2 * q + 1);
+  }
+  if ((np & 1) && blockIdx.x == 0 && threadIdx.x == 0)
+    hacc += particle_hash<double>(xp + 3 * (np - 1), 3, np - 1);
+  block_add_hash(hacc, hash);
+}
+
 __global__ void k_scatter(const int* __restrict__ key, const int* __restrict__ slot,
                           const int* __restrict__ start, int64_t np, int* __restrict__ idx) {
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np;
@@ -266,7 +285,11 @@ cudaError_t position_hash(const T* xp, int64_t ldxp, int64_t np, int dim,
   cudaError_t e = cudaMemsetAsync(hash, 0, sizeof(unsigned long long), st);
   if (e) return e;
   if (np > 0) {
-    k_hash<T><<<grid_for(np, 256), 256, 0, st>>>(xp, ldxp, np, dim, hash);
+    if (sizeof(T) == 8 && dim == 3 && ldxp == 3 && (reinterpret_cast<uintptr_t>(xp) & 15) == 0)
+      k_hash_xyz_pairs<<<grid_for((np + 1) / 2, 256), 256, 0, st>>>(
+          reinterpret_cast<const double*>(xp), np, hash);
+    else
+      k_hash<T><<<grid_for(np, 256), 256, 0, st>>>(xp, ldxp, np, dim, hash);
     count_launch();
   }
   return cudaGetLastError();

@@ -104,29 +104,46 @@ def test_config2_round_trip_properties():
                        torch.from_numpy(res[0][0] * 2))
 
 
-def test_m2p_reuses_p2m_order_only_for_identical_positions():
+def _sorts_since_last_read():
+    """Cell sorts the library ran since the previous read (device timing on)."""
+    import ctypes as C
+    ms, n = C.c_double(0.0), C.c_int64(0)
+    assert ppmg.lib().ppmg_kernel_timing_read(2, C.byref(ms), C.byref(n)) == 0
+    return int(n.value)
+
+
+@pytest.mark.parametrize("n", [20000, 20001])
+def test_m2p_reuses_p2m_order_only_for_identical_positions(n):
     """M2P after P2M of the same positions reuses P2M's cell order (fingerprint
-    match); after the positions change (even one particle, one ulp) it sorts
-    again.  Both must equal the oracle."""
+    match: no second sort); after the positions change (even one particle, one
+    ulp) it sorts again.  Both must equal the oracle.  An odd count covers the
+    last particle of the paired fingerprint reads."""
     rng = np.random.default_rng(95)
     t = registered(3, 16)
     g = [2, 2, 2]
     lb, ub = box_bounds(t, g)
-    xp = random_particles(rng, 3, 20000)
-    up = np.asfortranarray(rng.standard_normal((3, 20000)))
+    xp = random_particles(rng, 3, n)
+    up = np.asfortranarray(rng.standard_normal((3, n)))
     shape = (3,) + tuple(ub[a] - lb[a] + 1 for a in range(3)) + (1,)
-    for mode in (0, 1):
-        ppmg.set_precision(mode)
-        f = np.zeros(shape, order="F")
-        assert ppmg.ppm_interp_p2m(xp, 20000, up, 3, t.topo_id, t.mesh_id, 2, g, f) == 0
-        for moved in (False, True):
-            xq = xp.copy(order="F")
-            if moved:
-                xq[0, 7] = np.nextafter(xq[0, 7], 2.0)
-                xq[:, 100:200] = xq[:, 100:200][:, ::-1]
-            out = np.zeros((3, 20000), order="F")
-            assert ppmg.ppm_interp_m2p(xq, 20000, out, 3, t.topo_id, t.mesh_id, 2, g, f) == 0
-            ref = O.m2p(t, xq, f, lb, ub, 3, 2, g)
-            tol = 0.0 if mode == 0 else 1e-6
-            assert max_rel(out, ref) <= tol, (mode, moved)
-    ppmg.set_precision(0)
+    ppmg.lib().ppmg_kernel_timing(1)
+    try:
+        for mode in (0, 1):
+            ppmg.set_precision(mode)
+            f = np.zeros(shape, order="F")
+            _sorts_since_last_read()
+            assert ppmg.ppm_interp_p2m(xp, n, up, 3, t.topo_id, t.mesh_id, 2, g, f) == 0
+            assert _sorts_since_last_read() == 1
+            for moved in (False, True):
+                xq = xp.copy(order="F")
+                if moved:
+                    xq[0, 7] = np.nextafter(xq[0, 7], 2.0)
+                    xq[:, 100:200] = xq[:, 100:200][:, ::-1]
+                out = np.zeros((3, n), order="F")
+                assert ppmg.ppm_interp_m2p(xq, n, out, 3, t.topo_id, t.mesh_id, 2, g, f) == 0
+                assert _sorts_since_last_read() == (1 if moved else 0), (mode, moved)
+                ref = O.m2p(t, xq, f, lb, ub, 3, 2, g)
+                tol = 0.0 if mode == 0 else 1e-6
+                assert max_rel(out, ref) <= tol, (mode, moved)
+    finally:
+        ppmg.lib().ppmg_kernel_timing(0)
+        ppmg.set_precision(0)
