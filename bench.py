@@ -46,6 +46,20 @@ CONFIGS = {
 }
 
 
+L2_BYTES = 126 * 2**20  # B200 L2
+
+
+class L2Flush:
+    """Writes a buffer twice the L2 size between timed steps (outside their
+    events) when a workload's inputs are smaller than the L2."""
+
+    def __init__(self, torch, device):
+        self.buf = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=device)
+
+    def __call__(self):
+        self.buf.fill_(1.0)
+
+
 def hbm_peak():
     try:
         with open(PEAKS) as fh:
@@ -373,7 +387,8 @@ def run_remesh(args):
         "dtype": "mixed" if args.precision != "fp64" else "f64",
         "config": {"mesh": f"{nc}^3 periodic", "particles": n, "lda": 3, "kernel": "M'4",
                    "ghostsize": 2, "new_particles": npn,
-                   "data": "cell centres + 8 smooth modes (max 0.5 h), vortex-tube strengths"},
+                   "data": "cell centres + 8 smooth modes (max 0.5 h), vortex-tube strengths",
+                   "l2": "inputs larger than L2 (xp/up/field each > 126 MB)"},
         "path": "device arrays through the _dev twins (comp_weights, remesh, create_part)",
         "e2e": {"value": n / best, "unit": "particles/s", "ms_per_step": best * 1e3,
                 "path": "host-pointer entry points, host<->device copies inside, wall clock"}}))
@@ -414,22 +429,30 @@ def run_adjoint(args):
     for _ in range(max(args.warmup, 3)):
         step()
     torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
+    # the inputs (100 MB of positions, a 2 MB field) fit in the L2: flush it
+    # between steps, outside each step's events
+    flush = L2Flush(torch, dev)
+    ms = 0.0
     for _ in range(args.steps):
+        flush()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
         step()
-    e1.record(stream)
+        e1.record(stream)
+        e1.synchronize()
+        ms += e0.elapsed_time(e1)
     torch.cuda.synchronize()
     assert ppmg.sync_status(4, 1) == 0, ppmg.last_error()
-    ms = e0.elapsed_time(e1) / args.steps
+    ms /= args.steps
     print(json.dumps({
         "workload": "adjoint", "metric": "particles/s for forward P2M + adjoint (dL/dw, dL/dx)",
         "value": n / (ms / 1e3), "unit": "particles/s", "ms_per_step": ms,
         "steps": args.steps, "warmup": max(args.warmup, 3), "higher_is_better": True,
         "dtype": "mixed" if args.precision != "fp64" else "f64",
         "config": {"mesh": f"{nc}^3 periodic", "particles": n, "lda": 1,
-                   "data": "uniform positions, w ~ N(0,1), target T ~ N(0,1) per node"}}))
+                   "data": "uniform positions, w ~ N(0,1), target T ~ N(0,1) per node",
+                   "l2": "L2 flushed between timed steps (outside the steps' events)"}}))
 
 
 def main():
@@ -515,6 +538,13 @@ def main():
         if i1 or i2:
             raise RuntimeError(f"library error {ppmg.last_error()}")
 
+    # inputs (positions, strengths, field) below the L2 size: flush between steps
+    in_bytes = min(xp.numel() * 8, up.numel() * 8, field.numel() * 8)
+    flush = L2Flush(torch, dev) if in_bytes < L2_BYTES else None
+    l2_note = ("inputs larger than L2 (xp/up/field each > 126 MB)" if flush is None else
+               "L2 flushed between timed steps (a 252 MB buffer written outside the steps' "
+               "events); ms_per_step sums the steps' own events")
+
     def timed(prec):
         ppmg.set_precision(prec)
         for _ in range(args.warmup):
@@ -533,6 +563,8 @@ def main():
         ev0.record(stream)
         p2m_ms = []
         for k in range(args.steps):
+            if flush is not None:
+                flush()
             evp[0].record(stream)
             ppmg.ppm_interp_p2m(xp, n, up, 3, 1, 1, 2, g, field)
             evp[1].record(stream)
@@ -547,7 +579,10 @@ def main():
         ppmg.lib().ppmg_kernel_timing(0)
         kparts = [kernel_time(part) for part in range(3)]
         assert ppmg.sync_status(1, 1) == 0, ppmg.last_error()
-        ms = ev0.elapsed_time(ev1) / args.steps
+        if flush is None:
+            ms = ev0.elapsed_time(ev1) / args.steps
+        else:  # the steps' own events: the flushes between them are not timed
+            ms = float(sum(a + b for a, b in p2m_ms)) / args.steps
         if world > 1:
             ms = max_over_ranks(ms, dist, dev)
             dist.barrier()
@@ -718,7 +753,7 @@ def main():
                                     f"{nc}x{nc}x{nc * world} periodic mesh") +
                                    f", {n} particles per GPU ({CONFIGS[args.config][2]}), lda 3, "
                                    f"ghostsize 2",
-                       "l2": "inputs larger than L2 (xp/up/field each > 126 MB)",
+                       "l2": l2_note,
                        "parallelism": "1 periodic subdomain" if world == 1 else
                        f"{world} z-slab subdomains of a {nc}x{nc}x{nc * world} periodic mesh, "
                        f"ghost put/get between neighbouring slabs over "
