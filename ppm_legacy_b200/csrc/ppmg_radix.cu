@@ -1,14 +1,19 @@
-// ppmg_radix.cu -- stable LSD radix sort of particles into cell order that
-// moves their packed records with the keys (declared in ppmg_sort.cuh).
+// ppmg_radix.cu -- stable LSD radix sort of particles into cell order, with
+// their packed records and strengths placed in that order (declared in
+// ppmg_sort.cuh).
 //
 // The counting sort of ppmg_sort.cu scatters particle ids to random cell
 // slots and then gathers every particle's position and strengths from random
 // addresses; on large unordered particle sets those random accesses, not the
 // arithmetic, set its time.  Here every pass reads its input in order and
-// writes it grouped by one digit of the cell key: a sub-tile of 4096
+// writes it grouped by one digit of the cell key: a sub-tile of 8192
 // particles is ranked in shared memory and leaves as runs of equal digit, so
-// both the reads and the writes are coalesced.  The first pass builds the keys and the
-// records from xp / up; the later passes move (key, id, record, strengths).
+// both the reads and the writes are coalesced.  The first count pass builds
+// the keys from xp and writes each particle's record and strengths as one
+// row of 16-byte units (one 32-byte sector in the mixed form); the passes
+// move only (key, id), and one gather then copies every row into the sorted
+// planes.  Carrying the 32-64 byte payload through every pass cost more than
+// the single gather of one sector per particle.
 // The sort is stable and starts from particle-id order, so particles of one
 // cell end in ascending id -- the fill order of ppm_util_rank3d.f:525-533.
 #include <cuda_runtime.h>
@@ -22,10 +27,10 @@ namespace {
 constexpr int kCThreads = 512;                  // count kernel (full occupancy in one wave)
 constexpr int kRThreads = 1024;                 // move kernel
 constexpr int kRWarps = kRThreads / 32;
-constexpr int kRItems = 4;                      // items per thread and sub-tile
-constexpr int kRSub = kRThreads * kRItems;      // 4096 items per sub-tile
-constexpr int kRWarpItems = kRSub / kRWarps;    // 128 consecutive items per warp
-constexpr int kRMaxBits = 9;                    // >= 8 items per digit and sub-tile
+constexpr int kRItems = 8;                      // items per thread and sub-tile
+constexpr int kRSub = kRThreads * kRItems;      // 8192 items per sub-tile
+constexpr int kRWarpItems = kRSub / kRWarps;    // 256 consecutive items per warp
+constexpr int kRMaxBits = 9;                    // >= 16 items per digit and sub-tile
 constexpr int kRMaxBuckets = 1 << kRMaxBits;
 constexpr int kRSlots = kRMaxBuckets + 32;      // + the invalid bucket of the first pass
 constexpr int kRDigitsPerThread = (kRMaxBuckets + 1 + kRThreads - 1) / kRThreads;
@@ -59,10 +64,11 @@ struct CountArgs {
   int ncell, shift, bits, subs, ntiles;
   const int* key_in;
   int* hist;  // [digit * ntiles + tile]
-  // first pass: keys, records and strengths in particle order
+  // first pass: keys in particle order, and every particle's record and
+  // strength units side by side (iu 16-byte units per particle)
   int* key0;
-  V* rec0;
-  V* us0;
+  uint4* aos;
+  int iu;
   int* err;
   T* zout;
   int64_t ldz;
@@ -94,10 +100,20 @@ __device__ __forceinline__ typename Vec4<CT>::type make_us(const T* u, int lda, 
   return w;
 }
 
+// A float4 / double4 as its 16-byte units (streaming stores: the units are
+// read back once, in sorted order, by k_gather_units).
+template <class V>
+__device__ __forceinline__ void store_units(uint4* dst, const V& v) {
+  const uint4* u = reinterpret_cast<const uint4*>(&v);
+#pragma unroll
+  for (int t = 0; t < (int)(sizeof(V) / 16); ++t) __stcs(dst + t, u[t]);
+}
+
 // Digit histogram of each tile (subs sub-tiles of consecutive items).  The
-// first pass computes the keys from the positions, writes keys, records and
-// strengths in particle order, counts invalid particles, zeroes their output
-// rows and accumulates the position fingerprint.
+// first pass computes the keys from the positions, writes the keys and each
+// particle's record and strength units in particle order, counts invalid
+// particles, zeroes their output rows and accumulates the position
+// fingerprint.
 template <class T, class CT, bool FIRST>
 __global__ void __launch_bounds__(kCThreads) k_radix_count(CountArgs<T, CT> A) {
   using V = typename Vec4<CT>::type;
@@ -132,9 +148,11 @@ __global__ void __launch_bounds__(kCThreads) k_radix_count(CountArgs<T, CT> A) {
         r.w = __int_as_float(k);
       else
         r.w = (double)k;
-      store_vec(A.rec0, i, A.np, r);
+      constexpr int RU = (int)(sizeof(V) / 16);
+      uint4* row = A.aos + i * A.iu;
+      store_units(row, r);
       for (int ch = 0; ch < A.nchunk; ++ch)
-        store_vec(A.us0 + (int64_t)ch * A.np, i, A.np, make_us<T, CT>(A.up + i * A.ldup, A.lda, ch));
+        store_units(row + RU * (1 + ch), make_us<T, CT>(A.up + i * A.ldup, A.lda, ch));
     } else {
       k = A.key_in[i];
     }
@@ -147,19 +165,14 @@ __global__ void __launch_bounds__(kCThreads) k_radix_count(CountArgs<T, CT> A) {
 }
 
 struct MoveArgs {
-  int64_t np;     // plane stride of the records / strengths (16-byte units)
+  int64_t np;     // items of the first pass
   int* d_nvalid;  // written by the first pass, read by the later ones
   int ncell, shift, bits, subs, ntiles;
-  int rplanes, nplanes;  // record planes; record + strength planes
-  const int* hist;       // exclusive-scanned, [digit * ntiles + tile]
+  const int* hist;  // exclusive-scanned, [digit * ntiles + tile]
   const int* key_in;
-  const int* id_in;
-  const uint4* rec_in;
-  const uint4* us_in;
+  const int* id_in;  // not read by the first pass (ids = item positions)
   int* key_out;
   int* id_out;
-  uint4* rec_out;
-  uint4* us_out;
   int* wait_flag;  // set when a bulk copy never completes
 };
 
@@ -204,38 +217,33 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
-// Shared memory of k_radix_move: two key buffers (16 KB each), two plane
-// buffers (64 KB each), the 16-bit inverse map and per-warp digit counts,
-// the per-digit offsets and the mbarriers (~209 KB: one CTA of 32 warps per
-// SM, enough warps to cover the shared-memory latency of the ranking).
-constexpr size_t kMoveSmem = 2 * sizeof(int) * (size_t)kRSub + 2 * sizeof(uint4) * (size_t)kRSub +
+// Shared memory of k_radix_move: two key and two id buffers (kRSub entries
+// each), the 16-bit inverse map and per-warp digit counts, the per-digit
+// offsets and the mbarriers.
+constexpr size_t kMoveSmem = 4 * sizeof(int) * (size_t)kRSub +
                              sizeof(unsigned short) * (size_t)(kRSub + kRWarps * kRSlots) +
-                             sizeof(int) * (size_t)(3 * kRSlots + 64) + 6 * sizeof(uint64_t);
+                             sizeof(int) * (size_t)(3 * kRSlots + 64) + 4 * sizeof(uint64_t);
 
-// One stable pass.  Every tile walks its sub-tiles in order.  The inputs of
-// a sub-tile arrive by TMA bulk copies on two independent double-buffered
-// streams: keys (one 16 KB unit per sub-tile, issued two sub-tiles ahead)
-// and the units of ids (16 KB; not in the first pass, whose ids are the
-// item positions) and 16-byte planes of records and strengths (64 KB),
-// issued two units ahead, each stream completing on its own mbarriers.  The
-// keys are ranked by digit (warp w owns items [128w, 128w+128), ranked round
-// by round with one ballot per digit bit); inv[] maps every sorted position of the
-// sub-tile to its item, so the ids and each plane are written in digit runs
-// straight from their buffer.
+// One stable pass over (key, id) pairs.  Every tile walks its sub-tiles in
+// order.  The keys and the ids of a sub-tile arrive by TMA bulk copies issued
+// two sub-tiles ahead into double buffers (the first pass reads no ids: they
+// are the item positions), each completing on its own mbarrier.  The keys are
+// ranked by digit (warp w owns items [kRWarpItems w, kRWarpItems (w+1)),
+// ranked round by round with one ballot per digit bit); inv[] maps every
+// sorted position of the sub-tile to its item, so keys and ids leave in digit
+// runs.
 template <bool FIRST>
 __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
   extern __shared__ __align__(128) unsigned char smem[];
   int* kb = reinterpret_cast<int*>(smem);                             // [2][kRSub] keys
-  uint4* pb = reinterpret_cast<uint4*>(kb + 2 * kRSub);               // [2][kRSub] planes
-  unsigned short* inv = reinterpret_cast<unsigned short*>(pb + 2 * kRSub);  // [kRSub]
+  int* ib = kb + 2 * kRSub;                                           // [2][kRSub] ids
+  unsigned short* inv = reinterpret_cast<unsigned short*>(ib + 2 * kRSub);  // [kRSub]
   unsigned short* whist = inv + kRSub;                                // [kRWarps][kRSlots]
   int* run = reinterpret_cast<int*>(whist + kRWarps * kRSlots);       // next output slot per digit
   int* dst = run + kRSlots;                                           // digit start in the sub-tile
   int* tot = dst + kRSlots;                                           // digit count of the sub-tile
   int* sw = tot + kRSlots;                                            // block scan scratch [33]
-  // [0,1] keys full, [2,3] plane buffers full, [4,5] plane buffers released
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sw + 64);
-  __shared__ int s_fail;  // a bulk copy never completed: the tile gives up
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sw + 64);               // [0,1] keys, [2,3] ids
 
   const int nb = 1 << A.bits;
   const int nbk = FIRST ? nb + 1 : nb;
@@ -253,53 +261,31 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
   const int64_t t0 = (int64_t)blockIdx.x * A.subs * kRSub;
   if (t0 >= n) return;
   const int nsc = (int)min((int64_t)A.subs, (n - t0 + kRSub - 1) / kRSub);
-  const int NU = A.nplanes + (FIRST ? 0 : 1);  // stream units per sub-tile: [ids,] planes
-  const int total_p = nsc * NU;
 
   for (int d = tid; d < nbk; d += kRThreads) run[d] = A.hist[(int64_t)d * A.ntiles + blockIdx.x];
   if (tid == 0) {
 #pragma unroll
     for (int i = 0; i < 4; ++i) mbar_init(&bar[i]);
-    // a plane buffer is released once every warp has read it
-    mbar_init_count(&bar[4], kRWarps);
-    mbar_init_count(&bar[5], kRWarps);
-    s_fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
 
   auto sub_n = [&](int sub) { return (int)min((int64_t)kRSub, n - (t0 + (int64_t)sub * kRSub)); };
-  // keys of sub-tile s into kb[s & 1] (rounded up to 16 bytes: the key
-  // arrays are allocated 16 entries long)
-  auto issue_keys = [&](int s) {
+  // keys (and ids) of sub-tile s into buffer s & 1, rounded up to 16 bytes
+  // (the key and id arrays are allocated 16 entries long)
+  auto issue = [&](int s) {
     if (s >= nsc) return;
     const int64_t base = t0 + (int64_t)s * kRSub;
     const uint32_t bytes = (uint32_t)((sub_n(s) * 4 + 15) & ~15);
-    uint64_t* br = &bar[s & 1];
-    mbar_expect_tx(br, bytes);
-    bulk_load(kb + (s & 1) * kRSub, A.key_in + base, bytes, br);
-  };
-  // stream unit u (sub-tile u / NU; unit u % NU: the ids unless FIRST, then
-  // the planes) into pb[u & 1]
-  auto issue_plane = [&](int u) {
-    if (u >= total_p) return;
-    const int s = u / NU, pl = u - s * NU - (FIRST ? 0 : 1);
-    const int64_t base = t0 + (int64_t)s * kRSub;
-    uint64_t* br = &bar[2 + (u & 1)];
-    if (pl < 0) {  // ids (rounded up to 16 bytes like the keys)
-      const uint32_t bytes = (uint32_t)((sub_n(s) * 4 + 15) & ~15);
-      mbar_expect_tx(br, bytes);
-      bulk_load(pb + (u & 1) * kRSub, A.id_in + base, bytes, br);
-      return;
+    mbar_expect_tx(&bar[s & 1], bytes);
+    bulk_load(kb + (s & 1) * kRSub, A.key_in + base, bytes, &bar[s & 1]);
+    if (!FIRST) {
+      mbar_expect_tx(&bar[2 + (s & 1)], bytes);
+      bulk_load(ib + (s & 1) * kRSub, A.id_in + base, bytes, &bar[2 + (s & 1)]);
     }
-    const uint4* src = pl < A.rplanes ? A.rec_in + (int64_t)pl * A.np
-                                      : A.us_in + (int64_t)(pl - A.rplanes) * A.np;
-    const uint32_t bytes = (uint32_t)sub_n(s) * 16u;
-    mbar_expect_tx(br, bytes);
-    bulk_load(pb + (u & 1) * kRSub, src + base, bytes, br);
   };
-  // every thread waits; all give up together (copies still outstanding on
-  // either stream are waited for once more, with the same bound)
+  // every thread waits; all give up together (copies still outstanding are
+  // waited for once more, with the same bound)
   auto wait_on = [&](uint64_t* br, int use) -> bool {
     const bool ok = mbar_wait(br, (uint32_t)((use >> 1) & 1));
     if (__syncthreads_and(ok)) return true;
@@ -309,12 +295,9 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
   };
 
   if (tid == 0) {
-    issue_keys(0);
-    issue_keys(1);
-    issue_plane(0);
-    issue_plane(1);
+    issue(0);
+    issue(1);
   }
-  int u = 0;  // next plane unit
   for (int sub = 0; sub < nsc; ++sub) {
     const int64_t base = t0 + (int64_t)sub * kRSub;
     const int subn = sub_n(sub);
@@ -383,68 +366,26 @@ __global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
         const int d = digit_of<FIRST>(key[r], A.shift, mask, nb, A.ncell);
         inv[lpos[r] + dst[d] + wh[d]] = (unsigned short)(w * kRWarpItems + r * 32 + lane);
       }
-    __syncthreads();
-    // keys (first pass: and ids); thread t takes the sorted positions
-    // j = t + 1024 q
-    int gdst[kRItems], lix[kRItems];
+    __syncthreads();  // inv[] complete
+    // the ids of this sub-tile (later passes) must have landed
+    if (!FIRST && !wait_on(&bar[2 + (sub & 1)], sub)) return;
+    // keys and ids; thread t takes the sorted positions j = t + kRThreads q
+    const int* sids = ib + (sub & 1) * kRSub;
 #pragma unroll
     for (int q = 0; q < kRItems; ++q) {
       const int j = tid + q * kRThreads;
-      gdst[q] = -1;
-      lix[q] = 0;
       if (j < subn) {
         const int li = inv[j];
-        lix[q] = li;
         const int kk = skeys[li];
         const int d = digit_of<FIRST>(kk, A.shift, mask, nb, A.ncell);
-        gdst[q] = run[d] + (j - dst[d]);
-        __stcs(A.key_out + gdst[q], kk);
-        if (FIRST) __stcs(A.id_out + gdst[q], (int)(base + li));
+        const int g = run[d] + (j - dst[d]);
+        __stcs(A.key_out + g, kk);
+        __stcs(A.id_out + g, FIRST ? (int)(base + li) : sids[li]);
       }
     }
     __syncthreads();
-    if (tid == 0) issue_keys(sub + 2);
-    // ids, then the record and strength planes.  No block barrier per
-    // unit: every thread waits for the unit's copy itself, each warp
-    // releases the buffer on bar[4 + b] once it has read its items, and
-    // thread 0 refills the buffer when all warps have released it.
-    for (int pl = FIRST ? 0 : -1; pl < A.nplanes; ++pl, ++u) {
-      const int b = u & 1;
-      const uint32_t par = (uint32_t)((u >> 1) & 1);
-      const bool ok = *(volatile int*)&s_fail == 0 && mbar_wait(&bar[2 + b], par);
-      if (ok) {
-        const uint4* sb = pb + b * kRSub;
-        if (pl < 0) {
-          const int* sid = reinterpret_cast<const int*>(sb);
-#pragma unroll
-          for (int q = 0; q < kRItems; ++q)
-            if (gdst[q] >= 0) __stcs(A.id_out + gdst[q], sid[lix[q]]);
-        } else {
-          uint4* out = pl < A.rplanes ? A.rec_out + (int64_t)pl * A.np
-                                      : A.us_out + (int64_t)(pl - A.rplanes) * A.np;
-#pragma unroll
-          for (int q = 0; q < kRItems; ++q)
-            if (gdst[q] >= 0) __stcs(out + gdst[q], sb[lix[q]]);
-        }
-      } else {
-        s_fail = 1;
-      }
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&bar[4 + b]);
-      if (tid == 0) {
-        if (*(volatile int*)&s_fail == 0 && mbar_wait(&bar[4 + b], par))
-          issue_plane(u + 2);
-        else
-          s_fail = 1;
-      }
-    }
     for (int d = tid; d < nbk; d += kRThreads) run[d] += tot[d];
-    // a give-up ends the tile together, once the copies in flight are done
-    if (__syncthreads_or(*(volatile int*)&s_fail != 0)) {
-      if (tid == 0) atomicExch(A.wait_flag, 1);
-      for (int i = 0; i < 4; ++i) mbar_wait(&bar[i], 0u), mbar_wait(&bar[i], 1u);
-      return;
-    }
+    if (tid == 0) issue(sub + 2);
   }
 }
 
@@ -481,6 +422,45 @@ __global__ void k_fill_gaps(const int4* __restrict__ gaps, const int* __restrict
   }
 }
 
+// Payload of the sorted order: sorted position s takes the units of particle
+// ids[s] from its row of aos (IU units; in the mixed form with lda <= 4 a
+// row is one 32-byte sector) into the planes, units 0 .. ru-1 to rec and the
+// rest to us.  The lanes of one particle are adjacent, so a row costs one
+// sector request and a warp's stores to a plane are contiguous.  Four units
+// per thread are in flight at once (the reads land at random rows).
+template <int IU>
+__global__ void __launch_bounds__(256) k_gather_units(const int* __restrict__ ids,
+                                                      const int* __restrict__ d_nvalid,
+                                                      const uint4* __restrict__ aos, int iu_rt,
+                                                      int ru, int64_t np, uint4* __restrict__ rec,
+                                                      uint4* __restrict__ us) {
+  constexpr int kU = 4;
+  const int iu = IU > 0 ? IU : iu_rt;
+  const int64_t n = (int64_t)*d_nvalid * iu;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t g0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g0 < n; g0 += kU * stride) {
+    int64_t s[kU];
+    int t[kU], id[kU];
+#pragma unroll
+    for (int k = 0; k < kU; ++k) {
+      const int64_t g = g0 + k * stride;
+      s[k] = g / iu;
+      t[k] = (int)(g - s[k] * iu);
+      id[k] = g < n ? __ldcs(ids + s[k]) : 0;
+    }
+    uint4 v[kU];
+#pragma unroll
+    for (int k = 0; k < kU; ++k)
+      if (g0 + k * stride < n) v[k] = __ldcs(aos + (int64_t)id[k] * iu + t[k]);
+#pragma unroll
+    for (int k = 0; k < kU; ++k)
+      if (g0 + k * stride < n) {
+        uint4* dst = t[k] < ru ? rec + (int64_t)t[k] * np : us + (int64_t)(t[k] - ru) * np;
+        __stcs(dst + s[k], v[k]);
+      }
+  }
+}
+
 int bit_length(int64_t v) {
   int b = 0;
   while (v > 0) {
@@ -500,14 +480,15 @@ cudaError_t radix_sort_records(const KeyParams& kp, const T* xp, int64_t ldxp, c
   using V = typename Vec4<CT>::type;
   constexpr int RU = (int)(sizeof(V) / 16);
   const int nchunk = up ? (lda + 3) / 4 : 0;
+  const int IU = RU * (1 + nchunk);  // 16-byte units per particle: record, strengths
   const size_t n = (size_t)(np > 0 ? np : 1);
   const size_t nus = n * (size_t)(nchunk > 0 ? nchunk : 1);
   const size_t nk = n + 16;  // bulk copies of keys round up to 16 bytes
   cudaError_t e;
   if ((e = ws.key.ensure(sizeof(int) * nk)) || (e = ws.key2.ensure(sizeof(int) * nk)) ||
       (e = ws.idx.ensure(sizeof(int) * nk)) || (e = ws.idx2.ensure(sizeof(int) * nk)) ||
-      (e = ws.rec.ensure(sizeof(V) * n)) || (e = ws.rec2.ensure(sizeof(V) * n)) ||
-      (e = ws.us.ensure(sizeof(V) * nus)) || (e = ws.us2.ensure(sizeof(V) * nus)) ||
+      (e = ws.rec.ensure(sizeof(V) * n)) || (e = ws.rec2.ensure(sizeof(uint4) * n * IU)) ||
+      (e = ws.us.ensure(sizeof(V) * nus)) ||
       (e = ws.start.ensure(sizeof(int) * (size_t)(ncell + 1))) ||
       (e = ws.err.ensure(sizeof(int) * 4)))
     return e;
@@ -532,8 +513,6 @@ cudaError_t radix_sort_records(const KeyParams& kp, const T* xp, int64_t ldxp, c
   int* d_nvalid = ws.err.as<int>() + 2;
   DevBuf* keys[2] = {&ws.key, &ws.key2};
   DevBuf* ids[2] = {&ws.idx, &ws.idx2};
-  DevBuf* recs[2] = {&ws.rec, &ws.rec2};
-  DevBuf* uss[2] = {&ws.us, &ws.us2};
   for (int p = 0; p < passes; ++p) {
     const int shift = p * bits;
     const int pb = nbits - shift < bits ? nbits - shift : bits;
@@ -558,8 +537,8 @@ cudaError_t radix_sort_records(const KeyParams& kp, const T* xp, int64_t ldxp, c
     C.key_in = keys[in]->as<int>();
     C.hist = ws.hist.as<int>();
     C.key0 = keys[in]->as<int>();
-    C.rec0 = recs[in]->as<V>();
-    C.us0 = uss[in]->as<V>();
+    C.aos = ws.rec2.as<uint4>();
+    C.iu = IU;
     C.err = err_counter;
     C.zout = zout;
     C.ldz = ldz;
@@ -581,22 +560,33 @@ cudaError_t radix_sort_records(const KeyParams& kp, const T* xp, int64_t ldxp, c
     M.bits = pb;
     M.subs = subs;
     M.ntiles = ntiles;
-    M.rplanes = RU;
-    M.nplanes = RU * (1 + nchunk);
     M.hist = ws.hist.as<int>();
     M.key_in = keys[in]->as<int>();
     M.id_in = ids[in]->as<int>();
-    M.rec_in = recs[in]->as<uint4>();
-    M.us_in = uss[in]->as<uint4>();
     M.key_out = keys[out]->as<int>();
     M.id_out = ids[out]->as<int>();
-    M.rec_out = recs[out]->as<uint4>();
-    M.us_out = uss[out]->as<uint4>();
     M.wait_flag = wait_flag;
     if (p == 0)
       k_radix_move<true><<<ntiles, kRThreads, kMoveSmem, st>>>(M);
     else
       k_radix_move<false><<<ntiles, kRThreads, kMoveSmem, st>>>(M);
+    count_launch();
+  }
+  // records and strengths into the sorted order (the last pass wrote set 0)
+  {
+    const int64_t units = np * (int64_t)IU;
+    const int64_t gb = (units + 256 * 4 - 1) / (256 * 4);
+    const int grid = (int)(gb < 148 * 16 ? gb : 148 * 16);
+    uint4* rec = ws.rec.as<uint4>();
+    uint4* us = ws.us.as<uint4>();
+    const uint4* aos = ws.rec2.as<uint4>();
+    const int* sid = ws.idx.as<int>();
+    switch (IU) {
+      case 1: k_gather_units<1><<<grid, 256, 0, st>>>(sid, d_nvalid, aos, IU, RU, np, rec, us); break;
+      case 2: k_gather_units<2><<<grid, 256, 0, st>>>(sid, d_nvalid, aos, IU, RU, np, rec, us); break;
+      case 4: k_gather_units<4><<<grid, 256, 0, st>>>(sid, d_nvalid, aos, IU, RU, np, rec, us); break;
+      default: k_gather_units<0><<<grid, 256, 0, st>>>(sid, d_nvalid, aos, IU, RU, np, rec, us); break;
+    }
     count_launch();
   }
   // cell offsets from the sorted keys

@@ -38,7 +38,7 @@ void DevBuf::release() {
 Workspace::~Workspace() {
   DevBuf* all[] = {&key, &slot, &idx, &count, &start, &bsum, &rec, &us, &err,
                    &big, &tiles, &h_xp, &h_up, &h_field, &h_aux, &w1d,
-                   &key2, &idx2, &rec2, &us2, &hist, &gaps};
+                   &key2, &idx2, &rec2, &hist, &gaps};
   for (DevBuf* b : all) b->release();
   if (h_err_pinned) cudaFreeHost(h_err_pinned);
 }

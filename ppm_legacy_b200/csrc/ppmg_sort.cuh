@@ -27,7 +27,7 @@ struct DevBuf {
 // Scratch of one handle (device memory, grown on demand, reused).
 struct Workspace {
   DevBuf key, slot, idx, count, start, bsum, rec, us, err, big, tiles;
-  DevBuf key2, idx2, rec2, us2, hist, gaps;  // radix sort: second buffer set, histograms
+  DevBuf key2, idx2, rec2, hist, gaps;  // radix sort: second key/id set, record rows, histograms
   DevBuf h_xp, h_up, h_field, h_aux;  // device mirrors for host-pointer calls
   DevBuf w1d;                          // comp_weights state: sorted 1D weights
   int* h_err_pinned = nullptr;         // pinned host copy of the error word
@@ -88,7 +88,8 @@ cudaError_t pack_records(const KeyParams& kp, const T* xp, int64_t ldxp, const T
                          Workspace& ws, cudaStream_t st);
 
 // Stable LSD radix sort of the particles by cell (the order of bin_sort:
-// ascending id inside a cell) that carries their packed records along.  On
+// ascending id inside a cell) of (key, id) pairs, followed by one gather of
+// the packed records and strengths into the sorted order.  On
 // return (stream-ordered), for sorted positions s < np:
 //   ws.key[s]  cell of the particle (ncell for an invalid one; those sort last)
 //   ws.idx[s]  particle id

@@ -105,10 +105,14 @@ def test_ghost_widths(nc, g):
     check_p2m(t, xp, up, 2, g, 0)
 
 
-@pytest.mark.parametrize("n", [1, 2, 4095, 4096, 4097, 8193])
-def test_ragged_particle_counts(n):
-    rng = np.random.default_rng(n)
-    t = registered(3, 8)
+@pytest.mark.parametrize("n,nc", [(1, 8), (2, 8), (4095, 8), (4096, 8), (4097, 8), (8191, 8),
+                                  (8192, 8), (8193, 8), (16385, 8), (8191, 40), (8193, 40),
+                                  (24577, 40)])
+def test_ragged_particle_counts(n, nc):
+    """Particle counts around the radix sort's 8192-item sub-tile, with one
+    sort pass (8^3 cells) and two (40^3 cells)."""
+    rng = np.random.default_rng(n + nc)
+    t = registered(3, nc)
     xp = random_particles(rng, 3, n)
     up = rng.standard_normal((3, n))
     check_p2m(t, xp, up, 2, [2, 2, 2], 0)
