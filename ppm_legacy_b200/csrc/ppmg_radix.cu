@@ -6,7 +6,7 @@
 // slots and then gathers every particle's position and strengths from random
 // addresses; on large unordered particle sets those random accesses, not the
 // arithmetic, set its time.  Here every pass reads its input in order and
-// writes it grouped by one digit of the cell key: a sub-tile of 8192
+// writes it grouped by one digit of the cell key: a sub-tile of 4096
 // particles is ranked in shared memory and leaves as runs of equal digit, so
 // both the reads and the writes are coalesced.  The first count pass builds
 // the keys from xp and writes each particle's record and strengths as one
@@ -25,12 +25,12 @@ namespace ppmg {
 namespace {
 
 constexpr int kCThreads = 512;                  // count kernel (full occupancy in one wave)
-constexpr int kRThreads = 1024;                 // move kernel
+constexpr int kRThreads = 512;                  // move kernel (two CTAs per SM)
 constexpr int kRWarps = kRThreads / 32;
 constexpr int kRItems = 8;                      // items per thread and sub-tile
-constexpr int kRSub = kRThreads * kRItems;      // 8192 items per sub-tile
+constexpr int kRSub = kRThreads * kRItems;      // 4096 items per sub-tile
 constexpr int kRWarpItems = kRSub / kRWarps;    // 256 consecutive items per warp
-constexpr int kRMaxBits = 9;                    // >= 16 items per digit and sub-tile
+constexpr int kRMaxBits = 9;                    // >= 8 items per digit and sub-tile
 constexpr int kRMaxBuckets = 1 << kRMaxBits;
 constexpr int kRSlots = kRMaxBuckets + 32;      // + the invalid bucket of the first pass
 constexpr int kRDigitsPerThread = (kRMaxBuckets + 1 + kRThreads - 1) / kRThreads;
@@ -219,7 +219,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
 
 // Shared memory of k_radix_move: two key and two id buffers (kRSub entries
 // each), the 16-bit inverse map and per-warp digit counts, the per-digit
-// offsets and the mbarriers.
+// offsets and the mbarriers (~98 KB: two CTAs of 16 warps per SM, so one
+// CTA's ranking overlaps the other's barriers and stores).
 constexpr size_t kMoveSmem = 4 * sizeof(int) * (size_t)kRSub +
                              sizeof(unsigned short) * (size_t)(kRSub + kRWarps * kRSlots) +
                              sizeof(int) * (size_t)(3 * kRSlots + 64) + 4 * sizeof(uint64_t);
@@ -233,7 +234,7 @@ constexpr size_t kMoveSmem = 4 * sizeof(int) * (size_t)kRSub +
 // sorted position of the sub-tile to its item, so keys and ids leave in digit
 // runs.
 template <bool FIRST>
-__global__ void __launch_bounds__(kRThreads, 1) k_radix_move(MoveArgs A) {
+__global__ void __launch_bounds__(kRThreads, 2) k_radix_move(MoveArgs A) {
   extern __shared__ __align__(128) unsigned char smem[];
   int* kb = reinterpret_cast<int*>(smem);                             // [2][kRSub] keys
   int* ib = kb + 2 * kRSub;                                           // [2][kRSub] ids

@@ -109,7 +109,7 @@ def test_ghost_widths(nc, g):
                                   (8192, 8), (8193, 8), (16385, 8), (8191, 40), (8193, 40),
                                   (24577, 40)])
 def test_ragged_particle_counts(n, nc):
-    """Particle counts around the radix sort's 8192-item sub-tile, with one
+    """Particle counts around the radix sort's 4096-item sub-tile, with one
     sort pass (8^3 cells) and two (40^3 cells)."""
     rng = np.random.default_rng(n + nc)
     t = registered(3, nc)
