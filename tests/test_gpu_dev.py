@@ -147,3 +147,46 @@ def test_m2p_reuses_p2m_order_only_for_identical_positions(n):
     finally:
         ppmg.lib().ppmg_kernel_timing(0)
         ppmg.set_precision(0)
+
+
+@pytest.mark.parametrize("lda", [5, 8])
+def test_mixed_many_components_against_oracle(lda):
+    """Mixed precision with lda > 4: the sort's record rows carry two strength
+    chunks (three 16-byte units per particle) and P2M runs one launch per
+    chunk.  P2M and M2P agree with the FP64 oracle to <= 1e-6.  The cluster
+    puts thousands of particles into single cells; there the partial sums of
+    a staging unit, plain FP32 before the compensated fold, bound the
+    conservation of total strength to ~3e-9 of sum |u| (1e-10 holds at the
+    benchmark densities, test_config2_round_trip_properties)."""
+    rng = np.random.default_rng(500 + lda)
+    nc = 24
+    t = registered(3, nc)
+    g = [2, 2, 2]
+    n = 30000
+    # a dense cluster (several staging units per layer) over a uniform background
+    xp = np.concatenate([random_particles(rng, 3, n // 2),
+                         np.clip(0.4 + 0.03 * rng.standard_normal((3, n - n // 2)), 0.0, 0.999)],
+                        axis=1)
+    up = rng.standard_normal((lda, n))
+    ref, lb, ub = O.p2m(t, xp, up, 2, g)
+    shape = ref.shape
+    dxp, dup = colmajor(xp), colmajor(up)
+    ppmg.set_precision(1)
+    try:
+        f = colmajor(np.zeros(shape))
+        assert ppmg.ppm_interp_p2m(dxp, n, dup, lda, t.topo_id, t.mesh_id, 2, g, f) == 0
+        assert ppmg.sync_status(t.topo_id, t.mesh_id) == 0
+        fh = f.cpu().numpy()
+        s = tuple(slice(g[a], g[a] + nc + 1) for a in range(3))
+        assert max_rel(fh[(slice(None),) + s], ref[(slice(None),) + s]) < 1e-6
+        tot = fh[(slice(None),) + tuple(slice(g[a], g[a] + nc) for a in range(3))].sum(
+            axis=(1, 2, 3, 4))
+        np.testing.assert_allclose(tot, up.sum(axis=1), rtol=0,
+                                   atol=1e-8 * np.abs(up).sum(axis=1).max())
+        out = colmajor(np.zeros((lda, n)))
+        assert ppmg.ppm_interp_m2p(dxp, n, out, lda, t.topo_id, t.mesh_id, 2, g, f) == 0
+        assert ppmg.sync_status(t.topo_id, t.mesh_id) == 0
+        oref = O.m2p(t, xp, fh, lb, ub, lda, 2, g)
+        assert max_rel(out.cpu().numpy(), oref) < 1e-6
+    finally:
+        ppmg.set_precision(0)
