@@ -10,10 +10,10 @@
 // particles is ranked in shared memory and leaves as runs of equal digit, so
 // both the reads and the writes are coalesced.  The first count pass builds
 // the keys from xp and writes each particle's record and strengths as one
-// row of 16-byte units (one 32-byte sector in the mixed form); the passes
-// move only (key, id), and one gather then copies every row into the sorted
-// planes.  Carrying the 32-64 byte payload through every pass cost more than
-// the single gather of one sector per particle.
+// row of 16-byte units (32 bytes in the mixed form); the passes move only
+// (key, id), and one gather then copies every row into the sorted planes.
+// A random row read costs DRAM about 128 bytes, yet carrying the 32-64 byte
+// payload through every pass cost more than that single random read.
 // The sort is stable and starts from particle-id order, so particles of one
 // cell end in ascending id -- the fill order of ppm_util_rank3d.f:525-533.
 #include <cuda_runtime.h>
