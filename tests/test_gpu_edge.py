@@ -134,3 +134,44 @@ def test_positions_on_faces_and_near_the_upper_face():
     up = np.asfortranarray(np.random.default_rng(5).standard_normal((2, xp.shape[1])))
     check_p2m(t, xp, up, 2, [2, 2, 2], 0)
     check_p2m(t, xp, up, 1, [1, 1, 1], 0)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_m2p_non_finite_positions(mode):
+    """M2P with non-finite positions among ~9000 valid ones (more than two
+    sort sub-tiles): the sort drops them into its invalid bucket, their rows
+    of up are zero, info = -2 / errno 503, and every valid particle still
+    gets the oracle's value (FP64 bit for bit, mixed to <= 1e-6)."""
+    rng = np.random.default_rng(77 + mode)
+    t = registered(3, 12)
+    g = [2, 2, 2]
+    n = 9001
+    xp = random_particles(rng, 3, n)
+    bad = np.array([0, 3, 4095, 4096, 8191, 9000])
+    xp[0, bad[:2]] = np.nan
+    xp[1, bad[2]] = np.inf
+    xp[2, bad[3]] = -np.inf
+    xp[:, bad[4]] = np.nan
+    xp[2, bad[5]] = np.nan
+    ok = np.ones(n, dtype=bool)
+    ok[bad] = False
+    src = random_particles(rng, 3, 3000)
+    # the GPU's field: every periodic image holds its node's value, the
+    # field the oracle's M2P reads as given and the GPU's reads with wrap
+    f, _, lb, _ = p2m_both(t, src, rng.standard_normal((3, 3000)), 2, g)
+    ub = [int(t.Nm[a]) + 2 for a in range(3)]
+    out = np.full((3, n), 7.0, order="F")
+    ppmg.set_precision(mode)
+    try:
+        info = ppmg.ppm_interp_m2p(np.asfortranarray(xp), n, out, 3, t.topo_id, t.mesh_id, 2, g, f)
+        err = ppmg.last_error()  # before the next library call replaces it
+    finally:
+        ppmg.set_precision(0)
+    assert info == -2
+    assert err[1] == 503
+    assert np.all(out[:, ~ok] == 0.0)
+    ref = O.m2p(t, np.asfortranarray(xp[:, ok]), f, lb, ub, 3, 2, g)
+    if mode == 0:
+        assert np.array_equal(out[:, ok], ref)
+    else:
+        assert max_rel(out[:, ok], ref) < 1e-6
