@@ -119,6 +119,52 @@ def measured_traffic(kernel, np_):
         return None
 
 
+def _mesh_moments(torch, U, h):
+    """sum_n x_n^k f_n over the unique nodes U(lda, nx, ny, nz) (FP64), for
+    k = 0, 1, 2 and every axis: tensor [k, axis, component]."""
+    lda = U.shape[0]
+    out = torch.zeros((3, 3, lda), dtype=torch.float64, device=U.device)
+    for d in range(3):
+        s = U.sum(dim=[a + 1 for a in range(3) if a != d])  # (lda, n_d)
+        x = torch.arange(U.shape[1 + d], dtype=torch.float64, device=U.device) * h
+        for k in range(3):
+            out[k, d] = s @ x ** k
+    return out
+
+
+def _particle_moments(torch, xp, up):
+    """sum_p x_p^k u_p and sum_p |x_p^k u_p|: tensors [k, axis, component]."""
+    lda = up.shape[0]
+    val = torch.zeros((3, 3, lda), dtype=torch.float64, device=up.device)
+    mag = torch.zeros_like(val)
+    au = up.abs()
+    for d in range(3):
+        xd = xp[d]
+        for k in range(3):
+            xk = xd ** k
+            val[k, d] = up @ xk
+            mag[k, d] = au @ xk.abs()
+    return val, mag
+
+
+def moment_errors(torch, U, h, xp, up):
+    """Relative conservation error of moments 0, 1, 2 (max over axes and
+    components): |sum_n x^k f - sum_p x^k u| / sum_p |x^k u|."""
+    m = _mesh_moments(torch, U, h)
+    v, a = _particle_moments(torch, xp, up)
+    rel = (m - v).abs() / torch.where(a > 0, a, torch.ones_like(a))
+    return [float(rel[k].max()) for k in range(3)]
+
+
+def rel_errors(torch, a, ref):
+    """Normwise max and RMS relative error of a against ref."""
+    d = a - ref
+    den_max = float(ref.abs().max())
+    den_rms = float(torch.linalg.vector_norm(ref))
+    return (float(d.abs().max()) / (den_max or 1.0),
+            float(torch.linalg.vector_norm(d)) / (den_rms or 1.0))
+
+
 def slab_topology(ppmg, nc, world, topo_id=1, mesh_id=1):
     """The weak-scaling domain: world z-slabs of nc^3 cells, cubic cells of
     size 1/nc, periodic; slab r covers z in [r, r+1)."""
@@ -455,6 +501,48 @@ def run_adjoint(args):
                    "l2": "L2 flushed between timed steps (outside the steps' events)"}}))
 
 
+def launch_ranks(n):
+    """Re-run this command as n ranks on this node (torch.distributed.run on
+    127.0.0.1, a free port); returns the launcher's exit status."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={n}", "--master-addr", "127.0.0.1", "--master-port", str(port),
+           os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.call(cmd)
+
+
+def launch_check(args):
+    """Every rank joins the process group; rank 0 prints how many did."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    seen = 1
+    if world > 1:
+        if args.dist_backend == "nccl":
+            local = int(os.environ.get("LOCAL_RANK", "0"))
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+            dev = torch.device("cuda", local)
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+            dev = "cpu"
+        t = torch.ones(1, device=dev)
+        dist.all_reduce(t)
+        seen = int(t.item())
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({"launch_check": True, "n_gpus": world, "ranks_joined": seen,
+                          "backend": args.dist_backend if world > 1 else None}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -475,9 +563,21 @@ def main():
     ap.add_argument("--workload", default="roundtrip", choices=["roundtrip", "remesh", "adjoint"],
                     help="roundtrip: the metric (default); remesh / adjoint: the 256^3 remesh "
                          "and 128^3 adjoint workloads, one JSON line each")
+    ap.add_argument("--launch-check", action="store_true",
+                    help="start the ranks and the process group only (no GPU work) and print "
+                         "one line with the number of ranks that joined")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        # one process per GPU: start the N ranks here through torch.distributed.run
+        return launch_ranks(args.gpus)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world != args.gpus:
+        raise SystemExit(f"bench.py: --gpus {args.gpus} but {world} ranks were started "
+                         f"(WORLD_SIZE); launch with --nproc-per-node {args.gpus}")
+    if args.launch_check:
+        return launch_check(args)
     if args.workload == "remesh":
         return run_remesh(args)
     if args.workload == "adjoint":
@@ -488,7 +588,6 @@ def main():
 
     import ppm_legacy_b200 as ppmg
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0")) % max(torch.cuda.device_count(), 1)
     torch.cuda.set_device(local)
@@ -593,10 +692,54 @@ def main():
     sampler = ClockSampler(local)
     sampler.start()
     res = {}
+    snap = {}
     precs = {"both": [1, 0], "mixed": [1], "fp64": [0]}[args.precision]
     for prec in precs:
         res[prec] = timed(prec)
+        if world == 1 and len(precs) == 2:
+            # the last timed step's results of this form (accuracy block below)
+            snap[prec] = (field[:, g[0]:g[0] + nc, g[1]:g[1] + nc, g[2]:g[2] + nc, 0].clone(),
+                          out.clone())
     clocks = sampler.stop()
+
+    accuracy = None
+    if snap:
+        # Mixed form against the plain FP64 form on the benchmark's own data
+        # (the FP64 form matches the oracle to <= 1e-13 in the parity tests),
+        # and conservation of moments 0, 1, 2 by both forms.  Moment 0 is taken
+        # from the timed steps' fields over all particles; moments 1 and 2 per
+        # axis from one more P2M per form of the particles whose support does
+        # not wrap (stencil origin in [1, Nc-2) on every axis), since a wrapped
+        # node sits a period away from its particle.
+        h = 1.0 / nc
+        pm, rm = rel_errors(torch, snap[1][0], snap[0][0])
+        po, ro = rel_errors(torch, snap[1][1], snap[0][1])
+        xi = xp * nc
+        inner = torch.all((xi >= 1.0) & (xi < nc - 2.0), dim=0)
+        up_in = (up.t() * inner[:, None]).t()  # column-major like up
+        cons = {}
+        for prec in (1, 0):
+            e0 = moment_errors(torch, snap[prec][0], h, xp, up)[0]
+            ppmg.set_precision(prec)
+            if ppmg.ppm_interp_p2m(xp, n, up_in, 3, 1, 1, 2, g, field):
+                raise RuntimeError(f"library error {ppmg.last_error()}")
+            U = field[:, g[0]:g[0] + nc, g[1]:g[1] + nc, g[2]:g[2] + nc, 0]
+            e = moment_errors(torch, U, h, xp, up_in)
+            cons["mixed" if prec == 1 else "fp64"] = {"moment0": e0, "moment1": e[1],
+                                                      "moment2": e[2]}
+        assert ppmg.sync_status(1, 1) == 0, ppmg.last_error()
+        accuracy = {
+            "data": f"the benchmark's {nc}^3 data ({n} {CONFIGS[args.config][2]} particles, "
+                    f"lda 3), results of the last timed step of each form",
+            "mixed_vs_fp64": {"p2m_max_rel": pm, "p2m_rms_rel": rm,
+                              "m2p_max_rel": po, "m2p_rms_rel": ro},
+            "conservation": cons,
+            "moment_rule": ("|sum_n x_n^k f_n - sum_p x_p^k u_p| / sum_p |x_p^k u_p|, max over "
+                            "axes and components; k = 0 over all particles, k = 1, 2 over the "
+                            f"{int(inner.sum())} particles whose support does not wrap"),
+            "targets": {"max_rel": 1e-6, "moments": 1e-10},
+        }
+        del snap, up_in, inner, xi
 
     peak, peak_src = hbm_peak()
     head = precs[0]
@@ -759,7 +902,7 @@ def main():
                        f"ghost put/get between neighbouring slabs over "
                        f"{args.dist_backend.upper()}"},
             "roofline": roof, "forms": parts, "clocks": clocks, "gpu_launches": launches,
-            "e2e": e2e, "cpu_baseline": cb, "adjoint": adj,
+            "e2e": e2e, "cpu_baseline": cb, "adjoint": adj, "accuracy": accuracy,
         }
         print(json.dumps(line))
     if world > 1:

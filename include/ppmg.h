@@ -128,7 +128,10 @@ void ppmg_interp_p2m_sv_2d_dev(PPMG_P2M_V_ARGS(float), void* stream);
  * info = -2 (errnum 503) and launch nothing.
  * The first call on a device looks up the array's device address (this may
  * load the library's device code on that device): make it before any stream
- * capture.  All calls on a device share the array and each overwrites the
+ * capture.  The address is kept per device and looked up again when the
+ * device's context has changed (after a cudaDeviceReset).  Particles outside
+ * the subdomain are reported through ppmg_sync_status as for the _dev entry
+ * point (info = -1, errnum 405).  All calls on a device share the array and each overwrites the
  * previous call's contents (what must start at zero is cleared by the call):
  * calls whose GPU work overlaps -- different streams, or different host
  * threads -- race and corrupt each other's results; order them on one stream. */

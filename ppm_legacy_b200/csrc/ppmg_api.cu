@@ -2,7 +2,9 @@
 // registry (the geometry state the reference keeps in ppm_module_data*),
 // argument validation with the reference's info/errno conventions, and the
 // host-pointer (synchronous) and device-pointer (stream-ordered) pipelines.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <cmath>
 #include <cstdio>
@@ -1886,9 +1888,29 @@ constexpr int kNoAllocMaxDevices = 64;
 
 std::mutex g_noalloc_mu;
 void* g_noalloc_base[kNoAllocMaxDevices] = {};
+CUcontext g_noalloc_ctx[kNoAllocMaxDevices] = {};
+
+// The calling thread's current CUDA context (the device's primary context for
+// runtime-API callers), through the driver entry point the runtime exposes,
+// so that the library needs no link-time dependency on libcuda.
+CUcontext current_context() {
+  static PFN_cuCtxGetCurrent_v4000 get = [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      fn = nullptr;
+    return reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(fn);
+  }();
+  CUcontext c = nullptr;
+  if (get == nullptr || get(&c) != CUDA_SUCCESS) return nullptr;
+  return c;
+}
 
 // Device address of the scratch array on the current device.  The first call
 // on a device looks it up (which may load this library's device code there).
+// The address belongs to the device's context: after a cudaDeviceReset the
+// next call finds a new context and looks the address up again.
 void* noalloc_scratch(int* info, const char* caller) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
@@ -1898,7 +1920,10 @@ void* noalloc_scratch(int* info, const char* caller) {
     return nullptr;
   }
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (g_noalloc_base[dev] == nullptr) {
+  // no current context yet (a thread's first CUDA call) also means a lookup,
+  // which makes the device's primary context current
+  const CUcontext ctx = current_context();
+  if (g_noalloc_base[dev] == nullptr || ctx == nullptr || ctx != g_noalloc_ctx[dev]) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, ppmg_noalloc_scratch);
     if (e != cudaSuccess) { cuda_fail(info, e, caller); return nullptr; }
@@ -1907,6 +1932,7 @@ void* noalloc_scratch(int* info, const char* caller) {
       return nullptr;
     }
     g_noalloc_base[dev] = p;
+    g_noalloc_ctx[dev] = current_context();
   }
   return g_noalloc_base[dev];
 }

@@ -69,3 +69,54 @@ def max_rel(a, ref):
 def rms_rel(a, ref):
     den = np.sqrt((ref ** 2).sum())
     return float(np.sqrt(((a - ref) ** 2).sum()) / (den if den > 0 else 1.0))
+
+
+def interior_mask(xp, nc, lo=0.0, hi=1.0):
+    """Particles whose M'4 support stays inside one periodic image of the box:
+    stencil origin xi = (x - lo) / h in [1, nc - 2) on every axis, so the
+    nodes i0-1 .. i0+2 never wrap.  Moments 1 and 2 of the deposited field
+    equal the particles' only for these (the node coordinate of a wrapped
+    node is a period away from the particle)."""
+    h = (hi - lo) / nc
+    xi = (np.asarray(xp)[:3] - lo) / h
+    return np.all((xi >= 1.0) & (xi < nc - 2.0), axis=0)
+
+
+def mesh_moments(U, h, lo=0.0):
+    """sum_n x_n^k f_n over the unique nodes U(lda, nx, ny, nz) for k = 0, 1, 2
+    and every axis: array [k, axis, component] (k = 0 repeated per axis)."""
+    U = np.asarray(U, dtype=np.float64)
+    lda = U.shape[0]
+    out = np.zeros((3, 3, lda))
+    for d in range(3):
+        other = tuple(a + 1 for a in range(3) if a != d)
+        s = U.sum(axis=other)  # (lda, n_d)
+        x = lo + np.arange(U.shape[1 + d]) * h
+        for k in range(3):
+            out[k, d] = s @ (x ** k)
+    return out
+
+
+def particle_moments(xp, up):
+    """sum_p x_p^k u_p and sum_p |x_p^k u_p|: arrays [k, axis, component]."""
+    xp = np.asarray(xp, dtype=np.float64)[:3]
+    up = np.asarray(up, dtype=np.float64)
+    up = up if up.ndim == 2 else up[None]
+    lda = up.shape[0]
+    val = np.zeros((3, 3, lda))
+    mag = np.zeros((3, 3, lda))
+    for d in range(3):
+        for k in range(3):
+            xk = xp[d] ** k
+            val[k, d] = up @ xk
+            mag[k, d] = np.abs(up) @ np.abs(xk)
+    return val, mag
+
+
+def moment_errors(U, h, xp, up, lo=0.0):
+    """Relative conservation error of moments 0, 1, 2 (max over axes and
+    components): |sum_n x^k f - sum_p x^k u| / sum_p |x^k u|."""
+    m = mesh_moments(U, h, lo)
+    v, a = particle_moments(xp, up)
+    rel = np.abs(m - v) / np.where(a > 0, a, 1.0)
+    return [float(rel[k].max()) for k in range(3)]

@@ -1,0 +1,139 @@
+"""Parity at the benchmark configurations' own sizes and data.
+
+Config 2: 128^3 periodic mesh, one particle per cell jittered (2,097,152
+particles), lda 3, both precision forms against the oracle.
+Config 5 shape at 128^3: the clustered distribution of the 512^3 workload
+(50% uniform + 4 Gaussian blobs, sigma 0.05: the same particles per cell as
+at 512^3, up to ~60 in the blob cores), 2,097,152 particles, lda 3.
+Config 3: the 256^3 remeshing workload with its exact generator (cell
+centres displaced by 8 Fourier modes, vortex-tube strengths) through
+comp_weights, remesh and create_part.
+
+Accuracy metrics (normwise, over the real unique nodes or the particles):
+max |a - ref| / max |ref| and ||a - ref||_2 / ||ref||_2.  Conservation: moment
+0 over all particles, moments 1 and 2 per axis over the particles whose
+support does not wrap (a separate P2M of those particles).
+"""
+import numpy as np
+import pytest
+
+import ppm_legacy_b200 as ppmg
+from _util import (box_bounds, interior_mask, jittered_particles, max_rel, moment_errors,
+                   periodic_fill, rms_rel, topo_for, unique_view)
+from oracle import oracle as O
+
+pytestmark = [pytest.mark.gpu, pytest.mark.slow]
+
+_next_id = [1300]
+
+
+def registered(nc):
+    _next_id[0] += 1
+    t = topo_for(3, nc, topo_id=_next_id[0], mesh_id=1)
+    assert ppmg.register(t) == 0, ppmg.last_error()
+    return t
+
+
+def clustered_particles(rng, n):
+    """50% uniform + 4 Gaussian blobs (sigma 0.05, centres in [0.2, 0.8)^3),
+    wrapped into [0, 1)^3: the distribution of the 512^3 benchmark."""
+    nu = n // 2
+    nb = (n - nu) // 4
+    parts = [rng.random((3, nu))]
+    centres = 0.2 + 0.6 * rng.random((4, 3))
+    for b in range(4):
+        m = nb if b < 3 else n - nu - 3 * nb
+        parts.append((centres[b][:, None] + 0.05 * rng.standard_normal((3, m))) % 1.0)
+    xp = np.concatenate(parts, axis=1)
+    return np.asfortranarray(np.where(xp >= 1.0, 0.0, xp))
+
+
+def _p2m(t, xp, up, g):
+    lb, ub = box_bounds(t, g)
+    f = np.zeros((up.shape[0],) + tuple(ub[a] - lb[a] + 1 for a in range(3)) + (1,), order="F")
+    info = ppmg.ppm_interp_p2m(xp, xp.shape[1], up, up.shape[0], t.topo_id, t.mesh_id, 2, g, f)
+    assert info == 0, ppmg.last_error()
+    return f, lb
+
+
+def _m2p(t, xp, f, lda, g):
+    out = np.zeros((lda, xp.shape[1]), order="F")
+    info = ppmg.ppm_interp_m2p(xp, xp.shape[1], out, lda, t.topo_id, t.mesh_id, 2, g, f)
+    assert info == 0, ppmg.last_error()
+    return out
+
+
+@pytest.mark.parametrize("dist", ["jittered", "clustered"])
+def test_config_128_round_trip_against_oracle(dist):
+    """P2M and M2P at 128^3 with 2,097,152 particles, lda 3, in both forms."""
+    rng = np.random.default_rng(2 if dist == "jittered" else 5)
+    nc = 128
+    h = 1.0 / nc
+    t = registered(nc)
+    g = [2, 2, 2]
+    xp = jittered_particles(rng, 3, nc) if dist == "jittered" else clustered_particles(rng, nc ** 3)
+    if dist == "jittered":  # the particles arrive in random order, as in the benchmark
+        xp = np.asfortranarray(xp[:, rng.permutation(xp.shape[1])])
+    n = xp.shape[1]
+    up = np.asfortranarray(rng.standard_normal((3, n)))
+    ref, lbo, ubo = O.p2m(t, xp, up, 2, g)
+    ref_u = unique_view(ref, lbo, [nc] * 3, 3)
+    O.ghost_get(t, ref, lbo, ubo, g)
+    ref_out = O.m2p(t, xp, ref, lbo, ubo, 3, 2, g)
+    inner = interior_mask(xp, nc)
+    up_in = np.asfortranarray(np.where(inner[None, :], up, 0.0))
+    try:
+        for mode, tol in ((0, 1e-13), (1, 1e-6)):
+            ppmg.set_precision(mode)
+            f, lb = _p2m(t, xp, up, g)
+            fu = unique_view(f, lb, [nc] * 3, 3)
+            assert max_rel(fu, ref_u) < tol and rms_rel(fu, ref_u) < tol
+            # real nodes 1..Nm, node Nm a copy of node 1 (the reference's put)
+            real = (slice(None),) + (slice(1 - lb[0], nc + 2 - lb[0]),) * 3 + (0,)
+            assert max_rel(f[real], ref[real]) < tol
+            e0 = moment_errors(fu, h, xp, up)[0]
+            assert e0 < 1e-10, (mode, e0)
+            out = _m2p(t, xp, f, 3, g)
+            assert max_rel(out, ref_out) < tol and rms_rel(out, ref_out) < tol
+            if mode == 0:
+                # M2P alone on the oracle's own field: the same terms in the same
+                # order, bit for bit
+                assert np.array_equal(_m2p(t, xp, ref, 3, g), ref_out)
+            fi, lbi = _p2m(t, xp, up_in, g)
+            e = moment_errors(unique_view(fi, lbi, [nc] * 3, 3), h, xp, up_in)
+            assert max(e) < 1e-10, (mode, e)
+    finally:
+        ppmg.set_precision(0)
+
+
+def test_config3_remesh_chain_against_oracle():
+    """comp_weights -> remesh -> create_part (cutoff (1e-8, huge) on |u|_2,
+    resetpos) on the 256^3 remeshing workload, FP64 form: field within 1e-13
+    of the oracle, the new particles equal in number and order, their
+    strengths within 1e-13 and positions equal."""
+    from bench import _cfg3_particles
+    nc = 256
+    xp, up = _cfg3_particles(nc)
+    n = xp.shape[1]
+    t = registered(nc)
+    g = [2, 2, 2]
+    ppmg.set_precision(0)
+    assert ppmg.ppm_rmsh_comp_weights(xp, n, t.topo_id, t.mesh_id, 2) == 0, ppmg.last_error()
+    lb, ub = box_bounds(t, g)
+    f = np.zeros((3,) + tuple(ub[a] - lb[a] + 1 for a in range(3)) + (1,), order="F")
+    assert ppmg.ppm_rmsh_remesh(xp, n, up, 3, t.topo_id, t.mesh_id, 2, g, f) == 0, \
+        ppmg.last_error()
+    wo, lst, si = O.comp_weights(t, xp, 2)
+    fo, lbo, ubo = O.remesh(t, xp, up, 2, g, wo, lst, si)
+    del wo
+    real = (slice(None),) + (slice(1 - lb[0], nc + 2 - lb[0]),) * 3 + (0,)
+    assert max_rel(f[real], fo[real]) < 1e-13
+    assert rms_rel(f[real], fo[real]) < 1e-13
+    cut = [1e-8, 1e300]
+    info, npn, upn, xpn, _ = ppmg.ppm_rmsh_create_part(f, t.topo_id, t.mesh_id, cut, lda=3,
+                                                       resetpos=True, ghostsize=g)
+    assert info == 0, ppmg.last_error()
+    no, upo, xpo, _ = O.create_part(t, fo, lbo, ubo, cut)
+    assert npn == no and no > nc ** 3 - 64
+    assert np.array_equal(xpn, xpo)
+    assert max_rel(upn, upo) < 1e-13

@@ -227,3 +227,29 @@ def test_oracle_poisson_recovers_an_analytic_solution():
     # the mean of omega (the zero mode) does not enter phi
     got2 = O.poisson((lam * phi + 3.0)[None], L)[0]
     assert np.abs(got2 - phi).max() < 1e-12
+
+
+def test_p2m_conserves_moments_0_1_2():
+    """The oracle's P2M conserves total strength for every particle and, for
+    particles whose support does not wrap, moments 1 and 2 per axis (M'4
+    reproduces polynomials of degree <= 2); bsp2 conserves moments 0 and 1."""
+    from _util import interior_mask, moment_errors, unique_view
+    rng = np.random.default_rng(31)
+    nc = 24
+    h = 1.0 / nc
+    t = topo_for(3, nc)
+    g = [2, 2, 2]
+    xp = random_particles(rng, 3, 4000)
+    up = rng.standard_normal((3, 4000))
+    inner = interior_mask(xp, nc)
+    assert 0 < inner.sum() < xp.shape[1]
+    for kernel, deg in ((2, 2), (1, 1)):
+        f, lb, _ = O.p2m(t, xp, up, kernel, g)
+        e0 = moment_errors(unique_view(f, lb, [nc] * 3, 3), h, xp, up)[0]
+        assert e0 < 1e-14
+        ui = np.where(inner[None, :], up, 0.0)
+        f, lb, _ = O.p2m(t, xp, ui, kernel, g)
+        errs = moment_errors(unique_view(f, lb, [nc] * 3, 3), h, xp, ui)
+        assert max(errs[: deg + 1]) < 1e-13, errs
+        if deg < 2:  # CIC does not reproduce x^2 (it adds f(1-f) h^2 per particle)
+            assert errs[2] > 1e-6
