@@ -91,8 +91,14 @@ def test_config_128_round_trip_against_oracle(dist):
             # real nodes 1..Nm, node Nm a copy of node 1 (the reference's put)
             real = (slice(None),) + (slice(1 - lb[0], nc + 2 - lb[0]),) * 3 + (0,)
             assert max_rel(f[real], ref[real]) < tol
+            # conservation bound: FP64 to rounding; mixed 5e-10 at this size.  The
+            # mixed form's product rounding (FP32, ~6e-8 of each term, unbiased)
+            # averages down as 1/sqrt(Np): the 1e-10 target holds at the 512^3
+            # benchmark size (134M particles, measured ~1.5e-11 there), and 2.1M
+            # particles give ~8x that
+            mtol = 1e-13 if mode == 0 else 5e-10
             e0 = moment_errors(fu, h, xp, up)[0]
-            assert e0 < 1e-10, (mode, e0)
+            assert e0 < mtol, (mode, e0)
             out = _m2p(t, xp, f, 3, g)
             assert max_rel(out, ref_out) < tol and rms_rel(out, ref_out) < tol
             if mode == 0:
@@ -105,7 +111,7 @@ def test_config_128_round_trip_against_oracle(dist):
                 assert np.array_equal(_m2p(t, xp, F, 3, g), O.m2p(t, xp, F, lbo, ubo, 3, 2, g))
             fi, lbi = _p2m(t, xp, up_in, g)
             e = moment_errors(unique_view(fi, lbi, [nc] * 3, 3), h, xp, up_in)
-            assert max(e) < 1e-10, (mode, e)
+            assert max(e) < mtol, (mode, e)
     finally:
         ppmg.set_precision(0)
 
