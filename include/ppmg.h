@@ -81,10 +81,70 @@ void ppmg_mesh_unregister(int topo_id, int mesh_id, int* info);
  * slabs, M2P and the adjoint read their field's z ghost planes, create_part
  * skips the slab's shared upper node plane; the exchange between the slabs
  * (the ghost put / get of ppm_map_field_ghost, ppm_map_field_send.f) is the
- * caller's, e.g. ppm_legacy_b200.halo over torch.distributed.  The
- * standalone ghost mapping and the allocation-free P2M return info = -2
- * (errno 503) on a slab. */
+ * caller's: through a transport registered with ppmg_halo_set_transport
+ * (below), or ppm_legacy_b200.halo over torch.distributed.  Without a
+ * transport the standalone ghost mapping returns info = -2 (errno 503) on a
+ * slab; the allocation-free P2M always does. */
 void ppmg_mesh_set_local_sub(int topo_id, int mesh_id, int isub, int* info);
+
+/* ---- ghost exchange between z-slab subdomains ---------------------------
+ * The inter-subdomain part of ppm_map_field_ghost (ppm/src/ppm_map_field_ghost.f:392-670,
+ * the blocks of ppm_map_field_ghost_init.f:234-447 for a cut along z, moved
+ * by ppm_map_field_send.f and added / copied by ppm_map_field_pop_3d.f).
+ * z is field_up's slowest axis, so every block is a run of whole node planes
+ * (all ldf rows, the field's full x-y extent), contiguous in memory.  With nz
+ * the local slab's cell layers (real nodes 1..nz+1, node nz+1 shared with the
+ * slab above) and g the z ghost width:
+ *   put: planes nz+1..nz+1+g go up, planes 1-g..1 go down; what arrives from
+ *        below is added to planes 1..1+g, from above to planes nz+1-g..nz+1
+ *        (both copies of a shared plane end with the full sum);
+ *   get: planes nz+1-g..nz go up, planes 2..1+g go down; what arrives from
+ *        below replaces planes 1-g..0, from above planes nz+2..nz+1+g.
+ * Tags name the direction of travel. */
+#define PPMG_HALO_TAG_UP 17   /* a block travelling to the slab above */
+#define PPMG_HALO_TAG_DOWN 18 /* a block travelling to the slab below */
+
+typedef struct {
+  int peer;      /* subdomain (0-based) on the other side */
+  int tag;       /* PPMG_HALO_TAG_UP or PPMG_HALO_TAG_DOWN */
+  void* buf;     /* the block: `bytes` contiguous bytes */
+  int64_t bytes;
+} ppmg_halo_block;
+
+/* The caller's transport (MPI, NCCL, ...): move the blocks and return 0, or
+ * nonzero on failure.  Each send must reach the receive of the same tag on
+ * the peer.  Blocks are device memory (on_device = 1, the calls of the
+ * `_dev` entry points; `stream` is the caller's stream, on which the sent
+ * blocks are produced and after which the received blocks are read) or host
+ * memory (on_device = 0, the host entry points; stream is NULL).  Every
+ * subdomain's process calls it with the same exchange in the same order. */
+typedef int (*ppmg_halo_fn)(void* ctx, int nsend, const ppmg_halo_block* sends, int nrecv,
+                            const ppmg_halo_block* recvs, int on_device, void* stream);
+
+/* Register (fn != NULL) or remove (fn == NULL) the transport of a slab
+ * handle.  With a transport, ppmg_map_field_ghost_{d,s}[_dev] on the slab
+ * performs the put or get with the neighbouring slabs, and the 3D P2M and
+ * remesh on the slab end with the ghost put, as ppm_interp_p2m.f:3665-3718
+ * and ppm_rmsh_remesh.f:876-924 end theirs.  A transport that fails gives
+ * info = -1, errno 2 (ppm_err_mpi_fail, ppm_error.h:153). */
+void ppmg_halo_set_transport(int topo_id, int mesh_id, ppmg_halo_fn fn, void* ctx, int* info);
+
+/* The blocks of one exchange, from the geometry alone (no device, no
+ * handle): the slab isub of nsubs z-slabs given as in ppmg_mesh_register
+ * (istart, nnodes: [nsubs][3], Nmz: global nodes along z), a field_up(ldf,
+ * f_lb:f_ub) and maptype ppm_param_map_ghost_put (6) or _get (5).  Outputs,
+ * index 0 = towards / from the slab above, 1 = the slab below:
+ *   *count      elements per block (whole planes, ldf rows each);
+ *   send_off[b] element offset into field_up of the block sent to
+ *               send_peer[b] with tag send_tag[b] (0: UP, 1: DOWN);
+ *   recv_off[b] element offset of the planes the block arriving from
+ *               recv_peer[b] with tag recv_tag[b] is added to (put) or
+ *               copied into (get). */
+void ppmg_halo_plan(int nsubs, const int* istart, const int* nnodes, int Nmz, int isub,
+                    int64_t ldf, const int64_t* f_lb, const int64_t* f_ub, const int* ghostsize,
+                    int maptype, int64_t* count, int* send_peer, int* send_tag,
+                    int64_t* send_off, int* recv_peer, int* recv_tag, int64_t* recv_off,
+                    int* info);
 
 /* Wait for all work of the handle's `_dev` calls on `stream` and return the
  * data-dependent status latched since the last call (info/errno as above). */

@@ -14,7 +14,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libppmg.so")
 BUILD_DIR = os.path.join(HERE, "_build")
 SOURCES = ["ppmg_sort.cu", "ppmg_radix.cu", "ppmg_p2m.cu", "ppmg_m2p.cu", "ppmg_rmsh.cu", "ppmg_map.cu",
-           "ppmg_fd.cu", "ppmg_api.cu"]
+           "ppmg_fd.cu", "ppmg_halo.cu", "ppmg_api.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
          "--expt-relaxed-constexpr"]

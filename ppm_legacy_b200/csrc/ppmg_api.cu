@@ -23,6 +23,7 @@
 #include "ppmg_rmsh.cuh"
 #include "ppmg_map.cuh"
 #include "ppmg_fd.cuh"
+#include "ppmg_halo.cuh"
 #include "ppmg_sort.cuh"
 
 namespace ppmg {
@@ -59,6 +60,12 @@ struct Handle {
   // the local subdomain is one z-slab of the domain: z is not periodic
   // within it, its neighbours' slabs hold the ghost nodes' owners
   bool open_z = false;
+  int Nm_global_z = 0;  // global nodes along z (Nm[2] becomes the slab's)
+  // transport of the ghost exchange with the neighbouring slabs (caller's)
+  ppmg_halo_fn halo_fn = nullptr;
+  void* halo_ctx = nullptr;
+  DevBuf halo_rbuf;                     // blocks received by a put (device)
+  std::vector<unsigned char> halo_host;  // host staging of the host entry points
   Geom g{};
   Workspace ws;       // P2M / M2P / adjoint / ghost / clist scratch
   Workspace ws_rmsh;  // comp_weights -> remesh state (ppm_module_data_rmsh)
@@ -475,6 +482,11 @@ bool field_is_box(const Handle& h, const int64_t* f_lb, const int64_t* f_ub, con
 }
 
 template <class T>
+int slab_exchange(Handle& h, T* field, int64_t ldf, const int64_t* f_lb, const int64_t* f_ub,
+                  const int* ghost, bool put, bool host_transport, cudaStream_t st, int* info,
+                  const char* caller);
+
+template <class T>
 void p2m_host(const T* xp, int64_t ldxp, int64_t Np, const T* up, int64_t ldup, int lda,
               int topo_id, int mesh_id, int kernel, const int* ghostsize, T* field_up,
               int64_t ldf, const int64_t* f_lb, const int64_t* f_ub, int* info, int dim,
@@ -505,6 +517,10 @@ void p2m_host(const T* xp, int64_t ldxp, int64_t Np, const T* up, int64_t ldup, 
   if (p2m_pipeline<T>(*h, dxp, ldxp, Np, dup, ldup, lda, kernel, ghostsize, dfield, ldf, f_lb,
                       f_ub, false, st, info, caller))
     return;
+  // a z-slab ends with the ghost put, as ppm_interp_p2m.f:3665-3718 does
+  if (h->open_z && h->halo_fn &&
+      slab_exchange<T>(*h, dfield, ldf, f_lb, f_ub, ghostsize, true, true, st, info, caller))
+    return;
   e = cudaMemcpyAsync(field_up, dfield, sizeof(T) * (size_t)nf, cudaMemcpyDeviceToHost, st);
   if (e) { cuda_fail(info, e, caller); return; }
   read_status(*h, st, info, caller);
@@ -527,8 +543,12 @@ void p2m_dev(const T* xp, int64_t ldxp, int64_t Np, const T* up, int64_t ldup, i
   Handle* h = get_checked(topo_id, mesh_id, dim, caller, info, dim == 3);
   if (!h) return;
   std::lock_guard<std::mutex> lk(h->mu);
-  p2m_pipeline<T>(*h, xp, ldxp, Np, up, ldup, lda, kernel, ghostsize, field_up, ldf, f_lb,
-                  f_ub, false, st, info, caller);
+  if (p2m_pipeline<T>(*h, xp, ldxp, Np, up, ldup, lda, kernel, ghostsize, field_up, ldf, f_lb,
+                      f_ub, false, st, info, caller))
+    return;
+  // a z-slab ends with the ghost put, as ppm_interp_p2m.f:3665-3718 does
+  if (h->open_z && h->halo_fn)
+    slab_exchange<T>(*h, field_up, ldf, f_lb, f_ub, ghostsize, true, false, st, info, caller);
 }
 
 template <class T>
@@ -692,6 +712,73 @@ int ghost_pipeline(Handle& h, T* field, int64_t ldf, int lda, const int64_t* f_l
   return 0;
 }
 
+// The ghost exchange of a z-slab handle with its neighbours through the
+// caller's transport, on the device field `field` (the caller's for the `_dev`
+// entry points, the mirror of the host entry points).  host_transport: the
+// transport sees host staging buffers (host entry points) instead of device
+// memory.  put: received blocks are added to the planes they belong to; get:
+// they replace the ghost planes.
+template <class T>
+int slab_exchange(Handle& h, T* field, int64_t ldf, const int64_t* f_lb, const int64_t* f_ub,
+                  const int* ghost, bool put, bool host_transport, cudaStream_t st, int* info,
+                  const char* caller) {
+  if (h.halo_fn == nullptr)
+    return fail(info, kErrorError, kErrArgument,
+                std::string(caller) + ": z-slab subdomain without a halo transport "
+                                      "(ppmg_halo_set_transport)");
+  HaloPlan pl;
+  const char* why = halo_plan(h.nsubs, h.istart.data(), h.nnodes.data(), h.Nm_global_z,
+                              h.local_sub, ldf, f_lb, f_ub, ghost[2], put, pl);
+  if (why) return fail(info, kErrorError, kErrArgument, std::string(caller) + ": " + why);
+  if (pl.count == 0) return 0;
+  const size_t bytes = sizeof(T) * (size_t)pl.count;
+  T* rbuf[2];
+  cudaError_t e = cudaSuccess;
+  if (put) {
+    if ((e = h.halo_rbuf.ensure(2 * bytes))) return cuda_fail(info, e, caller);
+    rbuf[0] = h.halo_rbuf.as<T>();
+    rbuf[1] = rbuf[0] + pl.count;
+  } else {  // a get receives straight into the ghost planes (never sent)
+    rbuf[0] = field + pl.recv_off[0];
+    rbuf[1] = field + pl.recv_off[1];
+  }
+  ppmg_halo_block sends[2], recvs[2];
+  int rc = 0;
+  if (!host_transport) {
+    for (int b = 0; b < 2; ++b) {
+      sends[b] = {pl.send_peer[b], pl.send_tag[b], field + pl.send_off[b], (int64_t)bytes};
+      recvs[b] = {pl.recv_peer[b], pl.recv_tag[b], rbuf[b], (int64_t)bytes};
+    }
+    rc = h.halo_fn(h.halo_ctx, 2, sends, 2, recvs, 1, st);
+  } else {
+    h.halo_host.resize(4 * bytes);
+    unsigned char* hb = h.halo_host.data();
+    for (int b = 0; b < 2 && !e; ++b)
+      e = cudaMemcpyAsync(hb + b * bytes, field + pl.send_off[b], bytes, cudaMemcpyDeviceToHost,
+                          st);
+    if (!e) e = cudaStreamSynchronize(st);
+    if (e) return cuda_fail(info, e, caller);
+    for (int b = 0; b < 2; ++b) {
+      sends[b] = {pl.send_peer[b], pl.send_tag[b], hb + b * bytes, (int64_t)bytes};
+      recvs[b] = {pl.recv_peer[b], pl.recv_tag[b], hb + (2 + b) * bytes, (int64_t)bytes};
+    }
+    rc = h.halo_fn(h.halo_ctx, 2, sends, 2, recvs, 0, nullptr);
+    for (int b = 0; b < 2 && !rc && !e; ++b)
+      e = cudaMemcpyAsync(rbuf[b], hb + (2 + b) * bytes, bytes, cudaMemcpyHostToDevice, st);
+    if (!e) e = cudaStreamSynchronize(st);  // the staging is reused by the next call
+    if (e) return cuda_fail(info, e, caller);
+  }
+  if (rc != 0)
+    return fail(info, kErrorFatal, 2,
+                std::string(caller) + ": the halo transport failed (returned " +
+                    std::to_string(rc) + ")");
+  if (put)
+    for (int b = 0; b < 2 && !e; ++b)
+      e = launch_plane_add<T>(field + pl.recv_off[b], rbuf[b], pl.count, st);
+  if (e) return cuda_fail(info, e, caller);
+  return 0;
+}
+
 template <class T>
 void ghost_host(T* field_up, int64_t ldf, int lda, const int64_t* f_lb, const int64_t* f_ub,
                 int topo_id, int mesh_id, const int* ghostsize, int maptype, int* info,
@@ -700,17 +787,25 @@ void ghost_host(T* field_up, int64_t ldf, int lda, const int64_t* f_lb, const in
   if (info) *info = 0;
   Handle* hh = find_handle(topo_id, mesh_id);
   if (!hh) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": topo_id/mesh_id is invalid"); return; }
-  Handle* h = get_checked(topo_id, mesh_id, hh->dim, caller, info);
+  // a z-slab handle maps through its halo transport
+  Handle* h = get_checked(topo_id, mesh_id, hh->dim, caller, info, hh->halo_fn != nullptr);
   if (!h) return;
   if (lda < 1 || ldf < lda) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": lda inconsistent"); return; }
+  if (h->open_z && maptype != kMapGhostGet && maptype != kMapGhostPut) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": maptype must be ghost_get (5) or ghost_put (6)"); return; }
   std::lock_guard<std::mutex> lk(h->mu);
   cudaStream_t st = h->stream;
   cudaError_t e;
   const int64_t nf = field_elems(*h, ldf, f_lb, f_ub);
   T* dfield = mirror<T>(h->ws.h_field, field_up, nf, st, e);
   if (e) { cuda_fail(info, e, caller); return; }
-  if (ghost_pipeline<T>(*h, dfield, ldf, lda, f_lb, f_ub, ghostsize, maptype, st, info, caller))
+  if (h->open_z) {
+    if (slab_exchange<T>(*h, dfield, ldf, f_lb, f_ub, ghostsize, maptype == kMapGhostPut, true,
+                         st, info, caller))
+      return;
+  } else if (ghost_pipeline<T>(*h, dfield, ldf, lda, f_lb, f_ub, ghostsize, maptype, st, info,
+                               caller)) {
     return;
+  }
   e = cudaMemcpyAsync(field_up, dfield, sizeof(T) * (size_t)nf, cudaMemcpyDeviceToHost, st);
   if (!e) e = cudaStreamSynchronize(st);
   if (e) cuda_fail(info, e, caller);
@@ -781,6 +876,7 @@ void ppmg_mesh_register(int topo_id, int mesh_id, int dim, const double* min_phy
   h->dim = dim;
   h->nsubs = nsubs;
   for (int a = 0; a < 3; ++a) h->Nm[a] = a < dim ? Nm[a] : 2;
+  h->Nm_global_z = h->Nm[2];
   for (int f = 0; f < 6; ++f) h->bcdef[f] = f < 2 * dim ? bcdef[f] : kBcPeriodic;
   h->min_sub.assign(min_sub, min_sub + 3 * nsubs);
   h->max_sub.assign(max_sub, max_sub + 3 * nsubs);
@@ -861,6 +957,40 @@ void ppmg_mesh_set_local_sub(int topo_id, int mesh_id, int isub, int* info) {
   h->local_sub = isub;
   h->sort_cached = false;
   h->w_valid = false;
+}
+
+void ppmg_halo_set_transport(int topo_id, int mesh_id, ppmg_halo_fn fn, void* ctx, int* info) {
+  clear_error();
+  if (info) *info = 0;
+  Handle* h = find_handle(topo_id, mesh_id);
+  if (!h) { fail(info, kErrorError, ppmg::kErrArgument, "ppmg_halo_set_transport: topo_id/mesh_id is invalid"); return; }
+  if (h->nsubs < 2 || h->dim != 3) { fail(info, kErrorError, ppmg::kErrArgument, "ppmg_halo_set_transport: the mesh has one subdomain (no neighbours to exchange with)"); return; }
+  std::lock_guard<std::mutex> lk(h->mu);
+  h->halo_fn = fn;
+  h->halo_ctx = fn ? ctx : nullptr;
+}
+
+void ppmg_halo_plan(int nsubs, const int* istart, const int* nnodes, int Nmz, int isub,
+                    int64_t ldf, const int64_t* f_lb, const int64_t* f_ub, const int* ghostsize,
+                    int maptype, int64_t* count, int* send_peer, int* send_tag,
+                    int64_t* send_off, int* recv_peer, int* recv_tag, int64_t* recv_off,
+                    int* info) {
+  clear_error();
+  if (info) *info = 0;
+  if (maptype != kMapGhostGet && maptype != kMapGhostPut) { fail(info, kErrorError, ppmg::kErrArgument, "ppmg_halo_plan: maptype must be ghost_get (5) or ghost_put (6)"); return; }
+  HaloPlan pl;
+  const char* why = halo_plan(nsubs, istart, nnodes, Nmz, isub, ldf, f_lb, f_ub, ghostsize[2],
+                              maptype == kMapGhostPut, pl);
+  if (why) { fail(info, kErrorError, ppmg::kErrArgument, std::string("ppmg_halo_plan: ") + why); return; }
+  *count = pl.count;
+  for (int b = 0; b < 2; ++b) {
+    send_peer[b] = pl.send_peer[b];
+    send_tag[b] = pl.send_tag[b];
+    send_off[b] = pl.send_off[b];
+    recv_peer[b] = pl.recv_peer[b];
+    recv_tag[b] = pl.recv_tag[b];
+    recv_off[b] = pl.recv_off[b];
+  }
 }
 
 void ppmg_mesh_unregister(int topo_id, int mesh_id, int* info) {
@@ -1050,10 +1180,17 @@ static void ghost_dev(T* field_up, int64_t ldf, int lda, const int64_t* f_lb, co
   if (info) *info = 0;
   Handle* hh = find_handle(topo_id, mesh_id);
   if (!hh) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": topo_id/mesh_id is invalid"); return; }
-  Handle* h = get_checked(topo_id, mesh_id, hh->dim, caller, info);
+  // a z-slab handle maps through its halo transport
+  Handle* h = get_checked(topo_id, mesh_id, hh->dim, caller, info, hh->halo_fn != nullptr);
   if (!h) return;
   if (lda < 1 || ldf < lda) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": lda inconsistent"); return; }
   std::lock_guard<std::mutex> lk(h->mu);
+  if (h->open_z) {
+    if (maptype != kMapGhostGet && maptype != kMapGhostPut) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": maptype must be ghost_get (5) or ghost_put (6)"); return; }
+    slab_exchange<T>(*h, field_up, ldf, f_lb, f_ub, ghostsize, maptype == kMapGhostPut, false,
+                     stream, info, caller);
+    return;
+  }
   ghost_pipeline<T>(*h, field_up, ldf, lda, f_lb, f_ub, ghostsize, maptype, stream, info, caller);
 }
 }  // extern "C++"
@@ -1228,8 +1365,12 @@ static void remesh_common(const T* xp, int64_t ldxp, int64_t Np, const T* up,
   }
   if (dev) {
     // device arrays on the caller's stream; errors latch for ppmg_sync_status
-    p2m_pipeline<T>(*h, xp, ldxp, Np, up, ldup, lda, kernel, ghostsize, field_up, ldf, f_lb,
-                         f_ub, true, dst, info, caller);
+    if (p2m_pipeline<T>(*h, xp, ldxp, Np, up, ldup, lda, kernel, ghostsize, field_up, ldf, f_lb,
+                        f_ub, true, dst, info, caller))
+      return;
+    // a z-slab ends with the ghost put, as ppm_rmsh_remesh.f:876-924 does
+    if (h->open_z && h->halo_fn)
+      slab_exchange<T>(*h, field_up, ldf, f_lb, f_ub, ghostsize, true, false, dst, info, caller);
     return;
   }
   cudaStream_t st = h->stream;
@@ -1243,6 +1384,9 @@ static void remesh_common(const T* xp, int64_t ldxp, int64_t Np, const T* up,
   if (e) { cuda_fail(info, e, caller); return; }
   if (p2m_pipeline<T>(*h, dxp, ldxp, Np, dup, ldup, lda, kernel, ghostsize, dfield, ldf,
                            f_lb, f_ub, true, st, info, caller))
+    return;
+  if (h->open_z && h->halo_fn &&
+      slab_exchange<T>(*h, dfield, ldf, f_lb, f_ub, ghostsize, true, true, st, info, caller))
     return;
   e = cudaMemcpyAsync(field_up, dfield, sizeof(T) * (size_t)nf, cudaMemcpyDeviceToHost, st);
   if (e) { cuda_fail(info, e, caller); return; }

@@ -203,3 +203,196 @@ class DistComm:
         import torch.distributed as dist
         r = self._rank(s)
         return r if self.group is None else dist.get_global_rank(self.group, r)
+
+
+# ---- the library's own exchange (ppmg_halo_plan, ppmg_halo_set_transport) ----
+#
+# With a transport registered on a slab handle, the C-ABI performs the
+# exchange itself: ppmg_map_field_ghost_* on the slab does the put or get, and
+# the 3D P2M and remesh end with the put.  The library decides which planes
+# travel where (ppmg_halo_plan) and adds or copies what arrives; the transport
+# only moves bytes.  CTransport registers a Python mover as that transport.
+
+import ctypes as _C  # noqa: E402
+import threading as _threading  # noqa: E402
+
+
+class HaloBlock(_C.Structure):
+    """ppmg_halo_block: one contiguous block to send or receive."""
+    _fields_ = [("peer", _C.c_int), ("tag", _C.c_int), ("buf", _C.c_void_p),
+                ("bytes", _C.c_int64)]
+
+
+HALO_FN = _C.CFUNCTYPE(_C.c_int, _C.c_void_p, _C.c_int, _C.POINTER(HaloBlock), _C.c_int,
+                       _C.POINTER(HaloBlock), _C.c_int, _C.c_void_p)
+
+_c_transports: dict = {}
+
+
+def plan(topo, isub, ldf, field_lb, field_ub, ghost, put):
+    """The library's blocks of one exchange of slab isub (ppmg_halo_plan):
+    {"count": elements per block, "send": [(peer, tag, offset)] * 2,
+    "recv": [(peer, tag, offset)] * 2}, offsets in elements into field_up,
+    index 0 towards / from the slab above, 1 the slab below.  Host logic
+    only: needs no GPU."""
+    from ._lib import int_array, last_error, lib
+    ist = np.ascontiguousarray(topo.istart, dtype=np.int32)
+    nn = np.ascontiguousarray(topo.nnodes, dtype=np.int32)
+    cnt = _C.c_int64(0)
+    sp, st, rp, rt = ((_C.c_int * 2)() for _ in range(4))
+    so, ro = (_C.c_int64 * 2)(), (_C.c_int64 * 2)()
+    info = _C.c_int(0)
+    lib().ppmg_halo_plan(int(topo.nsubs), ist.ctypes.data, nn.ctypes.data, int(topo.Nm[2]),
+                         int(isub), int(ldf), int_array(field_lb, _C.c_int64),
+                         int_array(field_ub, _C.c_int64), int_array(ghost), 6 if put else 5,
+                         _C.byref(cnt), sp, st, so, rp, rt, ro, _C.byref(info))
+    if info.value != 0:
+        raise ValueError(last_error()[2])
+    return {"count": cnt.value, "send": [(sp[b], st[b], so[b]) for b in range(2)],
+            "recv": [(rp[b], rt[b], ro[b]) for b in range(2)]}
+
+
+def has_c_transport(topo_id, mesh_id) -> bool:
+    return (int(topo_id), int(mesh_id)) in _c_transports
+
+
+def c_transport(topo_id, mesh_id):
+    """The CTransport registered on a handle, or None."""
+    return _c_transports.get((int(topo_id), int(mesh_id)))
+
+
+class CTransport:
+    """A Python mover registered as the halo transport of slab handle
+    (topo_id, mesh_id) whose local subdomain is isub.  mover.exchange(me,
+    sends, recvs, on_device, stream) moves blocks given as (peer, tag,
+    address, nbytes); an exception becomes a nonzero status (the C call then
+    fails with errno 2)."""
+
+    def __init__(self, topo_id, mesh_id, isub, mover):
+        from ._lib import last_error, lib
+        self.key = (int(topo_id), int(mesh_id))
+        self.isub = int(isub)
+        self.mover = mover
+        self._fn = HALO_FN(self._call)  # kept alive as long as the registration
+        info = _C.c_int(0)
+        lib().ppmg_halo_set_transport(self.key[0], self.key[1], _C.cast(self._fn, _C.c_void_p),
+                                      None, _C.byref(info))
+        if info.value != 0:
+            raise RuntimeError(last_error()[2])
+        _c_transports[self.key] = self
+
+    def _call(self, ctx, ns, sends, nr, recvs, on_device, stream):
+        try:
+            s = [(sends[i].peer, sends[i].tag, sends[i].buf, sends[i].bytes) for i in range(ns)]
+            r = [(recvs[i].peer, recvs[i].tag, recvs[i].buf, recvs[i].bytes) for i in range(nr)]
+            self.mover.exchange(self.isub, s, r, bool(on_device), stream)
+            return 0
+        except Exception:  # noqa: BLE001 -- reported through the library's info
+            import traceback
+            traceback.print_exc()
+            return 1
+
+    def close(self):
+        from ._lib import lib
+        info = _C.c_int(0)
+        lib().ppmg_halo_set_transport(self.key[0], self.key[1], None, None, _C.byref(info))
+        _c_transports.pop(self.key, None)
+
+
+def _cudart():
+    from cuda.bindings import runtime as rt
+    return rt
+
+
+def _read_block(addr, nbytes, on_device, stream):
+    """The bytes of a block (device blocks after the work on `stream`)."""
+    if not on_device:
+        return _C.string_at(addr, nbytes)
+    rt = _cudart()
+    (err,) = rt.cudaStreamSynchronize(stream or 0)
+    out = bytearray(nbytes)
+    buf = (_C.c_char * nbytes).from_buffer(out)
+    (err2,) = rt.cudaMemcpy(_C.addressof(buf), addr, nbytes, rt.cudaMemcpyKind.cudaMemcpyDeviceToHost)
+    if err != rt.cudaError_t.cudaSuccess or err2 != rt.cudaError_t.cudaSuccess:
+        raise RuntimeError(f"halo block read failed: {err} {err2}")
+    return bytes(out)
+
+
+def _write_block(addr, data, on_device):
+    if not on_device:
+        _C.memmove(addr, data, len(data))
+        return
+    rt = _cudart()
+    src = (_C.c_char * len(data)).from_buffer_copy(data)
+    (err,) = rt.cudaMemcpy(addr, _C.addressof(src), len(data),
+                           rt.cudaMemcpyKind.cudaMemcpyHostToDevice)
+    if err != rt.cudaError_t.cudaSuccess:
+        raise RuntimeError(f"halo block write failed: {err}")
+
+
+class ThreadMover:
+    """Slabs held by one process, each exchanging from a host thread of its
+    own (their C calls run concurrently): a send is matched with the receive
+    of the same (source, destination, tag).  Blocks travel through host
+    memory.  A receive waits at most `timeout` seconds."""
+
+    def __init__(self, timeout=60.0):
+        self.cv = _threading.Condition()
+        self.box = {}
+        self.timeout = timeout
+
+    def exchange(self, me, sends, recvs, on_device, stream):
+        posted = [((me, peer, tag), _read_block(addr, n, on_device, stream))
+                  for peer, tag, addr, n in sends]
+        with self.cv:
+            for k, data in posted:
+                self.box[k] = data
+            self.cv.notify_all()
+        for peer, tag, addr, n in recvs:
+            key = (peer, me, tag)
+            with self.cv:
+                if not self.cv.wait_for(lambda: key in self.box, timeout=self.timeout):
+                    raise TimeoutError(f"slab {me}: no block from {peer} (tag {tag})")
+                data = self.box.pop(key)
+            if len(data) != n:
+                raise ValueError("slab exchange: block sizes differ between neighbours")
+            _write_block(addr, data, on_device)
+
+
+class DistMover:
+    """torch.distributed point-to-point (subdomain s on rank s, or
+    sub_to_rank[s]): one batch of isend / irecv.  Blocks go through tensors
+    on the process group's side (host memory for gloo, the current device for
+    NCCL)."""
+
+    def __init__(self, group=None, sub_to_rank=None):
+        self.group = group
+        self.sub_to_rank = sub_to_rank
+
+    def _peer(self, s):
+        import torch.distributed as dist
+        r = int(s if self.sub_to_rank is None else self.sub_to_rank[s])
+        return r if self.group is None else dist.get_global_rank(self.group, r)
+
+    def exchange(self, me, sends, recvs, on_device, stream):
+        import torch
+        import torch.distributed as dist
+        nccl = dist.get_backend(self.group) == "nccl"
+        dev = torch.device("cuda", torch.cuda.current_device()) if nccl else torch.device("cpu")
+
+        def tensor_of(data):
+            return torch.frombuffer(bytearray(data), dtype=torch.uint8).to(dev)
+
+        ops, bufs = [], []
+        for peer, tag, addr, n in sends:
+            t = tensor_of(_read_block(addr, n, on_device, stream))
+            ops.append(dist.P2POp(dist.isend, t, self._peer(peer), self.group, tag))
+        for peer, tag, addr, n in recvs:
+            t = torch.empty(n, dtype=torch.uint8, device=dev)
+            bufs.append((t, addr))
+            ops.append(dist.P2POp(dist.irecv, t, self._peer(peer), self.group, tag))
+        if ops:
+            for req in dist.batch_isend_irecv(ops):
+                req.wait()
+        for t, addr in bufs:
+            _write_block(addr, t.cpu().numpy().tobytes(), on_device)

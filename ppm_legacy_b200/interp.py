@@ -106,6 +106,13 @@ def _slab_exchange(field_up, topo_id, mesh_id, ghostsize, lb, put):
     fn({isub: field_up}, t, list(ghostsize), [int(v) for v in lb], halo.comm_for(topo_id, mesh_id))
 
 
+def _python_exchange(topo_id, mesh_id):
+    """A slab handle whose exchange runs in Python (ppm_legacy_b200.halo):
+    one without a transport registered in the library (halo.CTransport),
+    whose C calls then leave the exchange to their caller."""
+    return _topo.is_slab(topo_id, mesh_id) and not halo.has_c_transport(topo_id, mesh_id)
+
+
 def ppm_interp_p2m(xp, Np, up, *args, field_lb=None, exchange=True):
     """ppm_interp_p2m(xp, Np, up, [lda,] topo_id, mesh_id, kernel, ghostsize, field_up).
 
@@ -134,7 +141,7 @@ def ppm_interp_p2m(xp, Np, up, *args, field_lb=None, exchange=True):
             raise TypeError("device (torch) arrays use the vector variant (pass lda)")
         getattr(lib(), name)(_addr(xp), xp.shape[0], int(Np), _addr(up), topo_id, mesh_id,
                              kernel, g, _addr(field_up), lb, ub, C.byref(info))
-    if exchange and _topo.is_slab(topo_id, mesh_id):
+    if exchange and _python_exchange(topo_id, mesh_id):
         _slab_exchange(field_up, topo_id, mesh_id, ghostsize, lb, True)
     return info.value
 
@@ -176,7 +183,13 @@ def ppm_interp_p2m_adjoint(xp, Np, up, lda, topo_id, mesh_id, kernel, r_field, d
     _check(xp, up, r_field, dw, dx)
     lb, ub = _bounds(r_field, 3, True, ghostsize, field_lb)
     if exchange and _topo.is_slab(topo_id, mesh_id):
-        _slab_exchange(r_field, topo_id, mesh_id, ghostsize, lb, False)
+        if halo.has_c_transport(topo_id, mesh_id):
+            info = ppm_map_field_ghost(r_field, int(lda), topo_id, mesh_id, ghostsize,
+                                       P.ppm_param_map_ghost_get, field_lb=field_lb)
+            if info != 0:
+                return info
+        else:
+            _slab_exchange(r_field, topo_id, mesh_id, ghostsize, lb, False)
     info = C.c_int(0)
     a = (_addr(xp), xp.shape[0], int(Np), _addr(up), up.shape[0], int(lda), topo_id, mesh_id,
          kernel, _addr(r_field), r_field.shape[0], lb, ub, _addr(dw), dw.shape[0], _addr(dx),
@@ -205,7 +218,7 @@ def ppm_map_field_ghost(field_up, *args, field_lb=None):
     _check(field_up)
     dim = field_up.ndim - (2 if vector else 1)
     lb, ub = _bounds(field_up, dim, vector, ghostsize, field_lb)
-    if _topo.is_slab(topo_id, mesh_id):
+    if _python_exchange(topo_id, mesh_id):
         if int(maptype) not in (P.ppm_param_map_ghost_get, P.ppm_param_map_ghost_put):
             return -2
         _slab_exchange(field_up, topo_id, mesh_id, ghostsize, lb,
@@ -292,7 +305,7 @@ def ppm_rmsh_remesh(xp, Np, up, *args, field_lb=None, exchange=True):
         getattr(lib(), f"ppmg_rmsh_remesh_{k}v_{dim}d_dev")(*a, _stream())
     else:
         getattr(lib(), f"ppmg_rmsh_remesh_{k}v_{dim}d")(*a)
-    if exchange and _topo.is_slab(topo_id, mesh_id):
+    if exchange and _python_exchange(topo_id, mesh_id):
         _slab_exchange(field_up, topo_id, mesh_id, ghostsize, lb, True)
     return info.value
 
