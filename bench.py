@@ -375,6 +375,89 @@ def _cfg3_particles(nc, seed=3):
     return xp, up
 
 
+def cfg3_particles_dev(torch, nc, device, seed=3):
+    """The 256^3 remesh workload generated on the device (the construction of
+    _cfg3_particles with torch's seeded generator): cell centres displaced by
+    8 Fourier modes (integer wavevectors, |k|_inf in [1, 4], random unit
+    directions and phases, amplitudes summing to 0.5 h), vortex-tube
+    strengths.  Returns column-major xp(3, n), up(3, n)."""
+    g = torch.Generator(device="cpu")
+    g.manual_seed(seed)
+    h = 1.0 / nc
+    i = (torch.arange(nc, dtype=torch.float64, device=device) + 0.5) * h
+    X = i[:, None, None].expand(nc, nc, nc)   # x slowest here; flattened in F order below
+    Y = i[None, :, None].expand(nc, nc, nc)
+    Z = i[None, None, :].expand(nc, nc, nc)
+    # Fortran order of the node (x fastest): transpose to (z, y, x) then flatten
+    x = torch.stack([X.permute(2, 1, 0).reshape(-1), Y.permute(2, 1, 0).reshape(-1),
+                     Z.permute(2, 1, 0).reshape(-1)])
+    d = torch.zeros_like(x)
+    amps = torch.rand(8, generator=g, dtype=torch.float64)
+    amps *= 0.5 * h / amps.sum()
+    for m in range(8):
+        k = torch.randint(-4, 5, (3,), generator=g)
+        while int(k.abs().max()) < 1:
+            k = torch.randint(-4, 5, (3,), generator=g)
+        e = torch.randn(3, generator=g, dtype=torch.float64)
+        e /= e.norm()
+        ph = float(torch.rand(1, generator=g, dtype=torch.float64)) * 2 * np.pi
+        kx = (k.to(torch.float64).to(device)[:, None] * x).sum(0)
+        d += float(amps[m]) * e.to(device)[:, None] * torch.sin(2 * np.pi * kx + ph)[None, :]
+    xp = torch.remainder(x + d, 1.0)
+    xp = torch.where(xp >= 1.0, torch.zeros_like(xp), xp)
+    tp = 2 * np.pi
+    s, c = torch.sin(tp * xp), torch.cos(tp * xp)
+    up = torch.stack([s[0] * c[1] * c[2], c[0] * s[1] * c[2], -2 * c[0] * c[1] * s[2]])
+    return xp.t().contiguous().t(), up.t().contiguous().t()
+
+
+def remesh_extra(torch, ppmg, dev, warmup, steps, peak):
+    """One remeshing step on the 256^3 workload (comp_weights, remesh with
+    M'4, lda 3, ghostsize 2, create_part with cutoff (1e-8, huge) on |u|_2 and
+    resetpos) through the device entry points, timed with CUDA events; bytes
+    per step: P2M's Np (24 + 24) + N^3 24, the create_part read N^3 24, the
+    new particles' writes np_new (24 + 24)."""
+    nc = 256
+    xp, up = cfg3_particles_dev(torch, nc, dev)
+    n = xp.shape[1]
+    t = ppmg.cartesian(3, nc, topo_id=3, mesh_id=1)
+    assert ppmg.register(t) == 0, ppmg.last_error()
+    g = [2, 2, 2]
+    ext = nc + 1 + 2 * g[0]
+    f = torch.zeros((1, ext, ext, ext, 3), device=dev, dtype=torch.float64).permute(4, 3, 2, 1, 0)
+    cut = [1e-8, 1e300]
+    stream = torch.cuda.current_stream()
+
+    def step():
+        assert ppmg.ppm_rmsh_comp_weights(xp, n, 3, 1, 2) == 0, ppmg.last_error()
+        assert ppmg.ppm_rmsh_remesh(xp, n, up, 3, 3, 1, 2, g, f) == 0, ppmg.last_error()
+        info, npn, _, _, _ = ppmg.ppm_rmsh_create_part(f, 3, 1, cut, lda=3, resetpos=True,
+                                                       ghostsize=g)
+        assert info == 0, ppmg.last_error()
+        return npn
+
+    for _ in range(max(warmup, 3)):
+        npn = step()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        npn = step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    assert ppmg.sync_status(3, 1) == 0, ppmg.last_error()
+    ppmg.unregister(t)
+    ms = e0.elapsed_time(e1) / steps
+    B = n * (24 + 24) + nc ** 3 * 24 + nc ** 3 * 24 + npn * (24 + 24)
+    return {"workload": f"remesh: {nc}^3 periodic, {n} particles (cell centres + 8 smooth "
+                        "modes, vortex-tube strengths), comp_weights + remesh + create_part",
+            "ms_per_step": ms, "particles_per_s": n / (ms / 1e3), "new_particles": npn,
+            "alg_bytes": B, "achieved_gbs": B / (ms / 1e3) / 1e9,
+            "frac_of_hbm_roofline": B / (ms / 1e3) / 1e9 / peak, "steps": steps,
+            "l2": "inputs larger than L2 (xp/up/field each > 126 MB)"}
+
+
 def run_remesh(args):
     """One remeshing step on the 256^3 workload: ppm_rmsh_comp_weights +
     ppm_rmsh_remesh (M'4, lda 3, ghostsize 2) + ppm_rmsh_create_part (cutoff
@@ -384,7 +467,10 @@ def run_remesh(args):
     import torch
     import ppm_legacy_b200 as ppmg
     nc = 256
-    xp, up = _cfg3_particles(nc)
+    dev = torch.device("cuda", 0)
+    dx, du = cfg3_particles_dev(torch, nc, dev)
+    xp = np.asfortranarray(dx.cpu().numpy())
+    up = np.asfortranarray(du.cpu().numpy())
     n = xp.shape[1]
     t = ppmg.cartesian(3, nc, topo_id=3, mesh_id=1)
     assert ppmg.register(t) == 0, ppmg.last_error()
@@ -401,9 +487,6 @@ def run_remesh(args):
         assert info == 0, ppmg.last_error()
         return npn
 
-    dev = torch.device("cuda", 0)
-    dx = torch.from_numpy(np.ascontiguousarray(xp.T)).to(dev).t()
-    du = torch.from_numpy(np.ascontiguousarray(up.T)).to(dev).t()
     df = torch.zeros((1, ext, ext, ext, 3), device=dev, dtype=torch.float64).permute(4, 3, 2, 1, 0)
     stream = torch.cuda.current_stream()
     for _ in range(max(args.warmup, 1)):
@@ -557,6 +640,8 @@ def main():
     ap.add_argument("--cpu-warmup", type=int, default=0)
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"])
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the sorted-input round trip and the 256^3 remesh workload")
     ap.add_argument("--dist-backend", default="nccl", choices=["nccl", "gloo"],
                     help="N > 1: the process-group backend (gloo stages the slab exchange "
                          "through host memory)")
@@ -876,6 +961,50 @@ def main():
                "path": "host-pointer C-ABI (ppmg_interp_p2m_dv_3d, ppmg_interp_m2p_dv_3d), "
                        "pinned host buffers"}
 
+    extra = None
+    if world == 1 and not args.no_extra:
+        # (1) the same particles in cell order, as ppm_rmsh_create_part emits
+        # them (or a caller that keeps its particles sorted): the sort's
+        # gather reads and M2P's result rows become nearly sequential
+        ppmg.set_precision(head)
+        cells = torch.floor(xp * nc).to(torch.int64).clamp_(0, nc - 1)
+        order = torch.argsort(cells[0] + nc * (cells[1] + nc * cells[2]), stable=True)
+        del cells
+        xs = xp[:, order].t().contiguous().t()
+        us = up[:, order].t().contiguous().t()
+        del order
+        for _ in range(max(args.warmup, 3)):
+            ppmg.ppm_interp_p2m(xs, n, us, 3, 1, 1, 2, g, field)
+            ppmg.ppm_interp_m2p(xs, n, out, 3, 1, 1, 2, g, field)
+        assert ppmg.sync_status(1, 1) == 0, ppmg.last_error()
+        torch.cuda.synchronize()
+        for part in range(3):
+            kernel_time(part)
+        ppmg.lib().ppmg_kernel_timing(1)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            ppmg.ppm_interp_p2m(xs, n, us, 3, 1, 1, 2, g, field)
+            ppmg.ppm_interp_m2p(xs, n, out, 3, 1, 1, 2, g, field)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ppmg.lib().ppmg_kernel_timing(0)
+        sp = [kernel_time(part) for part in range(3)]
+        assert ppmg.sync_status(1, 1) == 0, ppmg.last_error()
+        sms = e0.elapsed_time(e1) / args.steps
+        del xs, us
+        sorted_in = {
+            "workload": "the round trip above with the particles given in cell order",
+            "ms_per_step": sms, "particles_per_s": n / (sms / 1e3),
+            "frac_of_hbm_roofline": B / (sms / 1e3) / 1e9 / peak,
+            "parts_ms_per_launch": {nm: (sp[i][0] / sp[i][1] if sp[i][1] else None)
+                                    for i, nm in enumerate(names)},
+            "form": "mixed" if head == 1 else "fp64", "steps": args.steps}
+        # (2) the remeshing workload (comp_weights + remesh + create_part, 256^3)
+        extra = {"sorted_input": sorted_in,
+                 "remesh": remesh_extra(torch, ppmg, dev, args.warmup, args.steps, peak)}
+
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline(args)
@@ -903,6 +1032,7 @@ def main():
                        f"{args.dist_backend.upper()}"},
             "roofline": roof, "forms": parts, "clocks": clocks, "gpu_launches": launches,
             "e2e": e2e, "cpu_baseline": cb, "adjoint": adj, "accuracy": accuracy,
+            "extra": extra,
         }
         print(json.dumps(line))
     if world > 1:
