@@ -395,6 +395,19 @@ void ppmg_map_part_route_d_dev(const double* xp, int64_t ldxp, int64_t Np, int t
                                int mesh_id, int* perm, int64_t* counts, int* info, void* stream);
 void ppmg_map_part_route_s_dev(const float* xp, int64_t ldxp, int64_t Np, int topo_id,
                                int mesh_id, int* perm, int64_t* counts, int* info, void* stream);
+/* Global routing (ppm_map_part_global, ppm/src/ppm_map_part_global.f:355-420):
+ * every particle to the slab that contains it among all nsubs slabs (<= 255;
+ * closed-lower / open-upper, x and y inside the domain).  perm receives the
+ * particle ids grouped by destination slab 0..nsubs-1 and then those in no
+ * slab, each group in ascending id; counts (host, nsubs+1) the group sizes.
+ * Particles in no slab are left out of the exchange without an error, as in
+ * the reference (ppm_map_part_global.f:437-442). */
+void ppmg_map_part_global_route_d_dev(const double* xp, int64_t ldxp, int64_t Np, int topo_id,
+                                      int mesh_id, int* perm, int64_t* counts, int* info,
+                                      void* stream);
+void ppmg_map_part_global_route_s_dev(const float* xp, int64_t ldxp, int64_t Np, int topo_id,
+                                      int mesh_id, int* perm, int64_t* counts, int* info,
+                                      void* stream);
 void ppmg_map_part_gather_d_dev(const double* src, int64_t lds, int lda, const int* perm,
                                 int64_t n, double* dst, int64_t ldd, int* info, void* stream);
 void ppmg_map_part_gather_s_dev(const float* src, int64_t lds, int lda, const int* perm,

@@ -79,6 +79,8 @@ SIGNATURES = {
     "ppmg_fdsolver_poisson_3d_s_dev": ([_pd, _i64, _i, _pi64, _pi64, _i, _i, _pi, _pi, _vp], None),
     "ppmg_map_part_route_d_dev": ([_pd, _i64, _i64, _i, _i, _pd, _pi64, _pi, _vp], None),
     "ppmg_map_part_route_s_dev": ([_pd, _i64, _i64, _i, _i, _pd, _pi64, _pi, _vp], None),
+    "ppmg_map_part_global_route_d_dev": ([_pd, _i64, _i64, _i, _i, _pd, _pi64, _pi, _vp], None),
+    "ppmg_map_part_global_route_s_dev": ([_pd, _i64, _i64, _i, _i, _pd, _pi64, _pi, _vp], None),
     "ppmg_map_part_gather_d_dev": ([_pd, _i64, _i, _pd, _i64, _pd, _i64, _pi, _vp], None),
     "ppmg_map_part_gather_s_dev": ([_pd, _i64, _i, _pd, _i64, _pd, _i64, _pi, _vp], None),
     "ppmg_util_rank2d_d_dev": (_RANK + [_vp], None),

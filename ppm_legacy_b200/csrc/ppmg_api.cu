@@ -1743,6 +1743,67 @@ static void route_common(const T* xp, int64_t ldxp, int64_t Np, int topo_id, int
              " particles lie in no neighbouring subdomain");
 }
 
+// ppm_map_part_global on z-slabs: every particle to the slab that contains it
+// (ppm_map_part_global.f:355-420).  counts[0..nsubs]: particles per slab, then
+// those in none (dropped without an error, ppm_map_part_global.f:437-442).
+template <class T>
+static void groute_common(const T* xp, int64_t ldxp, int64_t Np, int topo_id, int mesh_id,
+                          int* perm, int64_t* counts, int* info, cudaStream_t st,
+                          const char* caller) {
+  clear_error();
+  if (info) *info = 0;
+  if (Np < 0 || (Np > 0 && ldxp < 3) || Np >= (int64_t)1 << 31) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": invalid sizes"); return; }
+  Handle* h = get_checked(topo_id, mesh_id, 3, caller, info, true);
+  if (!h) return;
+  std::lock_guard<std::mutex> lk(h->mu);
+  const int ns = h->nsubs;
+  if (ns > kMaxGlobalSubs) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": more than 255 subdomains"); return; }
+  if (ns > 1 && !h->open_z) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": select the local slab first (ppmg_mesh_set_local_sub)"); return; }
+  if (counts)
+    for (int c = 0; c <= ns; ++c) counts[c] = 0;
+  if (Np == 0) return;
+  GlobalRouteParams R{};
+  R.nsubs = ns;
+  for (int a = 0; a < 2; ++a) {
+    R.lo[a] = h->g.min_phys[a];
+    R.hi[a] = h->g.max_phys[a];
+    R.lof[a] = (float)R.lo[a];
+    R.hif[a] = (float)R.hi[a];
+  }
+  const int nblk = route_blocks(Np);
+  Workspace& ws = h->ws_map;
+  const size_t ncls = (size_t)ns + 1;
+  cudaError_t e;
+  if ((e = ws.key.ensure((size_t)Np)) || (e = ws.count.ensure(sizeof(int) * ncls * nblk)) ||
+      (e = ws.start.ensure(sizeof(int) * ncls * nblk)) ||
+      (e = ws.h_aux.ensure(sizeof(double) * 2 * (size_t)ns))) { cuda_fail(info, e, caller); return; }
+  std::vector<double> zb(2 * (size_t)ns);
+  for (int q = 0; q < ns; ++q) {
+    zb[q] = h->min_sub[3 * q + 2];
+    zb[ns + q] = h->max_sub[3 * q + 2];
+  }
+  double* dz = ws.h_aux.as<double>();
+  if ((e = cudaMemcpyAsync(dz, zb.data(), sizeof(double) * 2 * ns, cudaMemcpyHostToDevice, st))) { cuda_fail(info, e, caller); return; }
+  R.zlo = dz;
+  R.zhi = dz + ns;
+  if ((e = launch_route_global<T>(R, xp, ldxp, Np, static_cast<unsigned char*>(ws.key.p),
+                                  ws.count.as<int>(), ws.start.as<int>(), perm, ws, st))) {
+    cuda_fail(info, e, caller);
+    return;
+  }
+  // class starts off[c * nblk]; the call returns once they are read (zb's
+  // staging also lives until then)
+  std::vector<int> cs(ncls, 0);
+  for (size_t c = 1; c < ncls && !e; ++c)
+    e = cudaMemcpyAsync(&cs[c], ws.start.as<int>() + c * nblk, sizeof(int),
+                        cudaMemcpyDeviceToHost, st);
+  if (!e) e = cudaStreamSynchronize(st);
+  if (e) { cuda_fail(info, e, caller); return; }
+  if (counts)
+    for (size_t c = 0; c < ncls; ++c)
+      counts[c] = (c + 1 < ncls ? cs[c + 1] : (int)Np) - cs[c];
+}
+
 template <class T>
 static void gather_common(const T* src, int64_t lds, int lda, const int* perm, int64_t n, T* dst,
                           int64_t ldd, int* info, cudaStream_t st, const char* caller) {
@@ -1765,6 +1826,18 @@ void ppmg_map_part_route_s_dev(const float* xp, int64_t ldxp, int64_t Np, int to
                                void* stream) {
   route_common<float>(xp, ldxp, Np, topo_id, mesh_id, perm, counts, info, (cudaStream_t)stream,
                       "ppmg_map_part_route_s_dev");
+}
+void ppmg_map_part_global_route_d_dev(const double* xp, int64_t ldxp, int64_t Np, int topo_id,
+                                      int mesh_id, int* perm, int64_t* counts, int* info,
+                                      void* stream) {
+  groute_common<double>(xp, ldxp, Np, topo_id, mesh_id, perm, counts, info, (cudaStream_t)stream,
+                        "ppmg_map_part_global_route_d_dev");
+}
+void ppmg_map_part_global_route_s_dev(const float* xp, int64_t ldxp, int64_t Np, int topo_id,
+                                      int mesh_id, int* perm, int64_t* counts, int* info,
+                                      void* stream) {
+  groute_common<float>(xp, ldxp, Np, topo_id, mesh_id, perm, counts, info, (cudaStream_t)stream,
+                       "ppmg_map_part_global_route_s_dev");
 }
 void ppmg_map_part_gather_d_dev(const double* src, int64_t lds, int lda, const int* perm,
                                 int64_t n, double* dst, int64_t ldd, int* info, void* stream) {

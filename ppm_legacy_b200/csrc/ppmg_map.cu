@@ -96,6 +96,88 @@ __global__ void __launch_bounds__(kRouteThreads) k_route_scatter(const unsigned 
   }
 }
 
+// Global routing: the class of every item is its slab (the reference tests
+// the subdomains from the last to the first, ppm_map_part_global.f:355-420;
+// slabs do not overlap, so the first hit is the only one) or nsubs.
+template <class T>
+__global__ void __launch_bounds__(kRouteThreads) k_groute_count(GlobalRouteParams R,
+                                                                const T* xp, int64_t ldxp,
+                                                                int64_t np, unsigned char* dest,
+                                                                int* bc, int nblk) {
+  constexpr bool F = sizeof(T) == 4;
+  __shared__ int cnt[kMaxGlobalSubs + 1];
+  __shared__ T zl[kMaxGlobalSubs], zh[kMaxGlobalSubs];
+  const int ncls = R.nsubs + 1;
+  for (int c = threadIdx.x; c < ncls; c += kRouteThreads) cnt[c] = 0;
+  for (int q = threadIdx.x; q < R.nsubs; q += kRouteThreads) {
+    zl[q] = (T)R.zlo[q];  // the positions' own precision, as the reference compares
+    zh[q] = (T)R.zhi[q];
+  }
+  __syncthreads();
+  const int64_t b0 = (int64_t)blockIdx.x * kRouteChunk;
+  const int64_t b1 = min(np, b0 + kRouteChunk);
+  for (int64_t i = b0 + threadIdx.x; i < b1; i += kRouteThreads) {
+    const T* x = xp + i * ldxp;
+    bool inxy = true;
+    for (int a = 0; a < 2; ++a) {
+      const T lo = F ? (T)R.lof[a] : (T)R.lo[a], hi = F ? (T)R.hif[a] : (T)R.hi[a];
+      inxy = inxy && x[a] >= lo && x[a] < hi;
+    }
+    int c = R.nsubs;
+    if (inxy)
+      for (int q = R.nsubs - 1; q >= 0; --q)
+        if (x[2] >= zl[q] && x[2] < zh[q]) {
+          c = q;
+          break;
+        }
+    dest[i] = (unsigned char)c;
+    atomicAdd(&cnt[c], 1);
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < ncls; c += kRouteThreads)
+    bc[(int64_t)c * nblk + blockIdx.x] = cnt[c];
+}
+
+// Stable scatter into ncls classes: rounds of 256 items in order; lanes of
+// one class in a warp are found with __match_any_sync, the warps' counts per
+// class are kept in shared memory (zeroed by their writers after use).
+__global__ void __launch_bounds__(kRouteThreads) k_groute_scatter(const unsigned char* dest,
+                                                                  int64_t np, const int* off,
+                                                                  int nblk, int ncls,
+                                                                  int* perm) {
+  constexpr int W = kRouteThreads / 32;
+  __shared__ int wcnt[kMaxGlobalSubs + 1][W];
+  __shared__ int run[kMaxGlobalSubs + 1];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int c = threadIdx.x; c < ncls; c += kRouteThreads) {
+    run[c] = off[(int64_t)c * nblk + blockIdx.x];
+    for (int ww = 0; ww < W; ++ww) wcnt[c][ww] = 0;
+  }
+  __syncthreads();
+  const int64_t b0 = (int64_t)blockIdx.x * kRouteChunk;
+  const int64_t b1 = min(np, b0 + kRouteChunk);
+  for (int64_t base = b0; base < b1; base += kRouteThreads) {
+    const int64_t i = base + threadIdx.x;
+    const int c = i < b1 ? (int)dest[i] : -1;
+    const unsigned m = __match_any_sync(0xffffffffu, c);
+    const bool leader = lane == __ffs(m) - 1;
+    if (c >= 0 && leader) wcnt[c][w] = __popc(m);
+    __syncthreads();
+    if (c >= 0) {
+      int before = run[c];
+      for (int ww = 0; ww < w; ++ww) before += wcnt[c][ww];
+      before += __popc(m & ((1u << lane) - 1u));
+      perm[before] = (int)i;
+    }
+    __syncthreads();
+    if (c >= 0 && leader) {
+      atomicAdd(&run[c], wcnt[c][w]);
+      wcnt[c][w] = 0;
+    }
+    __syncthreads();
+  }
+}
+
 template <class T>
 __global__ void k_gather_cols(const T* src, int64_t lds, int lda, const int* perm, int64_t n,
                               T* dst, int64_t ldd) {
@@ -127,6 +209,23 @@ cudaError_t launch_route(const RouteParams& R, const T* xp, int64_t ldxp, int64_
 }
 
 template <class T>
+cudaError_t launch_route_global(const GlobalRouteParams& R, const T* xp, int64_t ldxp,
+                                int64_t np, unsigned char* dest, int* bc, int* off, int* perm,
+                                Workspace& ws, cudaStream_t st) {
+  if (np <= 0) return cudaSuccess;
+  if (R.nsubs < 1 || R.nsubs > kMaxGlobalSubs) return cudaErrorInvalidValue;
+  const int nblk = route_blocks(np);
+  const int ncls = R.nsubs + 1;
+  k_groute_count<T><<<nblk, kRouteThreads, 0, st>>>(R, xp, ldxp, np, dest, bc, nblk);
+  count_launch();
+  cudaError_t e = scan_exclusive(bc, off, (int64_t)ncls * nblk, ws, st);
+  if (e) return e;
+  k_groute_scatter<<<nblk, kRouteThreads, 0, st>>>(dest, np, off, nblk, ncls, perm);
+  count_launch();
+  return cudaGetLastError();
+}
+
+template <class T>
 cudaError_t launch_gather_cols(const T* src, int64_t lds, int lda, const int* perm, int64_t n,
                                T* dst, int64_t ldd, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
@@ -143,6 +242,12 @@ template cudaError_t launch_route<double>(const RouteParams&, const double*, int
 template cudaError_t launch_route<float>(const RouteParams&, const float*, int64_t, int64_t,
                                          unsigned char*, int*, int*, int*, Workspace&,
                                          cudaStream_t);
+template cudaError_t launch_route_global<double>(const GlobalRouteParams&, const double*,
+                                                 int64_t, int64_t, unsigned char*, int*, int*,
+                                                 int*, Workspace&, cudaStream_t);
+template cudaError_t launch_route_global<float>(const GlobalRouteParams&, const float*, int64_t,
+                                                int64_t, unsigned char*, int*, int*, int*,
+                                                Workspace&, cudaStream_t);
 template cudaError_t launch_gather_cols<double>(const double*, int64_t, int, const int*, int64_t,
                                                 double*, int64_t, cudaStream_t);
 template cudaError_t launch_gather_cols<float>(const float*, int64_t, int, const int*, int64_t,

@@ -156,3 +156,111 @@ def ppm_map_part_partial(xp, Np, topo_id, mesh_id, props=(), comm=None):
                          t, c)
     x2, p2 = out[isub]
     return info, int(x2.shape[1]), x2, p2
+
+
+# ---- ppm_map_part_global: every particle to the slab that contains it --------
+
+TAG_GSIZE, TAG_GDATA = 80, 100
+
+
+def device_route_global(topo_id, mesh_id, xp, nsubs):
+    """(info, perm, [count to slab 0 .. nsubs-1, count in no slab]) of the
+    slab's particles (ppmg_map_part_global_route on the current stream)."""
+    import torch
+    n = int(xp.shape[1])
+    perm = torch.empty(max(n, 1), dtype=torch.int32, device=xp.device)
+    cnt = (C.c_int64 * (int(nsubs) + 1))()
+    info = C.c_int(0)
+    k = "d" if xp.dtype == torch.float64 else "s"
+    getattr(lib(), f"ppmg_map_part_global_route_{k}_dev")(
+        xp.data_ptr(), xp.stride(1), n, int(topo_id), int(mesh_id), perm.data_ptr(), cnt,
+        C.byref(info), torch.cuda.current_stream().cuda_stream)
+    return info.value, perm, [int(c) for c in cnt]
+
+
+def map_global(parts: dict, topo, comm, route=device_route_global, gather=device_gather):
+    """parts {isub: (topo_id, mesh_id, xp, [props])} of the slabs this process
+    holds; returns (info, {isub: (xp_new, [props_new])}).  The exchange is
+    all-pairs: sizes first (one to every other slab), then the non-empty
+    particle blocks, in the same operation order on every rank."""
+    import torch
+    ns = int(topo.nsubs)
+    info_all = 0
+    packed, counts = {}, {}
+    for s, (tid, mid, xp, props) in parts.items():
+        n = int(xp.shape[1])
+        info, perm, cnt = route(tid, mid, xp, ns)
+        if info and not info_all:
+            info_all = info
+        counts[s] = cnt
+        packed[s] = [gather(a, perm, n) for a in [xp] + list(props)]
+    dev = next(iter(parts.values()))[2].device
+    sends, recvs = [], []
+    for s, c in counts.items():
+        for q in range(ns):
+            if q == s:
+                continue
+            sends.append((s, q, TAG_GSIZE, torch.tensor([c[q]], dtype=torch.int64, device=dev)))
+            recvs.append((s, q, TAG_GSIZE, torch.zeros(1, dtype=torch.int64, device=dev)))
+    got = comm.exchange(sends, recvs)
+    arrive = {}
+    for (s, src, _, _), g in zip(recvs, got):
+        arrive.setdefault(s, {})[src] = int(g.item())
+    sends, recvs, want = [], [], []
+    for s, c in counts.items():
+        start = [0]
+        for v in c:
+            start.append(start[-1] + v)
+        for k, P in enumerate(packed[s]):
+            rows = _rows(P)
+            for q in range(ns):
+                if q == s:
+                    continue
+                if c[q]:
+                    sends.append((s, q, TAG_GDATA + k, rows[start[q]:start[q] + c[q]]))
+                nq = arrive[s].get(q, 0)
+                if nq:
+                    recvs.append((s, q, TAG_GDATA + k, torch.empty((nq, rows.shape[1]),
+                                                                  dtype=P.dtype,
+                                                                  device=P.device)))
+                    want.append((s, k, q))
+    got = comm.exchange(sends, recvs)
+    blocks = {key: g for key, g in zip(want, got)}
+    out = {}
+    for s, c in counts.items():
+        start = sum(c[:s])
+        n_new = c[s] + sum(arrive[s].get(q, 0) for q in range(ns) if q != s)
+        arrays = []
+        for k, P in enumerate(packed[s]):
+            rows = _rows(P)
+            res = torch.empty((max(n_new, 1), rows.shape[1]), dtype=P.dtype, device=P.device)
+            res[:c[s]].copy_(rows[start:start + c[s]])
+            pos = c[s]
+            for q in range(ns):
+                nq = arrive[s].get(q, 0) if q != s else 0
+                if nq:
+                    res[pos:pos + nq].copy_(blocks[(s, k, q)])
+                    pos += nq
+            arrays.append(res.t()[:, :n_new])
+        out[s] = (arrays[0], arrays[1:])
+    return info_all, out
+
+
+def ppm_map_part_global(xp, Np, topo_id, mesh_id, props=(), comm=None):
+    """ppm_map_part_global for the slab this process holds: returns
+    (info, Np_new, xp_new, [props_new]).  Every particle goes to the slab
+    that contains it, however far it moved; particles in no slab are left
+    out, without an error (ppm_map_part_global.f:437-442).  The new list is
+    the kept particles in their order, then the arrivals by ascending source
+    slab (each in the source's order).  xp and props are column-major device
+    arrays (ld, Np); every rank of the slab decomposition calls it."""
+    r = _topo.local_sub(topo_id, mesh_id)
+    if r is None:
+        raise ValueError("ppm_map_part_global: unknown topo_id/mesh_id")
+    t, isub = r
+    n = int(Np)
+    c = comm if comm is not None else halo.comm_for(topo_id, mesh_id)
+    info, out = map_global({isub: (topo_id, mesh_id, xp[:, :n], list(p[:, :n] for p in props))},
+                           t, c)
+    x2, p2 = out[isub]
+    return info, int(x2.shape[1]), x2, p2
