@@ -80,7 +80,7 @@ def make_before(t, world, n=300):
     for s in range(world):
         rng = np.random.default_rng(700 + s)
         x = scattered_particles(t, s, n, rng)
-        before[s] = (x, np.arange(s * 1000, s * 1000 + n)[None, :],
+        before[s] = (x, np.arange(s * 10 ** 6, s * 10 ** 6 + n)[None, :],  # unique ids
                      np.asfortranarray(rng.standard_normal((2, n))))
     return before
 
