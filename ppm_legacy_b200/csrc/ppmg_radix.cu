@@ -74,6 +74,7 @@ struct CountArgs {
   int64_t ldz;
   int nz;
   unsigned long long* hash;
+  const int* unsorted;  // 0: the first pass found the keys in order (later passes skip)
 };
 
 // Digit of a key; in the first pass invalid particles (key ncell) take the
@@ -123,6 +124,7 @@ __global__ void __launch_bounds__(kCThreads) k_radix_count(CountArgs<T, CT> A) {
   const unsigned mask = (unsigned)nb - 1u;
   for (int d = threadIdx.x; d < nbk; d += kCThreads) sh[d] = 0;
   __syncthreads();
+  if (!FIRST && *A.unsorted == 0) return;  // keys already in order: nothing to count
   const int64_t n = FIRST ? A.np : (int64_t)*A.d_nvalid;
   const int64_t t0 = (int64_t)blockIdx.x * A.subs * kRSub;
   const int64_t t1 = min(n, t0 + (int64_t)A.subs * kRSub);
@@ -174,6 +176,7 @@ struct MoveArgs {
   int* key_out;
   int* id_out;
   int* wait_flag;  // set when a bulk copy never completes
+  const int* unsorted;  // 0: the first pass found the keys in order (the passes skip)
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -259,6 +262,7 @@ __global__ void __launch_bounds__(kRThreads, 2) k_radix_move(MoveArgs A) {
   const int64_t n = FIRST ? A.np : (int64_t)*A.d_nvalid;
   if (FIRST && blockIdx.x == 0 && tid == 0)
     *A.d_nvalid = A.hist[(int64_t)nb * A.ntiles];  // start of the invalid bucket
+  if (*A.unsorted == 0) return;  // keys already in order: k_sorted_finish takes over
   const int64_t t0 = (int64_t)blockIdx.x * A.subs * kRSub;
   if (t0 >= n) return;
   const int nsc = (int)min((int64_t)A.subs, (n - t0 + kRSub - 1) / kRSub);
@@ -394,6 +398,38 @@ __global__ void __launch_bounds__(kRThreads, 2) k_radix_move(MoveArgs A) {
 // (start[ncell] = the valid count): position s writes the cells between the
 // previous key and its own; runs of more than kRGapRun empty cells go to a
 // list that k_fill_gaps writes.
+// Particles that arrive in cell order (those ppm_rmsh_create_part emits, or a
+// caller that keeps its particles sorted) need no pass: *unsorted stays 0
+// when no key of the first pass exceeds its successor (invalid particles,
+// key ncell, then sit at the end already).
+// Each thread checks four consecutive keys (one 16-byte load; the key arrays
+// are 16-entry padded and 16-byte aligned) and the next group's first key.
+__global__ void k_keys_sorted(const int* __restrict__ key, int64_t np, int* unsorted) {
+  const int64_t ng = (np + 3) / 4;
+  bool bad = false;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < ng;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int4 k = reinterpret_cast<const int4*>(key)[q];
+    const int64_t i = 4 * q;
+    const int v[4] = {k.x, k.y, k.z, k.w};
+#pragma unroll
+    for (int j = 0; j < 3; ++j) bad |= i + j + 1 < np && v[j] > v[j + 1];
+    if (i + 4 < np) bad |= v[3] > key[i + 4];
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) *unsorted = 1;
+}
+
+// The sorted order of keys found in order: the keys as they are, identity ids.
+__global__ void k_sorted_finish(const int* __restrict__ unsorted, const int* __restrict__ key0,
+                                int64_t np, int* __restrict__ key, int* __restrict__ id) {
+  if (*unsorted != 0) return;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < np;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (key != key0) key[i] = key0[i];
+    id[i] = (int)i;
+  }
+}
+
 __global__ void k_cell_starts(const int* __restrict__ key, const int* __restrict__ d_nvalid,
                               int ncell, int* __restrict__ start, int4* __restrict__ gaps,
                               int* __restrict__ ngaps, int gapcap) {
@@ -491,7 +527,7 @@ cudaError_t radix_sort_records(const KeyParams& kp, const T* xp, int64_t ldxp, c
       (e = ws.rec.ensure(sizeof(V) * n)) || (e = ws.rec2.ensure(sizeof(uint4) * n * IU)) ||
       (e = ws.us.ensure(sizeof(V) * nus)) ||
       (e = ws.start.ensure(sizeof(int) * (size_t)(ncell + 1))) ||
-      (e = ws.err.ensure(sizeof(int) * 4)))
+      (e = ws.err.ensure(sizeof(int) * 8)))
     return e;
   if (hash && (e = cudaMemsetAsync(hash, 0, sizeof(unsigned long long), st))) return e;
   if (np == 0) return cudaMemsetAsync(ws.start.p, 0, sizeof(int) * (size_t)(ncell + 1), st);
@@ -512,8 +548,13 @@ cudaError_t radix_sort_records(const KeyParams& kp, const T* xp, int64_t ldxp, c
                                 (int)kMoveSmem)))
     return e;
   int* d_nvalid = ws.err.as<int>() + 2;
+  int* unsorted = ws.err.as<int>() + 4;
+  if ((e = cudaMemsetAsync(unsorted, 0, sizeof(int), st))) return e;
   DevBuf* keys[2] = {&ws.key, &ws.key2};
   DevBuf* ids[2] = {&ws.idx, &ws.idx2};
+  const int gk = (int)((np + 255) / 256 < 148 * 16 ? (np + 255) / 256 : 148 * 16);
+  const int64_t g4 = ((np + 3) / 4 + 255) / 256;
+  const int gk4 = (int)(g4 < 148 * 8 ? g4 : 148 * 8);
   for (int p = 0; p < passes; ++p) {
     const int shift = p * bits;
     const int pb = nbits - shift < bits ? nbits - shift : bits;
@@ -545,10 +586,14 @@ cudaError_t radix_sort_records(const KeyParams& kp, const T* xp, int64_t ldxp, c
     C.ldz = ldz;
     C.nz = nz;
     C.hash = hash;
-    if (p == 0)
+    C.unsorted = unsorted;
+    if (p == 0) {
       k_radix_count<T, CT, true><<<ntiles, kCThreads, 0, st>>>(C);
-    else
+      k_keys_sorted<<<gk4, 256, 0, st>>>(keys[in]->as<int>(), np, unsorted);
+      count_launch();
+    } else {
       k_radix_count<T, CT, false><<<ntiles, kCThreads, 0, st>>>(C);
+    }
     count_launch();
     if ((e = scan_exclusive(ws.hist.as<int>(), ws.hist.as<int>(), (int64_t)ntiles * nbk, ws,
                             st)))
@@ -567,10 +612,18 @@ cudaError_t radix_sort_records(const KeyParams& kp, const T* xp, int64_t ldxp, c
     M.key_out = keys[out]->as<int>();
     M.id_out = ids[out]->as<int>();
     M.wait_flag = wait_flag;
+    M.unsorted = unsorted;
     if (p == 0)
       k_radix_move<true><<<ntiles, kRThreads, kMoveSmem, st>>>(M);
     else
       k_radix_move<false><<<ntiles, kRThreads, kMoveSmem, st>>>(M);
+    count_launch();
+  }
+  // keys found in order: set 0 takes them as they are, with identity ids
+  {
+    const int first_in = ((passes - 1) & 1) ^ 1;  // the set the first pass read its keys into
+    k_sorted_finish<<<gk, 256, 0, st>>>(unsorted, keys[first_in]->as<int>(), np,
+                                        ws.key.as<int>(), ws.idx.as<int>());
     count_launch();
   }
   // records and strengths into the sorted order (the last pass wrote set 0)
