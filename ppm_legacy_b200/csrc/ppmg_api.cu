@@ -72,6 +72,7 @@ struct Handle {
   Workspace ws_map;   // particle routing between slabs
   Workspace ws_fd;    // Poisson solver buffers
   FFTPlans fft;       // its cuFFT plans
+  SlabFFTPlans fft_slab;  // the slab form's plans (z-slab handles)
   cudaStream_t stream = nullptr;
   int* d_status = nullptr;  // [0] particles outside the sub, [1] non-finite
   // position fingerprints: [0] of the sort held in ws, [1] of an M2P's xp
@@ -93,6 +94,7 @@ struct Handle {
   int64_t w_np = 0;
   ~Handle() {
     fft.release();
+    fft_slab.release();
     if (stream) cudaStreamDestroy(stream);
     if (d_status) cudaFree(d_status);
     if (d_hash) cudaFree(d_hash);
@@ -712,6 +714,40 @@ int ghost_pipeline(Handle& h, T* field, int64_t ldf, int lda, const int64_t* f_l
   return 0;
 }
 
+// One call of the caller's transport on device blocks.  host_transport (the
+// host entry points): the transport sees host staging copies of them.
+// Returns the transport's status (a CUDA error of the staging in e).
+int run_transport(Handle& h, int ns, const ppmg_halo_block* sends, int nr,
+                  const ppmg_halo_block* recvs, bool host_transport, cudaStream_t st,
+                  cudaError_t& e) {
+  e = cudaSuccess;
+  if (!host_transport) return h.halo_fn(h.halo_ctx, ns, sends, nr, recvs, 1, st);
+  size_t tot = 0;
+  for (int b = 0; b < ns; ++b) tot += (size_t)sends[b].bytes;
+  for (int b = 0; b < nr; ++b) tot += (size_t)recvs[b].bytes;
+  h.halo_host.resize(tot > 0 ? tot : 1);
+  unsigned char* hb = h.halo_host.data();
+  std::vector<ppmg_halo_block> hs(sends, sends + ns), hr(recvs, recvs + nr);
+  size_t o = 0;
+  for (int b = 0; b < ns && !e; ++b) {
+    hs[b].buf = hb + o;
+    e = cudaMemcpyAsync(hb + o, sends[b].buf, (size_t)sends[b].bytes, cudaMemcpyDeviceToHost, st);
+    o += (size_t)sends[b].bytes;
+  }
+  for (int b = 0; b < nr; ++b) {
+    hr[b].buf = hb + o;
+    o += (size_t)recvs[b].bytes;
+  }
+  if (!e) e = cudaStreamSynchronize(st);
+  if (e) return 0;
+  const int rc = h.halo_fn(h.halo_ctx, ns, hs.data(), nr, hr.data(), 0, nullptr);
+  for (int b = 0; b < nr && !rc && !e; ++b)
+    e = cudaMemcpyAsync(recvs[b].buf, hr[b].buf, (size_t)recvs[b].bytes, cudaMemcpyHostToDevice,
+                        st);
+  if (!e) e = cudaStreamSynchronize(st);  // the staging is reused by the next call
+  return rc;
+}
+
 // The ghost exchange of a z-slab handle with its neighbours through the
 // caller's transport, on the device field `field` (the caller's for the `_dev`
 // entry points, the mirror of the host entry points).  host_transport: the
@@ -743,31 +779,12 @@ int slab_exchange(Handle& h, T* field, int64_t ldf, const int64_t* f_lb, const i
     rbuf[1] = field + pl.recv_off[1];
   }
   ppmg_halo_block sends[2], recvs[2];
-  int rc = 0;
-  if (!host_transport) {
-    for (int b = 0; b < 2; ++b) {
-      sends[b] = {pl.send_peer[b], pl.send_tag[b], field + pl.send_off[b], (int64_t)bytes};
-      recvs[b] = {pl.recv_peer[b], pl.recv_tag[b], rbuf[b], (int64_t)bytes};
-    }
-    rc = h.halo_fn(h.halo_ctx, 2, sends, 2, recvs, 1, st);
-  } else {
-    h.halo_host.resize(4 * bytes);
-    unsigned char* hb = h.halo_host.data();
-    for (int b = 0; b < 2 && !e; ++b)
-      e = cudaMemcpyAsync(hb + b * bytes, field + pl.send_off[b], bytes, cudaMemcpyDeviceToHost,
-                          st);
-    if (!e) e = cudaStreamSynchronize(st);
-    if (e) return cuda_fail(info, e, caller);
-    for (int b = 0; b < 2; ++b) {
-      sends[b] = {pl.send_peer[b], pl.send_tag[b], hb + b * bytes, (int64_t)bytes};
-      recvs[b] = {pl.recv_peer[b], pl.recv_tag[b], hb + (2 + b) * bytes, (int64_t)bytes};
-    }
-    rc = h.halo_fn(h.halo_ctx, 2, sends, 2, recvs, 0, nullptr);
-    for (int b = 0; b < 2 && !rc && !e; ++b)
-      e = cudaMemcpyAsync(rbuf[b], hb + (2 + b) * bytes, bytes, cudaMemcpyHostToDevice, st);
-    if (!e) e = cudaStreamSynchronize(st);  // the staging is reused by the next call
-    if (e) return cuda_fail(info, e, caller);
+  for (int b = 0; b < 2; ++b) {
+    sends[b] = {pl.send_peer[b], pl.send_tag[b], field + pl.send_off[b], (int64_t)bytes};
+    recvs[b] = {pl.recv_peer[b], pl.recv_tag[b], rbuf[b], (int64_t)bytes};
   }
+  const int rc = run_transport(h, 2, sends, 2, recvs, host_transport, st, e);
+  if (e) return cuda_fail(info, e, caller);
   if (rc != 0)
     return fail(info, kErrorFatal, 2,
                 std::string(caller) + ": the halo transport failed (returned " +
@@ -1610,10 +1627,12 @@ static void poisson_common(T* field_up, int64_t ldf, int lda, const int64_t* f_l
   if (info) *info = 0;
   Handle* hh = find_handle(topo_id, mesh_id);
   if (!hh) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": topo_id/mesh_id is invalid"); return; }
-  Handle* h = get_checked(topo_id, mesh_id, 3, caller, info);
+  // a z-slab solves with the other slabs through its halo transport
+  Handle* h = get_checked(topo_id, mesh_id, 3, caller, info, hh->halo_fn != nullptr);
   if (!h) return;
   if (lda < 1 || ldf < lda) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": lda inconsistent"); return; }
   if (!check_ghost(*h, ghostsize, caller, info)) return;
+  if (h->open_z && h->g.N[1] < h->nsubs) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": the slab solve needs at least as many y cells as slabs"); return; }
   std::lock_guard<std::mutex> lk(h->mu);
   int lo[3], hi[3];
   for (int a = 0; a < 3; ++a) {
@@ -1632,7 +1651,60 @@ static void poisson_common(T* field_up, int64_t ldf, int lda, const int64_t* f_l
   }
   double len[3];
   for (int a = 0; a < 3; ++a) len[a] = h->g.max_phys[a] - h->g.min_phys[a];
-  const int bad = fd_poisson<T>(h->fft, h->ws_fd, h->g.N, len, dfield, fd, lda, st, e);
+  int bad = 0;
+  if (h->open_z) {
+    // ppm_fdsolver_solve_slab: xy transforms on the slab, z on the pencils
+    std::vector<int> z0(h->nsubs), nz(h->nsubs);
+    for (int q = 0; q < h->nsubs; ++q) {
+      z0[q] = h->istart[3 * q + 2] - 1;
+      nz[q] = h->nnodes[3 * q + 2] - 1;
+    }
+    SlabSolve sl;
+    sl.P = h->nsubs;
+    sl.me = h->local_sub;
+    sl.N[0] = h->g.N[0];
+    sl.N[1] = h->g.N[1];
+    sl.N[2] = h->Nm_global_z - 1;
+    for (int a = 0; a < 3; ++a) sl.len[a] = len[a];
+    sl.z0 = z0.data();
+    sl.nz = nz.data();
+    cudaError_t te = cudaSuccess;
+    BlockExchange xchg = [&](int ns, const ppmg_halo_block* sb, int nr,
+                             const ppmg_halo_block* rb) {
+      const int rc = run_transport(*h, ns, sb, nr, rb, !dev, st, te);
+      return te ? 1 : rc;
+    };
+    bad = fd_poisson_slab<T>(h->fft_slab, h->ws_fd, sl, dfield, fd, lda, st, xchg, e);
+    if (!e) e = te;
+    if (bad == 2) {
+      fail(info, kErrorFatal, 2, std::string(caller) + ": the halo transport failed");
+      return;
+    }
+    // the shared upper plane (node nz+1, the slab above's plane 1), then the
+    // z ghost planes, from the neighbours
+    if (!bad && !e) {
+      HaloPlan pl;
+      const char* why = halo_plan(h->nsubs, h->istart.data(), h->nnodes.data(), h->Nm_global_z,
+                                  h->local_sub, ldf, f_lb, f_ub, 0, true, pl);
+      if (why) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": " + why); return; }
+      // with g = 0 the put's blocks are single planes: nz+1 up, 1 down; the
+      // plane 1 travelling down replaces the lower slab's plane nz+1
+      const int64_t plane = pl.count;
+      const int nzl = h->g.N[2];
+      ppmg_halo_block sb = {pl.send_peer[1], 19, dfield + pl.send_off[1],
+                            (int64_t)(sizeof(T) * plane)};
+      ppmg_halo_block rb = {pl.recv_peer[1], 19,
+                            dfield + (int64_t)(nzl + 1 - f_lb[2]) * plane,
+                            (int64_t)(sizeof(T) * plane)};
+      const int rc = run_transport(*h, 1, &sb, 1, &rb, !dev, st, e);
+      if (e) { cuda_fail(info, e, caller); return; }
+      if (rc) { fail(info, kErrorFatal, 2, std::string(caller) + ": the halo transport failed"); return; }
+      if (slab_exchange<T>(*h, dfield, ldf, f_lb, f_ub, ghostsize, false, !dev, st, info, caller))
+        return;
+    }
+  } else {
+    bad = fd_poisson<T>(h->fft, h->ws_fd, h->g.N, len, dfield, fd, lda, st, e);
+  }
   if (bad) {
     fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": cuFFT plan or transform failed");
     return;

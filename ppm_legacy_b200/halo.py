@@ -333,12 +333,15 @@ def _write_block(addr, data, on_device):
 class ThreadMover:
     """Slabs held by one process, each exchanging from a host thread of its
     own (their C calls run concurrently): a send is matched with the receive
-    of the same (source, destination, tag).  Blocks travel through host
-    memory.  A receive waits at most `timeout` seconds."""
+    of the same (source, destination, tag), in the order they were posted
+    (a thread may post its next exchange before a peer took the last one).
+    Blocks travel through host memory.  A receive waits at most `timeout`
+    seconds."""
 
     def __init__(self, timeout=60.0):
+        import collections
         self.cv = _threading.Condition()
-        self.box = {}
+        self.box = collections.defaultdict(collections.deque)
         self.timeout = timeout
 
     def exchange(self, me, sends, recvs, on_device, stream):
@@ -346,14 +349,14 @@ class ThreadMover:
                   for peer, tag, addr, n in sends]
         with self.cv:
             for k, data in posted:
-                self.box[k] = data
+                self.box[k].append(data)
             self.cv.notify_all()
         for peer, tag, addr, n in recvs:
             key = (peer, me, tag)
             with self.cv:
-                if not self.cv.wait_for(lambda: key in self.box, timeout=self.timeout):
+                if not self.cv.wait_for(lambda: len(self.box[key]) > 0, timeout=self.timeout):
                     raise TimeoutError(f"slab {me}: no block from {peer} (tag {tag})")
-                data = self.box.pop(key)
+                data = self.box[key].popleft()
             if len(data) != n:
                 raise ValueError("slab exchange: block sizes differ between neighbours")
             _write_block(addr, data, on_device)
