@@ -146,6 +146,41 @@ void ppmg_halo_plan(int nsubs, const int* istart, const int* nnodes, int Nmz, in
                     int64_t* send_off, int* recv_peer, int* recv_tag, int64_t* recv_off,
                     int* info);
 
+/* ---- ghost exchange of any cartesian decomposition ------------------------
+ * Cuts along x, y and z (the subdomains of ppm_param_decomp_cartesian, each
+ * axis cut into intervals shared by all subdomains of the other axes).  A
+ * block is a box of the local field in its 1-based node indices, lo..hi
+ * inclusive per axis; it travels as all ldf rows of each node, x fastest
+ * (ldf * ext0 * ext1 * ext2 elements, ext = hi - lo + 1).  Along a cut axis
+ * the local nodes 1..nnodes hold the subdomain's real nodes (the last one
+ * shared with the next subdomain); along an uncut axis the box spans the
+ * whole field box 1-g..Nm+g.  With G the ghost-extended box of a subdomain
+ * and R its real box, in global node indices, and t in {-1, 0, 1} per cut
+ * axis (the periodic shift, N cells):
+ *   put: subdomain s sends G_s and (R_q + tN) to q, which adds it to its
+ *        nodes; every copy of a real node ends with the sum of all copies;
+ *   get: s sends (R_s and (G_q + tN)) minus (R_q + tN) to q, cut into at
+ *        most one box per cut axis, which q copies into its ghost nodes.
+ * Tags: 100 + 3 * d + k, d = (t0+1) + 3 (t1+1) + 9 (t2+1) the shift, k the
+ * piece; a send and its receive carry the same tag.  Slabs along z (cuts
+ * along z only) exchange whole planes instead (ppmg_halo_plan). */
+typedef struct {
+  int peer;       /* subdomain (0-based) on the other side */
+  int tag;
+  int64_t lo[3];  /* first node of the box per axis (local, 1-based) */
+  int64_t hi[3];  /* last node, inclusive */
+} ppmg_halo_box;
+
+/* The boxes of one exchange of subdomain isub (maptype 6 = put, 5 = get)
+ * from the geometry alone (istart, nnodes: [nsubs][3] as in
+ * ppmg_mesh_register; Nm: global nodes per axis).  *nsend / *nrecv get the
+ * box counts; at most `cap` boxes of each list are written (cap = 0 asks for
+ * the counts).  Receives are listed in the order they are applied. */
+void ppmg_halo_plan_boxes(int nsubs, const int* istart, const int* nnodes, const int* Nm,
+                          int isub, const int* ghostsize, int maptype, int cap,
+                          ppmg_halo_box* sends, int* nsend, ppmg_halo_box* recvs, int* nrecv,
+                          int* info);
+
 /* Wait for all work of the handle's `_dev` calls on `stream` and return the
  * data-dependent status latched since the last call (info/errno as above). */
 void ppmg_sync_status(int topo_id, int mesh_id, void* stream, int* info);

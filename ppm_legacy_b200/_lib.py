@@ -40,6 +40,8 @@ SIGNATURES = {
     "ppmg_halo_set_transport": ([_i, _i, _vp, _vp, _pi], None),
     "ppmg_halo_plan": ([_i, _pd, _pd, _i, _i, _i64, _pi64, _pi64, _pi, _i, _pi64, _pi, _pi, _pi64,
                         _pi, _pi, _pi64, _pi], None),
+    "ppmg_halo_plan_boxes": ([_i, _pd, _pd, _pi, _i, _pi, _i, _i, _vp, _pi, _vp, _pi, _pi],
+                             None),
     "ppmg_interp_p2m_adjoint_dv_3d": (_ADJ, None),
     "ppmg_interp_p2m_adjoint_dv_3d_dev": (_ADJ + [_vp], None),
     "ppmg_map_field_ghost_d": (_GHOST, None),

@@ -1010,6 +1010,32 @@ void ppmg_halo_plan(int nsubs, const int* istart, const int* nnodes, int Nmz, in
   }
 }
 
+void ppmg_halo_plan_boxes(int nsubs, const int* istart, const int* nnodes, const int* Nm,
+                          int isub, const int* ghostsize, int maptype, int cap,
+                          ppmg_halo_box* sends, int* nsend, ppmg_halo_box* recvs, int* nrecv,
+                          int* info) {
+  clear_error();
+  if (info) *info = 0;
+  if (maptype != kMapGhostGet && maptype != kMapGhostPut) { fail(info, kErrorError, ppmg::kErrArgument, "ppmg_halo_plan_boxes: maptype must be ghost_get (5) or ghost_put (6)"); return; }
+  std::vector<HaloBox> hs, hr;
+  const char* why = halo_boxes(nsubs, istart, nnodes, Nm, isub, ghostsize,
+                               maptype == kMapGhostPut, hs, hr);
+  if (why) { fail(info, kErrorError, ppmg::kErrArgument, std::string("ppmg_halo_plan_boxes: ") + why); return; }
+  auto out = [cap](const std::vector<HaloBox>& v, ppmg_halo_box* dst, int* n) {
+    *n = (int)v.size();
+    for (int i = 0; i < (int)v.size() && i < cap; ++i) {
+      dst[i].peer = v[i].peer;
+      dst[i].tag = v[i].tag;
+      for (int a = 0; a < 3; ++a) {
+        dst[i].lo[a] = v[i].lo[a];
+        dst[i].hi[a] = v[i].hi[a];
+      }
+    }
+  };
+  out(hs, sends, nsend);
+  out(hr, recvs, nrecv);
+}
+
 void ppmg_mesh_unregister(int topo_id, int mesh_id, int* info) {
   clear_error();
   if (info) *info = 0;

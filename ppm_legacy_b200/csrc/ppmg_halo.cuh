@@ -1,6 +1,8 @@
 // ppmg_halo.cuh -- blocks of the ghost exchange between z-slab subdomains.
 #pragma once
 
+#include <vector>
+
 #include "ppmg_common.cuh"
 
 namespace ppmg {
@@ -21,6 +23,31 @@ struct HaloPlan {
 const char* halo_plan(int nsubs, const int* istart, const int* nnodes, int Nmz, int isub,
                       int64_t ldf, const int64_t* f_lb, const int64_t* f_ub, int gz, bool put,
                       HaloPlan& out);
+
+// The exchange of any cartesian decomposition (cuts along one, two or three
+// axes): blocks are boxes of the local field, in its 1-based local node
+// indices (inclusive), for every neighbouring subdomain and periodic shift.
+struct HaloBox {
+  int peer, tag;
+  int64_t lo[3], hi[3];
+};
+// Builds the boxes of subdomain isub (istart, nnodes: [nsubs][3]; Nm: global
+// nodes per axis; g: ghost widths).  Returns 0, or a message describing the
+// argument that is wrong.
+const char* halo_boxes(int nsubs, const int* istart, const int* nnodes, const int Nm[3],
+                       int isub, const int g[3], bool put, std::vector<HaloBox>& sends,
+                       std::vector<HaloBox>& recvs);
+
+// Pack the boxes of field (ldf rows per node, element strides s[3], lower
+// bounds lb[3]) into buf (boxes back to back, in table order), or unpack buf
+// into them (add: the put's pop with add; else a copy).  tab: device table
+// of 8 int64 per box (lo[3], ext[3], buffer offset, elements), nbox boxes,
+// total elements tot.
+template <class T>
+cudaError_t launch_box_copy(T* field, int64_t ldf, const int64_t s[3], const int lb[3],
+                            const int64_t* tab, int nbox, int64_t tot, T* buf, int mode,
+                            cudaStream_t st);
+constexpr int kBoxPack = 0, kBoxCopy = 1, kBoxAdd = 2;
 
 // dst[i] += src[i] for i < n (the pop with add of a received block).
 template <class T>

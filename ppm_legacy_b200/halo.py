@@ -252,6 +252,37 @@ def plan(topo, isub, ldf, field_lb, field_ub, ghost, put):
             "recv": [(rp[b], rt[b], ro[b]) for b in range(2)]}
 
 
+class HaloBox(_C.Structure):
+    """ppmg_halo_box: one box of local field nodes (1-based, inclusive)."""
+    _fields_ = [("peer", _C.c_int), ("tag", _C.c_int), ("lo", _C.c_int64 * 3),
+                ("hi", _C.c_int64 * 3)]
+
+
+def plan_boxes(topo, isub, ghost, put):
+    """The library's boxes of one exchange of subdomain isub of a cartesian
+    decomposition (ppmg_halo_plan_boxes): {"send": [...], "recv": [...]},
+    each entry (peer, tag, lo(3), hi(3)) in local 1-based node indices,
+    receives in the order they are applied.  Host logic only."""
+    from ._lib import int_array, last_error, lib
+    ist = np.ascontiguousarray(topo.istart, dtype=np.int32)
+    nn = np.ascontiguousarray(topo.nnodes, dtype=np.int32)
+    ns, nr, info = _C.c_int(0), _C.c_int(0), _C.c_int(0)
+    args = (int(topo.nsubs), ist.ctypes.data, nn.ctypes.data, int_array(topo.Nm), int(isub),
+            int_array(ghost), 6 if put else 5)
+    lib().ppmg_halo_plan_boxes(*args, 0, None, _C.byref(ns), None, _C.byref(nr),
+                               _C.byref(info))
+    if info.value != 0:
+        raise ValueError(last_error()[2])
+    sb, rb = (HaloBox * max(ns.value, 1))(), (HaloBox * max(nr.value, 1))()
+    cap = max(ns.value, nr.value)
+    lib().ppmg_halo_plan_boxes(*args, cap, _C.addressof(sb), _C.byref(ns), _C.addressof(rb),
+                               _C.byref(nr), _C.byref(info))
+
+    def rows(b, n):
+        return [(b[i].peer, b[i].tag, tuple(b[i].lo), tuple(b[i].hi)) for i in range(n)]
+    return {"send": rows(sb, ns.value), "recv": rows(rb, nr.value)}
+
+
 def has_c_transport(topo_id, mesh_id) -> bool:
     return (int(topo_id), int(mesh_id)) in _c_transports
 
