@@ -74,17 +74,20 @@ void ppmg_mesh_unregister(int topo_id, int mesh_id, int* info);
 /* The subdomain (0-based isub) this GPU computes on: the one-entry
  * ppm_isublist of the process (ppm/src/ppm_topo_mkfield.f:311-319 builds the
  * reference's per-process sub list).  Required when nsubs > 1.  Supported
- * decomposition: slabs along z, every subdomain spanning x and y.  On a
- * slab the 3D P2M, M2P, P2M adjoint and remeshing (comp_weights, remesh,
- * create_part) compute on the local sub with z not periodic: P2M and remesh
- * leave in their z ghost planes the contributions owed to the neighbouring
- * slabs, M2P and the adjoint read their field's z ghost planes, create_part
- * skips the slab's shared upper node plane; the exchange between the slabs
- * (the ghost put / get of ppm_map_field_ghost, ppm_map_field_send.f) is the
- * caller's: through a transport registered with ppmg_halo_set_transport
- * (below), or ppm_legacy_b200.halo over torch.distributed.  Without a
- * transport the standalone ghost mapping returns info = -2 (errno 503) on a
- * slab; the allocation-free P2M always does. */
+ * decompositions: cartesian in 3D (ppm_param_decomp_cartesian and the
+ * pencil and slab cuts): every axis is either spanned by all subdomains or
+ * cut into intervals that all subdomains share, each interval starting on
+ * the previous one's last node.  Along a cut axis the local subdomain is not
+ * periodic: the 3D P2M, M2P, P2M adjoint and remeshing (comp_weights,
+ * remesh, create_part) compute on it alone, P2M and remesh leave in their
+ * ghost layers the contributions owed to the neighbours, M2P and the adjoint
+ * read their field's ghost layers, create_part skips the shared upper node
+ * of each cut axis; the exchange between the subdomains (the ghost put / get
+ * of ppm_map_field_ghost, ppm_map_field_send.f) is the caller's: through a
+ * transport registered with ppmg_halo_set_transport (below), or, for slabs
+ * along z, ppm_legacy_b200.halo over torch.distributed.  Without a transport
+ * the standalone ghost mapping returns info = -2 (errno 503) on a cut
+ * subdomain; the allocation-free P2M always does. */
 void ppmg_mesh_set_local_sub(int topo_id, int mesh_id, int isub, int* info);
 
 /* ---- ghost exchange between z-slab subdomains ---------------------------
@@ -121,11 +124,13 @@ typedef struct {
 typedef int (*ppmg_halo_fn)(void* ctx, int nsend, const ppmg_halo_block* sends, int nrecv,
                             const ppmg_halo_block* recvs, int on_device, void* stream);
 
-/* Register (fn != NULL) or remove (fn == NULL) the transport of a slab
- * handle.  With a transport, ppmg_map_field_ghost_{d,s}[_dev] on the slab
- * performs the put or get with the neighbouring slabs, and the 3D P2M and
- * remesh on the slab end with the ghost put, as ppm_interp_p2m.f:3665-3718
- * and ppm_rmsh_remesh.f:876-924 end theirs.  A transport that fails gives
+/* Register (fn != NULL) or remove (fn == NULL) the transport of a handle
+ * whose local subdomain is one of several.  With a transport,
+ * ppmg_map_field_ghost_{d,s}[_dev] on it performs the put or get with the
+ * neighbouring subdomains (whole planes for slabs along z, the boxes of
+ * ppmg_halo_plan_boxes otherwise), and the 3D P2M and remesh end with the
+ * ghost put, as ppm_interp_p2m.f:3665-3718 and ppm_rmsh_remesh.f:876-924
+ * end theirs.  A transport that fails gives
  * info = -1, errno 2 (ppm_err_mpi_fail, ppm_error.h:153). */
 void ppmg_halo_set_transport(int topo_id, int mesh_id, ppmg_halo_fn fn, void* ctx, int* info);
 
@@ -159,8 +164,10 @@ void ppmg_halo_plan(int nsubs, const int* istart, const int* nnodes, int Nmz, in
  * axis (the periodic shift, N cells):
  *   put: subdomain s sends G_s and (R_q + tN) to q, which adds it to its
  *        nodes; every copy of a real node ends with the sum of all copies;
- *   get: s sends (R_s and (G_q + tN)) minus (R_q + tN) to q, cut into at
- *        most one box per cut axis, which q copies into its ghost nodes.
+ *   get: s sends (R'_s and (G_q + tN)) minus (R_q + tN) to q, cut into at
+ *        most one box per cut axis, which q copies into its ghost nodes;
+ *        R'_s is R_s without its last node along each cut axis (the next
+ *        subdomain's first), so that no node arrives twice.
  * Tags: 100 + 3 * d + k, d = (t0+1) + 3 (t1+1) + 9 (t2+1) the shift, k the
  * piece; a send and its receive carry the same tag.  Slabs along z (cuts
  * along z only) exchange whole planes instead (ppmg_halo_plan). */
@@ -400,7 +407,11 @@ void ppmg_util_rank2d_s(const float* xp, int64_t ldxp, int64_t Np, const float* 
  * -1/|k|^2 (k_a = 2 pi / L_a times the wave number folded to |.| <= N_a/2,
  * the zero mode set to 0), and phi is written to every node of the box
  * 1-g:Nm+g (real nodes and their periodic images).  FFTs by cuFFT (the
- * reference uses FFTW); a z-slab handle returns info = -2. */
+ * reference uses FFTW).  On a slab along z with a halo transport the slab
+ * form solves the whole domain: xy transforms on every slab, an all-to-all
+ * to z pencils through the transport, the z transforms and the spectral
+ * step, and back; phi then fills the slab's box, its z ghost planes from the
+ * neighbours.  Other cuts return info = -2, errno 503. */
 void ppmg_fdsolver_poisson_3d_d(double* field_up, int64_t ldf, int lda, const int64_t* f_lb,
                                 const int64_t* f_ub, int topo_id, int mesh_id,
                                 const int* ghostsize, int* info);
@@ -423,7 +434,8 @@ void ppmg_fdsolver_poisson_3d_s_dev(float* field_up, int64_t ldf, int lda, const
  * receives the particle ids grouped by class: kept, to the slab below, to the
  * slab above, in no neighbour; each class in ascending id.  counts (host, 4)
  * receives the class sizes; the call returns once they are known.  Particles
- * in no neighbour give info = -2, errno 405.
+ * in no neighbour give info = -2, errno 405.  Slabs along z only (other
+ * cuts: info = -2, errno 503; the global routing below serves them).
  * gather: dst(0:lda-1, j) = src(0:lda-1, perm[j]) for j < n (device arrays;
  * positions or any particle property). */
 void ppmg_map_part_route_d_dev(const double* xp, int64_t ldxp, int64_t Np, int topo_id,
@@ -431,12 +443,13 @@ void ppmg_map_part_route_d_dev(const double* xp, int64_t ldxp, int64_t Np, int t
 void ppmg_map_part_route_s_dev(const float* xp, int64_t ldxp, int64_t Np, int topo_id,
                                int mesh_id, int* perm, int64_t* counts, int* info, void* stream);
 /* Global routing (ppm_map_part_global, ppm/src/ppm_map_part_global.f:355-420):
- * every particle to the slab that contains it among all nsubs slabs (<= 255;
- * closed-lower / open-upper, x and y inside the domain).  perm receives the
- * particle ids grouped by destination slab 0..nsubs-1 and then those in no
- * slab, each group in ascending id; counts (host, nsubs+1) the group sizes.
- * Particles in no slab are left out of the exchange without an error, as in
- * the reference (ppm_map_part_global.f:437-442). */
+ * every particle to the subdomain that contains it among all nsubs (<= 255;
+ * closed-lower / open-upper boxes min_sub .. max_sub on every axis; any
+ * registered decomposition).  perm receives the particle ids grouped by
+ * destination subdomain 0..nsubs-1 and then those in none, each group in
+ * ascending id; counts (host, nsubs+1) the group sizes.  Particles in no
+ * subdomain are left out of the exchange without an error, as in the
+ * reference (ppm_map_part_global.f:437-442). */
 void ppmg_map_part_global_route_d_dev(const double* xp, int64_t ldxp, int64_t Np, int topo_id,
                                       int mesh_id, int* perm, int64_t* counts, int* info,
                                       void* stream);

@@ -57,14 +57,20 @@ struct Handle {
   // the subdomain this GPU computes on (ppm_isublist of one entry): -1 until
   // ppmg_mesh_set_local_sub when nsubs > 1
   int local_sub = 0;
-  // the local subdomain is one z-slab of the domain: z is not periodic
-  // within it, its neighbours' slabs hold the ghost nodes' owners
-  bool open_z = false;
-  int Nm_global_z = 0;  // global nodes along z (Nm[2] becomes the slab's)
+  // cut axes: the local subdomain is one interval of several along them, not
+  // periodic within it; the neighbouring subdomains own its ghost nodes
+  bool open[3] = {false, false, false};
+  int Nm_global[3] = {1, 1, 1};  // global nodes (Nm becomes the subdomain's)
+  bool cut() const { return open[0] || open[1] || open[2]; }
+  // slabs along z: the exchange moves whole planes (ppmg_halo_plan)
+  bool slab() const { return open[2] && !open[0] && !open[1]; }
   // transport of the ghost exchange with the neighbouring slabs (caller's)
   ppmg_halo_fn halo_fn = nullptr;
   void* halo_ctx = nullptr;
   DevBuf halo_rbuf;                     // blocks received by a put (device)
+  DevBuf halo_sbuf;                     // packed blocks to send (box exchange)
+  DevBuf halo_tab;                      // box tables of the box exchange
+  std::vector<int64_t> halo_tab_host;
   std::vector<unsigned char> halo_host;  // host staging of the host entry points
   Geom g{};
   Workspace ws;       // P2M / M2P / adjoint / ghost / clist scratch
@@ -132,7 +138,7 @@ Handle* find_handle(int topo_id, int mesh_id) {
 // Checks shared by every hot-path entry point (the ppm_debug > 0 checks of
 // ppm_interp_p2m.f:338-410, always on here).
 Handle* get_checked(int topo_id, int mesh_id, int dim, const char* caller, int* info,
-                    bool slab_ok = false) {
+                    bool sub_ok = false) {
   Handle* h = find_handle(topo_id, mesh_id);
   if (!h) {
     fail(info, kErrorError, kErrArgument, std::string(caller) + ": topo_id/mesh_id is invalid");
@@ -149,11 +155,11 @@ Handle* get_checked(int topo_id, int mesh_id, int dim, const char* caller, int* 
              ": nsubs > 1: select this GPU's subdomain with ppmg_mesh_set_local_sub");
     return nullptr;
   }
-  if (h->open_z && !slab_ok) {
+  if (h->cut() && !sub_ok) {
     fail(info, kErrorError, kErrArgument,
          std::string(caller) +
-             ": a z-slab subdomain is supported by the 3D P2M and M2P; this routine needs one "
-             "periodic subdomain per GPU");
+             ": a subdomain of several is supported by the 3D P2M, M2P, adjoint, remeshing and "
+             "ghost mapping; this routine needs one periodic subdomain per GPU");
     return nullptr;
   }
   for (int f = 0; f < 2 * dim; ++f)
@@ -225,7 +231,7 @@ KeyParams make_kp(const Handle& h, int mode, bool quirk) {
     kp.minf[a] = (float)kp.min[a];
     kp.maxf[a] = (float)kp.max[a];
     kp.dxif[a] = a < h.dim ? (quirk ? h.g.dxiq_f[a] : h.g.dxi_f[a]) : 1.0f;
-    kp.open[a] = a == 2 && h.open_z ? 1 : 0;
+    kp.open[a] = h.open[a] ? 1 : 0;
   }
   return kp;
 }
@@ -282,6 +288,11 @@ int p2m_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, const T* up, 
   for (int a = 0; a < h.dim; ++a) {
     lo[a] = 1 - ghost[a];
     hi[a] = h.Nm[a] + ghost[a];
+    // along a cut axis the stencils reach HL - 1 nodes past the real ones,
+    // whose contributions the ghost layers carry to the neighbours
+    if (h.open[a] && ghost[a] < (kernel == kKernelMp4 ? 1 : 0))
+      return fail(info, kErrorError, kErrArgument,
+                  std::string(caller) + ": ghostsize too small for this kernel on a cut axis");
   }
   FieldDesc fd;
   if (!make_fd(h, ldf, f_lb, f_ub, lo, hi, fd, caller, info)) return *info;
@@ -323,14 +334,16 @@ int p2m_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, const T* up, 
   P.us = ws.us.p;
   P.field = field;
   P.fd = fd;
-  if (h.open_z) {
-    // a z-slab: every node plane of the written box 1-g:Nm+g is produced
-    // (ghost planes hold the contributions owed to the neighbouring slabs)
-    P.open_z = 1;
-    P.zlo = lo[2] - 1;
-    P.ze = hi[2] - lo[2] + 1;
-  }
-  if ((e = ws.tiles.ensure(p2m_scratch_bytes(h.dim, P.N, P.ze)))) return cuda_fail(info, e, caller);
+  P.span = cell_span(P.N);
+  for (int a = 0; a < h.dim; ++a)
+    if (h.open[a]) {
+      // a cut axis: every node of the written box 1-g:Nm+g is produced
+      // (ghost nodes hold the contributions owed to the neighbours)
+      P.open[a] = 1;
+      P.span.org[a] = lo[a] - 1;
+      P.span.ext[a] = hi[a] - lo[a] + 1;
+    }
+  if ((e = ws.tiles.ensure(p2m_scratch_bytes(h.dim, P.N, &P.span)))) return cuda_fail(info, e, caller);
   e = launch_p2m(P, h.dim, kernel, prec, lda, Np > 0 ? Np : 1, remesh, ws.tiles.p, st);
   if (e) return cuda_fail(info, e, caller);
   if (!remesh) {
@@ -375,13 +388,14 @@ int m2p_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, T* up, int64_
     lo[a] = 1;
     hi[a] = h.g.N[a];
   }
-  if (h.open_z) {
-    // a z-slab reads the node planes its stencils reach, ghost planes
-    // included (filled from the neighbouring slabs by a ghost get)
-    const int HL = kernel == kKernelMp4 ? 2 : 1;
-    lo[2] = 2 - HL;
-    hi[2] = h.g.N[2] + HL;
-  }
+  for (int a = 0; a < h.dim; ++a)
+    if (h.open[a]) {
+      // a cut axis: the nodes the stencils reach are read, ghost nodes
+      // included (filled from the neighbours by a ghost get)
+      const int HL = kernel == kKernelMp4 ? 2 : 1;
+      lo[a] = 2 - HL;
+      hi[a] = h.g.N[a] + HL;
+    }
   FieldDesc fd;
   if (!make_fd(h, ldf, f_lb, f_ub, lo, hi, fd, caller, info)) return *info;
   if (Np == 0) return 0;
@@ -396,7 +410,7 @@ int m2p_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, T* up, int64_
     h.sort_cached = false;
     // outside a z-slab: unassigned (405); else only non-finite positions fail
     e = sort_interp<T>(h, kp, xp, ldxp, (const T*)nullptr, 0, 0, Np, prec == M2P_FP64,
-                       h.d_status + (h.open_z ? 0 : 1), up, ldup, lda, st);
+                       h.d_status + (h.cut() ? 0 : 1), up, ldup, lda, st);
     if (e) return cuda_fail(info, e, caller);
   }
   const int* dnv = d_nvalid_of(h.ws, h.g.ncell);
@@ -411,13 +425,13 @@ int m2p_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, T* up, int64_
   P.up = up;
   P.ldup = ldup;
   P.lda = lda;
-  P.open_z = h.open_z ? 1 : 0;
+  for (int a = 0; a < 3; ++a) P.open[a] = h.open[a] ? 1 : 0;
   if (h.dim == 3) {
     TileItems ti;
     if ((e = h.ws.tiles.ensure(tile_items_bytes(P.N)))) return cuda_fail(info, e, caller);
-    // a z-slab's P2M items cover its node planes -g .. nz+g, not M2P's cell
-    // layers: M2P builds its own (the cell order itself is reused)
-    if (reuse && !h.open_z) {
+    // a cut subdomain's P2M items cover its nodes -g .. N+g, not M2P's
+    // cells: M2P builds its own (the cell order itself is reused)
+    if (reuse && !h.cut()) {
       ti = tile_items_view(h.ws.tiles.p, P.N);
     } else if ((e = make_tile_items(h.ws.start.as<int>(), P.N, Np, h.ws.tiles.p, ti, st))) {
       return cuda_fail(info, e, caller);
@@ -484,9 +498,9 @@ bool field_is_box(const Handle& h, const int64_t* f_lb, const int64_t* f_ub, con
 }
 
 template <class T>
-int slab_exchange(Handle& h, T* field, int64_t ldf, const int64_t* f_lb, const int64_t* f_ub,
-                  const int* ghost, bool put, bool host_transport, cudaStream_t st, int* info,
-                  const char* caller);
+int sub_exchange(Handle& h, T* field, int64_t ldf, const int64_t* f_lb, const int64_t* f_ub,
+                 const int* ghost, bool put, bool host_transport, cudaStream_t st, int* info,
+                 const char* caller);
 
 template <class T>
 void p2m_host(const T* xp, int64_t ldxp, int64_t Np, const T* up, int64_t ldup, int lda,
@@ -520,8 +534,8 @@ void p2m_host(const T* xp, int64_t ldxp, int64_t Np, const T* up, int64_t ldup, 
                       f_ub, false, st, info, caller))
     return;
   // a z-slab ends with the ghost put, as ppm_interp_p2m.f:3665-3718 does
-  if (h->open_z && h->halo_fn &&
-      slab_exchange<T>(*h, dfield, ldf, f_lb, f_ub, ghostsize, true, true, st, info, caller))
+  if (h->cut() && h->halo_fn &&
+      sub_exchange<T>(*h, dfield, ldf, f_lb, f_ub, ghostsize, true, true, st, info, caller))
     return;
   e = cudaMemcpyAsync(field_up, dfield, sizeof(T) * (size_t)nf, cudaMemcpyDeviceToHost, st);
   if (e) { cuda_fail(info, e, caller); return; }
@@ -549,8 +563,8 @@ void p2m_dev(const T* xp, int64_t ldxp, int64_t Np, const T* up, int64_t ldup, i
                       f_ub, false, st, info, caller))
     return;
   // a z-slab ends with the ghost put, as ppm_interp_p2m.f:3665-3718 does
-  if (h->open_z && h->halo_fn)
-    slab_exchange<T>(*h, field_up, ldf, f_lb, f_ub, ghostsize, true, false, st, info, caller);
+  if (h->cut() && h->halo_fn)
+    sub_exchange<T>(*h, field_up, ldf, f_lb, f_ub, ghostsize, true, false, st, info, caller);
 }
 
 template <class T>
@@ -619,12 +633,13 @@ int adjoint_pipeline(Handle& h, const double* xp, int64_t ldxp, int64_t Np, cons
     lo[a] = 1;
     hi[a] = h.g.N[a];
   }
-  if (h.open_z) {
-    // a z-slab reads r's z ghost planes (the adjoint of the put is a get)
-    const int HL = kernel == kKernelMp4 ? 2 : 1;
-    lo[2] = 2 - HL;
-    hi[2] = h.g.N[2] + HL;
-  }
+  for (int a = 0; a < 3; ++a)
+    if (h.open[a]) {
+      // a cut axis: r's ghost nodes are read (the adjoint of the put is a get)
+      const int HL = kernel == kKernelMp4 ? 2 : 1;
+      lo[a] = 2 - HL;
+      hi[a] = h.g.N[a] + HL;
+    }
   FieldDesc fd;
   if (!make_fd(h, ldf, f_lb, f_ub, lo, hi, fd, caller, info)) return *info;
   if (Np == 0) return 0;
@@ -637,7 +652,7 @@ int adjoint_pipeline(Handle& h, const double* xp, int64_t ldxp, int64_t Np, cons
     h.sort_cached = false;  // the work items below describe this sort only
     KeyParams kp = make_kp(h, KEY_INTERP_WRAP, false);
     e = sort_interp<double>(h, kp, xp, ldxp, nullptr, 0, 0, Np, prec == M2P_FP64,
-                            h.d_status + (h.open_z ? 0 : 1), dw, lddw, lda, st);
+                            h.d_status + (h.cut() ? 0 : 1), dw, lddw, lda, st);
     if (e) return cuda_fail(info, e, caller);
   }
   const int* dnv = d_nvalid_of(h.ws, h.g.ncell);
@@ -656,13 +671,13 @@ int adjoint_pipeline(Handle& h, const double* xp, int64_t ldxp, int64_t Np, cons
   P.ldupin = ldup;
   P.dx = dx;
   P.lddx = lddx;
-  P.open_z = h.open_z ? 1 : 0;
+  for (int a = 0; a < 3; ++a) P.open[a] = h.open[a] ? 1 : 0;
   for (int a = 0; a < 3; ++a) P.dxi[a] = h.g.dxi_d[a];
   if (lda <= 4) {
     TileItems ti;
     if ((e = h.ws.tiles.ensure(tile_items_bytes(P.N)))) return cuda_fail(info, e, caller);
-    // a z-slab's P2M items cover node planes, not cell layers: own items
-    if (reuse && !h.open_z) {
+    // a cut subdomain's P2M items cover nodes, not cells: own items
+    if (reuse && !h.cut()) {
       ti = tile_items_view(h.ws.tiles.p, P.N);
     } else if ((e = make_tile_items(h.ws.start.as<int>(), P.N, Np, h.ws.tiles.p, ti, st))) {
       return cuda_fail(info, e, caller);
@@ -763,7 +778,7 @@ int slab_exchange(Handle& h, T* field, int64_t ldf, const int64_t* f_lb, const i
                 std::string(caller) + ": z-slab subdomain without a halo transport "
                                       "(ppmg_halo_set_transport)");
   HaloPlan pl;
-  const char* why = halo_plan(h.nsubs, h.istart.data(), h.nnodes.data(), h.Nm_global_z,
+  const char* why = halo_plan(h.nsubs, h.istart.data(), h.nnodes.data(), h.Nm_global[2],
                               h.local_sub, ldf, f_lb, f_ub, ghost[2], put, pl);
   if (why) return fail(info, kErrorError, kErrArgument, std::string(caller) + ": " + why);
   if (pl.count == 0) return 0;
@@ -796,6 +811,137 @@ int slab_exchange(Handle& h, T* field, int64_t ldf, const int64_t* f_lb, const i
   return 0;
 }
 
+// The ghost exchange of a subdomain cut along several axes: boxes per
+// neighbour and periodic shift (halo_boxes), packed into one send buffer,
+// moved by the caller's transport into one receive buffer, then added (put)
+// or copied (get) into the field.  The get's boxes are disjoint: one launch
+// copies them all.  The put's may overlap (a corner node receives from up
+// to 7 neighbours): they are added in waves of disjoint boxes, each box after
+// every earlier box it overlaps, so every node sums in the plan's order.
+template <class T>
+int box_exchange(Handle& h, T* field, int64_t ldf, const int64_t* f_lb, const int64_t* f_ub,
+                 const int* ghost, bool put, bool host_transport, cudaStream_t st, int* info,
+                 const char* caller) {
+  if (h.halo_fn == nullptr)
+    return fail(info, kErrorError, kErrArgument,
+                std::string(caller) + ": subdomain without a halo transport "
+                                      "(ppmg_halo_set_transport)");
+  std::vector<HaloBox> sb, rb;
+  const char* why = halo_boxes(h.nsubs, h.istart.data(), h.nnodes.data(), h.Nm_global,
+                               h.local_sub, ghost, put, sb, rb);
+  if (why) return fail(info, kErrorError, kErrArgument, std::string(caller) + ": " + why);
+  for (const auto* v : {&sb, &rb})
+    for (const HaloBox& b : *v)
+      for (int a = 0; a < 3; ++a)
+        if (b.lo[a] < f_lb[a] || b.hi[a] > f_ub[a])
+          return fail(info, kErrorError, kErrArgument,
+                      std::string(caller) + ": field_up bounds do not cover the ghost layers");
+  // table rows: lo[3], ext[3], first index of the box in its launch, its
+  // offset in the buffer.  Rows: the sends, the receives, then the
+  // receives again grouped by the put's waves (a box goes one wave after
+  // the last earlier box it overlaps)
+  const int ns = (int)sb.size(), nr = (int)rb.size();
+  auto overlap = [&](const HaloBox& x, const HaloBox& y) {
+    for (int a = 0; a < 3; ++a)
+      if (x.hi[a] < y.lo[a] || y.hi[a] < x.lo[a]) return false;
+    return true;
+  };
+  std::vector<int> wave(nr, 0);
+  int nw = 0;
+  if (put)
+    for (int i = 0; i < nr; ++i) {
+      for (int j = 0; j < i; ++j)
+        if (wave[j] >= wave[i] && overlap(rb[i], rb[j])) wave[i] = wave[j] + 1;
+      nw = wave[i] + 1 > nw ? wave[i] + 1 : nw;
+    }
+  std::vector<int64_t>& tab = h.halo_tab_host;
+  tab.assign(8 * (size_t)(ns + 2 * nr), 0);
+  std::vector<int64_t> elems(ns + nr);
+  int64_t tot[2] = {0, 0};
+  auto row = [&](int r, const HaloBox& b, int64_t first, int64_t off) {
+    int64_t* t = tab.data() + 8 * (size_t)r;
+    for (int a = 0; a < 3; ++a) {
+      t[a] = b.lo[a];
+      t[3 + a] = b.hi[a] - b.lo[a] + 1;
+    }
+    t[6] = first;
+    t[7] = off;
+  };
+  for (int i = 0; i < ns + nr; ++i) {
+    const HaloBox& b = i < ns ? sb[i] : rb[i - ns];
+    int64_t n = ldf;
+    for (int a = 0; a < 3; ++a) n *= b.hi[a] - b.lo[a] + 1;
+    elems[i] = n;
+    int64_t& acc = tot[i < ns ? 0 : 1];
+    row(i, b, acc, acc);
+    acc += n;
+  }
+  std::vector<int> wfirst(nw + 1, 0);
+  std::vector<int64_t> wtot(nw, 0);
+  {
+    int r = ns + nr;
+    for (int w = 0; w < nw; ++w) {
+      wfirst[w] = r;
+      for (int i = 0; i < nr; ++i)
+        if (wave[i] == w) {
+          row(r++, rb[i], wtot[w], tab[8 * (size_t)(ns + i) + 7]);
+          wtot[w] += elems[ns + i];
+        }
+    }
+  }
+  cudaError_t e = cudaSuccess;
+  if ((e = h.halo_tab.ensure(sizeof(int64_t) * tab.size())) ||
+      (e = h.halo_sbuf.ensure(sizeof(T) * (size_t)(tot[0] > 0 ? tot[0] : 1))) ||
+      (e = h.halo_rbuf.ensure(sizeof(T) * (size_t)(tot[1] > 0 ? tot[1] : 1))))
+    return cuda_fail(info, e, caller);
+  int64_t* dtab = h.halo_tab.as<int64_t>();
+  T* sbuf = h.halo_sbuf.as<T>();
+  T* rbuf = h.halo_rbuf.as<T>();
+  if ((e = cudaMemcpyAsync(dtab, tab.data(), sizeof(int64_t) * tab.size(),
+                           cudaMemcpyHostToDevice, st)))
+    return cuda_fail(info, e, caller);
+  int64_t s[3];
+  int lb[3];
+  s[0] = ldf;
+  s[1] = ldf * (f_ub[0] - f_lb[0] + 1);
+  s[2] = s[1] * (f_ub[1] - f_lb[1] + 1);
+  for (int a = 0; a < 3; ++a) lb[a] = (int)f_lb[a];
+  if ((e = launch_box_copy<T>(field, ldf, s, lb, dtab, ns, tot[0], sbuf, kBoxPack, st)))
+    return cuda_fail(info, e, caller);
+  std::vector<ppmg_halo_block> sends(ns), recvs(nr);
+  for (int i = 0; i < ns; ++i)
+    sends[i] = {sb[i].peer, sb[i].tag, sbuf + tab[8 * (size_t)i + 7],
+                (int64_t)sizeof(T) * elems[i]};
+  for (int i = 0; i < nr; ++i)
+    recvs[i] = {rb[i].peer, rb[i].tag, rbuf + tab[8 * (size_t)(ns + i) + 7],
+                (int64_t)sizeof(T) * elems[ns + i]};
+  const int rc = run_transport(h, ns, sends.data(), nr, recvs.data(), host_transport, st, e);
+  if (e) return cuda_fail(info, e, caller);
+  if (rc != 0)
+    return fail(info, kErrorFatal, 2,
+                std::string(caller) + ": the halo transport failed (returned " +
+                    std::to_string(rc) + ")");
+  if (!put)
+    e = launch_box_copy<T>(field, ldf, s, lb, dtab + 8 * (size_t)ns, nr, tot[1], rbuf,
+                           kBoxCopy, st);
+  for (int w = 0; w < nw && !e; ++w)
+    e = launch_box_copy<T>(field, ldf, s, lb, dtab + 8 * (size_t)wfirst[w],
+                           (w + 1 < nw ? wfirst[w + 1] : ns + 2 * nr) - wfirst[w], wtot[w],
+                           rbuf, kBoxAdd, st);
+  if (e) return cuda_fail(info, e, caller);
+  return 0;
+}
+
+template <class T>
+int sub_exchange(Handle& h, T* field, int64_t ldf, const int64_t* f_lb, const int64_t* f_ub,
+                 const int* ghost, bool put, bool host_transport, cudaStream_t st, int* info,
+                 const char* caller) {
+  return h.slab() ? slab_exchange<T>(h, field, ldf, f_lb, f_ub, ghost, put, host_transport, st,
+                                     info, caller)
+                  : box_exchange<T>(h, field, ldf, f_lb, f_ub, ghost, put, host_transport, st,
+                                    info, caller);
+}
+
 template <class T>
 void ghost_host(T* field_up, int64_t ldf, int lda, const int64_t* f_lb, const int64_t* f_ub,
                 int topo_id, int mesh_id, const int* ghostsize, int maptype, int* info,
@@ -808,15 +954,15 @@ void ghost_host(T* field_up, int64_t ldf, int lda, const int64_t* f_lb, const in
   Handle* h = get_checked(topo_id, mesh_id, hh->dim, caller, info, hh->halo_fn != nullptr);
   if (!h) return;
   if (lda < 1 || ldf < lda) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": lda inconsistent"); return; }
-  if (h->open_z && maptype != kMapGhostGet && maptype != kMapGhostPut) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": maptype must be ghost_get (5) or ghost_put (6)"); return; }
+  if (h->cut() && maptype != kMapGhostGet && maptype != kMapGhostPut) { fail(info, kErrorError, kErrArgument, std::string(caller) + ": maptype must be ghost_get (5) or ghost_put (6)"); return; }
   std::lock_guard<std::mutex> lk(h->mu);
   cudaStream_t st = h->stream;
   cudaError_t e;
   const int64_t nf = field_elems(*h, ldf, f_lb, f_ub);
   T* dfield = mirror<T>(h->ws.h_field, field_up, nf, st, e);
   if (e) { cuda_fail(info, e, caller); return; }
-  if (h->open_z) {
-    if (slab_exchange<T>(*h, dfield, ldf, f_lb, f_ub, ghostsize, maptype == kMapGhostPut, true,
+  if (h->cut()) {
+    if (sub_exchange<T>(*h, dfield, ldf, f_lb, f_ub, ghostsize, maptype == kMapGhostPut, true,
                          st, info, caller))
       return;
   } else if (ghost_pipeline<T>(*h, dfield, ldf, lda, f_lb, f_ub, ghostsize, maptype, st, info,
@@ -893,7 +1039,7 @@ void ppmg_mesh_register(int topo_id, int mesh_id, int dim, const double* min_phy
   h->dim = dim;
   h->nsubs = nsubs;
   for (int a = 0; a < 3; ++a) h->Nm[a] = a < dim ? Nm[a] : 2;
-  h->Nm_global_z = h->Nm[2];
+  for (int a = 0; a < 3; ++a) h->Nm_global[a] = h->Nm[a];
   for (int f = 0; f < 6; ++f) h->bcdef[f] = f < 2 * dim ? bcdef[f] : kBcPeriodic;
   h->min_sub.assign(min_sub, min_sub + 3 * nsubs);
   h->max_sub.assign(max_sub, max_sub + 3 * nsubs);
@@ -948,28 +1094,25 @@ void ppmg_mesh_set_local_sub(int topo_id, int mesh_id, int isub, int* info) {
   std::lock_guard<std::mutex> lk(h->mu);
   if (isub < 0 || isub >= h->nsubs) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": isub out of range"); return; }
   if (h->nsubs > 1) {
-    // supported decomposition: slabs along z, every subdomain spanning the
-    // whole domain in x and y (ppm_param_decomp_zpencil cut along z only)
+    // supported decompositions: cartesian (ppm_param_decomp_cartesian and
+    // the pencil / slab cuts, each axis cut into intervals shared by all
+    // subdomains), in 3D
     if (h->dim != 3) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": several subdomains are supported in 3D only"); return; }
-    for (int s = 0; s < h->nsubs; ++s)
-      for (int a = 0; a < 2; ++a)
-        if (h->istart[3 * s + a] != 1 || h->nnodes[3 * s + a] != h->Nm[a]) {
-          fail(info, kErrorError, ppmg::kErrArgument,
-               std::string(caller) + ": only a decomposition into z-slabs (each subdomain "
-                                     "spanning x and y) is supported");
-          return;
-        }
-    const int nz = h->nnodes[3 * isub + 2] - 1;
-    if (nz < 1) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": the subdomain has no cell layer"); return; }
+    if (const char* why = check_cartesian(h->nsubs, h->istart.data(), h->nnodes.data(),
+                                          h->Nm_global)) {
+      fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": " + why);
+      return;
+    }
     Geom& g = h->g;
-    g.N[2] = nz;
     for (int a = 0; a < 3; ++a) {
+      const int n = h->nnodes[3 * isub + a];
+      h->open[a] = n != h->Nm_global[a];
+      h->Nm[a] = n;
+      g.N[a] = n - 1;
       g.min_sub[a] = h->min_sub[3 * isub + a];
       g.max_sub[a] = h->max_sub[3 * isub + a];
     }
     g.ncell = (int64_t)g.N[0] * g.N[1] * g.N[2];
-    h->Nm[2] = nz + 1;
-    h->open_z = true;
   }
   h->local_sub = isub;
   h->sort_cached = false;
@@ -1228,9 +1371,9 @@ static void ghost_dev(T* field_up, int64_t ldf, int lda, const int64_t* f_lb, co
   if (!h) return;
   if (lda < 1 || ldf < lda) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": lda inconsistent"); return; }
   std::lock_guard<std::mutex> lk(h->mu);
-  if (h->open_z) {
+  if (h->cut()) {
     if (maptype != kMapGhostGet && maptype != kMapGhostPut) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": maptype must be ghost_get (5) or ghost_put (6)"); return; }
-    slab_exchange<T>(*h, field_up, ldf, f_lb, f_ub, ghostsize, maptype == kMapGhostPut, false,
+    sub_exchange<T>(*h, field_up, ldf, f_lb, f_ub, ghostsize, maptype == kMapGhostPut, false,
                      stream, info, caller);
     return;
   }
@@ -1412,8 +1555,8 @@ static void remesh_common(const T* xp, int64_t ldxp, int64_t Np, const T* up,
                         f_ub, true, dst, info, caller))
       return;
     // a z-slab ends with the ghost put, as ppm_rmsh_remesh.f:876-924 does
-    if (h->open_z && h->halo_fn)
-      slab_exchange<T>(*h, field_up, ldf, f_lb, f_ub, ghostsize, true, false, dst, info, caller);
+    if (h->cut() && h->halo_fn)
+      sub_exchange<T>(*h, field_up, ldf, f_lb, f_ub, ghostsize, true, false, dst, info, caller);
     return;
   }
   cudaStream_t st = h->stream;
@@ -1428,8 +1571,8 @@ static void remesh_common(const T* xp, int64_t ldxp, int64_t Np, const T* up,
   if (p2m_pipeline<T>(*h, dxp, ldxp, Np, dup, ldup, lda, kernel, ghostsize, dfield, ldf,
                            f_lb, f_ub, true, st, info, caller))
     return;
-  if (h->open_z && h->halo_fn &&
-      slab_exchange<T>(*h, dfield, ldf, f_lb, f_ub, ghostsize, true, true, st, info, caller))
+  if (h->cut() && h->halo_fn &&
+      sub_exchange<T>(*h, dfield, ldf, f_lb, f_ub, ghostsize, true, true, st, info, caller))
     return;
   e = cudaMemcpyAsync(field_up, dfield, sizeof(T) * (size_t)nf, cudaMemcpyDeviceToHost, st);
   if (e) { cuda_fail(info, e, caller); return; }
@@ -1658,7 +1801,8 @@ static void poisson_common(T* field_up, int64_t ldf, int lda, const int64_t* f_l
   if (!h) return;
   if (lda < 1 || ldf < lda) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": lda inconsistent"); return; }
   if (!check_ghost(*h, ghostsize, caller, info)) return;
-  if (h->open_z && h->g.N[1] < h->nsubs) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": the slab solve needs at least as many y cells as slabs"); return; }
+  if (h->cut() && !h->slab()) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": the FFT solver on several subdomains supports slabs along z only"); return; }
+  if (h->slab() && h->g.N[1] < h->nsubs) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": the slab solve needs at least as many y cells as slabs"); return; }
   std::lock_guard<std::mutex> lk(h->mu);
   int lo[3], hi[3];
   for (int a = 0; a < 3; ++a) {
@@ -1678,7 +1822,7 @@ static void poisson_common(T* field_up, int64_t ldf, int lda, const int64_t* f_l
   double len[3];
   for (int a = 0; a < 3; ++a) len[a] = h->g.max_phys[a] - h->g.min_phys[a];
   int bad = 0;
-  if (h->open_z) {
+  if (h->slab()) {
     // ppm_fdsolver_solve_slab: xy transforms on the slab, z on the pencils
     std::vector<int> z0(h->nsubs), nz(h->nsubs);
     for (int q = 0; q < h->nsubs; ++q) {
@@ -1690,7 +1834,7 @@ static void poisson_common(T* field_up, int64_t ldf, int lda, const int64_t* f_l
     sl.me = h->local_sub;
     sl.N[0] = h->g.N[0];
     sl.N[1] = h->g.N[1];
-    sl.N[2] = h->Nm_global_z - 1;
+    sl.N[2] = h->Nm_global[2] - 1;
     for (int a = 0; a < 3; ++a) sl.len[a] = len[a];
     sl.z0 = z0.data();
     sl.nz = nz.data();
@@ -1710,7 +1854,7 @@ static void poisson_common(T* field_up, int64_t ldf, int lda, const int64_t* f_l
     // z ghost planes, from the neighbours
     if (!bad && !e) {
       HaloPlan pl;
-      const char* why = halo_plan(h->nsubs, h->istart.data(), h->nnodes.data(), h->Nm_global_z,
+      const char* why = halo_plan(h->nsubs, h->istart.data(), h->nnodes.data(), h->Nm_global[2],
                                   h->local_sub, ldf, f_lb, f_ub, 0, true, pl);
       if (why) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": " + why); return; }
       // with g = 0 the put's blocks are single planes: nz+1 up, 1 down; the
@@ -1782,6 +1926,7 @@ static void route_common(const T* xp, int64_t ldxp, int64_t Np, int topo_id, int
   Handle* h = get_checked(topo_id, mesh_id, 3, caller, info, true);
   if (!h) return;
   if (Np < 0 || (Np > 0 && ldxp < 3) || Np >= (int64_t)1 << 31) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": invalid sizes"); return; }
+  if (h->cut() && !h->slab()) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": routing to the neighbours supports slabs along z only (ppmg_map_part_global_route routes on any decomposition)"); return; }
   std::lock_guard<std::mutex> lk(h->mu);
   // the local slab and its z neighbours (periodic across the domain's z faces)
   RouteParams R{};
@@ -1795,7 +1940,7 @@ static void route_common(const T* xp, int64_t ldxp, int64_t Np, int topo_id, int
   };
   for (int c = 0; c < 3; ++c) R.zlo[c] = R.zhi[c] = 0.0, R.zlof[c] = R.zhif[c] = 0.0f;
   box(0, s);
-  if (h->open_z) {
+  if (h->slab()) {
     const double lo = h->min_sub[3 * s + 2], hi = h->max_sub[3 * s + 2];
     for (int q = 0; q < h->nsubs; ++q) {
       if (q == s) continue;
@@ -1856,34 +2001,29 @@ static void groute_common(const T* xp, int64_t ldxp, int64_t Np, int topo_id, in
   std::lock_guard<std::mutex> lk(h->mu);
   const int ns = h->nsubs;
   if (ns > kMaxGlobalSubs) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": more than 255 subdomains"); return; }
-  if (ns > 1 && !h->open_z) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": select the local slab first (ppmg_mesh_set_local_sub)"); return; }
+  if (ns > 1 && !h->cut()) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": select the local subdomain first (ppmg_mesh_set_local_sub)"); return; }
   if (counts)
     for (int c = 0; c <= ns; ++c) counts[c] = 0;
   if (Np == 0) return;
   GlobalRouteParams R{};
   R.nsubs = ns;
-  for (int a = 0; a < 2; ++a) {
-    R.lo[a] = h->g.min_phys[a];
-    R.hi[a] = h->g.max_phys[a];
-    R.lof[a] = (float)R.lo[a];
-    R.hif[a] = (float)R.hi[a];
-  }
   const int nblk = route_blocks(Np);
   Workspace& ws = h->ws_map;
   const size_t ncls = (size_t)ns + 1;
   cudaError_t e;
   if ((e = ws.key.ensure((size_t)Np)) || (e = ws.count.ensure(sizeof(int) * ncls * nblk)) ||
       (e = ws.start.ensure(sizeof(int) * ncls * nblk)) ||
-      (e = ws.h_aux.ensure(sizeof(double) * 2 * (size_t)ns))) { cuda_fail(info, e, caller); return; }
-  std::vector<double> zb(2 * (size_t)ns);
-  for (int q = 0; q < ns; ++q) {
-    zb[q] = h->min_sub[3 * q + 2];
-    zb[ns + q] = h->max_sub[3 * q + 2];
-  }
+      (e = ws.h_aux.ensure(sizeof(double) * 6 * (size_t)ns))) { cuda_fail(info, e, caller); return; }
+  // the subdomain boxes, [6][ns]: min_sub x, y, z, then max_sub x, y, z
+  std::vector<double> zb(6 * (size_t)ns);
+  for (int q = 0; q < ns; ++q)
+    for (int a = 0; a < 3; ++a) {
+      zb[a * ns + q] = h->min_sub[3 * q + a];
+      zb[(3 + a) * ns + q] = h->max_sub[3 * q + a];
+    }
   double* dz = ws.h_aux.as<double>();
-  if ((e = cudaMemcpyAsync(dz, zb.data(), sizeof(double) * 2 * ns, cudaMemcpyHostToDevice, st))) { cuda_fail(info, e, caller); return; }
-  R.zlo = dz;
-  R.zhi = dz + ns;
+  if ((e = cudaMemcpyAsync(dz, zb.data(), sizeof(double) * 6 * ns, cudaMemcpyHostToDevice, st))) { cuda_fail(info, e, caller); return; }
+  R.box = dz;
   if ((e = launch_route_global<T>(R, xp, ldxp, Np, static_cast<unsigned char*>(ws.key.p),
                                   ws.count.as<int>(), ws.start.as<int>(), perm, ws, st))) {
     cuda_fail(info, e, caller);
@@ -2335,6 +2475,7 @@ void p2m_noalloc(const double* xp, int64_t ldxp, int64_t Np, const double* up, i
   P.TZ = p2m_tile_depth(3, P.N);
   P.cap = prec == P2M_FP64 ? 544 : 1088;
   P.c0 = 0;
+  P.span = cell_span(P.N);
   P.start = ws.start.as<int>();
   P.rec = ws.rec.p;
   P.us = ws.us.p;

@@ -1,8 +1,14 @@
-// ppmg_halo.cu -- the ghost exchange between z-slab subdomains: which planes
-// travel where (the blocks ppm_map_field_ghost_init.f:234-447 builds for a cut
-// along z) and the add of received blocks (ppm_map_field_pop_3d.f, pop with
-// add).  The transport that moves the blocks is the caller's.
+// ppmg_halo.cu -- the ghost exchange between subdomains: which nodes travel
+// where (the blocks ppm_map_field_ghost_init.f:234-447 builds: whole planes
+// for slabs along z, boxes per neighbour and periodic shift for cuts along
+// several axes), the packing of boxes and the add of received blocks
+// (ppm_map_field_pop_3d.f, pop with add).  The transport that moves the
+// blocks is the caller's.
 #include "ppmg_halo.cuh"
+
+#include <array>
+#include <map>
+#include <set>
 
 namespace ppmg {
 
@@ -53,25 +59,57 @@ const char* halo_plan(int nsubs, const int* istart, const int* nnodes, int Nmz, 
   return nullptr;
 }
 
+const char* check_cartesian(int nsubs, const int* istart, const int* nnodes, const int Nm[3]) {
+  if (nsubs < 1) return "no subdomain";
+  std::vector<std::vector<int>> starts(3);
+  for (int a = 0; a < 3; ++a) {
+    // an axis is cut when the subdomains do not span it; all of them agree
+    const bool cut = nnodes[a] != Nm[a];
+    std::map<int, int> iv;  // istart -> nnodes of the axis' intervals
+    for (int q = 0; q < nsubs; ++q) {
+      const int i0 = istart[3 * q + a], n = nnodes[3 * q + a];
+      if ((n != Nm[a]) != cut) return "the subdomains are not a cartesian decomposition";
+      if (n < 2 || i0 < 1) return "a subdomain has no cell along an axis";
+      auto it = iv.find(i0);
+      if (it != iv.end() && it->second != n)
+        return "the subdomains are not a cartesian decomposition";
+      iv[i0] = n;
+    }
+    // the intervals tile 1 .. Nm, each starting on the last node of the previous
+    int next = 1;
+    for (auto& kv : iv) {
+      if (kv.first != next) return "the subdomains are not a cartesian decomposition";
+      next = kv.first + kv.second - 1;
+      starts[a].push_back(kv.first);
+    }
+    if (next != Nm[a]) return "the subdomains do not cover the mesh";
+  }
+  // every combination of the axes' intervals is one subdomain
+  if ((int64_t)starts[0].size() * starts[1].size() * starts[2].size() != nsubs)
+    return "the subdomains are not a cartesian decomposition";
+  std::set<std::array<int, 3>> seen;
+  for (int q = 0; q < nsubs; ++q)
+    if (!seen.insert({istart[3 * q], istart[3 * q + 1], istart[3 * q + 2]}).second)
+      return "two subdomains share a box";
+  return nullptr;
+}
+
 const char* halo_boxes(int nsubs, const int* istart, const int* nnodes, const int Nm[3],
                        int isub, const int g[3], bool put, std::vector<HaloBox>& sends,
                        std::vector<HaloBox>& recvs) {
   sends.clear();
   recvs.clear();
   if (nsubs < 2 || isub < 0 || isub >= nsubs) return "isub / nsubs out of range";
-  // an axis is cut when the subdomains do not span it; all of them agree
+  if (const char* why = check_cartesian(nsubs, istart, nnodes, Nm)) return why;
   bool open[3];
   int64_t N[3];
   for (int a = 0; a < 3; ++a) {
     open[a] = nnodes[3 * isub + a] != Nm[a];
     N[a] = Nm[a] - 1;
     if (g[a] < 0) return "negative ghost width";
-    for (int q = 0; q < nsubs; ++q) {
-      if ((nnodes[3 * q + a] != Nm[a]) != open[a])
-        return "the subdomains are not a cartesian decomposition";
-      if (open[a] && (nnodes[3 * q + a] < 2 || g[a] > nnodes[3 * q + a] - 1))
+    for (int q = 0; q < nsubs; ++q)
+      if (open[a] && g[a] > nnodes[3 * q + a] - 1)
         return "a ghost width exceeds a subdomain's cells";
-    }
   }
   auto box = [&](int q, int a, bool ghosts, int64_t& lo, int64_t& hi) {
     if (!open[a]) {
@@ -82,12 +120,15 @@ const char* halo_boxes(int nsubs, const int* istart, const int* nnodes, const in
       hi = istart[3 * q + a] + nnodes[3 * q + a] - 1 + (ghosts ? g[a] : 0);
     }
   };
-  // block of one (sender S, receiver Rv, shift t of the receiver's real box
-  // in the sender's frame) in global node indices of the sender's frame.
-  // put: G_S and (R_Rv + tN); get: the part of (G_Rv + tN) and R_S outside
+  // block of one (sender S, receiver Rv, shift t of the receiver's box in
+  // the sender's frame) in global node indices of the sender's frame.
+  // put: G_S and (R_Rv + tN); get: the part of (G_Rv + tN) and R'_S outside
   // (R_Rv + tN), cut into at most one box per cut axis (the standard
-  // decomposition of a box minus a box), k its index.  Non-cut axes span
-  // the whole field box (their images are every subdomain's own).
+  // decomposition of a box minus a box), k its index.  R'_S is R_S without
+  // its last node along every cut axis (that node is the next subdomain's
+  // first): every node is then sent by one subdomain only, and the boxes a
+  // get receives never overlap.  Non-cut axes span the whole field box
+  // (their images are every subdomain's own).
   auto blocks = [&](int S, int Rv, const int t[3], std::vector<std::pair<int, HaloBox>>& out) {
     out.clear();
     int64_t jl[3], jh[3], rl[3], rh[3];
@@ -98,6 +139,7 @@ const char* halo_boxes(int nsubs, const int* istart, const int* nnodes, const in
         box(Rv, a, false, ql, qh);
       } else {
         box(S, a, false, sl, sh);
+        if (open[a]) --sh;
         box(Rv, a, true, ql, qh);
       }
       if (open[a]) {
@@ -203,8 +245,9 @@ const char* halo_boxes(int nsubs, const int* istart, const int* nnodes, const in
 
 namespace {
 
-// One thread per element of all boxes (boxes back to back in the buffer);
-// a box is found by binary search over the table's buffer offsets.
+// One thread per element of the launch's boxes (index space: the boxes back
+// to back in table order); a box is found by binary search over the rows'
+// first indices, and its elements sit in the buffer from the row's offset.
 template <class T>
 __global__ void k_box_copy(T* __restrict__ field, int64_t ldf, int64_t s0, int64_t s1,
                            int64_t s2, int lb0, int lb1, int lb2,
@@ -219,6 +262,7 @@ __global__ void k_box_copy(T* __restrict__ field, int64_t ldf, int64_t s0, int64
     }
     const int64_t* b = tab + 8 * lo;
     int64_t r = i - b[6];
+    const int64_t j = b[7] + r;  // the element's place in the buffer
     const int64_t c = r % ldf;
     r /= ldf;
     const int64_t x = r % b[3];
@@ -227,11 +271,11 @@ __global__ void k_box_copy(T* __restrict__ field, int64_t ldf, int64_t s0, int64
     const int64_t z = r / b[4];
     const int64_t o = (b[0] + x - lb0) * s0 + (b[1] + y - lb1) * s1 + (b[2] + z - lb2) * s2 + c;
     if (mode == kBoxPack)
-      buf[i] = field[o];
+      buf[j] = field[o];
     else if (mode == kBoxCopy)
-      field[o] = buf[i];
+      field[o] = buf[j];
     else
-      field[o] += buf[i];
+      field[o] += buf[j];
   }
 }
 

@@ -24,6 +24,13 @@ const char* halo_plan(int nsubs, const int* istart, const int* nnodes, int Nmz, 
                       int64_t ldf, const int64_t* f_lb, const int64_t* f_ub, int gz, bool put,
                       HaloPlan& out);
 
+// Whether the subdomains (istart, nnodes: [nsubs][3], 1-based) form a
+// cartesian decomposition of the mesh of Nm nodes per axis: along every axis
+// either all of them span the mesh or all are cut, the intervals tile
+// 1 .. Nm (each starting on the previous one's last node), and every
+// combination of the axes' intervals is one subdomain.  0, or why not.
+const char* check_cartesian(int nsubs, const int* istart, const int* nnodes, const int Nm[3]);
+
 // The exchange of any cartesian decomposition (cuts along one, two or three
 // axes): blocks are boxes of the local field, in its 1-based local node
 // indices (inclusive), for every neighbouring subdomain and periodic shift.
@@ -39,10 +46,12 @@ const char* halo_boxes(int nsubs, const int* istart, const int* nnodes, const in
                        std::vector<HaloBox>& recvs);
 
 // Pack the boxes of field (ldf rows per node, element strides s[3], lower
-// bounds lb[3]) into buf (boxes back to back, in table order), or unpack buf
-// into them (add: the put's pop with add; else a copy).  tab: device table
-// of 8 int64 per box (lo[3], ext[3], buffer offset, elements), nbox boxes,
-// total elements tot.
+// bounds lb[3]) into buf, or unpack buf into them (add: the put's pop with
+// add; else a copy); each box travels as all ldf rows of its nodes, x
+// fastest.  tab: device table of 8 int64 per box (lo[3], ext[3], the box's
+// first index in the launch's index space -- the boxes back to back in table
+// order, tot elements in all -- and its offset in buf), nbox boxes.  The
+// boxes of one launch must not overlap unless every one only reads field.
 template <class T>
 cudaError_t launch_box_copy(T* field, int64_t ldf, const int64_t s[3], const int lb[3],
                             const int64_t* tab, int nbox, int64_t tot, T* buf, int mode,

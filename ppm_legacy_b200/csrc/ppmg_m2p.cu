@@ -17,10 +17,10 @@ namespace ppmg {
 
 namespace {
 
-// 0-based node plane of stencil plane z: periodic wrap, or (a z-slab) the
-// plane itself, ghost planes included
-__device__ __forceinline__ int zplane(const M2PParams& P, int z) {
-  return P.open_z ? z : wrap_index(z, P.N[2]);
+// 0-based node of stencil node n along axis a: periodic wrap, or (a cut
+// axis) the node itself, ghost nodes included
+__device__ __forceinline__ int node_at(const M2PParams& P, int a, int n) {
+  return P.open[a] ? n : wrap_index(n, P.N[a]);
 }
 
 template <int S, class CT, bool EXACT>
@@ -94,9 +94,9 @@ __global__ void __launch_bounds__(256) k_m2p3d(M2PParams P) {
   int64_t ox[S], oy[S], oz[S];
 #pragma unroll
   for (int i = 0; i < S; ++i) {
-    ox[i] = (int64_t)(wrap_index(cx - (HL - 1) + i, P.N[0]) + 1 - P.fd.lb[0]) * P.fd.s[0];
-    oy[i] = (int64_t)(wrap_index(cy - (HL - 1) + i, P.N[1]) + 1 - P.fd.lb[1]) * P.fd.s[1];
-    oz[i] = (int64_t)(zplane(P, cz - (HL - 1) + i) + 1 - P.fd.lb[2]) * P.fd.s[2];
+    ox[i] = (int64_t)(node_at(P, 0, cx - (HL - 1) + i) + 1 - P.fd.lb[0]) * P.fd.s[0];
+    oy[i] = (int64_t)(node_at(P, 1, cy - (HL - 1) + i) + 1 - P.fd.lb[1]) * P.fd.s[1];
+    oz[i] = (int64_t)(node_at(P, 2, cz - (HL - 1) + i) + 1 - P.fd.lb[2]) * P.fd.s[2];
   }
   const FT* F = static_cast<const FT*>(P.field);
   FT* up = static_cast<FT*>(P.up) + (int64_t)P.idx[s] * P.ldup;
@@ -200,9 +200,9 @@ __global__ void __launch_bounds__(256) k_adjoint3d(M2PParams P) {
   int64_t ox[S], oy[S], oz[S];
 #pragma unroll
   for (int i = 0; i < S; ++i) {
-    ox[i] = (int64_t)(wrap_index(cx - (HL - 1) + i, P.N[0]) + 1 - P.fd.lb[0]) * P.fd.s[0];
-    oy[i] = (int64_t)(wrap_index(cy - (HL - 1) + i, P.N[1]) + 1 - P.fd.lb[1]) * P.fd.s[1];
-    oz[i] = (int64_t)(zplane(P, cz - (HL - 1) + i) + 1 - P.fd.lb[2]) * P.fd.s[2];
+    ox[i] = (int64_t)(node_at(P, 0, cx - (HL - 1) + i) + 1 - P.fd.lb[0]) * P.fd.s[0];
+    oy[i] = (int64_t)(node_at(P, 1, cy - (HL - 1) + i) + 1 - P.fd.lb[1]) * P.fd.s[1];
+    oz[i] = (int64_t)(node_at(P, 2, cz - (HL - 1) + i) + 1 - P.fd.lb[2]) * P.fd.s[2];
   }
   const double* F = static_cast<const double*>(P.field);
   const int64_t p = P.idx[s];
@@ -292,9 +292,9 @@ constexpr size_t m2p_ring_bytes() {
          LC * sizeof(CT);
 }
 
-// OZ: a z-slab subdomain (P.open_z), compiled apart so that the periodic
-// gather keeps its plane loads unconditional.
-template <int S, class CT, bool EXACT, class FT, int LC, bool ADJ = false, bool OZ = false>
+// OPEN: a subdomain cut along some axis (P.open), compiled apart so that
+// the periodic gather keeps its column and plane loads unconditional.
+template <int S, class CT, bool EXACT, class FT, int LC, bool ADJ = false, bool OPEN = false>
 __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
   using V = typename Vec4<CT>::type;
   constexpr int HL = S / 2;
@@ -327,18 +327,26 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
   // global offset of node column q of plane z (component c0)
   auto col_off = [&](int q, int64_t oz) {
     const int r = q / WX, qx = q - r * WX;
-    const int xw = wrap_index(X0 - (HL - 1) + qx, P.N[0]);
-    const int yw = wrap_index(Y0 - (HL - 1) + r, P.N[1]);
+    int xw = X0 - (HL - 1) + qx, yw = Y0 - (HL - 1) + r;
+    if (!OPEN || !P.open[0]) xw = wrap_index(xw, P.N[0]);
+    if (!OPEN || !P.open[1]) yw = wrap_index(yw, P.N[1]);
     return (int64_t)(xw + 1 - P.fd.lb[0]) * P.fd.s[0] +
            (int64_t)(yw + 1 - P.fd.lb[1]) * P.fd.s[1] + oz + P.c0;
   };
   auto plane_oz = [&](int z) {
-    return (int64_t)((OZ ? z : wrap_index(z, P.N[2])) + 1 - P.fd.lb[2]) * P.fd.s[2];
+    return (int64_t)((OPEN && P.open[2] ? z : wrap_index(z, P.N[2])) + 1 - P.fd.lb[2]) *
+           P.fd.s[2];
   };
-  // a z-slab loads only the planes its cell layers 0 .. N2-1 read (a step
-  // past the last layer would reach one plane beyond the required box)
-  auto plane_ok = [&](int z) {
-    return !OZ || (z >= -(HL - 1) && z <= P.N[2] - 1 + HL);
+  // along a cut axis only the nodes the cells 0 .. N-1 reach are read (the
+  // columns of a tile past the last cell, and a step past the last layer,
+  // would reach beyond the required box)
+  auto in_reach = [&](int a, int n) { return n >= -(HL - 1) && n <= P.N[a] - 1 + HL; };
+  auto plane_ok = [&](int z) { return !OPEN || !P.open[2] || in_reach(2, z); };
+  auto col_ok = [&](int q) {
+    if (!OPEN) return true;
+    const int r = q / WX, qx = q - r * WX;
+    return (!P.open[0] || in_reach(0, X0 - (HL - 1) + qx)) &&
+           (!P.open[1] || in_reach(1, Y0 - (HL - 1) + r));
   };
   // row ranges of cell layers cz .. cz+LPS-1: thread 16 l + r loads row r of
   // layer cz + l
@@ -379,8 +387,13 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
     const int slot = wrap_index(z, R);
     const int64_t oz = plane_oz(z);
     for (int q = tid; q < NCOL; q += 256) {
-      const int64_t o = col_off(q, oz);
       CT* d = ring + (size_t)q * CS + slot * LC;
+      if (!col_ok(q)) {
+#pragma unroll
+        for (int a = 0; a < LC; ++a) d[a] = CT(0);
+        continue;
+      }
+      const int64_t o = col_off(q, oz);
 #pragma unroll
       for (int a = 0; a < LC; ++a) d[a] = (CT)__ldg(F + o + a);
     }
@@ -408,11 +421,11 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
 #pragma unroll
         for (int k = 0; k < PER; ++k) {
           const int q = tid + 256 * k;
-          if constexpr (OZ) {
+          if constexpr (OPEN) {
 #pragma unroll
             for (int a = 0; a < LC; ++a) pre[l][k][a] = CT(0);
           }
-          if (q < NCOL && ok) {
+          if (q < NCOL && ok && col_ok(q)) {
             const int64_t o = col_off(q, oz);
 #pragma unroll
             for (int a = 0; a < LC; ++a) pre[l][k][a] = (CT)__ldg(F + o + a);
@@ -588,7 +601,7 @@ __global__ void __launch_bounds__(256) k_m2p3d_tile(M2PParams P) {
 template <int S, class CT, bool EXACT, class FT>
 cudaError_t launch_tile_lc(const M2PParams& P, int lc, cudaStream_t st) {
   auto go = [&](auto kern, auto kern_oz, size_t smem) {
-    auto k = P.open_z ? kern_oz : kern;
+    auto k = P.open[0] || P.open[1] || P.open[2] ? kern_oz : kern;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e) return e;
@@ -663,8 +676,9 @@ cudaError_t launch_m2p(const M2PParams& P0, int dim, int kernel, M2PPrec prec, c
 
 template <int S, class CT, int LC>
 cudaError_t launch_adjoint_tile(const M2PParams& P, cudaStream_t st) {
-  auto kern = P.open_z ? k_m2p3d_tile<S, CT, false, double, LC, true, true>
-                       : k_m2p3d_tile<S, CT, false, double, LC, true>;
+  auto kern = P.open[0] || P.open[1] || P.open[2]
+                  ? k_m2p3d_tile<S, CT, false, double, LC, true, true>
+                  : k_m2p3d_tile<S, CT, false, double, LC, true>;
   const size_t smem = m2p_ring_bytes<S, CT, LC>();
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);

@@ -23,7 +23,7 @@ struct M2PParams {
   int64_t ldup;
   int lda;
   int c0;             // first component of this launch (tile kernel)
-  int open_z;         // z-slab subdomain: node planes read without periodic wrap in z
+  int open[3];        // cut axes: nodes read without periodic wrap (ghosts included)
   // 3D tile kernel: cell offsets and work items
   const int* start;
   const int4* items;

@@ -96,40 +96,37 @@ __global__ void __launch_bounds__(kRouteThreads) k_route_scatter(const unsigned 
   }
 }
 
-// Global routing: the class of every item is its slab (the reference tests
-// the subdomains from the last to the first, ppm_map_part_global.f:355-420;
-// slabs do not overlap, so the first hit is the only one) or nsubs.
+// Global routing: the class of every item is its subdomain (the reference
+// tests the subdomains from the last to the first, ppm_map_part_global.f:355-420;
+// the boxes do not overlap, so the first hit is the only one) or nsubs.
 template <class T>
 __global__ void __launch_bounds__(kRouteThreads) k_groute_count(GlobalRouteParams R,
                                                                 const T* xp, int64_t ldxp,
                                                                 int64_t np, unsigned char* dest,
                                                                 int* bc, int nblk) {
-  constexpr bool F = sizeof(T) == 4;
   __shared__ int cnt[kMaxGlobalSubs + 1];
-  __shared__ T zl[kMaxGlobalSubs], zh[kMaxGlobalSubs];
+  __shared__ T bl[3][kMaxGlobalSubs], bh[3][kMaxGlobalSubs];
   const int ncls = R.nsubs + 1;
   for (int c = threadIdx.x; c < ncls; c += kRouteThreads) cnt[c] = 0;
-  for (int q = threadIdx.x; q < R.nsubs; q += kRouteThreads) {
-    zl[q] = (T)R.zlo[q];  // the positions' own precision, as the reference compares
-    zh[q] = (T)R.zhi[q];
-  }
+  for (int q = threadIdx.x; q < R.nsubs; q += kRouteThreads)
+    for (int a = 0; a < 3; ++a) {
+      // the positions' own precision, as the reference compares
+      bl[a][q] = (T)R.box[a * R.nsubs + q];
+      bh[a][q] = (T)R.box[(3 + a) * R.nsubs + q];
+    }
   __syncthreads();
   const int64_t b0 = (int64_t)blockIdx.x * kRouteChunk;
   const int64_t b1 = min(np, b0 + kRouteChunk);
   for (int64_t i = b0 + threadIdx.x; i < b1; i += kRouteThreads) {
     const T* x = xp + i * ldxp;
-    bool inxy = true;
-    for (int a = 0; a < 2; ++a) {
-      const T lo = F ? (T)R.lof[a] : (T)R.lo[a], hi = F ? (T)R.hif[a] : (T)R.hi[a];
-      inxy = inxy && x[a] >= lo && x[a] < hi;
-    }
+    const T x0 = x[0], x1 = x[1], x2 = x[2];
     int c = R.nsubs;
-    if (inxy)
-      for (int q = R.nsubs - 1; q >= 0; --q)
-        if (x[2] >= zl[q] && x[2] < zh[q]) {
-          c = q;
-          break;
-        }
+    for (int q = R.nsubs - 1; q >= 0; --q)
+      if (x0 >= bl[0][q] && x0 < bh[0][q] && x1 >= bl[1][q] && x1 < bh[1][q] &&
+          x2 >= bl[2][q] && x2 < bh[2][q]) {
+        c = q;
+        break;
+      }
     dest[i] = (unsigned char)c;
     atomicAdd(&cnt[c], 1);
   }

@@ -25,20 +25,16 @@ cudaError_t launch_route(const RouteParams& R, const T* xp, int64_t ldxp, int64_
                          unsigned char* dest, int* bc, int* off, int* perm, Workspace& ws,
                          cudaStream_t st);
 
-// Global routing (ppm_map_part_global): every particle to the z-slab that
-// contains it among all nsubs slabs (<= kMaxGlobalSubs), x and y inside
-// [lo, hi); slab s spans [zlo[s], zhi[s]) (device arrays).  Class nsubs:
-// in no slab.  perm (np ints) receives the ids grouped by class 0..nsubs,
+// Global routing (ppm_map_part_global): every particle to the subdomain
+// that contains it among all nsubs (<= kMaxGlobalSubs), subdomain s spanning
+// [min_sub, max_sub) on every axis (R.box).  Class nsubs: in no subdomain.  perm (np ints) receives the ids grouped by class 0..nsubs,
 // each class in ascending id; off (device, (nsubs + 1) * route_blocks(np))
 // ends holding the exclusive class-major offsets, so class c starts at
 // off[c * nblk].
 constexpr int kMaxGlobalSubs = 255;
 struct GlobalRouteParams {
   int nsubs;
-  double lo[2], hi[2];
-  float lof[2], hif[2];
-  const double* zlo;
-  const double* zhi;
+  const double* box;  // device [6][nsubs]: min_sub x, y, z, then max_sub x, y, z
 };
 template <class T>
 cudaError_t launch_route_global(const GlobalRouteParams& R, const T* xp, int64_t ldxp,

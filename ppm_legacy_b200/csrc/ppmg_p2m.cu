@@ -54,8 +54,8 @@ __device__ __forceinline__ void emit_node(const P2MParams& P, int x, int y, int 
   for (int a = 0; a < DIM; ++a) {
     // 1-based images n+1+t*N within [box_lo, box_hi]
     const int N = P.N[a];
-    if (a == 2 && P.open_z) {
-      // no periodic images along an open axis: the node itself
+    if (P.open[a]) {
+      // no periodic images along a cut axis: the node itself
       lo[a] = hi[a] = 0;
     } else if (P.fd.box_lo[a] > 1 - N && P.fd.box_hi[a] < 2 * N + 1) {
       // ghost layers narrower than the mesh: t in {-1, 0, 1}
@@ -204,9 +204,10 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
 
   if ((int)blockIdx.x >= *P.nitems) return;
   const int4 it = P.items[blockIdx.x];
-  const int tiles_x = (P.N[0] + kTileX - 1) / kTileX;
-  const int X0 = (it.x % tiles_x) * kTileX;
-  const int Y0 = (it.x / tiles_x) * kTileY;
+  const int tiles_x = (P.span.ext[0] + kTileX - 1) / kTileX;
+  const int X0 = P.span.org[0] + (it.x % tiles_x) * kTileX;
+  const int Y0 = P.span.org[1] + (it.x / tiles_x) * kTileY;
+  const int XE = P.span.org[0] + P.span.ext[0], YE = P.span.org[1] + P.span.ext[1];
   const int Z0 = it.y, Z1 = it.z;
   const int cap = P.cap;
 
@@ -229,8 +230,8 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
   const int tid = threadIdx.x;
   const int tx = tid % kTX, ty = tid / kTX;
   const int x0 = X0 + 2 * tx, y = Y0 + ty;
-  const bool act0 = x0 < P.N[0] && y < P.N[1];
-  const bool act1 = x0 + 1 < P.N[0] && y < P.N[1];
+  const bool act0 = x0 < XE && y < YE;
+  const bool act1 = x0 + 1 < XE && y < YE;
   const uint4* grec = static_cast<const uint4*>(P.rec);
   const uint4* gus = static_cast<const uint4*>(P.us);
 
@@ -246,17 +247,21 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
   // cell offsets of the staged cells of layer cz, kept in registers until published
   int pb[PERC], pe[PERC];
   auto load_counts = [&](int cz) {
-    // open z: the layers outside the slab hold no particles of this subdomain
-    const bool empty = P.open_z && (cz < 0 || cz >= P.N[2]);
+    // along a cut axis the cells outside 0 .. N-1 hold no particles of
+    // this subdomain
+    const bool empty = P.open[2] && (cz < 0 || cz >= P.N[2]);
     const int czw = empty ? 0 : wrap_index(cz, P.N[2]);
 #pragma unroll
     for (int k = 0; k < PERC; ++k) {
       const int q = tid + NT * k;
       pb[k] = pe[k] = 0;
-      if (q < NSC && !empty) {
-        const int r = q / WX, qx = q - r * WX;
-        const int cx = wrap_index(X0 - HL + qx, P.N[0]);
-        const int cy = wrap_index(Y0 - HL + r, P.N[1]);
+      const int r = q / WX, qx = q - r * WX;
+      const int ux = X0 - HL + qx, uy = Y0 - HL + r;
+      const bool out = (P.open[0] && (ux < 0 || ux >= P.N[0])) ||
+                       (P.open[1] && (uy < 0 || uy >= P.N[1]));
+      if (q < NSC && !empty && !out) {
+        const int cx = wrap_index(ux, P.N[0]);
+        const int cy = wrap_index(uy, P.N[1]);
         const int64_t c = (int64_t)cx + (int64_t)P.N[0] * (cy + (int64_t)P.N[1] * czw);
         pb[k] = P.start[c];
         pe[k] = P.start[c + 1];
@@ -520,17 +525,21 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
   }
 }
 
-// Per (xy tile, cell layer): particles in the tile's own cells of that layer.
-__global__ void k_layer_counts(const int* __restrict__ start, int N0, int N1, int N2,
-                               int tiles_x, int ntiles, int* __restrict__ lc) {
+// Per (xy tile, cell layer): particles in the tile's own cells of that layer
+// (tiles of the span from (ox, oy), ex x ey nodes; cells outside 0 .. N-1
+// count none).
+__global__ void k_layer_counts(const int* __restrict__ start, int N0, int N1, int N2, int ox,
+                               int oy, int ex, int ey, int tiles_x, int ntiles,
+                               int* __restrict__ lc) {
   const int64_t n = (int64_t)ntiles * N2;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const int tile = (int)(i / N2), cz = (int)(i % N2);
-    const int X0 = (tile % tiles_x) * kTileX, X1 = min(X0 + kTileX, N0);
-    const int Y0 = (tile / tiles_x) * kTileY, Y1 = min(Y0 + kTileY, N1);
+    const int tx0 = ox + (tile % tiles_x) * kTileX, ty0 = oy + (tile / tiles_x) * kTileY;
+    const int X0 = max(tx0, 0), X1 = min(min(tx0 + kTileX, ox + ex), N0);
+    const int Y0 = max(ty0, 0), Y1 = min(min(ty0 + kTileY, oy + ey), N1);
     int sum = 0;
-    for (int y = Y0; y < Y1; ++y) {
+    for (int y = Y0; y < Y1 && X0 < X1; ++y) {
       const int64_t c0 = (int64_t)X0 + (int64_t)N0 * (y + (int64_t)N1 * cz);
       sum += start[c0 + (X1 - X0)] - start[c0];
     }
@@ -799,43 +808,51 @@ int p2m_tile_depth(int dim, const int N[3]) {
   return tz < 8 ? (N[1] < 8 ? N[1] : 8) : tz;
 }
 
+TileSpan cell_span(const int N[3]) {
+  TileSpan sp;
+  for (int a = 0; a < 3; ++a) {
+    sp.org[a] = 0;
+    sp.ext[a] = N[a];
+  }
+  return sp;
+}
+
 namespace {
 constexpr int kMinTZ = 8, kMaxTZ = 64;
-int tiles_xy(const int N[3]) {
-  return ((N[0] + kTileX - 1) / kTileX) * ((N[1] + kTileY - 1) / kTileY);
+int tiles_xy(const TileSpan& sp) {
+  return ((sp.ext[0] + kTileX - 1) / kTileX) * ((sp.ext[1] + kTileY - 1) / kTileY);
 }
-int item_capacity(const int N[3], int ze) {
-  if (ze <= 0) ze = N[2];
-  return tiles_xy(N) * ((ze + kMinTZ - 1) / kMinTZ) + 1;
+int item_capacity(const TileSpan& sp) {
+  return tiles_xy(sp) * ((sp.ext[2] + kMinTZ - 1) / kMinTZ) + 1;
 }
+TileSpan span_of(const int N[3], const TileSpan* sp) { return sp ? *sp : cell_span(N); }
 }  // namespace
 
 // Layout: items[cap] | nitems (64 bytes) | unordered items[cap] | layer counts
-size_t tile_items_bytes(const int N[3], int ze) {
-  return 2 * sizeof(int4) * (size_t)item_capacity(N, ze) +
-         sizeof(int) * (size_t)tiles_xy(N) * N[2] + 64;
+size_t tile_items_bytes(const int N[3], const TileSpan* sp) {
+  const TileSpan s = span_of(N, sp);
+  return 2 * sizeof(int4) * (size_t)item_capacity(s) +
+         sizeof(int) * (size_t)tiles_xy(s) * N[2] + 64;
 }
 
-size_t p2m_scratch_bytes(int dim, const int N[3], int ze) {
-  return dim == 3 ? tile_items_bytes(N, ze) : 16;
+size_t p2m_scratch_bytes(int dim, const int N[3], const TileSpan* sp) {
+  return dim == 3 ? tile_items_bytes(N, sp) : 16;
 }
 
-TileItems tile_items_view(void* scratch, const int N[3], int ze) {
+TileItems tile_items_view(void* scratch, const int N[3], const TileSpan* sp) {
   TileItems t;
-  t.cap = item_capacity(N, ze);
+  t.cap = item_capacity(span_of(N, sp));
   t.items = static_cast<const int4*>(scratch);
   t.nitems = reinterpret_cast<const int*>(t.items + t.cap);
   return t;
 }
 
 cudaError_t make_tile_items(const int* start, const int N[3], int64_t nvalid, void* scratch,
-                            TileItems& out, cudaStream_t st, int zlo, int ze) {
-  if (ze <= 0) {
-    zlo = 0;
-    ze = N[2];
-  }
-  const int nt = tiles_xy(N);
-  const int cap_items = item_capacity(N, ze);
+                            TileItems& out, cudaStream_t st, const TileSpan* sp) {
+  const TileSpan s = span_of(N, sp);
+  const int zlo = s.org[2], ze = s.ext[2];
+  const int nt = tiles_xy(s);
+  const int cap_items = item_capacity(s);
   int4* items = static_cast<int4*>(scratch);
   int* nitems = reinterpret_cast<int*>(items + cap_items);
   int4* unordered = reinterpret_cast<int4*>(nitems + 16);
@@ -844,8 +861,8 @@ cudaError_t make_tile_items(const int* start, const int N[3], int64_t nvalid, vo
   if (e) return e;
   const int64_t nl = (int64_t)nt * N[2];
   const int gl = (int)((nl + 255) / 256 < 148 * 32 ? (nl + 255) / 256 : 148 * 32);
-  k_layer_counts<<<gl, 256, 0, st>>>(start, N[0], N[1], N[2], (N[0] + kTileX - 1) / kTileX, nt,
-                                     lc);
+  k_layer_counts<<<gl, 256, 0, st>>>(start, N[0], N[1], N[2], s.org[0], s.org[1], s.ext[0],
+                                     s.ext[1], (s.ext[0] + kTileX - 1) / kTileX, nt, lc);
   const int64_t tgt64 = nvalid / (148 * 2 * 8);
   const int target = (int)(tgt64 < 4096 ? 4096 : (tgt64 > (1 << 30) ? (1 << 30) : tgt64));
   k_make_items<<<(nt + 127) / 128, 128, 0, st>>>(lc, N[2], zlo, ze, nt, target, kMinTZ, kMaxTZ,
@@ -866,9 +883,7 @@ cudaError_t launch_p2m(const P2MParams& P0, int dim, int kernel, P2MPrec prec, i
   if (dim == 3) {
     // work items: xy tiles split along z into segments of similar particle count
     TileItems ti;
-    if ((e = make_tile_items(P0.start, P0.N, nvalid, scratch, ti, st, P0.open_z ? P0.zlo : 0,
-                             P0.open_z ? P0.ze : 0)))
-      return e;
+    if ((e = make_tile_items(P0.start, P0.N, nvalid, scratch, ti, st, &P0.span))) return e;
     Pw.items = ti.items;
     Pw.nitems = ti.nitems;
     Pw.item_cap = ti.cap;

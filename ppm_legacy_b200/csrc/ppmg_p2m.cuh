@@ -11,6 +11,16 @@ enum P2MPrec {
   P2M_FP32 = 2,   // single-precision API: FP32 throughout
 };
 
+// The 0-based node range org .. org+ext-1 per axis that a 3D tile grid
+// covers: the unique nodes 0 .. N-1 of a periodic axis (org 0, ext N), the
+// whole written box -g .. N+g of a cut axis (an axis along which the local
+// subdomain is one interval of several: no periodic images, cell layers
+// outside 0 .. N-1 hold none of its particles).
+struct TileSpan {
+  int org[3], ext[3];
+};
+TileSpan cell_span(const int N[3]);
+
 struct P2MParams {
   int N[3];            // cells per axis
   int TZ;              // tile depth along the sweep axis (z in 3D, y in 2D)
@@ -26,15 +36,15 @@ struct P2MParams {
   const int4* items;
   const int* nitems;
   int item_cap;
-  // open z (a z-slab subdomain): cell layers outside [0, N[2]) are empty,
-  // nodes have no periodic images along z, and the work items cover the
-  // ze node planes zlo .. zlo+ze-1 (0-based) of the written box
-  int open_z, zlo, ze;
+  // cut axes (open[a]: the subdomain is one interval of several along a)
+  // and the node range the work items cover (cell_span(N) without cuts)
+  int open[3];
+  TileSpan span;
 };
 
-// Device scratch launch_p2m needs (work items, per-layer counts); ze: node
-// planes the items cover (<= 0: N[2]).
-size_t p2m_scratch_bytes(int dim, const int N[3], int ze = 0);
+// Device scratch launch_p2m needs (work items, per-layer counts); sp: the
+// node range the items cover (nullptr: cell_span(N)).
+size_t p2m_scratch_bytes(int dim, const int N[3], const TileSpan* sp = nullptr);
 
 // Work items of the 3D tile kernels: (xy tile of kTileX x kTileY cells,
 // z0, z1) with z ranges split so every item holds a similar particle count.
@@ -43,13 +53,13 @@ struct TileItems {
   const int* nitems;  // device count
   int cap;            // grid size to launch (items beyond *nitems exit)
 };
-size_t tile_items_bytes(const int N[3], int ze = 0);
+size_t tile_items_bytes(const int N[3], const TileSpan* sp = nullptr);
 // The items a previous make_tile_items left in `scratch`.
-TileItems tile_items_view(void* scratch, const int N[3], int ze = 0);
-// Items over the z planes zlo .. zlo+ze-1 (ze <= 0: the cell layers 0 .. N[2]-1);
-// planes outside the cell layers count no particles.
+TileItems tile_items_view(void* scratch, const int N[3], const TileSpan* sp = nullptr);
+// Items over the xy tiles and z planes of the span sp (nullptr: the cells
+// 0 .. N-1); nodes outside the cells count no particles.
 cudaError_t make_tile_items(const int* start, const int N[3], int64_t nvalid, void* scratch,
-                            TileItems& out, cudaStream_t st, int zlo = 0, int ze = 0);
+                            TileItems& out, cudaStream_t st, const TileSpan* sp = nullptr);
 
 // Tile depth (nodes along the sweep axis per CTA) of the 2D gather.
 int p2m_tile_depth(int dim, const int N[3]);

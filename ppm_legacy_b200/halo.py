@@ -92,7 +92,45 @@ def _check(base, lbz, nz, g):
         raise ValueError("z ghost width exceeds the slab's cell layers")
 
 
+def is_slab_topology(topo) -> bool:
+    """Whether every subdomain spans x and y (cuts along z only)."""
+    return all(int(topo.nnodes[s, a]) == int(topo.Nm[a])
+               for s in range(topo.nsubs) for a in range(2))
+
+
+def _exchange_boxes(fields, topo, ghost, field_lb, comm, put: bool):
+    """The exchange of a decomposition cut along x or y as well: the boxes of
+    ppmg_halo_plan_boxes, every send packed before any receive is applied,
+    receives applied in the plan's order (adds of the put in that order)."""
+    sends, recvs = [], []
+    for s, f in fields.items():
+        base = _base(f)
+        lbv = field_lb[s] if isinstance(field_lb, dict) else field_lb
+        lb = [int(v) for v in lbv]
+        ext = [base.shape[3], base.shape[2], base.shape[1]]  # x, y, z nodes
+
+        def view(lo, hi, base=base, lb=lb, ext=ext):
+            for a in range(3):
+                if lo[a] < lb[a] or hi[a] > lb[a] + ext[a] - 1:
+                    raise ValueError("field_up bounds do not cover the ghost layers")
+            return base[0, lo[2] - lb[2]:hi[2] - lb[2] + 1, lo[1] - lb[1]:hi[1] - lb[1] + 1,
+                        lo[0] - lb[0]:hi[0] - lb[0] + 1]
+        p = plan_boxes(topo, s, [int(v) for v in ghost], put)
+        for peer, tag, lo, hi in p["send"]:
+            sends.append((s, peer, tag, view(lo, hi).clone()))
+        for peer, tag, lo, hi in p["recv"]:
+            recvs.append((s, peer, tag, view(lo, hi)))
+    got = comm.exchange(sends, recvs)
+    for (_, _, _, target), blk in zip(recvs, got):
+        if put:
+            target.add_(blk)
+        else:
+            target.copy_(blk)
+
+
 def _exchange(fields, topo, ghost, field_lb, comm, put: bool):
+    if not is_slab_topology(topo):
+        return _exchange_boxes(fields, topo, ghost, field_lb, comm, put)
     g = int(ghost[2]) if len(ghost) > 2 else int(ghost[-1])
     sends, recvs = [], []
     for s, f in fields.items():
@@ -126,13 +164,15 @@ def _exchange(fields, topo, ghost, field_lb, comm, put: bool):
 
 
 def put(fields: dict, topo, ghost, field_lb, comm) -> None:
-    """Ghost put between slabs: fields {isub: field_up} held by this process,
-    field_lb their lower bounds (one triple, or {isub: triple})."""
+    """Ghost put between subdomains: fields {isub: field_up} held by this
+    process, field_lb their lower bounds (one triple, or {isub: triple}).
+    Slabs along z exchange whole planes; other cartesian cuts the boxes of
+    plan_boxes."""
     _exchange(fields, topo, ghost, field_lb, comm, True)
 
 
 def get(fields: dict, topo, ghost, field_lb, comm) -> None:
-    """Ghost get between slabs (fills the z ghost planes)."""
+    """Ghost get between subdomains (fills the ghost layers of the cut axes)."""
     _exchange(fields, topo, ghost, field_lb, comm, False)
 
 

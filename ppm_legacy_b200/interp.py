@@ -99,15 +99,17 @@ def _split(up, args, name):
 
 
 def _slab_exchange(field_up, topo_id, mesh_id, ghostsize, lb, put):
-    """The z ghost exchange of a slab handle (every rank takes it, also after
-    a local error, so that no neighbour waits for a message never sent)."""
+    """The ghost exchange of a handle on one subdomain of several (every rank
+    takes it, also after a local error, so that no neighbour waits for a
+    message never sent)."""
     t, isub = _topo.local_sub(topo_id, mesh_id)
     fn = halo.put if put else halo.get
     fn({isub: field_up}, t, list(ghostsize), [int(v) for v in lb], halo.comm_for(topo_id, mesh_id))
 
 
 def _python_exchange(topo_id, mesh_id):
-    """A slab handle whose exchange runs in Python (ppm_legacy_b200.halo):
+    """A handle on one subdomain of several whose exchange runs in Python
+    (ppm_legacy_b200.halo):
     one without a transport registered in the library (halo.CTransport),
     whose C calls then leave the exchange to their caller."""
     return _topo.is_slab(topo_id, mesh_id) and not halo.has_c_transport(topo_id, mesh_id)
@@ -116,7 +118,7 @@ def _python_exchange(topo_id, mesh_id):
 def ppm_interp_p2m(xp, Np, up, *args, field_lb=None, exchange=True):
     """ppm_interp_p2m(xp, Np, up, [lda,] topo_id, mesh_id, kernel, ghostsize, field_up).
 
-    On a z-slab handle the ghost put with the neighbouring slabs follows the
+    On one subdomain of several the ghost put with the neighbours follows the
     local deposit (as the reference's P2M ends with ppm_map_field_ghost put);
     exchange=False leaves it to the caller (halo.put).
     """
@@ -176,9 +178,10 @@ def ppm_interp_p2m_adjoint(xp, Np, up, lda, topo_id, mesh_id, kernel, r_field, d
                            ghostsize=(0, 0, 0), field_lb=None, exchange=True):
     """Adjoint of P2M (3D, FP64): dw = M2P(r), dx = sum_a up(a) grad_x W . r(a).
 
-    On a z-slab handle the adjoint of P2M's ghost put is a ghost get: r's z
-    ghost planes are filled from the neighbouring slabs first (exchange=False:
-    the caller's); r then needs z ghost layers (ghostsize / field_lb).
+    On one subdomain of several the adjoint of P2M's ghost put is a ghost
+    get: r's ghost layers along the cut axes are filled from the neighbours
+    first (exchange=False: the caller's); r then needs those ghost layers
+    (ghostsize / field_lb).
     """
     _check(xp, up, r_field, dw, dx)
     lb, ub = _bounds(r_field, 3, True, ghostsize, field_lb)
@@ -206,8 +209,8 @@ def ppm_map_field_ghost(field_up, *args, field_lb=None):
 
     maptype ppm_param_map_ghost_get or ppm_param_map_ghost_put; the
     init/push/send/pop steps of the reference happen inside the call.  On a
-    z-slab handle this is the exchange with the neighbouring slabs
-    (ppm_legacy_b200.halo); x and y are periodic within the slab.
+    handle on one subdomain of several this is the exchange with the
+    neighbours (ppm_legacy_b200.halo); uncut axes are periodic within it.
     """
     if len(args) == 5:
         lda, topo_id, mesh_id, ghostsize, maptype = args
@@ -286,8 +289,8 @@ def ppm_rmsh_remesh(xp, Np, up, *args, field_lb=None, exchange=True):
     preallocated by the caller (the reference's ppm_alloc grow step) and is
     overwritten entirely (zeroed, then the remeshed field).  float32 arrays
     select the single-precision variants (_ss/_sv), which need weights from
-    a single-precision ppm_rmsh_comp_weights.  On a z-slab handle the ghost
-    put with the neighbouring slabs follows (exchange=False: the caller's).
+    a single-precision ppm_rmsh_comp_weights.  On one subdomain of several
+    the ghost put with the neighbours follows (exchange=False: the caller's).
     """
     vector, lda, topo_id, mesh_id, kernel, ghostsize, field_up = _split(up, args, "ppm_rmsh_remesh")
     _check(xp, up, field_up)

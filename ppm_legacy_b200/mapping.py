@@ -164,8 +164,9 @@ TAG_GSIZE, TAG_GDATA = 80, 100
 
 
 def device_route_global(topo_id, mesh_id, xp, nsubs):
-    """(info, perm, [count to slab 0 .. nsubs-1, count in no slab]) of the
-    slab's particles (ppmg_map_part_global_route on the current stream)."""
+    """(info, perm, [count to subdomain 0 .. nsubs-1, count in none]) of the
+    local subdomain's particles (ppmg_map_part_global_route on the current
+    stream)."""
     import torch
     n = int(xp.shape[1])
     perm = torch.empty(max(n, 1), dtype=torch.int32, device=xp.device)

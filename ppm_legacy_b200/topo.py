@@ -121,7 +121,9 @@ def local_sub(topo_id: int, mesh_id: int):
 
 
 def is_slab(topo_id: int, mesh_id: int) -> bool:
-    """Whether the handle computes on one z-slab of a decomposed domain."""
+    """Whether the handle computes on one subdomain of several (a z-slab or
+    any other cartesian cut): its exchange with the neighbours is then the
+    caller's, or the registered transport's."""
     r = local_sub(topo_id, mesh_id)
     return r is not None and r[0].nsubs > 1
 
@@ -130,7 +132,7 @@ def register(topo: Topology, isub=None) -> int:
     """Hand the geometry to libppmg (ppmg_mesh_register); returns info.
 
     isub: the subdomain this process's GPU computes on (needed when the
-    topology has several subdomains: a decomposition into z-slabs).
+    topology has several subdomains: a cartesian decomposition).
     """
     import ctypes as C
 

@@ -150,8 +150,8 @@ def test_slab_particle_outside_its_slab_is_unassigned():
 
 
 def test_slab_handle_refuses_other_routines():
-    """The C-ABI ghost mapping leaves the exchange between slabs to the host;
-    only z-slab decompositions are accepted."""
+    """Without a transport the C-ABI ghost mapping leaves the exchange between
+    slabs to the host; cartesian decompositions are accepted, others not."""
     import ctypes as C
     from ppm_legacy_b200._lib import int_array
     t = topo_for(3, 12, decomp=(1, 1, 2))
@@ -161,14 +161,23 @@ def test_slab_handle_refuses_other_routines():
     ppmg.lib().ppmg_map_field_ghost_d(F.ctypes.data, 1, 1, int_array([-1] * 3, C.c_int64),
                                       int_array([15, 15, 9], C.c_int64), hs[0].topo_id, 1,
                                       int_array([2, 2, 2]), 5, C.byref(info))
-    assert info.value == -2 and "slab" in ppmg.last_error()[2]
+    assert info.value == -2 and "subdomain of several" in ppmg.last_error()[2]
     t2 = topo_for(3, 12, decomp=(2, 1, 1), topo_id=7900)
     ppmg.register(t2)
     import ctypes as C
     info = C.c_int(0)
     ppmg.lib().ppmg_mesh_set_local_sub(7900, 1, 0, C.byref(info))
-    assert info.value == -2 and "z-slabs" in ppmg.last_error()[2]
-    for ts in hs + [t2]:
+    assert info.value == 0, ppmg.last_error()
+    ppmg.unregister(t2)
+    t3 = topo_for(3, 12, decomp=(2, 1, 1), topo_id=7901)
+    t3.nnodes = t3.nnodes.copy()
+    t3.istart = t3.istart.copy()
+    t3.nnodes[0, 0] -= 1  # the intervals no longer meet: not a cartesian cut
+    ppmg.register(t3)
+    ppmg.lib().ppmg_mesh_set_local_sub(7901, 1, 0, C.byref(info))
+    assert info.value == -2 and "cartesian" in ppmg.last_error()[2]
+    ppmg.unregister(t3)
+    for ts in hs:
         ppmg.unregister(ts)
 
 

@@ -121,15 +121,22 @@ def test_put_then_get(nc, decomp, kernel, g, lda):
         assert np.abs(local[s] - want[s]).max() <= 1e-13 * scale, s
 
 
-def test_get_never_writes_real_nodes():
-    t = topo_for(3, 12, decomp=(2, 2, 2))
-    g = (2, 2, 2)
+@pytest.mark.parametrize("decomp,g", [((2, 2, 2), (2, 2, 2)), ((3, 2, 1), (3, 1, 2)),
+                                       ((2, 2, 2), (6, 6, 6))])
+def test_get_fills_each_ghost_node_once(decomp, g):
+    """The get's boxes never touch a real node and cover every ghost node of a
+    cut axis exactly once (so that one launch may copy them all)."""
+    t = topo_for(3, 12, decomp=decomp)
     for s in range(t.nsubs):
+        cut = [int(t.nnodes[s, a]) != int(t.Nm[a]) for a in range(3)]
+        n = [int(t.nnodes[s, a]) if cut[a] else int(t.Nm[a]) for a in range(3)]
+        hits = np.zeros(tuple(n[a] + 2 * g[a] for a in range(3)), int)
         for _, _, lo, hi in halo.plan_boxes(t, s, g, put=False)["recv"]:
-            inside = all(lo[a] >= 1 and hi[a] <= int(t.nnodes[s, a]) for a in range(3))
-            assert not inside
-            # a box lies outside the real box along at least one axis
-            assert any(hi[a] < 1 or lo[a] > int(t.nnodes[s, a]) for a in range(3))
+            hits[sl(lo, hi, g)[1:]] += 1
+        inner = tuple(slice(g[a], g[a] + n[a]) if cut[a] else slice(None) for a in range(3))
+        want = np.ones_like(hits)
+        want[inner] = 0
+        assert np.array_equal(hits, want), s
 
 
 def test_plan_is_refused_for_bad_geometry():
@@ -141,3 +148,75 @@ def test_plan_is_refused_for_bad_geometry():
     bad.nnodes[0, 0] = int(bad.Nm[0])  # spans x while the others are cut
     with pytest.raises(ValueError):
         halo.plan_boxes(bad, 1, (1, 1, 1), put=True)
+
+
+# ---- the same exchange through ppm_legacy_b200.halo (torch tensors) --------
+
+torch = pytest.importorskip("torch")
+
+
+def fortran_fields(local):
+    return {s: torch.from_numpy(np.asfortranarray(local[s][..., None])) for s in local}
+
+
+@pytest.mark.parametrize("decomp,g", [((2, 2, 2), (2, 2, 2)), ((3, 1, 2), (1, 1, 2)),
+                                       ((1, 2, 1), (1, 2, 1))])
+def test_python_exchange_in_one_process(decomp, g):
+    t, local, want = case(12, decomp, 2, g, 2, seed=31)
+    scale = max(np.abs(w).max() for w in want.values())
+    f = fortran_fields(local)
+    lb = [1 - g[a] for a in range(3)]
+    halo.put(f, t, list(g), lb, halo.LocalComm())
+    for s in f:
+        r = real(t, s, g)
+        assert np.abs(f[s].numpy()[..., 0][r] - want[s][r]).max() <= 1e-13 * scale, s
+    halo.get(f, t, list(g), lb, halo.LocalComm())
+    for s in f:
+        assert np.abs(f[s].numpy()[..., 0] - want[s]).max() <= 1e-13 * scale, s
+
+
+def _rank_main(rank, world, port, decomp, g, out):
+    import os
+
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        t, local, want = case(12, decomp, 2, g, 2, seed=5)
+        scale = max(np.abs(w).max() for w in want.values())
+        f = fortran_fields({rank: local[rank]})
+        lb = [1 - g[a] for a in range(3)]
+        halo.put(f, t, list(g), lb, halo.DistComm())
+        r = real(t, rank, g)
+        assert np.abs(f[rank].numpy()[..., 0][r] - want[rank][r]).max() <= 1e-13 * scale
+        halo.get(f, t, list(g), lb, halo.DistComm())
+        assert np.abs(f[rank].numpy()[..., 0] - want[rank]).max() <= 1e-13 * scale
+        dist.barrier()
+        out.put((rank, "ok"))
+    except Exception as e:  # reported to the parent, which fails the test
+        out.put((rank, repr(e)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_python_exchange_over_gloo():
+    """One subdomain per rank of a 2 x 2 x 1 cut (each neighbour is reached
+    across two periodic shifts)."""
+    import socket
+
+    import torch.multiprocessing as mp
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    world, decomp, g = 4, (2, 2, 1), (2, 1, 1)
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, decomp, g, out))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(out.get(timeout=180) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert all(v == "ok" for v in res.values()), res
