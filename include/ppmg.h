@@ -450,6 +450,27 @@ void ppmg_map_part_route_s_dev(const float* xp, int64_t ldxp, int64_t Np, int to
  * ascending id; counts (host, nsubs+1) the group sizes.  Particles in no
  * subdomain are left out of the exchange without an error, as in the
  * reference (ppm_map_part_global.f:437-442). */
+/* Partial routing on any cartesian cut (ppm_map_part_partial,
+ * ppm/src/ppm_map_part_partial.f:288-420 over the neighbour list): as the
+ * global routing below, but only the local subdomain and its neighbours
+ * (ppmg_halo_neighbours) are destinations; particles in none of them go to
+ * the last group and give info = -2, errno 405 (ppm_map_part_partial.f:
+ * 480-485).  On slabs along z the destinations are the slab and its two z
+ * neighbours, the classes of ppmg_map_part_route_* in a per-subdomain
+ * layout. */
+void ppmg_map_part_partial_route_d_dev(const double* xp, int64_t ldxp, int64_t Np, int topo_id,
+                                       int mesh_id, int* perm, int64_t* counts, int* info,
+                                       void* stream);
+void ppmg_map_part_partial_route_s_dev(const float* xp, int64_t ldxp, int64_t Np, int topo_id,
+                                       int mesh_id, int* perm, int64_t* counts, int* info,
+                                       void* stream);
+/* The neighbours of subdomain isub of a cartesian cut, from the geometry
+ * alone (ascending, isub excluded): the subdomains whose boxes share a face,
+ * an edge or a corner with isub's, across the periodic faces too (the
+ * reference's ineighsubs for such a cut).  *nneigh gets their number; at
+ * most cap are written. */
+void ppmg_halo_neighbours(int nsubs, const int* istart, const int* nnodes, const int* Nm,
+                          int isub, int cap, int* neigh, int* nneigh, int* info);
 void ppmg_map_part_global_route_d_dev(const double* xp, int64_t ldxp, int64_t Np, int topo_id,
                                       int mesh_id, int* perm, int64_t* counts, int* info,
                                       void* stream);

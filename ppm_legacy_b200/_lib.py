@@ -40,6 +40,7 @@ SIGNATURES = {
     "ppmg_halo_set_transport": ([_i, _i, _vp, _vp, _pi], None),
     "ppmg_halo_plan": ([_i, _pd, _pd, _i, _i, _i64, _pi64, _pi64, _pi, _i, _pi64, _pi, _pi, _pi64,
                         _pi, _pi, _pi64, _pi], None),
+    "ppmg_halo_neighbours": ([_i, _pd, _pd, _pi, _i, _i, _vp, _pi, _pi], None),
     "ppmg_halo_plan_boxes": ([_i, _pd, _pd, _pi, _i, _pi, _i, _i, _vp, _pi, _vp, _pi, _pi],
                              None),
     "ppmg_interp_p2m_adjoint_dv_3d": (_ADJ, None),
@@ -83,6 +84,8 @@ SIGNATURES = {
     "ppmg_map_part_route_s_dev": ([_pd, _i64, _i64, _i, _i, _pd, _pi64, _pi, _vp], None),
     "ppmg_map_part_global_route_d_dev": ([_pd, _i64, _i64, _i, _i, _pd, _pi64, _pi, _vp], None),
     "ppmg_map_part_global_route_s_dev": ([_pd, _i64, _i64, _i, _i, _pd, _pi64, _pi, _vp], None),
+    "ppmg_map_part_partial_route_d_dev": ([_pd, _i64, _i64, _i, _i, _pd, _pi64, _pi, _vp], None),
+    "ppmg_map_part_partial_route_s_dev": ([_pd, _i64, _i64, _i, _i, _pd, _pi64, _pi, _vp], None),
     "ppmg_map_part_gather_d_dev": ([_pd, _i64, _i, _pd, _i64, _pd, _i64, _pi, _vp], None),
     "ppmg_map_part_gather_s_dev": ([_pd, _i64, _i, _pd, _i64, _pd, _i64, _pi, _vp], None),
     "ppmg_util_rank2d_d_dev": (_RANK + [_vp], None),

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -1992,7 +1993,7 @@ static void route_common(const T* xp, int64_t ldxp, int64_t Np, int topo_id, int
 template <class T>
 static void groute_common(const T* xp, int64_t ldxp, int64_t Np, int topo_id, int mesh_id,
                           int* perm, int64_t* counts, int* info, cudaStream_t st,
-                          const char* caller) {
+                          const char* caller, bool partial = false) {
   clear_error();
   if (info) *info = 0;
   if (Np < 0 || (Np > 0 && ldxp < 3) || Np >= (int64_t)1 << 31) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": invalid sizes"); return; }
@@ -2016,10 +2017,20 @@ static void groute_common(const T* xp, int64_t ldxp, int64_t Np, int topo_id, in
       (e = ws.h_aux.ensure(sizeof(double) * 6 * (size_t)ns))) { cuda_fail(info, e, caller); return; }
   // the subdomain boxes, [6][ns]: min_sub x, y, z, then max_sub x, y, z
   std::vector<double> zb(6 * (size_t)ns);
+  std::vector<char> reach(ns, 1);
+  if (partial) {
+    // ppm_map_part_partial: the local subdomain and its neighbours only; the
+    // others get empty boxes, so their particles land in no subdomain
+    std::vector<int> nb;
+    cart_neighbours(ns, h->istart.data(), h->nnodes.data(), h->Nm_global, h->local_sub, nb);
+    std::fill(reach.begin(), reach.end(), 0);
+    reach[h->local_sub] = 1;
+    for (int q : nb) reach[q] = 1;
+  }
   for (int q = 0; q < ns; ++q)
     for (int a = 0; a < 3; ++a) {
-      zb[a * ns + q] = h->min_sub[3 * q + a];
-      zb[(3 + a) * ns + q] = h->max_sub[3 * q + a];
+      zb[a * ns + q] = reach[q] ? h->min_sub[3 * q + a] : 0.0;
+      zb[(3 + a) * ns + q] = reach[q] ? h->max_sub[3 * q + a] : 0.0;
     }
   double* dz = ws.h_aux.as<double>();
   if ((e = cudaMemcpyAsync(dz, zb.data(), sizeof(double) * 6 * ns, cudaMemcpyHostToDevice, st))) { cuda_fail(info, e, caller); return; }
@@ -2040,6 +2051,12 @@ static void groute_common(const T* xp, int64_t ldxp, int64_t Np, int topo_id, in
   if (counts)
     for (size_t c = 0; c < ncls; ++c)
       counts[c] = (c + 1 < ncls ? cs[c + 1] : (int)Np) - cs[c];
+  // ppm_map_part_partial.f:480-485: particles beyond the neighbours are an error
+  const int64_t lost = Np - cs[ns];
+  if (partial && lost > 0)
+    fail(info, kErrorError, kErrPartUnass,
+         std::string(caller) + ": " + std::to_string(lost) +
+             " particles lie in no neighbouring subdomain (ppm_map_part_global moves them)");
 }
 
 template <class T>
@@ -2076,6 +2093,29 @@ void ppmg_map_part_global_route_s_dev(const float* xp, int64_t ldxp, int64_t Np,
                                       void* stream) {
   groute_common<float>(xp, ldxp, Np, topo_id, mesh_id, perm, counts, info, (cudaStream_t)stream,
                        "ppmg_map_part_global_route_s_dev");
+}
+void ppmg_map_part_partial_route_d_dev(const double* xp, int64_t ldxp, int64_t Np, int topo_id,
+                                       int mesh_id, int* perm, int64_t* counts, int* info,
+                                       void* stream) {
+  groute_common<double>(xp, ldxp, Np, topo_id, mesh_id, perm, counts, info, (cudaStream_t)stream,
+                        "ppmg_map_part_partial_route_d_dev", true);
+}
+void ppmg_map_part_partial_route_s_dev(const float* xp, int64_t ldxp, int64_t Np, int topo_id,
+                                       int mesh_id, int* perm, int64_t* counts, int* info,
+                                       void* stream) {
+  groute_common<float>(xp, ldxp, Np, topo_id, mesh_id, perm, counts, info, (cudaStream_t)stream,
+                       "ppmg_map_part_partial_route_s_dev", true);
+}
+void ppmg_halo_neighbours(int nsubs, const int* istart, const int* nnodes, const int* Nm,
+                          int isub, int cap, int* neigh, int* nneigh, int* info) {
+  clear_error();
+  if (info) *info = 0;
+  if (isub < 0 || isub >= nsubs) { fail(info, kErrorError, ppmg::kErrArgument, "ppmg_halo_neighbours: isub out of range"); return; }
+  if (const char* why = check_cartesian(nsubs, istart, nnodes, Nm)) { fail(info, kErrorError, ppmg::kErrArgument, std::string("ppmg_halo_neighbours: ") + why); return; }
+  std::vector<int> nb;
+  cart_neighbours(nsubs, istart, nnodes, Nm, isub, nb);
+  *nneigh = (int)nb.size();
+  for (int i = 0; i < (int)nb.size() && i < cap; ++i) neigh[i] = nb[i];
 }
 void ppmg_map_part_gather_d_dev(const double* src, int64_t lds, int lda, const int* perm,
                                 int64_t n, double* dst, int64_t ldd, int* info, void* stream) {

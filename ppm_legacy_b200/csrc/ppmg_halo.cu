@@ -94,6 +94,22 @@ const char* check_cartesian(int nsubs, const int* istart, const int* nnodes, con
   return nullptr;
 }
 
+void cart_neighbours(int nsubs, const int* istart, const int* nnodes, const int Nm[3], int isub,
+                     std::vector<int>& out) {
+  out.clear();
+  for (int q = 0; q < nsubs; ++q) {
+    if (q == isub) continue;
+    bool near = true;
+    for (int a = 0; a < 3 && near; ++a) {
+      const int s0 = istart[3 * isub + a], s1 = s0 + nnodes[3 * isub + a] - 1;
+      const int q0 = istart[3 * q + a], q1 = q0 + nnodes[3 * q + a] - 1;
+      near = q0 == s0 || q0 == s1 || q1 == s0 || (s1 == Nm[a] && q0 == 1) ||
+             (s0 == 1 && q1 == Nm[a]);
+    }
+    if (near) out.push_back(q);
+  }
+}
+
 const char* halo_boxes(int nsubs, const int* istart, const int* nnodes, const int Nm[3],
                        int isub, const int g[3], bool put, std::vector<HaloBox>& sends,
                        std::vector<HaloBox>& recvs) {

@@ -31,6 +31,14 @@ const char* halo_plan(int nsubs, const int* istart, const int* nnodes, int Nmz, 
 // combination of the axes' intervals is one subdomain.  0, or why not.
 const char* check_cartesian(int nsubs, const int* istart, const int* nnodes, const int Nm[3]);
 
+// The neighbours of subdomain isub in a cartesian decomposition (sorted,
+// isub excluded): the subdomains whose interval along every axis equals
+// isub's or touches it, across the periodic faces too (the subdomains whose
+// boxes share a face, an edge or a corner with isub's: the neighbour list
+// ppm_map_part_partial sends to).
+void cart_neighbours(int nsubs, const int* istart, const int* nnodes, const int Nm[3], int isub,
+                     std::vector<int>& out);
+
 // The exchange of any cartesian decomposition (cuts along one, two or three
 // axes): blocks are boxes of the local field, in its 1-based local node
 // indices (inclusive), for every neighbouring subdomain and periodic shift.

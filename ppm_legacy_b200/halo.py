@@ -323,6 +323,23 @@ def plan_boxes(topo, isub, ghost, put):
     return {"send": rows(sb, ns.value), "recv": rows(rb, nr.value)}
 
 
+def cart_neighbours(topo, isub):
+    """The neighbours of subdomain isub of a cartesian cut (ppmg_halo_neighbours):
+    ascending, isub excluded; the subdomains whose boxes share a face, an
+    edge or a corner with isub's, across the periodic faces too."""
+    from ._lib import int_array, last_error, lib
+    ist = np.ascontiguousarray(topo.istart, dtype=np.int32)
+    nn = np.ascontiguousarray(topo.nnodes, dtype=np.int32)
+    out = (_C.c_int * max(int(topo.nsubs), 1))()
+    cnt, info = _C.c_int(0), _C.c_int(0)
+    lib().ppmg_halo_neighbours(int(topo.nsubs), ist.ctypes.data, nn.ctypes.data,
+                               int_array(topo.Nm), int(isub), int(topo.nsubs),
+                               _C.addressof(out), _C.byref(cnt), _C.byref(info))
+    if info.value != 0:
+        raise ValueError(last_error()[2])
+    return [out[i] for i in range(cnt.value)]
+
+
 def has_c_transport(topo_id, mesh_id) -> bool:
     return (int(topo_id), int(mesh_id)) in _c_transports
 

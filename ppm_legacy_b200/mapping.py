@@ -1,20 +1,22 @@
-"""Particle redistribution between z-slab subdomains: the host mirror of
+"""Particle redistribution between subdomains: the host mirror of
 ``ppm_map_part_partial`` (ppm/src/ppm_map_part_partial.f with the push /
 send / pop of ppm_map_part_push.f, ppm_map_part_send.f, ppm_map_part_pop.f)
-for the slab decomposition of ppm_legacy_b200.halo.
+and ``ppm_map_part_global`` for the decompositions of ppm_legacy_b200.halo.
 
 After particles moved (and the client imposed the periodic bounds, as in
-PPM), every particle goes to the slab that contains it among its slab and
-the two z neighbours.  The routing and the packing run on the GPU
-(ppmg_map_part_route / ppmg_map_part_gather: one stable grouping of the
-particles by destination, then a gather per array); the blocks travel with
-the transports of ppm_legacy_b200.halo.  Sizes go first, then the particle
-blocks, in the same operation order on every rank.
+PPM), every particle goes to the subdomain that contains it among its own
+and the neighbours: on slabs along z the two z neighbours
+(ppmg_map_part_route), on other cartesian cuts up to 26 neighbours
+(ppmg_map_part_partial_route).  The routing and the packing run on the GPU
+(one stable grouping of the particles by destination, then a gather per
+array, ppmg_map_part_gather); the blocks travel with the transports of
+ppm_legacy_b200.halo.  Sizes go first, then the particle blocks, in the same
+operation order on every rank.
 
-The new particle list of a slab is its kept particles in their order, then
-those arriving from the slab below, then those from the slab above.  (The
-reference orders arrivals by its communication sequence; the set of
-particles is the same.)
+The new particle list is the kept particles in their order, then the
+arrivals: on slabs those from the slab below, then those from the slab
+above; on other cuts by ascending source subdomain.  (The reference orders
+arrivals by its communication sequence; the set of particles is the same.)
 """
 from __future__ import annotations
 
@@ -70,10 +72,16 @@ def device_route(topo_id, mesh_id, xp):
     return info.value, perm, [int(c) for c in cnt]
 
 
-def map_subs(parts: dict, topo, comm, route=device_route, gather=device_gather):
-    """parts {isub: (topo_id, mesh_id, xp, [props])} of the slabs this process
-    holds; returns (info, {isub: (xp_new, [props_new])}).  route / gather:
-    the device kernels (replaceable, for tests of the exchange on CPU)."""
+def map_subs(parts: dict, topo, comm, route=None, gather=device_gather):
+    """parts {isub: (topo_id, mesh_id, xp, [props])} of the subdomains this
+    process holds; returns (info, {isub: (xp_new, [props_new])}).  route /
+    gather: the device kernels (replaceable, for tests of the exchange on
+    CPU; route takes (topo_id, mesh_id, xp) on slabs, (topo_id, mesh_id, xp,
+    nsubs) on other cuts)."""
+    if not halo.is_slab_topology(topo):
+        return map_global(parts, topo, comm, route=route or device_route_partial, gather=gather,
+                          peers=lambda s: halo.cart_neighbours(topo, s))
+    route = route or device_route
     import torch
     info_all = 0
     packed, counts = {}, {}
@@ -141,10 +149,10 @@ def map_subs(parts: dict, topo, comm, route=device_route, gather=device_gather):
 
 
 def ppm_map_part_partial(xp, Np, topo_id, mesh_id, props=(), comm=None):
-    """ppm_map_part_partial for the slab this process holds: returns
+    """ppm_map_part_partial for the subdomain this process holds: returns
     (info, Np_new, xp_new, [props_new]).  xp and props are column-major
-    device arrays (ld, Np); every rank of the slab decomposition calls it.
-    info is -2 (errno 405) when particles lie in no neighbouring slab (they
+    device arrays (ld, Np); every rank of the decomposition calls it.  info
+    is -2 (errno 405) when particles lie in no neighbouring subdomain (they
     are dropped); the exchange takes place all the same."""
     r = _topo.local_sub(topo_id, mesh_id)
     if r is None:
@@ -158,7 +166,7 @@ def ppm_map_part_partial(xp, Np, topo_id, mesh_id, props=(), comm=None):
     return info, int(x2.shape[1]), x2, p2
 
 
-# ---- ppm_map_part_global: every particle to the slab that contains it --------
+# ---- ppm_map_part_global: every particle to the subdomain that contains it ----
 
 TAG_GSIZE, TAG_GDATA = 80, 100
 
@@ -179,13 +187,35 @@ def device_route_global(topo_id, mesh_id, xp, nsubs):
     return info.value, perm, [int(c) for c in cnt]
 
 
-def map_global(parts: dict, topo, comm, route=device_route_global, gather=device_gather):
-    """parts {isub: (topo_id, mesh_id, xp, [props])} of the slabs this process
-    holds; returns (info, {isub: (xp_new, [props_new])}).  The exchange is
-    all-pairs: sizes first (one to every other slab), then the non-empty
-    particle blocks, in the same operation order on every rank."""
+def device_route_partial(topo_id, mesh_id, xp, nsubs):
+    """As device_route_global, with only the local subdomain and its
+    neighbours as destinations (ppmg_map_part_partial_route): particles
+    beyond them land in the last group and give info -2, errno 405."""
+    import torch
+    n = int(xp.shape[1])
+    perm = torch.empty(max(n, 1), dtype=torch.int32, device=xp.device)
+    cnt = (C.c_int64 * (int(nsubs) + 1))()
+    info = C.c_int(0)
+    k = "d" if xp.dtype == torch.float64 else "s"
+    getattr(lib(), f"ppmg_map_part_partial_route_{k}_dev")(
+        xp.data_ptr(), xp.stride(1), n, int(topo_id), int(mesh_id), perm.data_ptr(), cnt,
+        C.byref(info), torch.cuda.current_stream().cuda_stream)
+    return info.value, perm, [int(c) for c in cnt]
+
+
+def map_global(parts: dict, topo, comm, route=device_route_global, gather=device_gather,
+               peers=None):
+    """parts {isub: (topo_id, mesh_id, xp, [props])} of the subdomains this
+    process holds; returns (info, {isub: (xp_new, [props_new])}).  Sizes go
+    first (one to every peer), then the non-empty particle blocks, in the same
+    operation order on every rank.  peers(s): the subdomains s exchanges with
+    (every other one by default, the global mapping; the neighbours for the
+    partial mapping)."""
     import torch
     ns = int(topo.nsubs)
+    if peers is None:
+        def peers(s):
+            return [q for q in range(ns) if q != s]
     info_all = 0
     packed, counts = {}, {}
     for s, (tid, mid, xp, props) in parts.items():
@@ -198,9 +228,7 @@ def map_global(parts: dict, topo, comm, route=device_route_global, gather=device
     dev = next(iter(parts.values()))[2].device
     sends, recvs = [], []
     for s, c in counts.items():
-        for q in range(ns):
-            if q == s:
-                continue
+        for q in peers(s):
             sends.append((s, q, TAG_GSIZE, torch.tensor([c[q]], dtype=torch.int64, device=dev)))
             recvs.append((s, q, TAG_GSIZE, torch.zeros(1, dtype=torch.int64, device=dev)))
     got = comm.exchange(sends, recvs)
@@ -214,9 +242,7 @@ def map_global(parts: dict, topo, comm, route=device_route_global, gather=device
             start.append(start[-1] + v)
         for k, P in enumerate(packed[s]):
             rows = _rows(P)
-            for q in range(ns):
-                if q == s:
-                    continue
+            for q in peers(s):
                 if c[q]:
                     sends.append((s, q, TAG_GDATA + k, rows[start[q]:start[q] + c[q]]))
                 nq = arrive[s].get(q, 0)
@@ -230,15 +256,15 @@ def map_global(parts: dict, topo, comm, route=device_route_global, gather=device
     out = {}
     for s, c in counts.items():
         start = sum(c[:s])
-        n_new = c[s] + sum(arrive[s].get(q, 0) for q in range(ns) if q != s)
+        n_new = c[s] + sum(arrive[s].get(q, 0) for q in peers(s))
         arrays = []
         for k, P in enumerate(packed[s]):
             rows = _rows(P)
             res = torch.empty((max(n_new, 1), rows.shape[1]), dtype=P.dtype, device=P.device)
             res[:c[s]].copy_(rows[start:start + c[s]])
             pos = c[s]
-            for q in range(ns):
-                nq = arrive[s].get(q, 0) if q != s else 0
+            for q in peers(s):
+                nq = arrive[s].get(q, 0)
                 if nq:
                     res[pos:pos + nq].copy_(blocks[(s, k, q)])
                     pos += nq
@@ -248,13 +274,14 @@ def map_global(parts: dict, topo, comm, route=device_route_global, gather=device
 
 
 def ppm_map_part_global(xp, Np, topo_id, mesh_id, props=(), comm=None):
-    """ppm_map_part_global for the slab this process holds: returns
-    (info, Np_new, xp_new, [props_new]).  Every particle goes to the slab
-    that contains it, however far it moved; particles in no slab are left
-    out, without an error (ppm_map_part_global.f:437-442).  The new list is
-    the kept particles in their order, then the arrivals by ascending source
-    slab (each in the source's order).  xp and props are column-major device
-    arrays (ld, Np); every rank of the slab decomposition calls it."""
+    """ppm_map_part_global for the subdomain this process holds: returns
+    (info, Np_new, xp_new, [props_new]).  Every particle goes to the
+    subdomain that contains it, however far it moved; particles in none are
+    left out, without an error (ppm_map_part_global.f:437-442).  The new list
+    is the kept particles in their order, then the arrivals by ascending
+    source subdomain (each in the source's order).  xp and props are
+    column-major device arrays (ld, Np); every rank of the decomposition
+    calls it."""
     r = _topo.local_sub(topo_id, mesh_id)
     if r is None:
         raise ValueError("ppm_map_part_global: unknown topo_id/mesh_id")

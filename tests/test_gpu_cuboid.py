@@ -373,3 +373,36 @@ def test_cuboid_refusals():
     assert ppmg.register(bad, isub=0) != 0
     assert "cartesian" in ppmg.last_error()[2] or "cover" in ppmg.last_error()[2]
     ppmg.unregister(bad)
+
+
+@pytest.mark.parametrize("decomp,far", [((2, 2, 2), 0), ((4, 2, 1), 9)])
+def test_cuboid_partial_mapping(decomp, far):
+    """ppm_map_part_partial on a cut along several axes: the device routing
+    over the neighbour list equals the rule restated on CPU, every subdomain
+    ends with exactly its particles (kept ones, then the arrivals by
+    ascending source), and particles beyond the neighbours give 405."""
+    from ppm_legacy_b200 import mapping
+    from test_map_cuboid import check, make_before, partial_rule
+    t = topo_for(3, 12, decomp=decomp)
+    hs = sub_handles(t)
+    try:
+        before = make_before(t, 3000, far)
+        for s, ts in enumerate(hs):
+            info, perm, cnt = mapping.device_route_partial(ts.topo_id, 1, dev_f(before[s][0]),
+                                                           t.nsubs)
+            errno = ppmg.last_error()[1]  # before the next library call clears it
+            cls = partial_rule(t, s, before[s][0])
+            want = np.concatenate([np.flatnonzero(cls == c) for c in range(t.nsubs + 1)])
+            assert np.array_equal(perm.cpu().numpy()[:len(want)], want), s
+            assert cnt == [int((cls == c).sum()) for c in range(t.nsubs + 1)]
+            assert info == (-2 if (cls == t.nsubs).any() else 0)
+            if info:
+                assert errno == 405
+        parts = {s: (ts.topo_id, 1, dev_f(before[s][0]),
+                     [dev_f(before[s][1]), dev_f(before[s][2])]) for s, ts in enumerate(hs)}
+        info, res = mapping.map_subs(parts, t, halo.LocalComm())
+        after = {s: (host(x), host(p[0]), host(p[1])) for s, (x, p) in res.items()}
+        check(t, before, after)
+        assert info == (-2 if far else 0)
+    finally:
+        release(hs)
