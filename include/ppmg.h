@@ -411,7 +411,12 @@ void ppmg_util_rank2d_s(const float* xp, int64_t ldxp, int64_t Np, const float* 
  * form solves the whole domain: xy transforms on every slab, an all-to-all
  * to z pencils through the transport, the z transforms and the spectral
  * step, and back; phi then fills the slab's box, its z ghost planes from the
- * neighbours.  Other cuts return info = -2, errno 503. */
+ * neighbours.  On other cartesian cuts (with a transport) omega's unique
+ * nodes go to P virtual z-slabs (slab q on subdomain q's process), the slab
+ * form solves there, and phi returns to every node of each subdomain's box
+ * 1-g:Nm+g, ghosts and images included (ppm_fdsolver_map_3d.f maps the
+ * field the same way); this needs at least as many y and z cells as
+ * subdomains (else info = -2, errno 503). */
 void ppmg_fdsolver_poisson_3d_d(double* field_up, int64_t ldf, int lda, const int64_t* f_lb,
                                 const int64_t* f_ub, int topo_id, int mesh_id,
                                 const int* ghostsize, int* info);

@@ -79,7 +79,8 @@ struct Handle {
   Workspace ws_map;   // particle routing between slabs
   Workspace ws_fd;    // Poisson solver buffers
   FFTPlans fft;       // its cuFFT plans
-  SlabFFTPlans fft_slab;  // the slab form's plans (z-slab handles)
+  SlabFFTPlans fft_slab;  // the slab form's plans (z-slab handles, virtual slabs of cuts)
+  DevBuf fd_slab;         // a cut's virtual z-slab of the field (the solve on cuts)
   cudaStream_t stream = nullptr;
   int* d_status = nullptr;  // [0] particles outside the sub, [1] non-finite
   // position fingerprints: [0] of the sort held in ws, [1] of an M2P's xp
@@ -1789,6 +1790,282 @@ void ppmg_rmsh_create_part_s_dev(const float* field_up, int64_t ldf, int lda,
 
 // ---- FFT Poisson solver ------------------------------------------------------------
 extern "C++" {
+// Unique-node boxes moved between two layouts through the caller's transport:
+// the send boxes packed from src (node strides ss, lower bounds slb), the
+// receive boxes unpacked into dst (dsd, dlb), nc components per node, the
+// boxes in each layout's own 1-based node indices.  Blocks to the local
+// subdomain are copied on the device (the i-th local send to the i-th local
+// receive).  The receive boxes must be disjoint.
+template <class T>
+int box_transfer(Handle& h, const T* src, const int64_t ss[3], const int slb[3],
+                 const std::vector<HaloBox>& sends, T* dst, const int64_t ds[3],
+                 const int dlb[3], const std::vector<HaloBox>& recvs, int nc,
+                 bool host_transport, cudaStream_t st, int* info, const char* caller) {
+  const int ns = (int)sends.size(), nr = (int)recvs.size();
+  std::vector<int64_t>& tab = h.halo_tab_host;
+  tab.assign(8 * (size_t)(ns + nr), 0);
+  std::vector<int64_t> elems(ns + nr);
+  int64_t tot[2] = {0, 0};
+  for (int i = 0; i < ns + nr; ++i) {
+    const HaloBox& b = i < ns ? sends[i] : recvs[i - ns];
+    int64_t* t = tab.data() + 8 * (size_t)i;
+    int64_t n = nc;
+    for (int a = 0; a < 3; ++a) {
+      t[a] = b.lo[a];
+      t[3 + a] = b.hi[a] - b.lo[a] + 1;
+      n *= t[3 + a];
+    }
+    int64_t& acc = tot[i < ns ? 0 : 1];
+    t[6] = acc;
+    t[7] = acc;
+    elems[i] = n;
+    acc += n;
+  }
+  cudaError_t e = cudaSuccess;
+  if ((e = h.halo_tab.ensure(sizeof(int64_t) * (tab.empty() ? 1 : tab.size()))) ||
+      (e = h.halo_sbuf.ensure(sizeof(T) * (size_t)(tot[0] > 0 ? tot[0] : 1))) ||
+      (e = h.halo_rbuf.ensure(sizeof(T) * (size_t)(tot[1] > 0 ? tot[1] : 1))))
+    return cuda_fail(info, e, caller);
+  int64_t* dtab = h.halo_tab.as<int64_t>();
+  T* sbuf = h.halo_sbuf.as<T>();
+  T* rbuf = h.halo_rbuf.as<T>();
+  if (!tab.empty() && (e = cudaMemcpyAsync(dtab, tab.data(), sizeof(int64_t) * tab.size(),
+                                           cudaMemcpyHostToDevice, st)))
+    return cuda_fail(info, e, caller);
+  if ((e = launch_box_copy<T>(const_cast<T*>(src), nc, ss, slb, dtab, ns, tot[0], sbuf, kBoxPack,
+                              st)))
+    return cuda_fail(info, e, caller);
+  // blocks to and from other subdomains go through the transport; the local
+  // ones pair up in order (the i-th local send is the i-th local receive)
+  std::vector<ppmg_halo_block> sb, rb;
+  std::vector<int> self_s, self_r;
+  for (int i = 0; i < ns; ++i) {
+    if (sends[i].peer == h.local_sub) {
+      self_s.push_back(i);
+      continue;
+    }
+    sb.push_back({sends[i].peer, sends[i].tag, sbuf + tab[8 * (size_t)i + 7],
+                  (int64_t)sizeof(T) * elems[i]});
+  }
+  for (int i = 0; i < nr; ++i) {
+    if (recvs[i].peer == h.local_sub) {
+      self_r.push_back(i);
+      continue;
+    }
+    rb.push_back({recvs[i].peer, recvs[i].tag, rbuf + tab[8 * (size_t)(ns + i) + 7],
+                  (int64_t)sizeof(T) * elems[ns + i]});
+  }
+  if (self_s.size() != self_r.size())
+    return fail(info, kErrorError, kErrArgument, std::string(caller) + ": inconsistent local blocks");
+  for (size_t k = 0; k < self_s.size() && !e; ++k) {
+    const int i = self_s[k], j = self_r[k];
+    if (elems[i] != elems[ns + j] || sends[i].tag != recvs[j].tag)
+      return fail(info, kErrorError, kErrArgument,
+                  std::string(caller) + ": inconsistent local blocks");
+    e = cudaMemcpyAsync(rbuf + tab[8 * (size_t)(ns + j) + 7], sbuf + tab[8 * (size_t)i + 7],
+                        sizeof(T) * (size_t)elems[i], cudaMemcpyDeviceToDevice, st);
+  }
+  if (e) return cuda_fail(info, e, caller);
+  const int rc = run_transport(h, (int)sb.size(), sb.data(), (int)rb.size(), rb.data(),
+                               host_transport, st, e);
+  if (e) return cuda_fail(info, e, caller);
+  if (rc != 0)
+    return fail(info, kErrorFatal, 2,
+                std::string(caller) + ": the halo transport failed (returned " +
+                    std::to_string(rc) + ")");
+  if ((e = launch_box_copy<T>(dst, nc, ds, dlb, dtab + 8 * (size_t)ns, nr, tot[1], rbuf, kBoxCopy,
+                              st)))
+    return cuda_fail(info, e, caller);
+  return 0;
+}
+
+// The FFT solver on a cut along several axes.  As ppm_fdsolver_solve_3d
+// maps the field onto the slab topology it transforms on
+// (ppm_fdsolver_map_3d.f), omega's unique nodes go to P virtual z-slabs
+// (slab q on subdomain q's process, N2 split evenly), the slab form solves
+// there, and phi comes back to every node of each subdomain's
+// ghost-extended box (its real nodes, ghost nodes and periodic images), so
+// no ghost get follows.  Tags: 200 forward, 300 + shift back.
+template <class T>
+int poisson_cut(Handle& h, T* field, int64_t ldf, const int64_t* f_lb, const int64_t* f_ub,
+                const int* ghost, int lda, const double len[3], bool host_transport,
+                cudaStream_t st, int* info, const char* caller) {
+  const int P = h.nsubs, me = h.local_sub;
+  int N[3];
+  for (int a = 0; a < 3; ++a) N[a] = h.Nm_global[a] - 1;
+  if (N[1] < P || N[2] < P)
+    return fail(info, kErrorError, kErrArgument,
+                std::string(caller) + ": the solve on a cut along several axes needs at least as "
+                                      "many y and z cells as subdomains");
+  std::vector<int> z0(P), nz(P);
+  for (int q = 0; q < P; ++q) {
+    z0[q] = (int)((int64_t)N[2] * q / P);
+    nz[q] = (int)((int64_t)N[2] * (q + 1) / P) - z0[q];
+  }
+  // global 1-based node boxes: a subdomain's unique real nodes (the last
+  // node of a cut axis is the next subdomain's), its ghost-extended box, a
+  // virtual slab's unique nodes
+  auto ist = [&](int q, int a) { return (int64_t)h.istart[3 * q + a]; };
+  auto nno = [&](int q, int a) { return (int64_t)h.nnodes[3 * q + a]; };
+  auto real_u = [&](int q, int a, int64_t& lo, int64_t& hi) {
+    lo = h.open[a] ? ist(q, a) : 1;
+    hi = h.open[a] ? ist(q, a) + nno(q, a) - 2 : N[a];
+  };
+  auto gbox = [&](int q, int a, int64_t& lo, int64_t& hi) {
+    lo = (h.open[a] ? ist(q, a) : 1) - ghost[a];
+    hi = (h.open[a] ? ist(q, a) + nno(q, a) - 1 : N[a] + 1) + ghost[a];
+  };
+  auto slab_u = [&](int q, int a, int64_t& lo, int64_t& hi) {
+    lo = a < 2 ? 1 : z0[q] + 1;
+    hi = a < 2 ? N[a] : z0[q] + nz[q];
+  };
+  auto local_off = [&](int q, int a) { return h.open[a] ? ist(q, a) - 1 : 0; };
+  // the slab buffer: lda x N0 x N1 x nz[me], nodes from (1, 1, 1)
+  const int64_t sn = (int64_t)lda * N[0] * N[1] * (nz[me] > 0 ? nz[me] : 1);
+  cudaError_t e = h.fd_slab.ensure(sizeof(T) * (size_t)sn);
+  if (e) return cuda_fail(info, e, caller);
+  T* slab = h.fd_slab.as<T>();
+  FieldDesc sfd{};
+  sfd.s[0] = lda;
+  sfd.s[1] = (int64_t)lda * N[0];
+  sfd.s[2] = (int64_t)lda * N[0] * N[1];
+  const int sub_[3] = {N[0], N[1], nz[me]};
+  for (int a = 0; a < 3; ++a) {
+    sfd.lb[a] = sfd.box_lo[a] = 1;
+    sfd.ub[a] = sfd.box_hi[a] = sub_[a];
+  }
+  int64_t fs[3];
+  int flb[3];
+  fs[0] = ldf;
+  fs[1] = ldf * (f_ub[0] - f_lb[0] + 1);
+  fs[2] = fs[1] * (f_ub[1] - f_lb[1] + 1);
+  for (int a = 0; a < 3; ++a) flb[a] = (int)f_lb[a];
+  const int slb[3] = {1, 1, 1};
+  // forward: R'_me and U_q (one box per pair)
+  std::vector<HaloBox> snd, rcv;
+  for (int q = 0; q < P; ++q) {
+    HaloBox b;
+    bool ok = true;
+    for (int a = 0; a < 3 && ok; ++a) {
+      int64_t rl, rh, ul, uh;
+      real_u(me, a, rl, rh);
+      slab_u(q, a, ul, uh);
+      b.lo[a] = rl > ul ? rl : ul;
+      b.hi[a] = rh < uh ? rh : uh;
+      ok = b.lo[a] <= b.hi[a];
+      b.lo[a] -= local_off(me, a);
+      b.hi[a] -= local_off(me, a);
+    }
+    if (ok) {
+      b.peer = q;
+      b.tag = 200;
+      snd.push_back(b);
+    }
+    ok = true;
+    for (int a = 0; a < 3 && ok; ++a) {
+      int64_t rl, rh, ul, uh;
+      real_u(q, a, rl, rh);
+      slab_u(me, a, ul, uh);
+      b.lo[a] = rl > ul ? rl : ul;
+      b.hi[a] = rh < uh ? rh : uh;
+      ok = b.lo[a] <= b.hi[a];
+      if (a == 2) {
+        b.lo[a] -= z0[me];
+        b.hi[a] -= z0[me];
+      }
+    }
+    if (ok) {
+      b.peer = q;
+      b.tag = 200;
+      rcv.push_back(b);
+    }
+  }
+  for (const HaloBox& b : snd)
+    for (int a = 0; a < 3; ++a)
+      if (b.lo[a] < f_lb[a] || b.hi[a] > f_ub[a])
+        return fail(info, kErrorError, kErrArgument,
+                    std::string(caller) + ": field_up bounds do not cover the real nodes");
+  if (box_transfer<T>(h, field, fs, flb, snd, slab, sfd.s, slb, rcv, lda, host_transport, st, info,
+                      caller))
+    return *info;
+  // the slab solve
+  SlabSolve sl;
+  sl.P = P;
+  sl.me = me;
+  for (int a = 0; a < 3; ++a) {
+    sl.N[a] = N[a];
+    sl.len[a] = len[a];
+  }
+  sl.z0 = z0.data();
+  sl.nz = nz.data();
+  cudaError_t te = cudaSuccess;
+  BlockExchange xchg = [&](int ns, const ppmg_halo_block* sb, int nr, const ppmg_halo_block* rb) {
+    const int rc = run_transport(h, ns, sb, nr, rb, host_transport, st, te);
+    return te ? 1 : rc;
+  };
+  const int bad = fd_poisson_slab<T>(h.fft_slab, h.ws_fd, sl, slab, sfd, lda, st, xchg, e);
+  if (!e) e = te;
+  if (bad == 2)
+    return fail(info, kErrorFatal, 2, std::string(caller) + ": the halo transport failed");
+  if (bad)
+    return fail(info, kErrorError, kErrArgument,
+                std::string(caller) + ": cuFFT plan or transform failed");
+  if (e) return cuda_fail(info, e, caller);
+  // back: G_q and (U_me + tN) from the slab, G_me and (U_q + tN) into the field
+  snd.clear();
+  rcv.clear();
+  auto dir = [](const int t[3]) { return (t[0] + 1) + 3 * (t[1] + 1) + 9 * (t[2] + 1); };
+  for (int q = 0; q < P; ++q) {
+    int t[3];
+    for (t[2] = -1; t[2] <= 1; ++t[2])
+      for (t[1] = -1; t[1] <= 1; ++t[1])
+        for (t[0] = -1; t[0] <= 1; ++t[0]) {
+          HaloBox b;
+          bool ok = true;
+          for (int a = 0; a < 3 && ok; ++a) {  // me sends to q, in my slab's nodes
+            int64_t gl, gh, ul, uh;
+            gbox(q, a, gl, gh);
+            slab_u(me, a, ul, uh);
+            ul += (int64_t)t[a] * N[a];
+            uh += (int64_t)t[a] * N[a];
+            b.lo[a] = gl > ul ? gl : ul;
+            b.hi[a] = gh < uh ? gh : uh;
+            ok = b.lo[a] <= b.hi[a];
+            const int64_t o = (int64_t)t[a] * N[a] + (a == 2 ? z0[me] : 0);
+            b.lo[a] -= o;
+            b.hi[a] -= o;
+          }
+          if (ok) {
+            b.peer = q;
+            b.tag = 300 + dir(t);
+            snd.push_back(b);
+          }
+          ok = true;
+          for (int a = 0; a < 3 && ok; ++a) {  // me receives from q, in my field's nodes
+            int64_t gl, gh, ul, uh;
+            gbox(me, a, gl, gh);
+            slab_u(q, a, ul, uh);
+            ul += (int64_t)t[a] * N[a];
+            uh += (int64_t)t[a] * N[a];
+            b.lo[a] = gl > ul ? gl : ul;
+            b.hi[a] = gh < uh ? gh : uh;
+            ok = b.lo[a] <= b.hi[a];
+            b.lo[a] -= local_off(me, a);
+            b.hi[a] -= local_off(me, a);
+          }
+          if (ok) {
+            b.peer = q;
+            b.tag = 300 + dir(t);
+            rcv.push_back(b);
+          }
+        }
+  }
+  if (box_transfer<T>(h, slab, sfd.s, slb, snd, field, fs, flb, rcv, lda, host_transport, st, info,
+                      caller))
+    return *info;
+  return 0;
+}
+
 template <class T>
 static void poisson_common(T* field_up, int64_t ldf, int lda, const int64_t* f_lb,
                            const int64_t* f_ub, int topo_id, int mesh_id, const int* ghostsize,
@@ -1802,7 +2079,6 @@ static void poisson_common(T* field_up, int64_t ldf, int lda, const int64_t* f_l
   if (!h) return;
   if (lda < 1 || ldf < lda) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": lda inconsistent"); return; }
   if (!check_ghost(*h, ghostsize, caller, info)) return;
-  if (h->cut() && !h->slab()) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": the FFT solver on several subdomains supports slabs along z only"); return; }
   if (h->slab() && h->g.N[1] < h->nsubs) { fail(info, kErrorError, ppmg::kErrArgument, std::string(caller) + ": the slab solve needs at least as many y cells as slabs"); return; }
   std::lock_guard<std::mutex> lk(h->mu);
   int lo[3], hi[3];
@@ -1873,6 +2149,10 @@ static void poisson_common(T* field_up, int64_t ldf, int lda, const int64_t* f_l
       if (slab_exchange<T>(*h, dfield, ldf, f_lb, f_ub, ghostsize, false, !dev, st, info, caller))
         return;
     }
+  } else if (h->cut()) {
+    // a cut along several axes: through virtual z-slabs and back
+    if (poisson_cut<T>(*h, dfield, ldf, f_lb, f_ub, ghostsize, lda, len, !dev, st, info, caller))
+      return;
   } else {
     bad = fd_poisson<T>(h->fft, h->ws_fd, h->g.N, len, dfield, fd, lda, st, e);
   }
