@@ -159,6 +159,15 @@ __device__ __forceinline__ void emit_node(const P2MParams& P, int x, int y, int 
   if (DIM == 2) {
     lo[2] = hi[2] = 0;
   }
+  if ((lo[0] | hi[0] | lo[1] | hi[1] | lo[2] | hi[2]) == 0) {
+    // the common case: the node has no image inside the box
+    const int64_t o = (int64_t)(n[0] + 1 - P.fd.lb[0]) * P.fd.s[0] +
+                      (int64_t)(n[1] + 1 - P.fd.lb[1]) * P.fd.s[1] +
+                      (DIM == 3 ? (int64_t)(n[2] + 1 - P.fd.lb[2]) * P.fd.s[2] : 0) + P.c0;
+#pragma unroll
+    for (int a = 0; a < LC; ++a) F[o + a] = (OT)v[a];
+    return;
+  }
   for (int tk = lo[2]; tk <= hi[2]; ++tk) {
     const int64_t oz =
         DIM == 3 ? (int64_t)(n[2] + 1 + tk * P.N[2] - P.fd.lb[2]) * P.fd.s[2] : 0;
