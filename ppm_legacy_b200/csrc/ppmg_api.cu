@@ -93,6 +93,9 @@ struct Handle {
   int cache_prec = -1;        // record precision: 0 FP64 (double4), 1 FP32 (float4)
   bool cache_quirk = false;   // the sort's keys used M2P's FP32 mesh spacing
   int64_t cache_np = -1, cache_ldxp = -1;
+  // ws.tiles holds work items of the tile gathers (M2P, adjoint) for the
+  // cached sort (a P2M by the row gather leaves items of its own shape)
+  bool items_m2p = false;
   bool dxi_same_d = false, dxi_same_f = false;
   std::mutex mu;
   // comp_weights state
@@ -350,6 +353,7 @@ int p2m_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, const T* up, 
   if (e) return cuda_fail(info, e, caller);
   if (!remesh) {
     h.sort_cached = true;
+    h.items_m2p = !p2m_row_gather(h.dim, prec);
     h.cache_quirk = false;
     h.cache_prec = prec == P2M_FP64 ? 0 : 1;
     h.cache_np = Np;
@@ -433,10 +437,12 @@ int m2p_pipeline(Handle& h, const T* xp, int64_t ldxp, int64_t Np, T* up, int64_
     if ((e = h.ws.tiles.ensure(tile_items_bytes(P.N)))) return cuda_fail(info, e, caller);
     // a cut subdomain's P2M items cover its nodes -g .. N+g, not M2P's
     // cells: M2P builds its own (the cell order itself is reused)
-    if (reuse && !h.cut()) {
+    if (reuse && !h.cut() && h.items_m2p) {
       ti = tile_items_view(h.ws.tiles.p, P.N);
     } else if ((e = make_tile_items(h.ws.start.as<int>(), P.N, Np, h.ws.tiles.p, ti, st))) {
       return cuda_fail(info, e, caller);
+    } else {
+      h.items_m2p = !h.cut();
     }
     P.start = h.ws.start.as<int>();
     P.items = ti.items;
@@ -679,10 +685,12 @@ int adjoint_pipeline(Handle& h, const double* xp, int64_t ldxp, int64_t Np, cons
     TileItems ti;
     if ((e = h.ws.tiles.ensure(tile_items_bytes(P.N)))) return cuda_fail(info, e, caller);
     // a cut subdomain's P2M items cover nodes, not cells: own items
-    if (reuse && !h.cut()) {
+    if (reuse && !h.cut() && h.items_m2p) {
       ti = tile_items_view(h.ws.tiles.p, P.N);
     } else if ((e = make_tile_items(h.ws.start.as<int>(), P.N, Np, h.ws.tiles.p, ti, st))) {
       return cuda_fail(info, e, caller);
+    } else {
+      h.items_m2p = !h.cut();
     }
     P.start = h.ws.start.as<int>();
     P.items = ti.items;

@@ -14,6 +14,8 @@
 // order: results are bitwise reproducible and need no atomics.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "ppmg_p2m.cuh"
 
 namespace ppmg {
@@ -132,6 +134,26 @@ __device__ __forceinline__ void weights(CT f, CT w[S]) {
 
 // Write one finished node value (components c0..c0+LC-1) to every image of
 // unique node (x, y, z) inside the written box.
+// The periodic images n+1+t*N (1-based) of unique node n along axis a that
+// lie in the written box: t = lo .. hi (0 .. 0 when the node has none).
+__device__ __forceinline__ void axis_images(const P2MParams& P, int a, int n, int& lo,
+                                            int& hi) {
+  const int N = P.N[a];
+  if (P.open[a]) {
+    // no periodic images along a cut axis: the node itself
+    lo = hi = 0;
+  } else if (P.fd.box_lo[a] > 1 - N && P.fd.box_hi[a] < 2 * N + 1) {
+    // ghost layers narrower than the mesh: t in {-1, 0, 1}
+    lo = n + 1 - N >= P.fd.box_lo[a] ? -1 : 0;
+    hi = n + 1 + N <= P.fd.box_hi[a] ? 1 : 0;
+  } else {
+    int tlo = (P.fd.box_lo[a] - n - 1 + 64 * N) / N - 64;  // ceil for negatives
+    if (n + 1 + tlo * N < P.fd.box_lo[a]) ++tlo;
+    lo = tlo;
+    hi = (P.fd.box_hi[a] - n - 1 + 64 * N) / N - 64;  // floor
+  }
+}
+
 template <int DIM, class OT, int LC>
 __device__ __forceinline__ void emit_node(const P2MParams& P, int x, int y, int z,
                                           const double v[LC]) {
@@ -139,23 +161,7 @@ __device__ __forceinline__ void emit_node(const P2MParams& P, int x, int y, int 
   const int n[3] = {x, y, z};
   int lo[3], hi[3];
 #pragma unroll
-  for (int a = 0; a < DIM; ++a) {
-    // 1-based images n+1+t*N within [box_lo, box_hi]
-    const int N = P.N[a];
-    if (P.open[a]) {
-      // no periodic images along a cut axis: the node itself
-      lo[a] = hi[a] = 0;
-    } else if (P.fd.box_lo[a] > 1 - N && P.fd.box_hi[a] < 2 * N + 1) {
-      // ghost layers narrower than the mesh: t in {-1, 0, 1}
-      lo[a] = n[a] + 1 - N >= P.fd.box_lo[a] ? -1 : 0;
-      hi[a] = n[a] + 1 + N <= P.fd.box_hi[a] ? 1 : 0;
-    } else {
-      int tlo = (P.fd.box_lo[a] - n[a] - 1 + 64 * N) / N - 64;  // ceil for negatives
-      if (n[a] + 1 + tlo * N < P.fd.box_lo[a]) ++tlo;
-      lo[a] = tlo;
-      hi[a] = (P.fd.box_hi[a] - n[a] - 1 + 64 * N) / N - 64;  // floor
-    }
-  }
+  for (int a = 0; a < DIM; ++a) axis_images(P, a, n[a], lo[a], hi[a]);
   if (DIM == 2) {
     lo[2] = hi[2] = 0;
   }
@@ -736,19 +742,506 @@ __global__ void __launch_bounds__(kTX * kTY, TM ? 3 : 2) k_p2m3d(P2MParams P) {
   }
 }
 
+// --------------------------------------------------------------------------
+// 3D row gather (FP32 arithmetic: the mixed form and the single-precision
+// API).
+// A CTA of kGW warps owns the kGW x-nodes X0 .. X0+kGW-1 and the 33-S node
+// rows Y0 .. Y0+32-S over a z-range [Z0, Z1) of its work item.  Warp w owns
+// x-node X0 + w; lane L owns cell row Y0 - HL + L (L = 0 .. 31).  For each
+// cell layer the particles of the (kGW+S-1) x 32 cells whose stencils reach
+// the tile are staged in shared memory (1D weights once per staged
+// particle); thread (w, L) then visits the particles of the S cells
+// X0-HL+w .. X0-HL+w+S-1 of its row -- exactly the particles whose
+// x-stencils reach node X0 + w -- and adds each one's contribution to the
+// S node rows (j) and S node planes (k) of its yz-stencil into registers
+// G[j][k][a]: one visit per (particle, x-node), S*S*LC FMAs each.
+// The node of row Y0 + L is the sum of G[S-1-d] over lanes L + d
+// (d = 0 .. S-1), taken by warp shuffles in a fixed order; lanes L >= 33-S
+// only supply rows.  G's planes form a z-window like the node window of
+// k_p2m3d: when the sweep leaves layer cz, plane cz-HL+1 is complete and is
+// written (with its periodic images); the window then shifts.
+// Compensation (COMP): G holds plain FP32 partials.  Once a lane of a warp
+// has added more than kFoldTerms particles since the warp's last fold, the
+// warp sums all of G's planes over its rows and folds them into the
+// per-node (hi, lo) window with an error-free TwoSum, then clears G; a node
+// is written as hi + lo + the partial of its plane, in FP64.  Every node is
+// produced by one thread in a fixed order: the results are deterministic.
+// S: stencil width (4 = M'4, 2 = bsp2).  OT: field type.  LC: components of
+// this launch (<= 4).  WST: 1D weights come from comp_weights.
+// --------------------------------------------------------------------------
+constexpr int kGW = 8;          // warps per CTA = x-nodes per tile
+constexpr int kFoldTerms = 48;  // plain FP32 terms per G entry before a fold
+
+template <int S>
+constexpr int g_rows() {
+  return 33 - S;  // node rows per tile
+}
+
+// Exclusive scan over n <= 3 * 32 * NW cell values (thread t owns cells
+// 3t .. 3t+2) by a CTA of NW warps; as scan_cells.
+template <int NW, class F>
+__device__ __forceinline__ void scan_cells_w(int n, F val, int* out, int* wsum, int* red) {
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int q0 = 3 * tid;
+  const int v0 = q0 < n ? val(q0) : 0;
+  const int v1 = q0 + 1 < n ? val(q0 + 1) : 0;
+  const int v2 = q0 + 2 < n ? val(q0 + 2) : 0;
+  const int s = v0 + v1 + v2;
+  int inc = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) wsum[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    const int w = lane < NW ? wsum[lane] : 0;
+    int wi = w;
+#pragma unroll
+    for (int o = 1; o < NW; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += t;
+    }
+    if (lane < NW) wsum[lane] = wi - w;
+    if (lane == NW - 1) red[0] = wi;
+  }
+  __syncthreads();
+  const int ex = inc - s + wsum[wid];
+  if (q0 < n) out[q0] = ex;
+  if (q0 + 1 < n) out[q0 + 1] = ex + v0;
+  if (q0 + 2 < n) out[q0 + 2] = ex + v0 + v1;
+  if (tid == 0) out[n] = red[0];
+}
+
+// 16-byte planes per staged particle of the row gather: wx, wz, and the
+// products wy(j) u(a) (S*LC values)
+template <int S, int LC>
+constexpr int g_wyu_units() {
+  return (S * LC + 3) / 4;
+}
+template <int S, class OT, int LC, bool WST>
+constexpr size_t p2m3g_smem(int cap) {
+  constexpr int NSC = (kGW + S - 1) * 32;
+  constexpr int IU = p2m_rec_units<S, float, OT, WST>() + 1;
+  // per slot: the weight planes, the raw next unit, 2 column bytes
+  return (size_t)cap * (16 * (2 + g_wyu_units<S, LC>()) + 16 * IU + 2) +
+         sizeof(int) * (size_t)(8 * NSC + 2);
+}
+// staging slots of the row gather: as many as fit in ~110 KB (two CTAs per
+// SM), a multiple of 16
+template <int S, class OT, int LC, bool WST>
+constexpr int p2m3g_cap() {
+  int cap = 2048;
+  while (cap > 64 && p2m3g_smem<S, OT, LC, WST>(cap) > (size_t)110 * 1024) cap -= 16;
+  return cap;
+}
+
+template <int S, bool COMP, class OT, int LC, bool WST>
+__global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
+  constexpr int HL = S / 2;
+  constexpr int HH = S / 2 - 1;
+  constexpr int TYN = g_rows<S>();
+  constexpr int WX = kGW + S - 1;  // staged columns
+  constexpr int NSC = WX * 32;     // staged cells (32 rows)
+  constexpr int NT = kGW * 32;
+  constexpr int PERC = (NSC + NT - 1) / NT;
+  constexpr int RU = p2m_rec_units<S, float, OT, WST>();
+  constexpr int IU = RU + 1;
+  static_assert(NSC <= 3 * NT, "staged cells exceed the scan width");
+  static_assert(S <= 4 && LC <= 4, "stencil / components");
+
+  if ((int)blockIdx.x >= *P.nitems) return;
+  const int4 it = P.items[blockIdx.x];
+  const int tiles_x = (P.span.ext[0] + kGW - 1) / kGW;
+  const int X0 = P.span.org[0] + (it.x % tiles_x) * kGW;
+  const int Y0 = P.span.org[1] + (it.x / tiles_x) * TYN;
+  const int XE = P.span.org[0] + P.span.ext[0], YE = P.span.org[1] + P.span.ext[1];
+  const int Z0 = it.y, Z1 = it.z;
+  constexpr int cap = p2m3g_cap<S, OT, LC, WST>();
+  constexpr int UW = g_wyu_units<S, LC>();
+
+  extern __shared__ __align__(16) unsigned char smem[];
+  float4* sWX = reinterpret_cast<float4*>(smem);
+  float4* sWZ = sWX + cap;
+  float4* sWYU = sWZ + cap;  // [UW][cap]: wy(j) u(a) at a * S + j
+  uint4* raw = reinterpret_cast<uint4*>(sWYU + UW * cap);  // [cap][IU] next unit
+  int* cnt = reinterpret_cast<int*>(raw + (size_t)cap * IU);  // layer: particles per cell
+  int* done = cnt + NSC;                                    // layer: particles already in units
+  int* cbase = done + NSC;                                  // layer: first sorted particle per cell
+  int* ubase = cbase + NSC;                                 // unit being issued: first particle per cell
+  int* offU = ubase + NSC;                                  // [2][NSC + 1] unit offsets per cell
+  int* nxb = offU + 2 * (NSC + 1);                          // next layer: cell ranges in flight
+  int* nxe = nxb + NSC;
+  unsigned char* sQ = reinterpret_cast<unsigned char*>(nxe + NSC);  // [2][cap] staged columns
+  const float* sWXf = reinterpret_cast<const float*>(sWX);
+  __shared__ int wsum[kGW];
+  __shared__ int red[2];
+
+  const int tid = threadIdx.x;
+  const int w = tid >> 5, L = tid & 31;
+  const int nx = X0 + w, ny = Y0 + L;
+  const bool owner = L < TYN && nx < XE && ny < YE;
+  const uint4* grec = static_cast<const uint4*>(P.rec);
+  const uint4* gus = static_cast<const uint4*>(P.us);
+
+  // G: plain FP32 partials, node rows j in pairs (j = 2J: .x, 2J + 1: .y);
+  // (hi, lo): the compensated sums of the node planes; the planes form a
+  // ring (slot = node plane mod S)
+  float2 G[S / 2][S][LC];
+  float hi[S][LC], lo[S][LC];
+#pragma unroll
+  for (int j = 0; j < S / 2; ++j)
+#pragma unroll
+    for (int k = 0; k < S; ++k)
+#pragma unroll
+      for (int a = 0; a < LC; ++a) G[j][k][a] = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int k = 0; k < S; ++k)
+#pragma unroll
+    for (int a = 0; a < LC; ++a) hi[k][a] = lo[k][a] = 0.f;
+  int nterm = 0;  // particles added to G since the warp's last fold
+
+  // the staged cells of this thread (q = tid + NT k): their xy offset in
+  // the cell numbering, -1 for cells outside the subdomain along a cut axis
+  int64_t cxy[PERC];
+#pragma unroll
+  for (int k = 0; k < PERC; ++k) {
+    const int q = tid + NT * k;
+    const int r = q / WX, qx = q - r * WX;
+    const int ux = X0 - HL + qx, uy = Y0 - HL + r;
+    const bool out = q >= NSC || (P.open[0] && (ux < 0 || ux >= P.N[0])) ||
+                     (P.open[1] && (uy < 0 || uy >= P.N[1]));
+    cxy[k] = out ? -1 : (int64_t)wrap_index(ux, P.N[0]) +
+                            (int64_t)P.N[0] * wrap_index(uy, P.N[1]);
+  }
+  const int64_t plane_cells = (int64_t)P.N[0] * P.N[1];
+  // this thread's node column: its offset in field_up when it has no
+  // periodic image along x or y (else every image is found per node)
+  bool col_img = true;
+  int64_t col_off = 0;
+  if (owner) {
+    int l0, h0, l1, h1;
+    axis_images(P, 0, nx, l0, h0);
+    axis_images(P, 1, ny, l1, h1);
+    col_img = (l0 | h0 | l1 | h1) != 0;
+    col_off = (int64_t)(nx + 1 - P.fd.lb[0]) * P.fd.s[0] +
+              (int64_t)(ny + 1 - P.fd.lb[1]) * P.fd.s[1] + P.c0;
+  }
+
+  auto load_counts = [&](int cz) {
+    const bool empty = P.open[2] && (cz < 0 || cz >= P.N[2]);
+    const int64_t zoff = empty ? 0 : plane_cells * wrap_index(cz, P.N[2]);
+#pragma unroll
+    for (int k = 0; k < PERC; ++k) {
+      const int q = tid + NT * k;
+      if (q >= NSC) continue;
+      if (!empty && cxy[k] >= 0) {
+        const int* src = P.start + zoff + cxy[k];
+        cp_async4(nxb + q, src);
+        cp_async4(nxe + q, src + 1);
+      } else {
+        nxb[q] = nxe[q] = 0;
+      }
+    }
+  };
+  auto publish = [&]() {
+#pragma unroll
+    for (int k = 0; k < PERC; ++k) {
+      const int q = tid + NT * k;
+      if (q < NSC) {
+        const int b = nxb[q], e = nxe[q];
+        cbase[q] = b;
+        cnt[q] = e - b;
+        done[q] = 0;
+      }
+    }
+  };
+  int left = 0;
+  auto plan = [&](int ob, bool first) -> int {
+    int* off = offU + ob * (NSC + 1);
+    if (first) {
+      scan_cells_w<kGW>(NSC, [&](int q) { return cnt[q]; }, off, wsum, red);
+      left = red[0];
+      if (left <= cap) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          const int q = 3 * tid + i;
+          if (q < NSC) {
+            ubase[q] = cbase[q];
+            done[q] = cnt[q];
+          }
+        }
+        const int n = left;
+        left = 0;
+        __syncthreads();
+        return n;
+      }
+    }
+    scan_cells_w<kGW>(NSC, [&](int q) { return cnt[q] > done[q] ? 1 : 0; }, off, wsum, red);
+    const int A = max(red[0], 1);
+    const int kk = cap / A, rem = cap - A * kk;
+    auto take_of = [&](int q) {
+      const int l = q < NSC ? cnt[q] - done[q] : 0;
+      return l > 0 ? min(l, kk + (off[q] < rem ? 1 : 0)) : 0;
+    };
+    const int t0 = take_of(3 * tid), t1 = take_of(3 * tid + 1), t2 = take_of(3 * tid + 2);
+    __syncthreads();
+    scan_cells_w<kGW>(
+        NSC, [&](int q) { const int i = q - 3 * tid; return i == 0 ? t0 : (i == 1 ? t1 : t2); },
+        off, wsum, red);
+    const int n = red[0];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const int q = 3 * tid + i;
+      if (q < NSC) {
+        ubase[q] = cbase[q] + done[q];
+        done[q] += i == 0 ? t0 : (i == 1 ? t1 : t2);
+      }
+    }
+    left -= n;
+    __syncthreads();
+    return n;
+  };
+  auto issue = [&](int ob) {
+    const int* off = offU + ob * (NSC + 1);
+    unsigned char* q8 = sQ + ob * cap;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const int q = 3 * tid + i;
+      if (q < NSC) {
+        const int o0 = off[q], o1 = off[q + 1];
+        const int64_t g0 = ubase[q];
+        for (int o = o0; o < o1; ++o) {
+          const int64_t s = g0 + (o - o0);
+          uint4* d = raw + (size_t)o * IU;
+#pragma unroll
+          for (int t = 0; t < RU; ++t) {
+            if constexpr (WST)
+              cp_async16(d + t, grec + s * RU + t);
+            else
+              cp_async16(d + t, grec + t * P.ps + s);
+          }
+          cp_async16(d + RU, gus + s);
+          q8[o] = (unsigned char)(q % WX);
+        }
+      }
+    }
+    cp_async_commit();
+  };
+  // the sum over the warp's rows of ring slot k, component a of G for the
+  // node row of this lane (lanes L .. L+S-1 contribute, nearest first)
+  auto g_at = [&](int j, int k, int a) -> float {
+    return (j & 1) ? G[j >> 1][k][a].y : G[j >> 1][k][a].x;
+  };
+  auto row_sum = [&](int k, int a) -> float {
+    float s = g_at(S - 1, k, a);
+#pragma unroll
+    for (int d = 1; d < S; ++d) s += __shfl_down_sync(0xffffffffu, g_at(S - 1 - d, k, a), d);
+    return s;
+  };
+
+  int cz = Z0 - HL;
+  const int zlast = Z1 - 1 + HH;
+  // ring slot of the node plane cz - HL + 1 (the first plane of layer cz)
+  int ph = wrap_index(cz - HL + 1, S);
+  load_counts(cz);
+  cp_async_wait_all();
+  publish();
+  if (cz < zlast) load_counts(cz + 1);
+  __syncthreads();
+  int n_cur = plan(0, true);
+  bool last_cur = left == 0;
+  issue(0);
+
+  for (int u = 0;; ++u) {
+    const int ub = u & 1;
+    cp_async_wait_all();
+    __syncthreads();
+    // 1. weights of unit u: raw -> structure-of-arrays slots
+    for (int i = tid; i < n_cur; i += NT) {
+      const uint4* r = raw + (size_t)i * IU;
+      float wv[3][4];
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) wv[d][k] = 0.f;
+      if constexpr (WST) {
+        const OT* wsrc = reinterpret_cast<const OT*>(r);
+#pragma unroll
+        for (int k = 0; k < S; ++k) {
+          wv[0][k] = (float)wsrc[k];
+          wv[1][k] = (float)wsrc[S + k];
+          wv[2][k] = (float)wsrc[2 * S + k];
+        }
+      } else {
+        const float4 rv = *reinterpret_cast<const float4*>(r);
+        weights<S, float>(rv.x, wv[0]);
+        weights<S, float>(rv.y, wv[1]);
+        weights<S, float>(rv.z, wv[2]);
+      }
+      sWX[i] = make_float4(wv[0][0], wv[0][1], wv[0][2], wv[0][3]);
+      sWZ[i] = make_float4(wv[2][0], wv[2][1], wv[2][2], wv[2][3]);
+      const float4 u4 = *reinterpret_cast<const float4*>(r + RU);
+      const float uu[4] = {u4.x, u4.y, u4.z, u4.w};
+      float f[4 * UW];
+#pragma unroll
+      for (int t = 0; t < 4 * UW; ++t) f[t] = 0.f;
+#pragma unroll
+      for (int aa = 0; aa < LC; ++aa)
+#pragma unroll
+        for (int j = 0; j < S; ++j) f[aa * S + j] = wv[1][j] * uu[aa];
+#pragma unroll
+      for (int t = 0; t < UW; ++t)
+        sWYU[t * cap + i] = make_float4(f[4 * t], f[4 * t + 1], f[4 * t + 2], f[4 * t + 3]);
+    }
+    __syncthreads();
+    // 2. plan and issue unit u+1 (the next layer's first unit when unit u
+    //    completes its layer)
+    const int cz_u = cz;
+    const bool last_u = last_cur;
+    const int n_u = n_cur;
+    bool more = true;
+    if (last_u) {
+      if (cz < zlast) {
+        ++cz;
+        publish();
+        if (cz < zlast) load_counts(cz + 1);
+        __syncthreads();
+        n_cur = plan(ub ^ 1, true);
+      } else {
+        more = false;
+      }
+    } else {
+      n_cur = plan(ub ^ 1, false);
+    }
+    if (more) {
+      last_cur = left == 0;
+      issue(ub ^ 1);
+    }
+    // 3.-5. with the ring phase a compile-time constant
+    auto body = [&](auto phc) {
+      constexpr int PH = decltype(phc)::value;
+      // 3. accumulate unit u: the particles of cells w .. w+S-1 of row L
+      if (n_u > 0) {
+        const int* off = offU + ub * (NSC + 1);
+        const unsigned char* q8 = sQ + ub * cap;
+        const int q0 = L * WX + w;
+        const int p0 = off[q0], p1 = off[q0 + S];
+        nterm += p1 - p0;
+        for (int p = p0; p < p1; ++p) {
+          // x-weight of node X0 + w in the stencil of a particle of column c
+          const int ix = w + S - 1 - (int)q8[p];
+          const float wxi = sWXf[4 * p + ix];
+          const float4 wz4 = sWZ[p];
+          float f[4 * UW];
+#pragma unroll
+          for (int t = 0; t < UW; ++t) {
+            const float4 v = sWYU[t * cap + p];
+            f[4 * t] = v.x;
+            f[4 * t + 1] = v.y;
+            f[4 * t + 2] = v.z;
+            f[4 * t + 3] = v.w;
+          }
+          const float wz[4] = {wz4.x, wz4.y, wz4.z, wz4.w};
+          const float2 wx2 = make_float2(wxi, wxi);
+          // (wx wy(2J) u(a), wx wy(2J+1) u(a)) times wz(k), packed FP32 pairs
+#pragma unroll
+          for (int J = 0; J < S / 2; ++J)
+#pragma unroll
+            for (int a = 0; a < LC; ++a) {
+              const float2 cu =
+                  __fmul2_rn(wx2, make_float2(f[a * S + 2 * J], f[a * S + 2 * J + 1]));
+#pragma unroll
+              for (int k = 0; k < S; ++k)
+                G[J][(PH + k) % S][a] =
+                    __ffma2_rn(cu, make_float2(wz[k], wz[k]), G[J][(PH + k) % S][a]);
+            }
+        }
+      }
+      // 4. fold G into the node ring once a lane has added kFoldTerms
+      //    particles since the warp's last fold
+      if constexpr (COMP) {
+        if (__any_sync(0xffffffffu, nterm > kFoldTerms)) {
+#pragma unroll
+          for (int k = 0; k < S; ++k)
+#pragma unroll
+            for (int a = 0; a < LC; ++a) {
+              const float s = row_sum(k, a);
+              two_sum_fold<float>(hi[k][a], lo[k][a], s);
+            }
+#pragma unroll
+          for (int j = 0; j < S / 2; ++j)
+#pragma unroll
+            for (int k = 0; k < S; ++k)
+#pragma unroll
+              for (int a = 0; a < LC; ++a) G[j][k][a] = make_float2(0.f, 0.f);
+          nterm = 0;
+        }
+      }
+      // 5. layer complete: node plane zc (slot PH) is final: write it and
+      //    clear its slot for plane zc + S
+      if (last_u) {
+        const int zc = cz_u - (HL - 1);
+        float s0[LC];
+#pragma unroll
+        for (int a = 0; a < LC; ++a) s0[a] = row_sum(PH, a);
+        if (owner && zc >= Z0 && zc < Z1) {
+          double v[LC];
+#pragma unroll
+          for (int a = 0; a < LC; ++a)
+            v[a] = COMP ? ((double)hi[PH][a] + (double)lo[PH][a]) + (double)s0[a]
+                        : (double)s0[a];
+          int l2, h2;
+          axis_images(P, 2, zc, l2, h2);
+          if (!col_img && (l2 | h2) == 0) {
+            OT* F = static_cast<OT*>(P.field) + col_off +
+                    (int64_t)(zc + 1 - P.fd.lb[2]) * P.fd.s[2];
+#pragma unroll
+            for (int a = 0; a < LC; ++a) F[a] = (OT)v[a];
+          } else {
+            emit_node<3, OT, LC>(P, nx, ny, zc, v);
+          }
+        }
+#pragma unroll
+        for (int a = 0; a < LC; ++a) {
+#pragma unroll
+          for (int j = 0; j < S / 2; ++j) G[j][PH][a] = make_float2(0.f, 0.f);
+          hi[PH][a] = lo[PH][a] = 0.f;
+        }
+      }
+    };
+    if constexpr (S == 4) {
+      switch (ph) {
+        case 0: body(std::integral_constant<int, 0>{}); break;
+        case 1: body(std::integral_constant<int, 1>{}); break;
+        case 2: body(std::integral_constant<int, 2>{}); break;
+        default: body(std::integral_constant<int, 3>{}); break;
+      }
+    } else {
+      if (ph == 0)
+        body(std::integral_constant<int, 0>{});
+      else
+        body(std::integral_constant<int, 1>{});
+    }
+    if (last_u) ph = ph + 1 == S ? 0 : ph + 1;
+    if (!more) break;
+  }
+}
+
 // Per (xy tile, cell layer): particles in the tile's own cells of that layer
 // (tiles of the span from (ox, oy), ex x ey nodes; cells outside 0 .. N-1
 // count none).
 __global__ void k_layer_counts(const int* __restrict__ start, int N0, int N1, int N2, int ox,
-                               int oy, int ex, int ey, int tiles_x, int ntiles,
-                               int* __restrict__ lc) {
+                               int oy, int ex, int ey, int tdx, int tdy, int tiles_x,
+                               int ntiles, int* __restrict__ lc) {
   const int64_t n = (int64_t)ntiles * N2;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const int tile = (int)(i / N2), cz = (int)(i % N2);
-    const int tx0 = ox + (tile % tiles_x) * kTileX, ty0 = oy + (tile / tiles_x) * kTileY;
-    const int X0 = max(tx0, 0), X1 = min(min(tx0 + kTileX, ox + ex), N0);
-    const int Y0 = max(ty0, 0), Y1 = min(min(ty0 + kTileY, oy + ey), N1);
+    const int tx0 = ox + (tile % tiles_x) * tdx, ty0 = oy + (tile / tiles_x) * tdy;
+    const int X0 = max(tx0, 0), X1 = min(min(tx0 + tdx, ox + ex), N0);
+    const int Y0 = max(ty0, 0), Y1 = min(min(ty0 + tdy, oy + ey), N1);
     int sum = 0;
     for (int y = Y0; y < Y1 && X0 < X1; ++y) {
       const int64_t c0 = (int64_t)X0 + (int64_t)N0 * (y + (int64_t)N1 * cz);
@@ -966,21 +1459,30 @@ __global__ void __launch_bounds__(kTile2) k_p2m2d(P2MParams P) {
 template <int S, class CT, bool COMP, class OT, int LC, bool WST>
 cudaError_t launch_lc(const P2MParams& P, int dim, cudaStream_t st) {
   if (dim == 3) {
-    // staging slots: as many as fit in ~110 KB (2 CTAs / SM), ~74 KB for the
-    // TMEM form (3 CTAs / SM)
     P2MParams Q = P;
     int cap = 2048;
-    // (the TMEM form up to 3 components: a 4-component window would spill)
-    constexpr bool TM = COMP && LC <= 3;
-    const size_t lim = (size_t)(TM ? 74 : 110) * 1024;
-    while (cap > 64 && p2m3d_smem<S, CT, OT, WST>(cap) > lim) cap -= 16;
-    Q.cap = cap;
-    const size_t smem = p2m3d_smem<S, CT, OT, WST>(cap);
-    auto kern = k_p2m3d<S, CT, COMP, OT, LC, WST, TM>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
-    kern<<<Q.item_cap, kTX * kTY, smem, st>>>(Q);
+    size_t smem;
+    cudaError_t e;
+    if constexpr (std::is_same<CT, float>::value) {
+      // row gather (FP32 arithmetic): two CTAs of 8 warps per SM, staging
+      // slots in ~110 KB each
+      cap = p2m3g_cap<S, OT, LC, WST>();
+      Q.cap = cap;
+      smem = p2m3g_smem<S, OT, LC, WST>(cap);
+      auto kern = k_p2m3g<S, COMP, OT, LC, WST>;
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      kern<<<Q.item_cap, kGW * 32, smem, st>>>(Q);
+    } else {
+      // tile gather (the FP64 form): staging slots in ~110 KB (2 CTAs / SM)
+      while (cap > 64 && p2m3d_smem<S, CT, OT, WST>(cap) > (size_t)110 * 1024) cap -= 16;
+      Q.cap = cap;
+      smem = p2m3d_smem<S, CT, OT, WST>(cap);
+      auto kern = k_p2m3d<S, CT, COMP, OT, LC, WST>;
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      kern<<<Q.item_cap, kTX * kTY, smem, st>>>(Q);
+    }
   } else {
     constexpr int WX = kTile2 + S - 1;
     constexpr int PS = ((2 * S + 4) + 3) / 4 * 4;
@@ -1034,40 +1536,51 @@ TileSpan cell_span(const int N[3]) {
 
 namespace {
 constexpr int kMinTZ = 8, kMaxTZ = 64;
-int tiles_xy(const TileSpan& sp) {
-  return ((sp.ext[0] + kTileX - 1) / kTileX) * ((sp.ext[1] + kTileY - 1) / kTileY);
+int tiles_xy(const TileSpan& sp, int tdx, int tdy) {
+  return ((sp.ext[0] + tdx - 1) / tdx) * ((sp.ext[1] + tdy - 1) / tdy);
 }
-int item_capacity(const TileSpan& sp) {
-  return tiles_xy(sp) * ((sp.ext[2] + kMinTZ - 1) / kMinTZ) + 1;
+int item_capacity(const TileSpan& sp, int tdx, int tdy) {
+  return tiles_xy(sp, tdx, tdy) * ((sp.ext[2] + kMinTZ - 1) / kMinTZ) + 1;
 }
 TileSpan span_of(const int N[3], const TileSpan* sp) { return sp ? *sp : cell_span(N); }
+size_t items_bytes(const TileSpan& s, int N2, int tdx, int tdy) {
+  return 2 * sizeof(int4) * (size_t)item_capacity(s, tdx, tdy) +
+         sizeof(int) * (size_t)tiles_xy(s, tdx, tdy) * N2 + 64;
+}
 }  // namespace
 
 // Layout: items[cap] | nitems (64 bytes) | unordered items[cap] | layer counts
 size_t tile_items_bytes(const int N[3], const TileSpan* sp) {
-  const TileSpan s = span_of(N, sp);
-  return 2 * sizeof(int4) * (size_t)item_capacity(s) +
-         sizeof(int) * (size_t)tiles_xy(s) * N[2] + 64;
+  return items_bytes(span_of(N, sp), N[2], kTileX, kTileY);
 }
 
 size_t p2m_scratch_bytes(int dim, const int N[3], const TileSpan* sp) {
-  return dim == 3 ? tile_items_bytes(N, sp) : 16;
+  if (dim != 3) return 16;
+  // the items of either 3D gather (tile gather or row gather)
+  const TileSpan s = span_of(N, sp);
+  const size_t a = items_bytes(s, N[2], kTileX, kTileY);
+  const size_t b = items_bytes(s, N[2], kGW, g_rows<2>());
+  const size_t c = items_bytes(s, N[2], kGW, g_rows<4>());
+  return a > b ? (a > c ? a : c) : (b > c ? b : c);
 }
+
+bool p2m_row_gather(int dim, P2MPrec prec) { return dim == 3 && prec != P2M_FP64; }
 
 TileItems tile_items_view(void* scratch, const int N[3], const TileSpan* sp) {
   TileItems t;
-  t.cap = item_capacity(span_of(N, sp));
+  t.cap = item_capacity(span_of(N, sp), kTileX, kTileY);
   t.items = static_cast<const int4*>(scratch);
   t.nitems = reinterpret_cast<const int*>(t.items + t.cap);
   return t;
 }
 
 cudaError_t make_tile_items(const int* start, const int N[3], int64_t nvalid, void* scratch,
-                            TileItems& out, cudaStream_t st, const TileSpan* sp) {
+                            TileItems& out, cudaStream_t st, const TileSpan* sp, int tdx,
+                            int tdy) {
   const TileSpan s = span_of(N, sp);
   const int zlo = s.org[2], ze = s.ext[2];
-  const int nt = tiles_xy(s);
-  const int cap_items = item_capacity(s);
+  const int nt = tiles_xy(s, tdx, tdy);
+  const int cap_items = item_capacity(s, tdx, tdy);
   int4* items = static_cast<int4*>(scratch);
   int* nitems = reinterpret_cast<int*>(items + cap_items);
   int4* unordered = reinterpret_cast<int4*>(nitems + 16);
@@ -1077,11 +1590,15 @@ cudaError_t make_tile_items(const int* start, const int N[3], int64_t nvalid, vo
   const int64_t nl = (int64_t)nt * N[2];
   const int gl = (int)((nl + 255) / 256 < 148 * 32 ? (nl + 255) / 256 : 148 * 32);
   k_layer_counts<<<gl, 256, 0, st>>>(start, N[0], N[1], N[2], s.org[0], s.org[1], s.ext[0],
-                                     s.ext[1], (s.ext[0] + kTileX - 1) / kTileX, nt, lc);
-  const int64_t tgt64 = nvalid / (148 * 2 * 8);
+                                     s.ext[1], tdx, tdy, (s.ext[0] + tdx - 1) / tdx, nt, lc);
+  // the tile gathers: ~16 items per SM (two CTAs per SM), 8-64 layers; the
+  // row gather (a dearer per-layer halo): ~8 per SM, 16-128
+  const bool rows = tdx == kGW;
+  const int64_t tgt64 = nvalid / (rows ? 148 * 8 : 148 * 2 * 8);
   const int target = (int)(tgt64 < 4096 ? 4096 : (tgt64 > (1 << 30) ? (1 << 30) : tgt64));
-  k_make_items<<<(nt + 127) / 128, 128, 0, st>>>(lc, N[2], zlo, ze, nt, target, kMinTZ, kMaxTZ,
-                                                 unordered, nitems);
+  k_make_items<<<(nt + 127) / 128, 128, 0, st>>>(lc, N[2], zlo, ze, nt, target,
+                                                 rows ? 2 * kMinTZ : kMinTZ,
+                                                 rows ? 2 * kMaxTZ : kMaxTZ, unordered, nitems);
   k_order_items<<<1, 1024, 0, st>>>(unordered, nitems, items);
   count_launch(3);
   out.items = items;
@@ -1098,7 +1615,11 @@ cudaError_t launch_p2m(const P2MParams& P0, int dim, int kernel, P2MPrec prec, i
   if (dim == 3) {
     // work items: xy tiles split along z into segments of similar particle count
     TileItems ti;
-    if ((e = make_tile_items(P0.start, P0.N, nvalid, scratch, ti, st, &P0.span))) return e;
+    const bool rows = p2m_row_gather(dim, prec);
+    const int tdy = rows ? (kernel == kKernelMp4 ? g_rows<4>() : g_rows<2>()) : kTileY;
+    if ((e = make_tile_items(P0.start, P0.N, nvalid, scratch, ti, st, &P0.span,
+                             rows ? kGW : kTileX, tdy)))
+      return e;
     Pw.items = ti.items;
     Pw.nitems = ti.nitems;
     Pw.item_cap = ti.cap;

@@ -58,8 +58,15 @@ size_t tile_items_bytes(const int N[3], const TileSpan* sp = nullptr);
 TileItems tile_items_view(void* scratch, const int N[3], const TileSpan* sp = nullptr);
 // Items over the xy tiles and z planes of the span sp (nullptr: the cells
 // 0 .. N-1); nodes outside the cells count no particles.
+// tdx x tdy: the tile of the kernel that uses them (kTileX x kTileY for the
+// tile gathers).
 cudaError_t make_tile_items(const int* start, const int N[3], int64_t nvalid, void* scratch,
-                            TileItems& out, cudaStream_t st, const TileSpan* sp = nullptr);
+                            TileItems& out, cudaStream_t st, const TileSpan* sp = nullptr,
+                            int tdx = kTileX, int tdy = kTileY);
+
+// Whether launch_p2m runs the 3D row gather (whose items are not the tile
+// gathers' items that M2P and the adjoint can reuse).
+bool p2m_row_gather(int dim, P2MPrec prec);
 
 // Tile depth (nodes along the sweep axis per CTA) of the 2D gather.
 int p2m_tile_depth(int dim, const int N[3]);

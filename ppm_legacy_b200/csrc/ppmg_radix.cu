@@ -179,47 +179,6 @@ struct MoveArgs {
   const int* unsorted;  // 0: the first pass found the keys in order (the passes skip)
 };
 
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_init_count(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
-               "r"(bytes)
-               : "memory");
-}
-// One-dimensional TMA bulk copy global -> this CTA's shared memory.
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes,
-                                          uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-          "r"(smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(bar))
-      : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}" : "=r"(ok) : "r"(smem_addr(bar)), "r"(parity) : "memory");
-  return ok != 0;
-}
-// Bounded wait for a phase of an mbarrier (false: gave up).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (int it = 0; it < kRWaitLimit; ++it)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-
 // Shared memory of k_radix_move: two key and two id buffers (kRSub entries
 // each), the 16-bit inverse map and per-warp digit counts, the per-digit
 // offsets and the mbarriers (~98 KB: two CTAs of 16 warps per SM, so one
@@ -292,10 +251,11 @@ __global__ void __launch_bounds__(kRThreads, 2) k_radix_move(MoveArgs A) {
   // every thread waits; all give up together (copies still outstanding are
   // waited for once more, with the same bound)
   auto wait_on = [&](uint64_t* br, int use) -> bool {
-    const bool ok = mbar_wait(br, (uint32_t)((use >> 1) & 1));
+    const bool ok = mbar_wait(br, (uint32_t)((use >> 1) & 1), kRWaitLimit);
     if (__syncthreads_and(ok)) return true;
     if (tid == 0) atomicExch(A.wait_flag, 1);
-    for (int i = 0; i < 4; ++i) mbar_wait(&bar[i], 0u), mbar_wait(&bar[i], 1u);
+    for (int i = 0; i < 4; ++i)
+      mbar_wait(&bar[i], 0u, kRWaitLimit), mbar_wait(&bar[i], 1u, kRWaitLimit);
     return false;
   };
 
