@@ -32,93 +32,6 @@ __device__ __forceinline__ void two_sum_fold(CT& hi, CT& lo, CT p) {
   lo = lo + e;
 }
 
-// Tensor memory (TMEM: 128 lanes x 512 columns of 32 bits per SM) holds the
-// mixed form's (hi, lo) window: thread t of a warp owns TMEM lane
-// 32 (warp % 4) + t and a run of columns.  32x32b loads and stores move n
-// consecutive columns of the thread's lane to / from n registers.
-template <int N>
-__device__ __forceinline__ void tmem_ld(uint32_t ta, uint32_t* r) {
-  if constexpr (N == 16) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-        "%11, %12, %13, %14, %15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-          "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(ta));
-  } else if constexpr (N == 8) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
-                   "=r"(r[6]), "=r"(r[7])
-                 : "r"(ta));
-  } else if constexpr (N == 4) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(ta));
-  } else {
-    static_assert(N == 16 || N == 8 || N == 4, "TMEM chunk");
-  }
-}
-template <int N>
-__device__ __forceinline__ void tmem_st(uint32_t ta, const uint32_t* r) {
-  if constexpr (N == 16) {
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-        "%11, %12, %13, %14, %15, %16};" ::"r"(ta),
-        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
-        "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
-        "r"(r[15]));
-  } else if constexpr (N == 8) {
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};"
-                 ::"r"(ta), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]),
-                 "r"(r[6]), "r"(r[7]));
-  } else if constexpr (N == 4) {
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(ta),
-                 "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]));
-  } else {
-    static_assert(N == 16 || N == 8 || N == 4, "TMEM chunk");
-  }
-}
-// n columns (a multiple of 4) in chunks of 16, 8 and 4
-template <int N>
-__device__ __forceinline__ void tmem_load(uint32_t ta, uint32_t* r) {
-  if constexpr (N >= 16) {
-    tmem_ld<16>(ta, r);
-    if constexpr (N > 16) tmem_load<N - 16>(ta + 16, r + 16);
-  } else if constexpr (N >= 8) {
-    tmem_ld<8>(ta, r);
-    if constexpr (N > 8) tmem_load<N - 8>(ta + 8, r + 8);
-  } else if constexpr (N >= 4) {
-    tmem_ld<4>(ta, r);
-  }
-}
-template <int N>
-__device__ __forceinline__ void tmem_store(uint32_t ta, const uint32_t* r) {
-  if constexpr (N >= 16) {
-    tmem_st<16>(ta, r);
-    if constexpr (N > 16) tmem_store<N - 16>(ta + 16, r + 16);
-  } else if constexpr (N >= 8) {
-    tmem_st<8>(ta, r);
-    if constexpr (N > 8) tmem_store<N - 8>(ta + 8, r + 8);
-  } else if constexpr (N >= 4) {
-    tmem_st<4>(ta, r);
-  }
-}
-__device__ __forceinline__ void tmem_wait_ld() {
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void tmem_wait_st() {
-  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void tmem_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tmem_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-// Columns of TMEM one CTA of k_p2m3d allocates (a power of 2 >= 32): two
-// warps per lane quarter, two node columns per thread, 2 S LC values each.
-constexpr int kTmemCols = 128;
 
 template <int S, class CT>
 __device__ __forceinline__ void weights(CT f, CT w[S]) {
@@ -298,10 +211,8 @@ constexpr size_t p2m3d_smem(int cap) {
          sizeof(int) * (size_t)(8 * NSC + 2);
 }
 
-// TM (with COMP): the (hi, lo) window in tensor memory instead of registers,
-// which lets three CTAs share an SM.
-template <int S, class CT, bool COMP, class OT, int LC, bool WST, bool TM = false>
-__global__ void __launch_bounds__(kTX * kTY, TM ? 3 : 2) k_p2m3d(P2MParams P) {
+template <int S, class CT, bool COMP, class OT, int LC, bool WST>
+__global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
   using V = typename Vec4<CT>::type;
   constexpr int HL = S / 2;
   constexpr int HH = S / 2 - 1;
@@ -315,8 +226,6 @@ __global__ void __launch_bounds__(kTX * kTY, TM ? 3 : 2) k_p2m3d(P2MParams P) {
   constexpr int IU = RU + UU;
   static_assert(NSC <= 3 * NT, "staged cells exceed the scan width");
 
-  static_assert(!TM || (COMP && 4 * 2 * S * LC <= kTmemCols && (2 * S * LC) % 4 == 0),
-                "TMEM window layout");
   if ((int)blockIdx.x >= *P.nitems) return;
   const int4 it = P.items[blockIdx.x];
   const int tiles_x = (P.span.ext[0] + kTileX - 1) / kTileX;
@@ -354,30 +263,6 @@ __global__ void __launch_bounds__(kTX * kTY, TM ? 3 : 2) k_p2m3d(P2MParams P) {
 
   CT acc[2][S][LC];  // window (or per-unit partials when COMP)
   CT hi[2][S][LC], lo[2][S][LC];
-  // TM: this thread's TMEM columns: node column e's window at tcol + e NV,
-  // (hi, lo) of slot k, component a at 2 (k LC + a)
-  constexpr int NV = 2 * S * LC;
-  uint32_t tcol = 0;
-  if constexpr (TM) {
-    __shared__ uint32_t s_tmem;
-    if (tid < 32) {
-      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                       (unsigned)__cvta_generic_to_shared(&s_tmem)),
-                   "r"(kTmemCols)
-                   : "memory");
-      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
-    tmem_fence_before();
-    __syncthreads();
-    tmem_fence_after();
-    const int w = tid >> 5;
-    tcol = s_tmem + ((uint32_t)(32 * (w & 3)) << 16) + (uint32_t)((w >> 2) * 2 * NV);
-    uint32_t z[NV];
-#pragma unroll
-    for (int i = 0; i < NV; ++i) z[i] = 0u;
-    tmem_store<NV>(tcol, z);
-    tmem_store<NV>(tcol + NV, z);
-  }
 #pragma unroll
   for (int e = 0; e < 2; ++e)
 #pragma unroll
@@ -609,66 +494,7 @@ __global__ void __launch_bounds__(kTX * kTY, TM ? 3 : 2) k_p2m3d(P2MParams P) {
         }
       }
     }
-    if constexpr (TM) {
-      // fold, and on the layer's last unit emit and shift, one node column
-      // at a time with its window loaded from TMEM (the same arithmetic as
-      // the register form below)
-      const int zc = cz_u - (HL - 1);
-      tmem_wait_st();
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        uint32_t r[NV];
-        tmem_load<NV>(tcol + e * NV, r);
-        tmem_wait_ld();
-        CT h[S][LC], l[S][LC];
-#pragma unroll
-        for (int k = 0; k < S; ++k)
-#pragma unroll
-          for (int a = 0; a < LC; ++a) {
-            h[k][a] = __uint_as_float(r[2 * (k * LC + a)]);
-            l[k][a] = __uint_as_float(r[2 * (k * LC + a) + 1]);
-          }
-#pragma unroll
-        for (int k = 0; k < S; ++k)
-#pragma unroll
-          for (int a = 0; a < LC; ++a) {
-            if (k == 0 && last_u) continue;
-            if (k == S - 1 && first_u)
-              h[k][a] = acc[e][k][a];
-            else
-              two_sum_fold<CT>(h[k][a], l[k][a], acc[e][k][a]);
-            acc[e][k][a] = CT(0);
-          }
-        if (last_u) {
-          if ((e == 0 ? act0 : act1) && zc >= Z0 && zc < Z1) {
-            double v[LC];
-#pragma unroll
-            for (int a = 0; a < LC; ++a)
-              v[a] = ((double)h[0][a] + (double)l[0][a]) + (double)acc[e][0][a];
-            emit_node<3, OT, LC>(P, x0 + e, y, zc, v);
-          }
-#pragma unroll
-          for (int a = 0; a < LC; ++a) acc[e][0][a] = CT(0);
-#pragma unroll
-          for (int k = 0; k < S - 1; ++k)
-#pragma unroll
-            for (int a = 0; a < LC; ++a) {
-              h[k][a] = h[k + 1][a];
-              l[k][a] = l[k + 1][a];
-            }
-#pragma unroll
-          for (int a = 0; a < LC; ++a) h[S - 1][a] = l[S - 1][a] = CT(0);
-        }
-#pragma unroll
-        for (int k = 0; k < S; ++k)
-#pragma unroll
-          for (int a = 0; a < LC; ++a) {
-            r[2 * (k * LC + a)] = __float_as_uint(h[k][a]);
-            r[2 * (k * LC + a) + 1] = __float_as_uint(l[k][a]);
-          }
-        tmem_store<NV>(tcol + e * NV, r);
-      }
-    } else if constexpr (COMP) {
+    if constexpr (COMP) {
       // fold the unit's partial sums (every unit: total strength stays
       // conserved to ~1e-11 of sum |u|)
       // Two slots skip the TwoSum: the newest slot on the layer's first unit
@@ -689,7 +515,7 @@ __global__ void __launch_bounds__(kTX * kTY, TM ? 3 : 2) k_p2m3d(P2MParams P) {
           }
     }
     // 4. layer complete: node zc = cz_u - (HL-1) of both columns is final: emit, shift
-    if (!TM && last_u) {
+    if (last_u) {
       const int zc = cz_u - (HL - 1);
 #pragma unroll
       for (int e = 0; e < 2; ++e) {
@@ -728,17 +554,6 @@ __global__ void __launch_bounds__(kTX * kTY, TM ? 3 : 2) k_p2m3d(P2MParams P) {
       }
     }
     if (!more) break;
-  }
-  if constexpr (TM) {
-    // every thread's TMEM traffic done, then the allocating warp frees it
-    tmem_wait_st();
-    tmem_fence_before();
-    __syncthreads();
-    tmem_fence_after();
-    if (tid < 32)
-      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tcol & 0xFFFFu),
-                   "r"(kTmemCols)
-                   : "memory");
   }
 }
 
