@@ -641,7 +641,7 @@ constexpr size_t p2m3g_smem(int cap) {
   constexpr int IU = p2m_rec_units<S, float, OT, WST>() + 1;
   // per slot: the weight planes, the raw next unit, 2 column bytes
   return (size_t)cap * (16 * (2 + g_wyu_units<S, LC>()) + 16 * IU + 2) +
-         sizeof(int) * (size_t)(8 * NSC + 2);
+         sizeof(int) * (size_t)(10 * NSC + 2);
 }
 // staging slots of the row gather: as many as fit in ~110 KB (two CTAs per
 // SM), a multiple of 16
@@ -686,9 +686,10 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
   int* cbase = done + NSC;                                  // layer: first sorted particle per cell
   int* ubase = cbase + NSC;                                 // unit being issued: first particle per cell
   int* offU = ubase + NSC;                                  // [2][NSC + 1] unit offsets per cell
-  int* nxb = offU + 2 * (NSC + 1);                          // next layer: cell ranges in flight
-  int* nxe = nxb + NSC;
-  unsigned char* sQ = reinterpret_cast<unsigned char*>(nxe + NSC);  // [2][cap] staged columns
+  // cell ranges of a layer, [layer parity][NSC]: loaded one layer ahead
+  int* nxb = offU + 2 * (NSC + 1);
+  int* nxe = nxb + 2 * NSC;
+  unsigned char* sQ = reinterpret_cast<unsigned char*>(nxe + 2 * NSC);  // [2][cap] staged columns
   const float* sWXf = reinterpret_cast<const float*>(sWX);
   __shared__ int wsum[kGW];
   __shared__ int red[2];
@@ -747,25 +748,27 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
   auto load_counts = [&](int cz) {
     const bool empty = P.open[2] && (cz < 0 || cz >= P.N[2]);
     const int64_t zoff = empty ? 0 : plane_cells * wrap_index(cz, P.N[2]);
+    int* b = nxb + (cz & 1) * NSC;
+    int* e = nxe + (cz & 1) * NSC;
 #pragma unroll
     for (int k = 0; k < PERC; ++k) {
       const int q = tid + NT * k;
       if (q >= NSC) continue;
       if (!empty && cxy[k] >= 0) {
         const int* src = P.start + zoff + cxy[k];
-        cp_async4(nxb + q, src);
-        cp_async4(nxe + q, src + 1);
+        cp_async4(b + q, src);
+        cp_async4(e + q, src + 1);
       } else {
-        nxb[q] = nxe[q] = 0;
+        b[q] = e[q] = 0;
       }
     }
   };
-  auto publish = [&]() {
+  auto publish = [&](int par) {
 #pragma unroll
     for (int k = 0; k < PERC; ++k) {
       const int q = tid + NT * k;
       if (q < NSC) {
-        const int b = nxb[q], e = nxe[q];
+        const int b = nxb[par * NSC + q], e = nxe[par * NSC + q];
         cbase[q] = b;
         cnt[q] = e - b;
         done[q] = 0;
@@ -844,6 +847,90 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
     }
     cp_async_commit();
   };
+  // Plan of a layer whose staged particles fit one unit, without block
+  // barriers.  Unit slots follow the staged cells in row-major order, so lane
+  // L of every warp walks row L (its WX cell ranges) for the prefix within
+  // the row, and a warp scan over the 32 row totals gives the row bases:
+  // every warp computes the same offsets.  Lane (w, L) keeps the offsets of
+  // its accumulation window (cells w and w+S of its row) in registers and
+  // issues the copies of cells w and w + kGW of its row.
+  int p0c = 0, p1c = 0;  // window offsets of the planned unit (this lane)
+  // the staged columns X0-HL .. X0-HL+WX-1 need no periodic wrap along x
+  const bool row_contig = X0 - HL >= 0 && X0 - HL + WX <= P.N[0];
+  auto row_plan = [&](int par, int ob, bool& fits) -> int {
+    const int* b = nxb + par * NSC + L * WX;
+    const int* e = nxe + par * NSC + L * WX;
+    int run = 0, ow = 0, ows = 0, o1 = 0, n1 = 0, b1 = 0, o2 = 0, n2 = 0, b2 = 0;
+    if (row_contig) {
+      // the row's staged cells are consecutive keys: their particles are one
+      // run of the sorted order, and offsets inside the row are differences
+      // of the cell starts
+      const int r0 = b[0];
+      run = e[WX - 1] - r0;
+      b1 = b[w];
+      n1 = e[w] - b1;
+      ow = o1 = b1 - r0;
+      ows = w + S < WX ? b[w + S] - r0 : run;
+      if (w + kGW < WX) {
+        b2 = b[w + kGW];
+        n2 = e[w + kGW] - b2;
+        o2 = b2 - r0;
+      }
+    } else {
+#pragma unroll
+      for (int qx = 0; qx < WX; ++qx) {
+        const int bb = b[qx], cc = e[qx] - bb;
+        if (qx == w) {
+          ow = run;
+          o1 = run;
+          n1 = cc;
+          b1 = bb;
+        }
+        if (qx == w + S) ows = run;
+        if (qx == w + kGW) {
+          o2 = run;
+          n2 = cc;
+          b2 = bb;
+        }
+        run += cc;
+      }
+      if (w + S == WX) ows = run;
+    }
+    int inc = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (L >= o) inc += t;
+    }
+    const int total = __shfl_sync(0xffffffffu, inc, 31);
+    fits = total <= cap;
+    if (fits) {
+      const int base = inc - run;
+      p0c = base + ow;
+      p1c = base + ows;
+      unsigned char* q8 = sQ + ob * cap;
+      auto copy_cell = [&](int o0, int n, int64_t g0, int qx) {
+        for (int i = 0; i < n; ++i) {
+          const int o = o0 + i;
+          const int64_t sp = g0 + i;
+          uint4* d = raw + (size_t)o * IU;
+#pragma unroll
+          for (int t = 0; t < RU; ++t) {
+            if constexpr (WST)
+              cp_async16(d + t, grec + sp * RU + t);
+            else
+              cp_async16(d + t, grec + t * P.ps + sp);
+          }
+          cp_async16(d + RU, gus + sp);
+          q8[o] = (unsigned char)qx;
+        }
+      };
+      copy_cell(base + o1, n1, b1, w);
+      if (w + kGW < WX) copy_cell(base + o2, n2, b2, w + kGW);
+      cp_async_commit();
+    }
+    return total;
+  };
   // the sum over the warp's rows of ring slot k, component a of G for the
   // node row of this lane (lanes L .. L+S-1 contribute, nearest first)
   auto g_at = [&](int j, int k, int a) -> float {
@@ -862,12 +949,18 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
   int ph = wrap_index(cz - HL + 1, S);
   load_counts(cz);
   cp_async_wait_all();
-  publish();
-  if (cz < zlast) load_counts(cz + 1);
   __syncthreads();
-  int n_cur = plan(0, true);
+  if (cz < zlast) load_counts(cz + 1);
+  bool fast_cur;
+  int n_cur = row_plan(cz & 1, 0, fast_cur);
+  if (!fast_cur) {
+    // more particles than one unit holds: block-wide plan of equal shares
+    publish(cz & 1);
+    __syncthreads();
+    n_cur = plan(0, true);
+    issue(0);
+  }
   bool last_cur = left == 0;
-  issue(0);
 
   for (int u = 0;; ++u) {
     const int ub = u & 1;
@@ -916,24 +1009,30 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
     const int cz_u = cz;
     const bool last_u = last_cur;
     const int n_u = n_cur;
+    const bool fast_u = fast_cur;
+    const int p0u = p0c, p1u = p1c;
     bool more = true;
     if (last_u) {
       if (cz < zlast) {
         ++cz;
-        publish();
+        // the ranges of layer cz + 1 go to the buffer layer cz - 1 used
         if (cz < zlast) load_counts(cz + 1);
-        __syncthreads();
-        n_cur = plan(ub ^ 1, true);
+        n_cur = row_plan(cz & 1, ub ^ 1, fast_cur);
+        if (!fast_cur) {
+          publish(cz & 1);
+          __syncthreads();
+          n_cur = plan(ub ^ 1, true);
+          issue(ub ^ 1);
+        }
       } else {
         more = false;
       }
     } else {
       n_cur = plan(ub ^ 1, false);
-    }
-    if (more) {
-      last_cur = left == 0;
+      fast_cur = false;
       issue(ub ^ 1);
     }
+    if (more) last_cur = left == 0;
     // 3.-5. with the ring phase a compile-time constant
     auto body = [&](auto phc) {
       constexpr int PH = decltype(phc)::value;
@@ -942,7 +1041,7 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
         const int* off = offU + ub * (NSC + 1);
         const unsigned char* q8 = sQ + ub * cap;
         const int q0 = L * WX + w;
-        const int p0 = off[q0], p1 = off[q0 + S];
+        const int p0 = fast_u ? p0u : off[q0], p1 = fast_u ? p1u : off[q0 + S];
         nterm += p1 - p0;
         for (int p = p0; p < p1; ++p) {
           // x-weight of node X0 + w in the stencil of a particle of column c
