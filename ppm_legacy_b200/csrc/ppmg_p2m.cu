@@ -1145,14 +1145,18 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
 
 // Per (xy tile, cell layer): particles in the tile's own cells of that layer
 // (tiles of the span from (ox, oy), ex x ey nodes; cells outside 0 .. N-1
-// count none).
+// count none), stored tile-major: lc[tile * N2 + cz] (k_make_items walks a
+// tile's layers in one thread).
 __global__ void k_layer_counts(const int* __restrict__ start, int N0, int N1, int N2, int ox,
                                int oy, int ex, int ey, int tdx, int tdy, int tiles_x,
                                int ntiles, int* __restrict__ lc) {
   const int64_t n = (int64_t)ntiles * N2;
+  // i = cz * ntiles + tile: neighbouring threads take neighbouring tiles of
+  // one layer, whose row ends share sectors of start[] (186 -> 83 us at 512^3
+  // against layer-fastest threads)
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const int tile = (int)(i / N2), cz = (int)(i % N2);
+    const int tile = (int)(i % ntiles), cz = (int)(i / ntiles);
     const int tx0 = ox + (tile % tiles_x) * tdx, ty0 = oy + (tile / tiles_x) * tdy;
     const int X0 = max(tx0, 0), X1 = min(min(tx0 + tdx, ox + ex), N0);
     const int Y0 = max(ty0, 0), Y1 = min(min(ty0 + tdy, oy + ey), N1);
@@ -1161,7 +1165,7 @@ __global__ void k_layer_counts(const int* __restrict__ start, int N0, int N1, in
       const int64_t c0 = (int64_t)X0 + (int64_t)N0 * (y + (int64_t)N1 * cz);
       sum += start[c0 + (X1 - X0)] - start[c0];
     }
-    lc[i] = sum;
+    lc[(int64_t)tile * N2 + cz] = sum;
   }
 }
 
