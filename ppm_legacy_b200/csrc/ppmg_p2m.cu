@@ -629,11 +629,19 @@ __device__ __forceinline__ void scan_cells_w(int n, F val, int* out, int* wsum, 
   if (tid == 0) out[n] = red[0];
 }
 
-// 16-byte planes per staged particle of the row gather: wx, wz, and the
-// products wy(j) u(a) (S*LC values)
+// 16-byte planes per staged particle of the row gather after wx and wz:
+// the products wy(j) u(a) (S*LC values), or, when those take more than two
+// planes, wy and u themselves (each visit then forms the products wy(j) u(a)
+// again: S*LC/2 more packed multiplies, one 16-byte shared load fewer for
+// lda 3; the accumulation is bound by its shared wavefronts rather than its
+// multiplies)
+template <int S, int LC>
+constexpr bool g_raw_u() {
+  return S * LC > 8;
+}
 template <int S, int LC>
 constexpr int g_wyu_units() {
-  return (S * LC + 3) / 4;
+  return g_raw_u<S, LC>() ? 2 : (S * LC + 3) / 4;
 }
 template <int S, class OT, int LC, bool WST>
 constexpr size_t p2m3g_smem(int cap) {
@@ -679,7 +687,8 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   float4* sWX = reinterpret_cast<float4*>(smem);
   float4* sWZ = sWX + cap;
-  float4* sWYU = sWZ + cap;  // [UW][cap]: wy(j) u(a) at a * S + j
+  float4* sWYU = sWZ + cap;  // [UW][cap]: wy(j) u(a) at a * S + j, or wy and u
+  constexpr bool RAWU = g_raw_u<S, LC>();
   uint4* raw = reinterpret_cast<uint4*>(sWYU + UW * cap);  // [cap][IU] next unit
   int* cnt = reinterpret_cast<int*>(raw + (size_t)cap * IU);  // layer: particles per cell
   int* done = cnt + NSC;                                    // layer: particles already in units
@@ -991,17 +1000,22 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
       sWX[i] = make_float4(wv[0][0], wv[0][1], wv[0][2], wv[0][3]);
       sWZ[i] = make_float4(wv[2][0], wv[2][1], wv[2][2], wv[2][3]);
       const float4 u4 = *reinterpret_cast<const float4*>(r + RU);
-      const float uu[4] = {u4.x, u4.y, u4.z, u4.w};
-      float f[4 * UW];
+      if constexpr (RAWU) {
+        sWYU[i] = make_float4(wv[1][0], wv[1][1], wv[1][2], wv[1][3]);
+        sWYU[cap + i] = u4;
+      } else {
+        const float uu[4] = {u4.x, u4.y, u4.z, u4.w};
+        float f[4 * UW];
 #pragma unroll
-      for (int t = 0; t < 4 * UW; ++t) f[t] = 0.f;
+        for (int t = 0; t < 4 * UW; ++t) f[t] = 0.f;
 #pragma unroll
-      for (int aa = 0; aa < LC; ++aa)
+        for (int aa = 0; aa < LC; ++aa)
 #pragma unroll
-        for (int j = 0; j < S; ++j) f[aa * S + j] = wv[1][j] * uu[aa];
+          for (int j = 0; j < S; ++j) f[aa * S + j] = wv[1][j] * uu[aa];
 #pragma unroll
-      for (int t = 0; t < UW; ++t)
-        sWYU[t * cap + i] = make_float4(f[4 * t], f[4 * t + 1], f[4 * t + 2], f[4 * t + 3]);
+        for (int t = 0; t < UW; ++t)
+          sWYU[t * cap + i] = make_float4(f[4 * t], f[4 * t + 1], f[4 * t + 2], f[4 * t + 3]);
+      }
     }
     __syncthreads();
     // 2. plan and issue unit u+1 (the next layer's first unit when unit u
@@ -1048,29 +1062,52 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
           const int ix = w + S - 1 - (int)q8[p];
           const float wxi = sWXf[4 * p + ix];
           const float4 wz4 = sWZ[p];
-          float f[4 * UW];
-#pragma unroll
-          for (int t = 0; t < UW; ++t) {
-            const float4 v = sWYU[t * cap + p];
-            f[4 * t] = v.x;
-            f[4 * t + 1] = v.y;
-            f[4 * t + 2] = v.z;
-            f[4 * t + 3] = v.w;
-          }
           const float wz[4] = {wz4.x, wz4.y, wz4.z, wz4.w};
-          const float2 wx2 = make_float2(wxi, wxi);
-          // (wx wy(2J) u(a), wx wy(2J+1) u(a)) times wz(k), packed FP32 pairs
-#pragma unroll
-          for (int J = 0; J < S / 2; ++J)
+          if constexpr (RAWU) {
+            const float4 wy4 = sWYU[p];
+            const float4 u4 = sWYU[cap + p];
+            const float uu[4] = {u4.x, u4.y, u4.z, u4.w};
+            const float wy[4] = {wy4.x, wy4.y, wy4.z, wy4.w};
+            const float2 wx2 = make_float2(wxi, wxi);
+            // (wx (wy(2J) u(a)), wx (wy(2J+1) u(a))) times wz(k), packed FP32
+            // pairs: the products in the order of the staged form
 #pragma unroll
             for (int a = 0; a < LC; ++a) {
-              const float2 cu =
-                  __fmul2_rn(wx2, make_float2(f[a * S + 2 * J], f[a * S + 2 * J + 1]));
+              const float2 u2 = make_float2(uu[a], uu[a]);
 #pragma unroll
-              for (int k = 0; k < S; ++k)
-                G[J][(PH + k) % S][a] =
-                    __ffma2_rn(cu, make_float2(wz[k], wz[k]), G[J][(PH + k) % S][a]);
+              for (int J = 0; J < S / 2; ++J) {
+                const float2 cu =
+                    __fmul2_rn(wx2, __fmul2_rn(make_float2(wy[2 * J], wy[2 * J + 1]), u2));
+#pragma unroll
+                for (int k = 0; k < S; ++k)
+                  G[J][(PH + k) % S][a] =
+                      __ffma2_rn(cu, make_float2(wz[k], wz[k]), G[J][(PH + k) % S][a]);
+              }
             }
+          } else {
+            float f[4 * UW];
+#pragma unroll
+            for (int t = 0; t < UW; ++t) {
+              const float4 v = sWYU[t * cap + p];
+              f[4 * t] = v.x;
+              f[4 * t + 1] = v.y;
+              f[4 * t + 2] = v.z;
+              f[4 * t + 3] = v.w;
+            }
+            const float2 wx2 = make_float2(wxi, wxi);
+            // (wx wy(2J) u(a), wx wy(2J+1) u(a)) times wz(k), packed FP32 pairs
+#pragma unroll
+            for (int J = 0; J < S / 2; ++J)
+#pragma unroll
+              for (int a = 0; a < LC; ++a) {
+                const float2 cu =
+                    __fmul2_rn(wx2, make_float2(f[a * S + 2 * J], f[a * S + 2 * J + 1]));
+#pragma unroll
+                for (int k = 0; k < S; ++k)
+                  G[J][(PH + k) % S][a] =
+                      __ffma2_rn(cu, make_float2(wz[k], wz[k]), G[J][(PH + k) % S][a]);
+              }
+          }
         }
       }
       // 4. fold G into the node ring once a lane has added kFoldTerms
