@@ -647,9 +647,11 @@ template <int S, class OT, int LC, bool WST>
 constexpr size_t p2m3g_smem(int cap) {
   constexpr int NSC = (kGW + S - 1) * 32;
   constexpr int IU = p2m_rec_units<S, float, OT, WST>() + 1;
-  // per slot: the weight planes, the raw next unit, 2 column bytes
-  return (size_t)cap * (16 * (2 + g_wyu_units<S, LC>()) + 16 * IU + 2) +
-         sizeof(int) * (size_t)(10 * NSC + 2);
+  // per slot: the weight planes and the raw next unit; per thread and unit
+  // buffer: the S-1 inner boundaries of its accumulation window
+  return (size_t)cap * (16 * (2 + g_wyu_units<S, LC>()) + 16 * IU) +
+         sizeof(int) * (size_t)(10 * NSC + 2) +
+         sizeof(unsigned short) * (size_t)(2 * (S - 1) * kGW * 32);
 }
 // staging slots of the row gather: as many as fit in ~110 KB (two CTAs per
 // SM), a multiple of 16
@@ -698,7 +700,8 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
   // cell ranges of a layer, [layer parity][NSC]: loaded one layer ahead
   int* nxb = offU + 2 * (NSC + 1);
   int* nxe = nxb + 2 * NSC;
-  unsigned char* sQ = reinterpret_cast<unsigned char*>(nxe + 2 * NSC);  // [2][cap] staged columns
+  // [2][S-1][NT]: inner cell boundaries of each lane's accumulation window
+  unsigned short* sB = reinterpret_cast<unsigned short*>(nxe + 2 * NSC);
   const float* sWXf = reinterpret_cast<const float*>(sWX);
   __shared__ int wsum[kGW];
   __shared__ int red[2];
@@ -832,7 +835,6 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
   };
   auto issue = [&](int ob) {
     const int* off = offU + ob * (NSC + 1);
-    unsigned char* q8 = sQ + ob * cap;
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
       const int q = 3 * tid + i;
@@ -850,7 +852,6 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
               cp_async16(d + t, grec + t * P.ps + s);
           }
           cp_async16(d + RU, gus + s);
-          q8[o] = (unsigned char)(q % WX);
         }
       }
     }
@@ -870,6 +871,9 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
     const int* b = nxb + par * NSC + L * WX;
     const int* e = nxe + par * NSC + L * WX;
     int run = 0, ow = 0, ows = 0, o1 = 0, n1 = 0, b1 = 0, o2 = 0, n2 = 0, b2 = 0;
+    int oin[S - 1];  // inner window boundaries (cells w+1 .. w+S-1), within the row
+#pragma unroll
+    for (int k = 0; k < S - 1; ++k) oin[k] = 0;
     if (row_contig) {
       // the row's staged cells are consecutive keys: their particles are one
       // run of the sorted order, and offsets inside the row are differences
@@ -880,6 +884,8 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
       n1 = e[w] - b1;
       ow = o1 = b1 - r0;
       ows = w + S < WX ? b[w + S] - r0 : run;
+#pragma unroll
+      for (int k = 0; k < S - 1; ++k) oin[k] = b[w + 1 + k] - r0;
       if (w + kGW < WX) {
         b2 = b[w + kGW];
         n2 = e[w + kGW] - b2;
@@ -896,6 +902,9 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
           b1 = bb;
         }
         if (qx == w + S) ows = run;
+#pragma unroll
+        for (int k = 0; k < S - 1; ++k)
+          if (qx == w + 1 + k) oin[k] = run;
         if (qx == w + kGW) {
           o2 = run;
           n2 = cc;
@@ -917,8 +926,10 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
       const int base = inc - run;
       p0c = base + ow;
       p1c = base + ows;
-      unsigned char* q8 = sQ + ob * cap;
-      auto copy_cell = [&](int o0, int n, int64_t g0, int qx) {
+#pragma unroll
+      for (int k = 0; k < S - 1; ++k)
+        sB[(ob * (S - 1) + k) * NT + tid] = (unsigned short)(base + oin[k]);
+      auto copy_cell = [&](int o0, int n, int64_t g0) {
         for (int i = 0; i < n; ++i) {
           const int o = o0 + i;
           const int64_t sp = g0 + i;
@@ -931,11 +942,10 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
               cp_async16(d + t, grec + t * P.ps + sp);
           }
           cp_async16(d + RU, gus + sp);
-          q8[o] = (unsigned char)qx;
         }
       };
-      copy_cell(base + o1, n1, b1, w);
-      if (w + kGW < WX) copy_cell(base + o2, n2, b2, w + kGW);
+      copy_cell(base + o1, n1, b1);
+      if (w + kGW < WX) copy_cell(base + o2, n2, b2);
       cp_async_commit();
     }
     return total;
@@ -1053,13 +1063,19 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
       // 3. accumulate unit u: the particles of cells w .. w+S-1 of row L
       if (n_u > 0) {
         const int* off = offU + ub * (NSC + 1);
-        const unsigned char* q8 = sQ + ub * cap;
         const int q0 = L * WX + w;
         const int p0 = fast_u ? p0u : off[q0], p1 = fast_u ? p1u : off[q0 + S];
+        // the window's inner cell boundaries: a particle of cell w + m
+        // (m boundaries at or below it) takes x-weight S-1-m for node X0 + w
+        int bnd[S - 1];
+#pragma unroll
+        for (int k = 0; k < S - 1; ++k)
+          bnd[k] = fast_u ? (int)sB[(ub * (S - 1) + k) * NT + tid] : off[q0 + 1 + k];
         nterm += p1 - p0;
         for (int p = p0; p < p1; ++p) {
-          // x-weight of node X0 + w in the stencil of a particle of column c
-          const int ix = w + S - 1 - (int)q8[p];
+          int ix = S - 1;
+#pragma unroll
+          for (int k = 0; k < S - 1; ++k) ix -= p >= bnd[k] ? 1 : 0;
           const float wxi = sWXf[4 * p + ix];
           const float4 wz4 = sWZ[p];
           const float wz[4] = {wz4.x, wz4.y, wz4.z, wz4.w};
