@@ -203,6 +203,22 @@ class DistComm:
     def _rank(self, s):
         return int(s if self.sub_to_rank is None else self.sub_to_rank[s])
 
+    def posting_order(self, sends, recvs):
+        """The order in which this rank posts its sends and receives.
+
+        NCCL pairs the point-to-point messages between two ranks in the
+        order they are posted and ignores tags (gloo matches tags).  Sends
+        are posted sorted by (destination rank, source subdomain, destination
+        subdomain, tag) and receives by (source rank, the same triple), so
+        the k-th send from rank A to rank B meets the k-th receive at B from
+        A whatever order the plans list them in.
+        """
+        so = sorted(range(len(sends)),
+                    key=lambda i: (self._rank(sends[i][1]), sends[i][0], sends[i][1], sends[i][2]))
+        ro = sorted(range(len(recvs)),
+                    key=lambda i: (self._rank(recvs[i][1]), recvs[i][1], recvs[i][0], recvs[i][2]))
+        return so, ro
+
     def exchange(self, sends, recvs):
         import torch
         import torch.distributed as dist
@@ -217,17 +233,20 @@ class DistComm:
         def wire(t):
             return t.to(dev) if t.device != dev else t.contiguous()
 
-        ops, bufs, local = [], [], {}
-        for src, dst, tag, t in sends:
+        so, ro = self.posting_order(sends, recvs)
+        ops, local = [], {}
+        bufs = [torch.empty_like(like, memory_format=torch.contiguous_format, device=dev)
+                for _, _, _, like in recvs]
+        for i in so:
+            src, dst, tag, t = sends[i]
             if self._rank(dst) == me:
                 local[(src, dst, tag)] = t
             else:
                 ops.append(dist.P2POp(dist.isend, wire(t), self._peer(dst), self.group, tag))
-        for dst, src, tag, like in recvs:
-            buf = torch.empty_like(like, memory_format=torch.contiguous_format, device=dev)
-            bufs.append(buf)
+        for i in ro:
+            dst, src, tag, like = recvs[i]
             if self._rank(src) != me:
-                ops.append(dist.P2POp(dist.irecv, buf, self._peer(src), self.group, tag))
+                ops.append(dist.P2POp(dist.irecv, bufs[i], self._peer(src), self.group, tag))
         if ops:
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
@@ -465,6 +484,9 @@ class DistMover:
         r = int(s if self.sub_to_rank is None else self.sub_to_rank[s])
         return r if self.group is None else dist.get_global_rank(self.group, r)
 
+    def _rank(self, s):
+        return int(s if self.sub_to_rank is None else self.sub_to_rank[s])
+
     def exchange(self, me, sends, recvs, on_device, stream):
         import torch
         import torch.distributed as dist
@@ -474,6 +496,10 @@ class DistMover:
         def tensor_of(data):
             return torch.frombuffer(bytearray(data), dtype=torch.uint8).to(dev)
 
+        # posted in the order of DistComm.posting_order: NCCL pairs the
+        # messages of two ranks in posting order, not by tag
+        sends = sorted(sends, key=lambda m: (self._rank(m[0]), me, m[0], m[1]))
+        recvs = sorted(recvs, key=lambda m: (self._rank(m[0]), m[0], me, m[1]))
         ops, bufs = [], []
         for peer, tag, addr, n in sends:
             t = tensor_of(_read_block(addr, n, on_device, stream))

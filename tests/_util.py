@@ -120,3 +120,42 @@ def moment_errors(U, h, xp, up, lo=0.0):
     v, a = particle_moments(xp, up)
     rel = np.abs(m - v) / np.where(a > 0, a, 1.0)
     return [float(rel[k].max()) for k in range(3)]
+
+
+class PairOrderComm:
+    """Every subdomain in this process, subdomain s on rank s, matched the way
+    NCCL matches point-to-point messages: the k-th send one rank posts to
+    another meets the k-th receive that rank posts from it, tags not
+    compared.  Each subdomain posts in the order DistComm.posting_order
+    gives, so a plan whose sides list their messages in different orders
+    fails here (shape mismatch or wrong values) as it would over NCCL."""
+
+    def __init__(self):
+        from ppm_legacy_b200 import halo
+        self.order = halo.DistComm()
+
+    def exchange(self, sends, recvs):
+        import collections
+        by_src = collections.defaultdict(list)
+        for i, m in enumerate(sends):
+            by_src[m[0]].append(i)
+        queues = collections.defaultdict(collections.deque)
+        for src, idx in by_src.items():
+            mine = [sends[i] for i in idx]
+            so, _ = self.order.posting_order(mine, [])
+            for k in so:
+                queues[(src, mine[k][1])].append(mine[k][3])
+        by_dst = collections.defaultdict(list)
+        for i, r in enumerate(recvs):
+            by_dst[r[0]].append(i)
+        out = [None] * len(recvs)
+        for dst, idx in by_dst.items():
+            mine = [recvs[i] for i in idx]
+            _, ro = self.order.posting_order([], mine)
+            for k in ro:
+                src, like = mine[k][1], mine[k][3]
+                blk = queues[(src, dst)].popleft()
+                if blk.shape != like.shape:
+                    raise ValueError("messages paired out of order (block shapes differ)")
+                out[idx[k]] = blk.clone()
+        return out

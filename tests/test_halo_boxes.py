@@ -13,6 +13,7 @@ import numpy as np
 import pytest
 
 from _util import random_particles, topo_for, unique_view
+import _util as U  # noqa: E402
 from oracle import oracle as O
 from ppm_legacy_b200 import halo
 
@@ -171,6 +172,24 @@ def test_python_exchange_in_one_process(decomp, g):
         r = real(t, s, g)
         assert np.abs(f[s].numpy()[..., 0][r] - want[s][r]).max() <= 1e-13 * scale, s
     halo.get(f, t, list(g), lb, halo.LocalComm())
+    for s in f:
+        assert np.abs(f[s].numpy()[..., 0] - want[s]).max() <= 1e-13 * scale, s
+
+
+@pytest.mark.parametrize("decomp,g", [((2, 2, 2), (2, 2, 2)), ((2, 1, 1), (2, 2, 2)),
+                                       ((3, 1, 2), (1, 1, 2)), ((1, 2, 1), (1, 2, 1))])
+def test_python_exchange_with_nccl_pairing(decomp, g):
+    # the boxes of one neighbour and periodic shift: several messages between
+    # the same two ranks, paired in posting order as NCCL pairs them
+    t, local, want = case(12, decomp, 2, g, 2, seed=37)
+    scale = max(np.abs(w).max() for w in want.values())
+    f = fortran_fields(local)
+    lb = [1 - g[a] for a in range(3)]
+    halo.put(f, t, list(g), lb, U.PairOrderComm())
+    for s in f:
+        r = real(t, s, g)
+        assert np.abs(f[s].numpy()[..., 0][r] - want[s][r]).max() <= 1e-13 * scale, s
+    halo.get(f, t, list(g), lb, U.PairOrderComm())
     for s in f:
         assert np.abs(f[s].numpy()[..., 0] - want[s]).max() <= 1e-13 * scale, s
 

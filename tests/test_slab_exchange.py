@@ -22,6 +22,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 sys.path.insert(0, ROOT)
 from _util import random_particles, topo_for, unique_view  # noqa: E402
+import _util as U  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 from ppm_legacy_b200 import halo  # noqa: E402
 
@@ -91,6 +92,22 @@ def test_put_then_get_in_one_process(nc, nslab, kernel, g, lda):
     for s in fields:
         check_put(t, s, fields[s].numpy(), want[s], g)
     halo.get(fields, t, [g] * 3, lb, halo.LocalComm())
+    for s in fields:
+        check_get(t, s, fields[s].numpy(), want[s], g)
+
+
+@pytest.mark.parametrize("nc,nslab,g", [(12, 2, 2), (12, 3, 1), (16, 4, 3)])
+def test_put_then_get_with_nccl_pairing(nc, nslab, g):
+    # NCCL pairs the messages of two ranks in posting order, not by tag: with
+    # two slabs both neighbours are the same rank, and the up and down blocks
+    # must still meet their own receives
+    t, local, want = case(nc, nslab, 2, g, 2, seed=nc + 7 * nslab)
+    fields = {s: torch.from_numpy(local[s]) for s in local}
+    lb = [1 - g] * 3
+    halo.put(fields, t, [g] * 3, lb, U.PairOrderComm())
+    for s in fields:
+        check_put(t, s, fields[s].numpy(), want[s], g)
+    halo.get(fields, t, [g] * 3, lb, U.PairOrderComm())
     for s in fields:
         check_get(t, s, fields[s].numpy(), want[s], g)
 
