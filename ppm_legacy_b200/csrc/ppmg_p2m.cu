@@ -211,8 +211,10 @@ constexpr size_t p2m3d_smem(int cap) {
          sizeof(int) * (size_t)(8 * NSC + 2);
 }
 
+// The FP64 form's gather (the compensated FP32 form runs in k_p2m3g).
 template <int S, class CT, bool COMP, class OT, int LC, bool WST>
 __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
+  static_assert(!COMP, "plain sums only");
   using V = typename Vec4<CT>::type;
   constexpr int HL = S / 2;
   constexpr int HH = S / 2 - 1;
@@ -261,14 +263,13 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
   const uint4* grec = static_cast<const uint4*>(P.rec);
   const uint4* gus = static_cast<const uint4*>(P.us);
 
-  CT acc[2][S][LC];  // window (or per-unit partials when COMP)
-  CT hi[2][S][LC], lo[2][S][LC];
+  CT acc[2][S][LC];  // the node window of the thread's two columns
 #pragma unroll
   for (int e = 0; e < 2; ++e)
 #pragma unroll
     for (int k = 0; k < S; ++k)
 #pragma unroll
-      for (int a = 0; a < LC; ++a) acc[e][k][a] = hi[e][k][a] = lo[e][k][a] = CT(0);
+      for (int a = 0; a < LC; ++a) acc[e][k][a] = CT(0);
 
   // cell ranges of the staged cells of layer cz: copied asynchronously into
   // nxb / nxe (each thread its own cells), published a unit or more later
@@ -400,7 +401,6 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
   __syncthreads();
   int n_cur = plan(0, true);
   bool last_cur = left == 0;  // the unit in flight completes its layer
-  bool first_cur = true;      // the unit in flight opens its layer
   issue(0);
 
   for (int u = 0;; ++u) {
@@ -442,8 +442,6 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
     //    completes its layer); its loads fly while unit u is accumulated
     const int cz_u = cz;
     const bool last_u = last_cur;
-    const bool first_u = first_cur;
-    first_cur = last_u;
     const int n_u = n_cur;
     bool more = true;
     if (last_u) {
@@ -494,26 +492,6 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
         }
       }
     }
-    if constexpr (COMP) {
-      // fold the unit's partial sums (every unit: total strength stays
-      // conserved to ~1e-11 of sum |u|)
-      // Two slots skip the TwoSum: the newest slot on the layer's first unit
-      // still holds (0, 0), so the fold is a move; slot 0 on the layer's last
-      // unit keeps its partial, which step 4 adds to (hi, lo) in FP64.
-#pragma unroll
-      for (int e = 0; e < 2; ++e)
-#pragma unroll
-        for (int k = 0; k < S; ++k)
-#pragma unroll
-          for (int a = 0; a < LC; ++a) {
-            if (k == 0 && last_u) continue;
-            if (k == S - 1 && first_u)
-              hi[e][k][a] = acc[e][k][a];
-            else
-              two_sum_fold<CT>(hi[e][k][a], lo[e][k][a], acc[e][k][a]);
-            acc[e][k][a] = CT(0);
-          }
-    }
     // 4. layer complete: node zc = cz_u - (HL-1) of both columns is final: emit, shift
     if (last_u) {
       const int zc = cz_u - (HL - 1);
@@ -522,35 +500,15 @@ __global__ void __launch_bounds__(kTX * kTY, 2) k_p2m3d(P2MParams P) {
         if ((e == 0 ? act0 : act1) && zc >= Z0 && zc < Z1) {
           double v[LC];
 #pragma unroll
-          for (int a = 0; a < LC; ++a)
-            v[a] = COMP ? ((double)hi[e][0][a] + (double)lo[e][0][a]) + (double)acc[e][0][a]
-                        : (double)acc[e][0][a];
+          for (int a = 0; a < LC; ++a) v[a] = (double)acc[e][0][a];
           emit_node<3, OT, LC>(P, x0 + e, y, zc, v);
-        }
-        if constexpr (COMP) {
-#pragma unroll
-          for (int a = 0; a < LC; ++a) acc[e][0][a] = CT(0);
         }
 #pragma unroll
         for (int k = 0; k < S - 1; ++k)
 #pragma unroll
-          for (int a = 0; a < LC; ++a) {
-            if constexpr (COMP) {
-              hi[e][k][a] = hi[e][k + 1][a];
-              lo[e][k][a] = lo[e][k + 1][a];
-            } else {
-              acc[e][k][a] = acc[e][k + 1][a];
-            }
-          }
+          for (int a = 0; a < LC; ++a) acc[e][k][a] = acc[e][k + 1][a];
 #pragma unroll
-        for (int a = 0; a < LC; ++a) {
-          if constexpr (COMP) {
-            hi[e][S - 1][a] = CT(0);
-            lo[e][S - 1][a] = CT(0);
-          } else {
-            acc[e][S - 1][a] = CT(0);
-          }
-        }
+        for (int a = 0; a < LC; ++a) acc[e][S - 1][a] = CT(0);
       }
     }
     if (!more) break;
