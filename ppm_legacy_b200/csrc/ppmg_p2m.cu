@@ -550,42 +550,6 @@ constexpr int g_rows() {
   return 33 - S;  // node rows per tile
 }
 
-// Exclusive scan over n <= 3 * 32 * NW cell values (thread t owns cells
-// 3t .. 3t+2) by a CTA of NW warps; as scan_cells.
-template <int NW, class F>
-__device__ __forceinline__ void scan_cells_w(int n, F val, int* out, int* wsum, int* red) {
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  const int q0 = 3 * tid;
-  const int v0 = q0 < n ? val(q0) : 0;
-  const int v1 = q0 + 1 < n ? val(q0 + 1) : 0;
-  const int v2 = q0 + 2 < n ? val(q0 + 2) : 0;
-  const int s = v0 + v1 + v2;
-  int inc = s;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int t = __shfl_up_sync(0xffffffffu, inc, o);
-    if (lane >= o) inc += t;
-  }
-  if (lane == 31) wsum[wid] = inc;
-  __syncthreads();
-  if (wid == 0) {
-    const int w = lane < NW ? wsum[lane] : 0;
-    int wi = w;
-#pragma unroll
-    for (int o = 1; o < NW; o <<= 1) {
-      const int t = __shfl_up_sync(0xffffffffu, wi, o);
-      if (lane >= o) wi += t;
-    }
-    if (lane < NW) wsum[lane] = wi - w;
-    if (lane == NW - 1) red[0] = wi;
-  }
-  __syncthreads();
-  const int ex = inc - s + wsum[wid];
-  if (q0 < n) out[q0] = ex;
-  if (q0 + 1 < n) out[q0 + 1] = ex + v0;
-  if (q0 + 2 < n) out[q0 + 2] = ex + v0 + v1;
-  if (tid == 0) out[n] = red[0];
-}
 
 // 16-byte planes per staged particle of the row gather after wx and wz:
 // the products wy(j) u(a) (S*LC values), or, when those take more than two
@@ -608,7 +572,7 @@ constexpr size_t p2m3g_smem(int cap) {
   // per slot: the weight planes and the raw next unit; per thread and unit
   // buffer: the S-1 inner boundaries of its accumulation window
   return (size_t)cap * (16 * (2 + g_wyu_units<S, LC>()) + 16 * IU) +
-         sizeof(int) * (size_t)(10 * NSC + 2) +
+         sizeof(int) * (size_t)(6 * NSC) +
          sizeof(unsigned short) * (size_t)(2 * (S - 1) * kGW * 32);
 }
 // staging slots of the row gather: as many as fit in ~110 KB (two CTAs per
@@ -631,7 +595,6 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
   constexpr int PERC = (NSC + NT - 1) / NT;
   constexpr int RU = p2m_rec_units<S, float, OT, WST>();
   constexpr int IU = RU + 1;
-  static_assert(NSC <= 3 * NT, "staged cells exceed the scan width");
   static_assert(S <= 4 && LC <= 4, "stencil / components");
 
   if ((int)blockIdx.x >= *P.nitems) return;
@@ -650,19 +613,15 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
   float4* sWYU = sWZ + cap;  // [UW][cap]: wy(j) u(a) at a * S + j, or wy and u
   constexpr bool RAWU = g_raw_u<S, LC>();
   uint4* raw = reinterpret_cast<uint4*>(sWYU + UW * cap);  // [cap][IU] next unit
-  int* cnt = reinterpret_cast<int*>(raw + (size_t)cap * IU);  // layer: particles per cell
-  int* done = cnt + NSC;                                    // layer: particles already in units
-  int* cbase = done + NSC;                                  // layer: first sorted particle per cell
-  int* ubase = cbase + NSC;                                 // unit being issued: first particle per cell
-  int* offU = ubase + NSC;                                  // [2][NSC + 1] unit offsets per cell
   // cell ranges of a layer, [layer parity][NSC]: loaded one layer ahead
-  int* nxb = offU + 2 * (NSC + 1);
+  int* nxb = reinterpret_cast<int*>(raw + (size_t)cap * IU);
   int* nxe = nxb + 2 * NSC;
+  // [unit parity][NSC]: particles of each cell taken by the units before
+  // (read by the plan of a unit) and with it (written by that plan)
+  int* dn = nxe + 2 * NSC;
   // [2][S-1][NT]: inner cell boundaries of each lane's accumulation window
-  unsigned short* sB = reinterpret_cast<unsigned short*>(nxe + 2 * NSC);
+  unsigned short* sB = reinterpret_cast<unsigned short*>(dn + 2 * NSC);
   const float* sWXf = reinterpret_cast<const float*>(sWX);
-  __shared__ int wsum[kGW];
-  __shared__ int red[2];
 
   const int tid = threadIdx.x;
   const int w = tid >> 5, L = tid & 31;
@@ -733,180 +692,158 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
       }
     }
   };
-  auto publish = [&](int par) {
-#pragma unroll
-    for (int k = 0; k < PERC; ++k) {
-      const int q = tid + NT * k;
-      if (q < NSC) {
-        const int b = nxb[par * NSC + q], e = nxe[par * NSC + q];
-        cbase[q] = b;
-        cnt[q] = e - b;
-        done[q] = 0;
-      }
-    }
-  };
-  int left = 0;
-  auto plan = [&](int ob, bool first) -> int {
-    int* off = offU + ob * (NSC + 1);
-    if (first) {
-      scan_cells_w<kGW>(NSC, [&](int q) { return cnt[q]; }, off, wsum, red);
-      left = red[0];
-      if (left <= cap) {
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-          const int q = 3 * tid + i;
-          if (q < NSC) {
-            ubase[q] = cbase[q];
-            done[q] = cnt[q];
-          }
-        }
-        const int n = left;
-        left = 0;
-        __syncthreads();
-        return n;
-      }
-    }
-    scan_cells_w<kGW>(NSC, [&](int q) { return cnt[q] > done[q] ? 1 : 0; }, off, wsum, red);
-    const int A = max(red[0], 1);
-    const int kk = cap / A, rem = cap - A * kk;
-    auto take_of = [&](int q) {
-      const int l = q < NSC ? cnt[q] - done[q] : 0;
-      return l > 0 ? min(l, kk + (off[q] < rem ? 1 : 0)) : 0;
-    };
-    const int t0 = take_of(3 * tid), t1 = take_of(3 * tid + 1), t2 = take_of(3 * tid + 2);
-    __syncthreads();
-    scan_cells_w<kGW>(
-        NSC, [&](int q) { const int i = q - 3 * tid; return i == 0 ? t0 : (i == 1 ? t1 : t2); },
-        off, wsum, red);
-    const int n = red[0];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      const int q = 3 * tid + i;
-      if (q < NSC) {
-        ubase[q] = cbase[q] + done[q];
-        done[q] += i == 0 ? t0 : (i == 1 ? t1 : t2);
-      }
-    }
-    left -= n;
-    __syncthreads();
-    return n;
-  };
-  auto issue = [&](int ob) {
-    const int* off = offU + ob * (NSC + 1);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      const int q = 3 * tid + i;
-      if (q < NSC) {
-        const int o0 = off[q], o1 = off[q + 1];
-        const int64_t g0 = ubase[q];
-        for (int o = o0; o < o1; ++o) {
-          const int64_t s = g0 + (o - o0);
-          uint4* d = raw + (size_t)o * IU;
-#pragma unroll
-          for (int t = 0; t < RU; ++t) {
-            if constexpr (WST)
-              cp_async16(d + t, grec + s * RU + t);
-            else
-              cp_async16(d + t, grec + t * P.ps + s);
-          }
-          cp_async16(d + RU, gus + s);
-        }
-      }
-    }
-    cp_async_commit();
-  };
-  // Plan of a layer whose staged particles fit one unit, without block
-  // barriers.  Unit slots follow the staged cells in row-major order, so lane
-  // L of every warp walks row L (its WX cell ranges) for the prefix within
-  // the row, and a warp scan over the 32 row totals gives the row bases:
-  // every warp computes the same offsets.  Lane (w, L) keeps the offsets of
-  // its accumulation window (cells w and w+S of its row) in registers and
-  // issues the copies of cells w and w + kGW of its row.
+  // Plan of a unit, without block barriers.  Unit slots follow the staged
+  // cells in row-major order, so lane L of every warp walks row L's cell
+  // ranges, and warp scans over the 32 rows give the row bases: every warp
+  // computes the same plan.  Lane (w, L) keeps its accumulation window's
+  // offsets (cells w .. w+S of its row) in registers and shared memory and
+  // copies the particles of cells w and w + kGW of its row.
+  // A layer's first unit takes all of its particles when they fit `cap`
+  // (O(1) row offsets when the staged columns need no periodic wrap, since
+  // the row's cells are then consecutive keys).  Else every unit gives each
+  // cell with particles left an equal share of `cap` (the first `rem` such
+  // cells one more), the taken counts kept per cell in dn.
   int p0c = 0, p1c = 0;  // window offsets of the planned unit (this lane)
+  int left = 0;          // particles of the layer not yet in a unit
   // the staged columns X0-HL .. X0-HL+WX-1 need no periodic wrap along x
   const bool row_contig = X0 - HL >= 0 && X0 - HL + WX <= P.N[0];
-  auto row_plan = [&](int par, int ob, bool& fits) -> int {
-    const int* b = nxb + par * NSC + L * WX;
-    const int* e = nxe + par * NSC + L * WX;
-    int run = 0, ow = 0, ows = 0, o1 = 0, n1 = 0, b1 = 0, o2 = 0, n2 = 0, b2 = 0;
-    int oin[S - 1];  // inner window boundaries (cells w+1 .. w+S-1), within the row
+  auto copy_cell = [&](int o0, int n, int64_t g0) {
+    for (int i = 0; i < n; ++i) {
+      const int o = o0 + i;
+      const int64_t sp = g0 + i;
+      uint4* d = raw + (size_t)o * IU;
 #pragma unroll
-    for (int k = 0; k < S - 1; ++k) oin[k] = 0;
-    if (row_contig) {
-      // the row's staged cells are consecutive keys: their particles are one
-      // run of the sorted order, and offsets inside the row are differences
-      // of the cell starts
-      const int r0 = b[0];
-      run = e[WX - 1] - r0;
-      b1 = b[w];
-      n1 = e[w] - b1;
-      ow = o1 = b1 - r0;
-      ows = w + S < WX ? b[w + S] - r0 : run;
-#pragma unroll
-      for (int k = 0; k < S - 1; ++k) oin[k] = b[w + 1 + k] - r0;
-      if (w + kGW < WX) {
-        b2 = b[w + kGW];
-        n2 = e[w + kGW] - b2;
-        o2 = b2 - r0;
+      for (int t = 0; t < RU; ++t) {
+        if constexpr (WST)
+          cp_async16(d + t, grec + sp * RU + t);
+        else
+          cp_async16(d + t, grec + t * P.ps + sp);
       }
-    } else {
-#pragma unroll
-      for (int qx = 0; qx < WX; ++qx) {
-        const int bb = b[qx], cc = e[qx] - bb;
-        if (qx == w) {
-          ow = run;
-          o1 = run;
-          n1 = cc;
-          b1 = bb;
-        }
-        if (qx == w + S) ows = run;
-#pragma unroll
-        for (int k = 0; k < S - 1; ++k)
-          if (qx == w + 1 + k) oin[k] = run;
-        if (qx == w + kGW) {
-          o2 = run;
-          n2 = cc;
-          b2 = bb;
-        }
-        run += cc;
-      }
-      if (w + S == WX) ows = run;
+      cp_async16(d + RU, gus + sp);
     }
+  };
+  // the row offsets (run: the row's total) become unit offsets, the window
+  // is published, and the owned cells are copied
+  auto finish_plan = [&](int ob, int run, int ow, int ows, const int* oin, int o1, int n1,
+                         int64_t b1, int o2, int n2, int64_t b2) -> int {
     int inc = run;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const int t = __shfl_up_sync(0xffffffffu, inc, o);
       if (L >= o) inc += t;
     }
-    const int total = __shfl_sync(0xffffffffu, inc, 31);
-    fits = total <= cap;
-    if (fits) {
-      const int base = inc - run;
-      p0c = base + ow;
-      p1c = base + ows;
+    const int n = __shfl_sync(0xffffffffu, inc, 31);
+    const int base = inc - run;
+    p0c = base + ow;
+    p1c = base + ows;
+#pragma unroll
+    for (int k = 0; k < S - 1; ++k)
+      sB[(ob * (S - 1) + k) * NT + tid] = (unsigned short)(base + oin[k]);
+    copy_cell(base + o1, n1, b1);
+    if (w + kGW < WX) copy_cell(base + o2, n2, b2);
+    cp_async_commit();
+    return n;
+  };
+  auto plan_unit = [&](int par, int ob, bool first) -> int {
+    const int* b = nxb + par * NSC + L * WX;
+    const int* e = nxe + par * NSC + L * WX;
+    int oin[S - 1];  // inner window boundaries (cells w+1 .. w+S-1), within the row
+#pragma unroll
+    for (int k = 0; k < S - 1; ++k) oin[k] = 0;
+    if (first) {
+      int run = 0, ow = 0, ows = 0, o1 = 0, n1 = 0, b1 = 0, o2 = 0, n2 = 0, b2 = 0;
+      if (row_contig) {
+        const int r0 = b[0];
+        run = e[WX - 1] - r0;
+        b1 = b[w];
+        n1 = e[w] - b1;
+        ow = o1 = b1 - r0;
+        ows = w + S < WX ? b[w + S] - r0 : run;
+#pragma unroll
+        for (int k = 0; k < S - 1; ++k) oin[k] = b[w + 1 + k] - r0;
+        if (w + kGW < WX) {
+          b2 = b[w + kGW];
+          n2 = e[w + kGW] - b2;
+          o2 = b2 - r0;
+        }
+      } else {
+#pragma unroll
+        for (int qx = 0; qx < WX; ++qx) {
+          const int bb = b[qx], cc = e[qx] - bb;
+          if (qx == w) {
+            ow = o1 = run;
+            n1 = cc;
+            b1 = bb;
+          }
+          if (qx == w + S) ows = run;
+#pragma unroll
+          for (int k = 0; k < S - 1; ++k)
+            if (qx == w + 1 + k) oin[k] = run;
+          if (qx == w + kGW) {
+            o2 = run;
+            n2 = cc;
+            b2 = bb;
+          }
+          run += cc;
+        }
+        if (w + S == WX) ows = run;
+      }
+      const int total = __reduce_add_sync(0xffffffffu, run);
+      if (total <= cap) {
+        left = 0;
+        return finish_plan(ob, run, ow, ows, oin, o1, n1, b1, o2, n2, b2);
+      }
+    }
+    // equal shares: dn[ob] holds the counts taken before (none on the
+    // layer's first unit), dn[ob ^ 1] gets the counts after this unit
+    const int* dc = dn + ob * NSC + L * WX;
+    int* dx = dn + (ob ^ 1) * NSC + L * WX;
+    int rl = 0, ra = 0;
+#pragma unroll
+    for (int qx = 0; qx < WX; ++qx) {
+      const int l = e[qx] - b[qx] - (first ? 0 : dc[qx]);
+      rl += l;
+      ra += l > 0 ? 1 : 0;
+    }
+    const int tot = __reduce_add_sync(0xffffffffu, rl);
+    const int A = max(__reduce_add_sync(0xffffffffu, ra), 1);
+    const int kk = cap / A, rem = cap - A * kk;
+    int rk = ra;  // rank of the row's first cell with particles left: exclusive scan
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, rk, o);
+      if (L >= o) rk += t;
+    }
+    rk -= ra;
+    int run = 0, ow = 0, ows = 0, o1 = 0, n1 = 0, o2 = 0, n2 = 0;
+    int64_t b1 = 0, b2 = 0;
+#pragma unroll
+    for (int qx = 0; qx < WX; ++qx) {
+      const int d = first ? 0 : dc[qx];
+      const int l = e[qx] - b[qx] - d;
+      const int t = l > 0 ? min(l, kk + (rk < rem ? 1 : 0)) : 0;
+      rk += l > 0 ? 1 : 0;
+      if (qx == w) {
+        ow = o1 = run;
+        n1 = t;
+        b1 = (int64_t)b[qx] + d;
+      }
+      if (qx == w + S) ows = run;
 #pragma unroll
       for (int k = 0; k < S - 1; ++k)
-        sB[(ob * (S - 1) + k) * NT + tid] = (unsigned short)(base + oin[k]);
-      auto copy_cell = [&](int o0, int n, int64_t g0) {
-        for (int i = 0; i < n; ++i) {
-          const int o = o0 + i;
-          const int64_t sp = g0 + i;
-          uint4* d = raw + (size_t)o * IU;
-#pragma unroll
-          for (int t = 0; t < RU; ++t) {
-            if constexpr (WST)
-              cp_async16(d + t, grec + sp * RU + t);
-            else
-              cp_async16(d + t, grec + t * P.ps + sp);
-          }
-          cp_async16(d + RU, gus + sp);
-        }
-      };
-      copy_cell(base + o1, n1, b1);
-      if (w + kGW < WX) copy_cell(base + o2, n2, b2);
-      cp_async_commit();
+        if (qx == w + 1 + k) oin[k] = run;
+      if (qx == w + kGW) {
+        o2 = run;
+        n2 = t;
+        b2 = (int64_t)b[qx] + d;
+      }
+      if (qx == w || qx == w + kGW) dx[qx] = d + t;
+      run += t;
     }
-    return total;
+    if (w + S == WX) ows = run;
+    const int n = finish_plan(ob, run, ow, ows, oin, o1, n1, b1, o2, n2, b2);
+    left = tot - n;
+    return n;
   };
   // the sum over the warp's rows of ring slot k, component a of G for the
   // node row of this lane (lanes L .. L+S-1 contribute, nearest first)
@@ -928,15 +865,7 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
   cp_async_wait_all();
   __syncthreads();
   if (cz < zlast) load_counts(cz + 1);
-  bool fast_cur;
-  int n_cur = row_plan(cz & 1, 0, fast_cur);
-  if (!fast_cur) {
-    // more particles than one unit holds: block-wide plan of equal shares
-    publish(cz & 1);
-    __syncthreads();
-    n_cur = plan(0, true);
-    issue(0);
-  }
+  int n_cur = plan_unit(cz & 1, 0, true);
   bool last_cur = left == 0;
 
   for (int u = 0;; ++u) {
@@ -991,7 +920,6 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
     const int cz_u = cz;
     const bool last_u = last_cur;
     const int n_u = n_cur;
-    const bool fast_u = fast_cur;
     const int p0u = p0c, p1u = p1c;
     bool more = true;
     if (last_u) {
@@ -999,20 +927,12 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
         ++cz;
         // the ranges of layer cz + 1 go to the buffer layer cz - 1 used
         if (cz < zlast) load_counts(cz + 1);
-        n_cur = row_plan(cz & 1, ub ^ 1, fast_cur);
-        if (!fast_cur) {
-          publish(cz & 1);
-          __syncthreads();
-          n_cur = plan(ub ^ 1, true);
-          issue(ub ^ 1);
-        }
+        n_cur = plan_unit(cz & 1, ub ^ 1, true);
       } else {
         more = false;
       }
     } else {
-      n_cur = plan(ub ^ 1, false);
-      fast_cur = false;
-      issue(ub ^ 1);
+      n_cur = plan_unit(cz & 1, ub ^ 1, false);
     }
     if (more) last_cur = left == 0;
     // 3.-5. with the ring phase a compile-time constant
@@ -1020,15 +940,12 @@ __global__ void __launch_bounds__(kGW * 32, 2) k_p2m3g(P2MParams P) {
       constexpr int PH = decltype(phc)::value;
       // 3. accumulate unit u: the particles of cells w .. w+S-1 of row L
       if (n_u > 0) {
-        const int* off = offU + ub * (NSC + 1);
-        const int q0 = L * WX + w;
-        const int p0 = fast_u ? p0u : off[q0], p1 = fast_u ? p1u : off[q0 + S];
+        const int p0 = p0u, p1 = p1u;
         // the window's inner cell boundaries: a particle of cell w + m
         // (m boundaries at or below it) takes x-weight S-1-m for node X0 + w
         int bnd[S - 1];
 #pragma unroll
-        for (int k = 0; k < S - 1; ++k)
-          bnd[k] = fast_u ? (int)sB[(ub * (S - 1) + k) * NT + tid] : off[q0 + 1 + k];
+        for (int k = 0; k < S - 1; ++k) bnd[k] = (int)sB[(ub * (S - 1) + k) * NT + tid];
         nterm += p1 - p0;
         for (int p = p0; p < p1; ++p) {
           int ix = S - 1;
