@@ -1104,20 +1104,50 @@ __global__ void k_layer_counts(const int* __restrict__ start, int N0, int N1, in
 __global__ void k_make_items(const int* __restrict__ lc, int N2, int zlo, int ze, int ntiles,
                              int target, int min_tz, int max_tz, int4* __restrict__ items,
                              int* __restrict__ nitems) {
-  const int tile = blockIdx.x * blockDim.x + threadIdx.x;
+  // one warp per tile: lane l holds layer c0 + l of a chunk of 32 and the
+  // chunk's inclusive prefix of the counts; the item ends are the layers the
+  // sequential rule below would cut at, found a chunk at a time by ballots
+  //   acc: particles since the item's first layer z0, len = ez + 1 - z0;
+  //   cut at ez when ez is the last layer, or when (acc >= target and
+  //   len >= min_tz, or len >= max_tz) and min_tz layers or more remain
+  const int lane = threadIdx.x & 31;
+  const int tile = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   if (tile >= ntiles) return;
-  int z0 = 0, acc = 0;
-  for (int ez = 0; ez < ze; ++ez) {
+  int z0 = 0, carry = 0;  // item start; its particles in the chunks before
+  for (int c0 = 0; c0 < ze; c0 += 32) {
+    const int ez = c0 + lane;
     const int cz = zlo + ez;
-    if (cz >= 0 && cz < N2) acc += lc[(int64_t)tile * N2 + cz];
-    const int len = ez + 1 - z0;
-    const bool want = (acc >= target && len >= min_tz) || len >= max_tz;
-    if (ez == ze - 1 || (want && ze - (ez + 1) >= min_tz)) {
-      const int q = atomicAdd(nitems, 1);
-      // weight: particles of the item's own cells + a per-layer cost
-      items[q] = make_int4(tile, zlo + z0, zlo + ez + 1, acc + 32 * len);
-      z0 = ez + 1;
-      acc = 0;
+    const int v = (ez < ze && cz >= 0 && cz < N2) ? lc[(int64_t)tile * N2 + cz] : 0;
+    int pre = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, pre, o);
+      if (lane >= o) pre += t;
+    }
+    for (;;) {
+      // the prefix up to the layer before z0 (or minus the carry when the
+      // item began in an earlier chunk)
+      const int at = z0 - c0 - 1;
+      const int pz = __shfl_sync(0xffffffffu, pre, at >= 0 ? at : 0);
+      const int s0 = at >= 0 ? pz : -carry;
+      const int acc = pre - s0;
+      const int len = ez + 1 - z0;
+      const bool want = (acc >= target && len >= min_tz) || len >= max_tz;
+      const bool cut = ez >= z0 && ez < ze && (ez == ze - 1 || (want && ze - (ez + 1) >= min_tz));
+      const unsigned m = __ballot_sync(0xffffffffu, cut);
+      if (m == 0) {
+        carry = __shfl_sync(0xffffffffu, acc, 31);  // the item's particles up to the chunk end
+        break;
+      }
+      const int f = __ffs(m) - 1;
+      if (lane == f) {
+        const int q = atomicAdd(nitems, 1);
+        // weight: particles of the item's own cells + a per-layer cost
+        items[q] = make_int4(tile, zlo + z0, zlo + ez + 1, acc + 32 * len);
+      }
+      z0 = c0 + f + 1;
+      carry = 0;
+      if (z0 >= c0 + 32 || z0 >= ze) break;
     }
   }
 }
@@ -1442,7 +1472,7 @@ cudaError_t make_tile_items(const int* start, const int N[3], int64_t nvalid, vo
   const bool rows = tdx == kGW;
   const int64_t tgt64 = nvalid / (rows ? 148 * 8 : 148 * 2 * 8);
   const int target = (int)(tgt64 < 4096 ? 4096 : (tgt64 > (1 << 30) ? (1 << 30) : tgt64));
-  k_make_items<<<(nt + 127) / 128, 128, 0, st>>>(lc, N[2], zlo, ze, nt, target,
+  k_make_items<<<(nt + 3) / 4, 128, 0, st>>>(lc, N[2], zlo, ze, nt, target,
                                                  rows ? 2 * kMinTZ : kMinTZ,
                                                  rows ? 2 * kMaxTZ : kMaxTZ, unordered, nitems);
   k_order_items<<<1, 1024, 0, st>>>(unordered, nitems, items);
